@@ -1,0 +1,161 @@
+/*
+ * sparseb.h — C ABI of the B200 block-sparse contraction library (libsparseb.so).
+ *
+ * Drop-in for SparseBackends' tensor-algebra entry point
+ *     SparseBackends.contract!(C, labelsC, A, labelsA, B, labelsB)
+ *     (SparseBackends/src/tensoralgebra/contract.jl:37-104)
+ * and the storage/conversion functions it relies on.  A Julia `ccall` shim (see
+ * INTEGRATION.md) replaces the Julia kernels with these calls; Python reaches
+ * the same symbols through ctypes (package sparsebackends_b200).
+ *
+ * Conventions (identical to the reference):
+ *  - all tensors are FP64; dense payloads are column-major;
+ *  - keys are 1-based integer tuples, one row of P (block-sparse/aliased) or N
+ *    (COO) int64 values per entry;
+ *  - block-sparse and aliased keys are kept sorted by the column-major linear
+ *    index of the prefix; COO keys keep the order given (dirty flag as in the
+ *    reference, sorted by sb_coo_sort);
+ *  - a label is two uint64 values (Index id, prime level), so a label vector
+ *    of rank n is 2*n uint64 values;
+ *  - sb_contract overwrites C (keys, payload) exactly like the reference kernels.
+ *
+ * Threading: one sb_ctx per host thread.  Every call enqueues device work on
+ * the context's stream; calls that must read device-computed structure flags
+ * (value-dependent block creation) synchronise that stream internally.
+ * No function allocates pinned host memory or blocks on other streams.
+ */
+#ifndef SPARSEB_H
+#define SPARSEB_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SB_API __attribute__((visibility("default")))
+#else
+#define SB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum sb_status {
+  SB_OK = 0,
+  SB_ERR_INVALID_ARG = 1,        /* bad pointer, rank, size or enum value                  */
+  SB_ERR_DIM_MISMATCH = 2,       /* shared-label extents or block sizes disagree            */
+  SB_ERR_LABEL = 3,              /* label missing / must be reduced / crosses prefix-tail   */
+  SB_ERR_UNSUPPORTED_LAYOUT = 4, /* C dense tail interleaves A and B kept axes              */
+  SB_ERR_UNSUPPORTED_TYPES = 5,  /* no kernel for this (C, A, B) storage combination        */
+  SB_ERR_OOM = 6,                /* device allocation failed                                */
+  SB_ERR_TIMEOUT = 7,            /* reserved: a bounded device wait gave up                 */
+  SB_ERR_CUDA = 8,               /* CUDA runtime error (message in sb_last_error)           */
+  SB_ERR_ASSERTION = 9           /* a precondition the reference asserts was violated      */
+} sb_status;
+
+typedef enum sb_kind {
+  SB_KIND_DENSE = 0,
+  SB_KIND_COO = 1,         /* COOTensor            (src/coo/storage.jl:1-6)              */
+  SB_KIND_BLOCKSPARSE = 2, /* NewBlockSparseSorted (src/blocksparse/storage.jl:3-9)      */
+  SB_KIND_ALIASED = 3      /* AliasedBlockSparse   (src/aliased/storage.jl:46-54)        */
+} sb_kind;
+
+typedef struct sb_ctx sb_ctx;
+typedef struct sb_tensor sb_tensor;
+
+/* ── context ─────────────────────────────────────────────────────────────── */
+/* Creates a context on `device` with its own non-blocking stream.            */
+SB_API sb_status sb_ctx_create(int device, unsigned flags, sb_ctx** out);
+SB_API sb_status sb_ctx_destroy(sb_ctx* ctx);
+/* Message of the last failing call on this context ("" if none).            */
+SB_API const char* sb_last_error(const sb_ctx* ctx);
+/* Use an external cudaStream_t (e.g. a Julia/torch stream) for all work.      */
+SB_API sb_status sb_ctx_set_stream(sb_ctx* ctx, void* cuda_stream);
+SB_API void* sb_ctx_get_stream(const sb_ctx* ctx);
+SB_API sb_status sb_ctx_synchronize(sb_ctx* ctx);
+/* Number of kernels this context has launched so far.                        */
+SB_API int64_t sb_ctx_launch_count(const sb_ctx* ctx);
+
+/* ── tensor creation (host arrays are copied to the device) ──────────────── */
+/* Dense tensor; data may be NULL (zeros).  Replaces the Array operands of
+ * contract! (e.g. ta/contract_bs_dense.jl:411, B::AbstractArray).            */
+SB_API sb_status sb_tensor_create_dense(sb_ctx* ctx, int nd, const int64_t* dims, const double* data,
+                                 sb_tensor** out);
+/* Same, from a device pointer (copied device-to-device).                     */
+SB_API sb_status sb_tensor_create_dense_device(sb_ctx* ctx, int nd, const int64_t* dims,
+                                        const double* d_data, sb_tensor** out);
+/* NewBlockSparseSorted{T,N,N2}(dims, blksize, keys, ids, data)
+ * (src/blocksparse/storage.jl:3-13).  keys: nblocks x P (row per block,
+ * 1-based), need not be sorted but must be unique; ids: 1-based slot of each
+ * key's payload in data (NULL means 1..nblocks); data: nblocks*blksize.
+ * nblocks = 0 gives the empty tensor of NewBlockSparseSorted{T,N,N2}(dims)
+ * (storage.jl:86-93).                                                        */
+SB_API sb_status sb_tensor_create_bs(sb_ctx* ctx, int nd, const int64_t* dims, int n_tail, int64_t nblocks,
+                              const int64_t* keys, const int64_t* ids, const double* data,
+                              sb_tensor** out);
+/* COOTensor{T,N}(dims, keys, vals, dirty) (src/coo/storage.jl:1-15).        */
+SB_API sb_status sb_tensor_create_coo(sb_ctx* ctx, int nd, const int64_t* dims, int64_t nnz,
+                               const int64_t* keys, const double* vals, int dirty, sb_tensor** out);
+/* AliasedBlockSparse{T,N,N2,P}(dims, blksize, templates, n_templates, keys,
+ * alias_ids, scalars) (src/aliased/storage.jl:46-59).                        */
+SB_API sb_status sb_tensor_create_aliased(sb_ctx* ctx, int nd, const int64_t* dims, int n_tail,
+                                   int64_t n_templates, const double* templates, int64_t nblocks,
+                                   const int64_t* keys, const int64_t* alias_ids,
+                                   const double* scalars, sb_tensor** out);
+SB_API sb_status sb_tensor_free(sb_tensor* t);
+
+/* ── queries and export ──────────────────────────────────────────────────── */
+/* dims must hold nd values (call with dims=NULL first to learn nd).          */
+SB_API sb_status sb_tensor_info(const sb_tensor* t, int* kind, int* nd, int64_t* dims, int* n_tail,
+                         int64_t* nkeys, int64_t* blksize, int64_t* n_templates, int* dirty);
+/* Block-sparse export in the reference layout: keys sorted column-major,
+ * ids = 1:n in that order, data packed accordingly.  Any pointer may be NULL. */
+SB_API sb_status sb_tensor_export_bs(sb_ctx* ctx, const sb_tensor* t, int64_t* keys, int64_t* ids,
+                              double* data);
+SB_API sb_status sb_tensor_export_coo(sb_ctx* ctx, const sb_tensor* t, int64_t* keys, double* vals);
+SB_API sb_status sb_tensor_export_aliased(sb_ctx* ctx, const sb_tensor* t, double* templates,
+                                   int64_t* keys, int64_t* alias_ids, double* scalars);
+SB_API sb_status sb_tensor_export_dense(sb_ctx* ctx, const sb_tensor* t, double* data);
+/* Device pointer and length (doubles) of the payload (dense data, block data,
+ * COO values or aliased templates), for zero-copy interop.                   */
+SB_API sb_status sb_tensor_device_data(const sb_tensor* t, double** d_ptr, int64_t* len);
+
+/* ── operations ──────────────────────────────────────────────────────────── */
+/* contract!(C, labelsC, A, labelsA, B, labelsB) (ta/contract.jl:37-104) with the
+ * type-dispatched kernels of ta/contract_{coo,coo_dense,coo_bs,bs_bs,bs_dense}.jl
+ * and ta/contract_aliased*.jl.  Supported (C, A, B) kinds:
+ *   (COO, COO, COO)              contract_coo.jl:93-170          one label
+ *   (BS, COO, DENSE)             contract_coo_dense.jl:48-125    one label
+ *   (BS, COO, BS)                contract_coo_bs.jl:14-241       one label
+ *   (BS, BS, BS)                 contract_bs_bs.jl:126-730       one or more labels
+ *   (BS, BS, DENSE)              contract_bs_dense.jl:34-619     one or more labels
+ *   (ALIASED, COO, DENSE)        contract_aliased_coo_dense.jl:34-164
+ *   (ALIASED, ALIASED, DENSE)    contract_aliased.jl, contract_aliased_shared.jl
+ *   (ALIASED, ALIASED, ALIASED)  contract_aliased.jl, contract_aliased_shared.jl
+ *   (DENSE, BS, BS)              contract_bs_bs_to_dense! (contract_bs_bs.jl:736-754)
+ * C must already have the output dims (and tail count); it is overwritten.   */
+SB_API sb_status sb_contract(sb_ctx* ctx, sb_tensor* C, const uint64_t* labelsC, int nC,
+                      const sb_tensor* A, const uint64_t* labelsA, int nA, const sb_tensor* B,
+                      const uint64_t* labelsB, int nB);
+/* permutedims for every kind (storage.jl:188-264, coo/storage.jl:153-166,
+ * aliased/storage.jl:172-236); perm is 1-based.  Block-sparse/aliased perms
+ * may not cross the prefix/tail boundary (storage.jl:126-132).               */
+SB_API sb_status sb_permutedims(sb_ctx* ctx, const sb_tensor* A, const int* perm, sb_tensor** out);
+/* sort_coo! (coo/storage.jl:182-189): column-major order, clears dirty.      */
+SB_API sb_status sb_coo_sort(sb_ctx* ctx, sb_tensor* A);
+/* blocksparse_from_dense(A, Val(N2); atol, rtol, dropzeros)
+ * (src/blocksparse/conversions.jl:21-75).                                    */
+SB_API sb_status sb_blocksparse_from_dense(sb_ctx* ctx, const sb_tensor* dense, int n_tail, double atol,
+                                    double rtol, int dropzeros, sb_tensor** out);
+/* coo_from_dense(A; atol, rtol) (src/coo/conversions.jl:13-26).              */
+SB_API sb_status sb_coo_from_dense(sb_ctx* ctx, const sb_tensor* dense, double atol, double rtol,
+                            sb_tensor** out);
+/* to_dense for COO / block-sparse / aliased (coo/conversions.jl:4-10,
+ * blocksparse/conversions.jl:83-187, aliased/conversions.jl:45-62).          */
+SB_API sb_status sb_to_dense(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out);
+/* to_blocksparse(::AliasedBlockSparse) (aliased/conversions.jl:18-32).       */
+SB_API sb_status sb_aliased_to_blocksparse(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPARSEB_H */

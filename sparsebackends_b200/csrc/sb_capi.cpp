@@ -1,0 +1,451 @@
+// extern "C" entry points of libsparseb (declared in include/sparseb.h).
+// No C++ exception crosses this boundary: every failure becomes an
+// sb_status and a message retrievable with sb_last_error().
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "sb_internal.hpp"
+
+using namespace sb;
+
+namespace {
+
+thread_local std::string g_noctx_error;
+
+template <class F>
+sb_status guard(sb_ctx* ctx, F&& f) {
+  try {
+    f();
+    if (ctx) ctx->impl.last_error.clear();
+    return SB_OK;
+  } catch (const Error& e) {
+    (ctx ? ctx->impl.last_error : g_noctx_error) = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    (ctx ? ctx->impl.last_error : g_noctx_error) = "host allocation failed";
+    return SB_ERR_OOM;
+  } catch (const std::exception& e) {
+    (ctx ? ctx->impl.last_error : g_noctx_error) = e.what();
+    return SB_ERR_INVALID_ARG;
+  }
+}
+
+std::vector<int64_t> read_dims(int nd, const int64_t* dims) {
+  require(nd >= 0 && nd <= 64, SB_ERR_INVALID_ARG, "rank out of range");
+  require(nd == 0 || dims != nullptr, SB_ERR_INVALID_ARG, "dims is NULL");
+  std::vector<int64_t> d(dims, dims + nd);
+  for (auto x : d) require(x >= 1, SB_ERR_ASSERTION, "all dims must be >= 1");
+  return d;
+}
+
+Labels read_labels(const uint64_t* p, int n) {
+  require(n >= 0 && (n == 0 || p != nullptr), SB_ERR_INVALID_ARG, "label array is NULL");
+  Labels l(n);
+  for (int i = 0; i < n; ++i) l[i] = Label{p[2 * i], p[2 * i + 1]};
+  return l;
+}
+
+sb_tensor* wrap(sb_ctx* ctx, TensorPtr t) {
+  auto* h = new sb_tensor;
+  h->impl = std::move(t);
+  h->owner = ctx;
+  return h;
+}
+
+void check_keys_in_range(const std::vector<int64_t>& keys, int64_t n, int klen, const std::vector<int64_t>& dims) {
+  for (int64_t i = 0; i < n; ++i)
+    for (int j = 0; j < klen; ++j) {
+      const int64_t v = keys[i * klen + j];
+      require(v >= 1 && v <= dims[j], SB_ERR_ASSERTION, "key coordinate out of bounds");
+    }
+}
+
+void check_ctx(sb_ctx* ctx) { require(ctx != nullptr, SB_ERR_INVALID_ARG, "context is NULL"); }
+void check_t(const sb_tensor* t) { require(t != nullptr && t->impl, SB_ERR_INVALID_ARG, "tensor is NULL"); }
+
+}  // namespace
+
+extern "C" {
+
+sb_status sb_ctx_create(int device, unsigned flags, sb_ctx** out) {
+  (void)flags;
+  return guard(nullptr, [&] {
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(device));
+    auto* c = new sb_ctx;
+    c->impl.device = device;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->impl.stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      delete c;
+      check_cuda(e, "cudaStreamCreateWithFlags");
+    }
+    c->impl.own_stream = true;
+    // Keep freed device memory cached in the stream-ordered pool.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    *out = c;
+  });
+}
+
+sb_status sb_ctx_destroy(sb_ctx* ctx) {
+  if (!ctx) return SB_OK;
+  cudaStreamSynchronize(ctx->impl.stream);
+  if (ctx->impl.own_stream) cudaStreamDestroy(ctx->impl.stream);
+  delete ctx;
+  return SB_OK;
+}
+
+const char* sb_last_error(const sb_ctx* ctx) { return ctx ? ctx->impl.last_error.c_str() : g_noctx_error.c_str(); }
+
+sb_status sb_ctx_set_stream(sb_ctx* ctx, void* stream) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    SB_CK(cudaStreamSynchronize(ctx->impl.stream));
+    if (ctx->impl.own_stream) cudaStreamDestroy(ctx->impl.stream);
+    ctx->impl.stream = static_cast<cudaStream_t>(stream);
+    ctx->impl.own_stream = false;
+  });
+}
+
+void* sb_ctx_get_stream(const sb_ctx* ctx) { return ctx ? static_cast<void*>(ctx->impl.stream) : nullptr; }
+
+sb_status sb_ctx_synchronize(sb_ctx* ctx) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    ctx->impl.sync();
+  });
+}
+
+int64_t sb_ctx_launch_count(const sb_ctx* ctx) { return ctx ? ctx->impl.launches : 0; }
+
+sb_status sb_tensor_create_dense(sb_ctx* ctx, int nd, const int64_t* dims, const double* data, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    auto t = make_tensor(&ctx->impl, DENSE, read_dims(nd, dims), nd);
+    const int64_t n = t->numel();
+    t->data = DevBuf(&ctx->impl, n * sizeof(double));
+    if (data) SB_CK(cudaMemcpyAsync(t->data.raw(), data, n * sizeof(double), cudaMemcpyHostToDevice, ctx->impl.stream));
+    else SB_CK(cudaMemsetAsync(t->data.raw(), 0, n * sizeof(double), ctx->impl.stream));
+    *out = wrap(ctx, std::move(t));
+  });
+}
+
+sb_status sb_tensor_create_dense_device(sb_ctx* ctx, int nd, const int64_t* dims, const double* d_data, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    require(out != nullptr && d_data != nullptr, SB_ERR_INVALID_ARG, "out or d_data is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    auto t = make_tensor(&ctx->impl, DENSE, read_dims(nd, dims), nd);
+    const int64_t n = t->numel();
+    t->data = DevBuf(&ctx->impl, n * sizeof(double));
+    SB_CK(cudaMemcpyAsync(t->data.raw(), d_data, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->impl.stream));
+    *out = wrap(ctx, std::move(t));
+  });
+}
+
+sb_status sb_tensor_create_bs(sb_ctx* ctx, int nd, const int64_t* dims, int n_tail, int64_t nblocks, const int64_t* keys,
+                              const int64_t* ids, const double* data, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    auto d = read_dims(nd, dims);
+    require((nd == 0 && n_tail == 0) || (n_tail > 0 && n_tail <= nd), SB_ERR_ASSERTION, "0 < N2 <= N required");
+    require(nblocks >= 0, SB_ERR_INVALID_ARG, "nblocks < 0");
+    require(nblocks == 0 || (keys && data) || (nd - n_tail == 0 && data), SB_ERR_INVALID_ARG, "keys/data NULL");
+    Ctx* c = &ctx->impl;
+    auto t = make_tensor(c, BS, d, n_tail);
+    const int P = t->P();
+    const int64_t blk = t->blksize();
+    std::vector<int64_t> k(nblocks * P);
+    if (P) std::copy(keys, keys + nblocks * P, k.begin());
+    check_keys_in_range(k, nblocks, P, d);
+    std::vector<int64_t> lin(nblocks), p(nblocks);
+    for (int64_t i = 0; i < nblocks; ++i) lin[i] = lin0(&k[i * P], d.data(), P);
+    std::iota(p.begin(), p.end(), 0);
+    std::stable_sort(p.begin(), p.end(), [&](int64_t a, int64_t b) { return lin[a] < lin[b]; });
+    for (int64_t i = 1; i < nblocks; ++i) require(lin[p[i]] != lin[p[i - 1]], SB_ERR_ASSERTION, "duplicate block key");
+    std::vector<int64_t> src_off(nblocks);
+    for (int64_t i = 0; i < nblocks; ++i) {
+      const int64_t id = ids ? ids[p[i]] : p[i] + 1;
+      require(id >= 1 && id <= nblocks, SB_ERR_ASSERTION, "block id out of range");
+      src_off[i] = (id - 1) * blk;
+    }
+    t->keys.resize(nblocks * P);
+    for (int64_t i = 0; i < nblocks; ++i) std::copy(&k[p[i] * P], &k[p[i] * P] + P, &t->keys[i * P]);
+    t->nkeys = nblocks;
+    t->data = DevBuf(c, nblocks * blk * sizeof(double));
+    if (nblocks) {
+      DevBuf raw(c, nblocks * blk * sizeof(double));
+      SB_CK(cudaMemcpyAsync(raw.raw(), data, nblocks * blk * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      bool packed = true;
+      for (int64_t i = 0; i < nblocks; ++i) packed = packed && src_off[i] == i * blk;
+      if (packed) {
+        t->data = std::move(raw);
+      } else {
+        std::vector<int64_t> idx(nblocks * blk);
+        for (int64_t i = 0; i < nblocks; ++i)
+          for (int64_t e = 0; e < blk; ++e) idx[i * blk + e] = src_off[i] + e;
+        DevBuf di = upload(c, idx);
+        SB_CK(launch_gather(raw.d(), di.as<int64_t>(), nblocks * blk, t->data.d(), c->stream));
+        c->note_launch();
+      }
+    }
+    *out = wrap(ctx, std::move(t));
+  });
+}
+
+sb_status sb_tensor_create_coo(sb_ctx* ctx, int nd, const int64_t* dims, int64_t nnz, const int64_t* keys,
+                               const double* vals, int dirty, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    auto d = read_dims(nd, dims);
+    require(nnz >= 0 && (nnz == 0 || (keys && vals)), SB_ERR_INVALID_ARG, "keys/vals NULL");
+    auto t = make_tensor(&ctx->impl, COO, d, 0);
+    t->keys.assign(keys, keys + nnz * nd);
+    check_keys_in_range(t->keys, nnz, nd, d);
+    t->nkeys = nnz;
+    t->dirty = dirty != 0;
+    t->data = DevBuf(&ctx->impl, nnz * sizeof(double));
+    if (nnz) SB_CK(cudaMemcpyAsync(t->data.raw(), vals, nnz * sizeof(double), cudaMemcpyHostToDevice, ctx->impl.stream));
+    *out = wrap(ctx, std::move(t));
+  });
+}
+
+sb_status sb_tensor_create_aliased(sb_ctx* ctx, int nd, const int64_t* dims, int n_tail, int64_t n_templates,
+                                   const double* templates, int64_t nblocks, const int64_t* keys,
+                                   const int64_t* alias_ids, const double* scalars, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    auto d = read_dims(nd, dims);
+    require(n_tail > 0 && n_tail <= nd, SB_ERR_ASSERTION, "0 < N2 <= N required");
+    require(n_templates >= 0 && nblocks >= 0, SB_ERR_INVALID_ARG, "negative count");
+    require(n_templates == 0 || templates, SB_ERR_INVALID_ARG, "templates NULL");
+    require(nblocks == 0 || (keys && alias_ids && scalars), SB_ERR_INVALID_ARG, "keys/alias_ids/scalars NULL");
+    Ctx* c = &ctx->impl;
+    auto t = make_tensor(c, ALIASED, d, n_tail);
+    const int P = t->P();
+    const int64_t blk = t->blksize();
+    std::vector<int64_t> k(keys, keys + nblocks * P);
+    check_keys_in_range(k, nblocks, P, d);
+    std::vector<int64_t> lin(nblocks), p(nblocks);
+    for (int64_t i = 0; i < nblocks; ++i) lin[i] = lin0(&k[i * P], d.data(), P);
+    std::iota(p.begin(), p.end(), 0);
+    std::stable_sort(p.begin(), p.end(), [&](int64_t a, int64_t b) { return lin[a] < lin[b]; });
+    for (int64_t i = 1; i < nblocks; ++i) require(lin[p[i]] != lin[p[i - 1]], SB_ERR_ASSERTION, "duplicate block key");
+    std::vector<double> sc(nblocks);
+    t->keys.resize(nblocks * P);
+    t->alias_ids.resize(nblocks);
+    for (int64_t i = 0; i < nblocks; ++i) {
+      std::copy(&k[p[i] * P], &k[p[i] * P] + P, &t->keys[i * P]);
+      t->alias_ids[i] = alias_ids[p[i]];
+      require(t->alias_ids[i] >= 1 && t->alias_ids[i] <= n_templates, SB_ERR_ASSERTION, "alias id out of range");
+      sc[i] = scalars[p[i]];
+    }
+    t->nkeys = nblocks;
+    t->n_templates = n_templates;
+    t->data = DevBuf(c, n_templates * blk * sizeof(double));
+    if (n_templates)
+      SB_CK(cudaMemcpyAsync(t->data.raw(), templates, n_templates * blk * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    t->scalars = upload(c, sc);
+    *out = wrap(ctx, std::move(t));
+  });
+}
+
+sb_status sb_tensor_free(sb_tensor* t) {
+  if (!t) return SB_OK;
+  sb_ctx* ctx = t->owner;
+  return guard(ctx, [&] {
+    if (ctx) SB_CK(cudaSetDevice(ctx->impl.device));
+    delete t;
+  });
+}
+
+sb_status sb_tensor_info(const sb_tensor* t, int* kind, int* nd, int64_t* dims, int* n_tail, int64_t* nkeys,
+                         int64_t* blksize, int64_t* n_templates, int* dirty) {
+  return guard(t ? t->owner : nullptr, [&] {
+    check_t(t);
+    const Tensor& x = *t->impl;
+    if (kind) *kind = x.kind;
+    if (nd) *nd = x.N();
+    if (dims) std::copy(x.dims.begin(), x.dims.end(), dims);
+    if (n_tail) *n_tail = x.n2;
+    if (nkeys) *nkeys = x.nkeys;
+    if (blksize) *blksize = (x.kind == BS || x.kind == ALIASED) ? x.blksize() : 0;
+    if (n_templates) *n_templates = x.n_templates;
+    if (dirty) *dirty = x.dirty ? 1 : 0;
+  });
+}
+
+sb_status sb_tensor_export_bs(sb_ctx* ctx, const sb_tensor* t, int64_t* keys, int64_t* ids, double* data) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(t);
+    const Tensor& x = *t->impl;
+    require(x.kind == BS, SB_ERR_INVALID_ARG, "not a block-sparse tensor");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    if (keys) std::copy(x.keys.begin(), x.keys.end(), keys);
+    if (ids)
+      for (int64_t i = 0; i < x.nkeys; ++i) ids[i] = i + 1;
+    if (data && x.nkeys) {
+      SB_CK(cudaMemcpyAsync(data, x.data.raw(), x.nkeys * x.blksize() * sizeof(double), cudaMemcpyDeviceToHost, ctx->impl.stream));
+      ctx->impl.sync();
+    }
+  });
+}
+
+sb_status sb_tensor_export_coo(sb_ctx* ctx, const sb_tensor* t, int64_t* keys, double* vals) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(t);
+    const Tensor& x = *t->impl;
+    require(x.kind == COO, SB_ERR_INVALID_ARG, "not a COO tensor");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    if (keys) std::copy(x.keys.begin(), x.keys.end(), keys);
+    if (vals && x.nkeys) {
+      SB_CK(cudaMemcpyAsync(vals, x.data.raw(), x.nkeys * sizeof(double), cudaMemcpyDeviceToHost, ctx->impl.stream));
+      ctx->impl.sync();
+    }
+  });
+}
+
+sb_status sb_tensor_export_aliased(sb_ctx* ctx, const sb_tensor* t, double* templates, int64_t* keys, int64_t* alias_ids,
+                                   double* scalars) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(t);
+    const Tensor& x = *t->impl;
+    require(x.kind == ALIASED, SB_ERR_INVALID_ARG, "not an aliased tensor");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    if (keys) std::copy(x.keys.begin(), x.keys.end(), keys);
+    if (alias_ids) std::copy(x.alias_ids.begin(), x.alias_ids.end(), alias_ids);
+    if (templates && x.n_templates)
+      SB_CK(cudaMemcpyAsync(templates, x.data.raw(), x.n_templates * x.blksize() * sizeof(double), cudaMemcpyDeviceToHost,
+                            ctx->impl.stream));
+    if (scalars && x.nkeys)
+      SB_CK(cudaMemcpyAsync(scalars, x.scalars.raw(), x.nkeys * sizeof(double), cudaMemcpyDeviceToHost, ctx->impl.stream));
+    ctx->impl.sync();
+  });
+}
+
+sb_status sb_tensor_export_dense(sb_ctx* ctx, const sb_tensor* t, double* data) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(t);
+    const Tensor& x = *t->impl;
+    require(x.kind == DENSE, SB_ERR_INVALID_ARG, "not a dense tensor");
+    require(data != nullptr, SB_ERR_INVALID_ARG, "data is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    SB_CK(cudaMemcpyAsync(data, x.data.raw(), x.numel() * sizeof(double), cudaMemcpyDeviceToHost, ctx->impl.stream));
+    ctx->impl.sync();
+  });
+}
+
+sb_status sb_tensor_device_data(const sb_tensor* t, double** d_ptr, int64_t* len) {
+  return guard(t ? t->owner : nullptr, [&] {
+    check_t(t);
+    if (d_ptr) *d_ptr = t->impl->data.d();
+    if (len) *len = t->impl->payload_len();
+  });
+}
+
+sb_status sb_contract(sb_ctx* ctx, sb_tensor* C, const uint64_t* labelsC, int nC, const sb_tensor* A,
+                      const uint64_t* labelsA, int nA, const sb_tensor* B, const uint64_t* labelsB, int nB) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(C);
+    check_t(A);
+    check_t(B);
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    contract(&ctx->impl, *C->impl, read_labels(labelsC, nC), *A->impl, read_labels(labelsA, nA), *B->impl,
+             read_labels(labelsB, nB));
+  });
+}
+
+sb_status sb_permutedims(sb_ctx* ctx, const sb_tensor* A, const int* perm, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    require(out != nullptr && (perm != nullptr || A->impl->N() == 0), SB_ERR_INVALID_ARG, "perm/out NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    const Tensor& x = *A->impl;
+    std::vector<int> p(perm, perm + x.N());
+    TensorPtr r;
+    switch (x.kind) {
+      case BS: r = bs_permute(&ctx->impl, x, p); break;
+      case ALIASED: r = aliased_permute(&ctx->impl, x, p); break;
+      case COO: r = coo_permute(&ctx->impl, x, p); break;
+      default: {
+        std::vector<int> s(p);
+        std::sort(s.begin(), s.end());
+        for (int i = 0; i < x.N(); ++i) require(s[i] == i + 1, SB_ERR_INVALID_ARG, "perm must be a permutation of 1:N");
+        r = dense_permute(&ctx->impl, x, p);
+      }
+    }
+    *out = wrap(ctx, std::move(r));
+  });
+}
+
+sb_status sb_coo_sort(sb_ctx* ctx, sb_tensor* A) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    require(A->impl->kind == COO, SB_ERR_INVALID_ARG, "not a COO tensor");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    coo_sort(&ctx->impl, *A->impl);
+  });
+}
+
+sb_status sb_blocksparse_from_dense(sb_ctx* ctx, const sb_tensor* dense, int n_tail, double atol, double rtol, int dropzeros,
+                                    sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(dense);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    *out = wrap(ctx, bs_from_dense(&ctx->impl, *dense->impl, n_tail, atol, rtol, dropzeros != 0));
+  });
+}
+
+sb_status sb_coo_from_dense(sb_ctx* ctx, const sb_tensor* dense, double atol, double rtol, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(dense);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    *out = wrap(ctx, coo_from_dense(&ctx->impl, *dense->impl, atol, rtol));
+  });
+}
+
+sb_status sb_to_dense(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    *out = wrap(ctx, to_dense(&ctx->impl, *A->impl));
+  });
+}
+
+sb_status sb_aliased_to_blocksparse(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    *out = wrap(ctx, aliased_to_bs(&ctx->impl, *A->impl));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,1587 @@
+// contract!(C, labelsC, A, labelsA, B, labelsB) on the device.
+//
+// Host side: label analysis, operand permutation plans, merge-join of the
+// sorted integer keys into block-pair lists, output key lists (the reference's
+// block-creation rules, including the value-dependent ones, whose flags are
+// computed on the device).  Device side: every floating-point value.
+//
+// Function-by-function correspondence (SparseBackends/src/tensoralgebra/):
+//   contract()                 contract.jl:37-104
+//   prefix_outer_bb()          contract_bs_bs.jl:173-263
+//   dense_bb()                 contract_bs_bs.jl:288-423
+//   shared_bb()                contract_bs_bs.jl:572-730
+//   prefix_outer_bd()          contract_bs_dense.jl:34-204 (Kahan)
+//   dense_bd()                 contract_bs_dense.jl:248-392
+//   shared_bd()                contract_bs_dense.jl:411-619
+//   coo_coo()                  contract_coo.jl:48-170
+//   coo_dense()                contract_coo_dense.jl:4-125
+//   coo_bs_prefix()            contract_coo_bs.jl:51-124
+//   coo_bs_dense_index()       contract_coo_bs.jl:140-241
+//   aliased_*()                contract_aliased_coo_dense.jl, contract_aliased.jl,
+//                              contract_aliased_shared.jl
+//   bs_bs_to_dense()           contract_bs_bs.jl:736-754
+#include <algorithm>
+#include <map>
+#include <numeric>
+#include <unordered_map>
+
+#include "sb_internal.hpp"
+
+namespace sb {
+namespace {
+
+int find(const Labels& l, const Label& x) {
+  for (size_t i = 0; i < l.size(); ++i)
+    if (l[i] == x) return static_cast<int>(i);
+  return -1;
+}
+bool has(const Labels& l, const Label& x) { return find(l, x) >= 0; }
+std::string lab_str(const Label& l) { return "(" + std::to_string(l.id) + "," + std::to_string(l.plev) + ")"; }
+
+int64_t prod(const std::vector<int64_t>& d, int lo, int hi) {
+  int64_t p = 1;
+  for (int i = lo; i < hi; ++i) p *= d[i];
+  return p;
+}
+
+// An operand after an optional permutation (owned copy) with its labels.
+struct Op {
+  const Tensor* t = nullptr;
+  TensorPtr owned;
+  Labels labels;
+  const Tensor& operator*() const { return *t; }
+  const Tensor* operator->() const { return t; }
+};
+
+Op view(const Tensor& t, const Labels& l) {
+  Op o;
+  o.t = &t;
+  o.labels = l;
+  return o;
+}
+
+Op permuted(Ctx* ctx, const Op& in, const std::vector<int>& perm) {
+  if (is_identity(perm)) {
+    Op o;
+    o.t = in.t;
+    o.labels = in.labels;
+    return o;
+  }
+  Op o;
+  switch (in.t->kind) {
+    case BS: o.owned = bs_permute(ctx, *in.t, perm); break;
+    case ALIASED: o.owned = aliased_permute(ctx, *in.t, perm); break;
+    case DENSE: o.owned = dense_permute(ctx, *in.t, perm); break;
+    default: o.owned = coo_permute(ctx, *in.t, perm); break;
+  }
+  o.t = o.owned.get();
+  for (int p : perm) o.labels.push_back(in.labels[p - 1]);
+  return o;
+}
+
+// _find_permutation_for_tensor (contract_bs_bs.jl:33-45); axisr is 1-based.
+std::vector<int> perm_r_last(int P, int N, int axisr) {
+  std::vector<int> perm;
+  if (axisr <= P) {
+    for (int a = 1; a <= P; ++a)
+      if (a != axisr) perm.push_back(a);
+    perm.push_back(axisr);
+    for (int a = P + 1; a <= N; ++a) perm.push_back(a);
+  } else {
+    for (int a = 1; a <= P; ++a) perm.push_back(a);
+    for (int a = P + 1; a <= N; ++a)
+      if (a != axisr) perm.push_back(a);
+    perm.push_back(axisr);
+  }
+  return perm;
+}
+
+// _permute_r_to_last_prefix (contract_bs_bs.jl:77-95)
+Op r_to_last_prefix(Ctx* ctx, const Op& in, const Label& r) {
+  const int ax = find(in.labels, r) + 1;
+  require(ax >= 1 && ax <= in->P(), SB_ERR_LABEL, "rlab must be in prefix to use prefix kernel");
+  if (ax == in->P()) return view(*in.t, in.labels);
+  return permuted(ctx, in, perm_r_last(in->P(), in->N(), ax));
+}
+
+enum class Mode { AthenB, BthenA, Interleaved };
+
+// _cdense_grouping_and_orders (contract_bs_bs.jl:470-505)
+Mode cdense_grouping(const Labels& Cdense, const Labels& keepA, const Labels& keepB, Labels* dkA, Labels* dkB) {
+  std::vector<int> origin;
+  for (auto& l : Cdense) {
+    if (has(keepA, l)) origin.push_back(1);
+    else if (has(keepB, l)) origin.push_back(0);
+    else fail(SB_ERR_LABEL, "Cdense label " + lab_str(l) + " not found in keepA/keepB");
+  }
+  int firstA = -1, lastA = -1, firstB = -1, lastB = -1;
+  for (int i = 0; i < static_cast<int>(origin.size()); ++i) {
+    if (origin[i]) { if (firstA < 0) firstA = i; lastA = i; }
+    else { if (firstB < 0) firstB = i; lastB = i; }
+  }
+  dkA->clear();
+  dkB->clear();
+  for (auto& l : Cdense) (has(keepA, l) ? dkA : dkB)->push_back(l);
+  if (firstB < 0 || firstA < 0) return Mode::AthenB;
+  if (lastA < firstB) return Mode::AthenB;
+  if (lastB < firstA) return Mode::BthenA;
+  return Mode::Interleaved;
+}
+
+bool same_set(const Labels& a, const Labels& b) {
+  if (a.size() != b.size()) return false;
+  for (auto& x : a)
+    if (!has(b, x)) return false;
+  return true;
+}
+
+// Output key collector: contributions arrive in the reference's iteration
+// order; C blocks end up sorted by column-major prefix index (the order that
+// _ensure_block!'s sorted insertion produces) with per-block contribution
+// lists kept in arrival order.
+struct CKeys {
+  int PC;
+  std::vector<int64_t> cdims;
+  std::unordered_map<int64_t, int> index;
+  std::vector<std::vector<int64_t>> keys;
+  std::vector<int64_t> lins;
+  std::vector<std::vector<int>> contribs;
+  int ncontrib = 0;
+
+  CKeys(const Tensor& C) : PC(C.P()), cdims(C.dims) {}
+
+  int touch(const std::vector<int64_t>& k) {
+    const int64_t l = lin0(k.data(), cdims.data(), PC);
+    auto it = index.find(l);
+    int id;
+    if (it == index.end()) {
+      id = static_cast<int>(keys.size());
+      index.emplace(l, id);
+      keys.push_back(k);
+      lins.push_back(l);
+      contribs.emplace_back();
+    } else {
+      id = it->second;
+    }
+    contribs[id].push_back(ncontrib++);
+    return id;
+  }
+  // Sorted order of local ids.
+  std::vector<int> order() const {
+    std::vector<int> o(keys.size());
+    std::iota(o.begin(), o.end(), 0);
+    std::sort(o.begin(), o.end(), [&](int a, int b) { return lins[a] < lins[b]; });
+    return o;
+  }
+  // Write sorted keys into C.
+  void commit_keys(Tensor& C, const std::vector<int>& ord) const {
+    C.keys.clear();
+    for (int id : ord) C.keys.insert(C.keys.end(), keys[id].begin(), keys[id].end());
+    C.nkeys = static_cast<int64_t>(ord.size());
+  }
+};
+
+void reset_output(Ctx* ctx, Tensor& C, int64_t nkeys, int64_t payload) {
+  C.keys.clear();
+  C.alias_ids.clear();
+  C.nkeys = nkeys;
+  C.n_templates = 0;
+  C.data = DevBuf(ctx, payload * sizeof(double));
+  C.scalars.reset();
+}
+
+// ── launch helpers ────────────────────────────────────────────────────────
+struct GemmPlan {
+  std::vector<GemmCBlock> cbs;
+  std::vector<GemmPair> pairs;
+  int cur = -1;
+  void add_cblock(int64_t c_off, int64_t M, int64_t N) {
+    require(M < (1LL << 31) && N < (1LL << 31), SB_ERR_INVALID_ARG, "block matrix extent exceeds 2^31");
+    cbs.push_back(GemmCBlock{c_off, static_cast<int32_t>(M), static_cast<int32_t>(N),
+                             static_cast<int32_t>(pairs.size()), static_cast<int32_t>(pairs.size())});
+  }
+  void add_pair(int64_t x_off, int64_t y_off, int64_t K, int64_t ldx, int64_t ldy) {
+    require(K < (1LL << 31) && ldx < (1LL << 31) && ldy < (1LL << 31), SB_ERR_INVALID_ARG,
+            "block matrix extent exceeds 2^31");
+    pairs.push_back(GemmPair{x_off, y_off, static_cast<int32_t>(K), static_cast<int32_t>(ldx),
+                             static_cast<int32_t>(ldy), 0});
+    cbs.back().pair_end = static_cast<int32_t>(pairs.size());
+  }
+  void launch(Ctx* ctx, const double* X, const double* Y, double* C, bool xT, bool yT) {
+    if (cbs.empty()) return;
+    // Tile shape from the (uniform) C block shape.
+    int64_t M = 0, N = 0;
+    for (auto& c : cbs) { M = std::max<int64_t>(M, c.M); N = std::max<int64_t>(N, c.N); }
+    GemmShape shape = GemmShape::T64x64;
+    if (N <= 32 && M >= 128) shape = GemmShape::T128x32;
+    else if (M <= 32 && N >= 128) shape = GemmShape::T32x128;
+    int bm, bn;
+    gemm_tile_dims(shape, &bm, &bn);
+    std::vector<GemmTile> tiles;
+    for (size_t c = 0; c < cbs.size(); ++c)
+      for (int n0 = 0; n0 < cbs[c].N; n0 += bn)
+        for (int m0 = 0; m0 < cbs[c].M; m0 += bm)
+          tiles.push_back(GemmTile{static_cast<int32_t>(c), m0, n0, 0});
+    DevBuf dc = upload(ctx, cbs), dp = upload(ctx, pairs), dt = upload(ctx, tiles);
+    SB_CK(launch_gemm_f64(X, Y, C, dc.as<GemmCBlock>(), dp.as<GemmPair>(), dt.as<GemmTile>(),
+                          static_cast<int64_t>(tiles.size()), xT, yT, shape, ctx->stream));
+    ctx->note_launch();
+  }
+};
+
+struct OuterPlan {
+  std::vector<OuterCBlock> cbs;
+  std::vector<OuterPair> pairs;
+  int64_t max_elems = 0;
+  void add_cblock(int64_t c_off, int64_t M, int64_t N) {
+    cbs.push_back(OuterCBlock{c_off, static_cast<int32_t>(M), static_cast<int32_t>(N),
+                              static_cast<int32_t>(pairs.size()), static_cast<int32_t>(pairs.size())});
+    max_elems = std::max(max_elems, M * N);
+  }
+  void add_pair(int64_t a_off, int64_t b_off) {
+    pairs.push_back(OuterPair{a_off, b_off});
+    cbs.back().pair_end = static_cast<int32_t>(pairs.size());
+  }
+  void launch(Ctx* ctx, const double* A, const double* B, double* C, bool kahan) {
+    if (cbs.empty()) return;
+    DevBuf dc = upload(ctx, cbs), dp = upload(ctx, pairs);
+    SB_CK(launch_outer_acc(A, B, C, dc.as<OuterCBlock>(), static_cast<int64_t>(cbs.size()), dp.as<OuterPair>(),
+                           max_elems, kahan, ctx->stream));
+    ctx->note_launch();
+  }
+};
+
+struct AxpyPlan {
+  std::vector<AxpySeg> segs;
+  std::vector<AxpyEntry> ents;
+  int64_t max_len = 0;
+  void add_seg(int64_t c_off, int64_t len) {
+    segs.push_back(AxpySeg{c_off, len, static_cast<int32_t>(ents.size()), static_cast<int32_t>(ents.size())});
+    max_len = std::max(max_len, len);
+  }
+  void add(int64_t src_off, int64_t alpha_idx) {
+    ents.push_back(AxpyEntry{src_off, alpha_idx});
+    segs.back().e_end = static_cast<int32_t>(ents.size());
+  }
+  void launch(Ctx* ctx, const double* src, const double* alpha, double* C) {
+    if (segs.empty()) return;
+    DevBuf ds = upload(ctx, segs), de = upload(ctx, ents);
+    SB_CK(launch_axpy_seg(src, alpha, C, ds.as<AxpySeg>(), static_cast<int64_t>(segs.size()), de.as<AxpyEntry>(),
+                          max_len, ctx->stream));
+    ctx->note_launch();
+  }
+};
+
+// Per-(block, slice) nonzero flags of a block-sparse tensor whose reduced
+// axis is the last tail axis (_slice_any_nonzero, contract_bs_bs.jl:280-285).
+std::vector<uint8_t> slice_flags(Ctx* ctx, const double* data, const std::vector<int64_t>& offs, int64_t R,
+                                 int64_t chunk) {
+  const int64_t nb = static_cast<int64_t>(offs.size());
+  if (nb == 0 || R == 0) return {};
+  DevBuf doff = upload(ctx, offs);
+  DevBuf fl(ctx, nb * R);
+  SB_CK(launch_slice_nonzero(data, doff.as<int64_t>(), nb, R, chunk, fl.as<uint8_t>(), ctx->stream));
+  ctx->note_launch();
+  return download<uint8_t>(ctx, fl.raw(), nb * R);
+}
+
+void check_c_dims(const Tensor& C, const Labels& lC, const Op& A, const Op& B) {
+  for (size_t j = 0; j < lC.size(); ++j) {
+    int ia = find(A.labels, lC[j]), ib = find(B.labels, lC[j]);
+    int64_t d = ia >= 0 ? A->dims[ia] : (ib >= 0 ? B->dims[ib] : -1);
+    require(d >= 0, SB_ERR_LABEL, "C label " + lab_str(lC[j]) + " not found in A or B");
+    require(d == C.dims[j], SB_ERR_DIM_MISMATCH, "C dim of label " + lab_str(lC[j]) + " does not match the operand");
+  }
+}
+
+// ══════════════════════════ BS × BS ══════════════════════════════════════
+
+void prefix_outer_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A, const Op& B, const Label& r) {
+  const int PA = A->P(), PB = B->P(), PC = C.P();
+  Labels Ad(A.labels.begin() + PA, A.labels.end()), Bd(B.labels.begin() + PB, B.labels.end()),
+      Cd(lC.begin() + PC, lC.end());
+  for (auto& l : Ad) require(!has(Bd, l), SB_ERR_ASSERTION, "outer kernel assumes disjoint dense labels");
+  Labels AB(Ad), BA(Bd);
+  AB.insert(AB.end(), Bd.begin(), Bd.end());
+  BA.insert(BA.end(), Ad.begin(), Ad.end());
+  int order;
+  if (Cd == AB) order = 1;
+  else if (Cd == BA) order = 2;
+  else fail(SB_ERR_UNSUPPORTED_LAYOUT, "C dense must be [A_dense...,B_dense...] or [B_dense..., A_dense...]");
+  require(C.blksize() == A->blksize() * B->blksize(), SB_ERR_DIM_MISMATCH, "C.blksize must equal A.blksize * B.blksize");
+  std::vector<int> src;
+  for (int j = 0; j < PC; ++j) {
+    int ia = find(A.labels, lC[j]), ib = find(B.labels, lC[j]);
+    if (ia >= 0) src.push_back(ia + 1);
+    else { require(ib >= 0, SB_ERR_LABEL, "Label not found in A or B"); src.push_back(-(ib + 1)); }
+  }
+  CKeys ck(C);
+  std::vector<std::pair<int64_t, int64_t>> pr;  // (a block, b block) per contribution
+  const int64_t nA = A->nkeys, nB = B->nkeys;
+  int64_t iA = 0, iB = 0;
+  std::vector<int64_t> k(PC);
+  while (iA < nA && iB < nB) {
+    const int64_t rvA = A->key(iA)[PA - 1], rvB = B->key(iB)[PB - 1];
+    if (rvA < rvB) { while (iA < nA && A->key(iA)[PA - 1] == rvA) ++iA; continue; }
+    if (rvB < rvA) { while (iB < nB && B->key(iB)[PB - 1] == rvB) ++iB; continue; }
+    const int64_t blo = iB;
+    while (iB < nB && B->key(iB)[PB - 1] == rvA) ++iB;
+    for (; iA < nA && A->key(iA)[PA - 1] == rvA; ++iA)
+      for (int64_t j = blo; j < iB; ++j) {
+        for (int q = 0; q < PC; ++q) k[q] = src[q] > 0 ? A->key(iA)[src[q] - 1] : B->key(j)[-src[q] - 1];
+        ck.touch(k);
+        pr.emplace_back(iA, j);
+      }
+  }
+  auto ord = ck.order();
+  const int64_t blkA = A->blksize(), blkB = B->blksize(), blkC = C.blksize();
+  reset_output(ctx, C, static_cast<int64_t>(ord.size()), static_cast<int64_t>(ord.size()) * blkC);
+  ck.commit_keys(C, ord);
+  OuterPlan op;
+  for (size_t c = 0; c < ord.size(); ++c) {
+    if (order == 1) op.add_cblock(static_cast<int64_t>(c) * blkC, blkA, blkB);
+    else op.add_cblock(static_cast<int64_t>(c) * blkC, blkB, blkA);
+    for (int ci : ck.contribs[ord[c]]) {
+      if (order == 1) op.add_pair(pr[ci].first * blkA, pr[ci].second * blkB);
+      else op.add_pair(pr[ci].second * blkB, pr[ci].first * blkA);
+    }
+  }
+  if (order == 1) op.launch(ctx, A->data.d(), B->data.d(), C.data.d(), false);
+  else op.launch(ctx, B->data.d(), A->data.d(), C.data.d(), false);
+}
+
+void dense_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Label& r) {
+  const int PA = A0->P(), PB = B0->P(), PC = C.P();
+  const int axA = find(A0.labels, r) + 1, axB = find(B0.labels, r) + 1;
+  require(axA > PA, SB_ERR_LABEL, "rlab must be in A dense tail");
+  require(axB > PB, SB_ERR_LABEL, "rlab must be in B dense tail");
+  Op A = axA != A0->N() ? permuted(ctx, A0, perm_r_last(PA, A0->N(), axA)) : view(*A0.t, A0.labels);
+  Op B = axB != B0->N() ? permuted(ctx, B0, perm_r_last(PB, B0->N(), axB)) : view(*B0.t, B0.labels);
+  const int64_t R = A->dims.back();
+  require(B->dims.back() == R, SB_ERR_DIM_MISMATCH, "reduction extents differ");
+  const int64_t chunkA = A->blksize() / R, chunkB = B->blksize() / R;
+  require(C.n2 == (A->n2 - 1) + (B->n2 - 1), SB_ERR_ASSERTION, "N2C must equal (N2A-1)+(N2B-1)");
+  require(C.blksize() == chunkA * chunkB, SB_ERR_DIM_MISMATCH, "C.blksize must equal chunkA*chunkB");
+  Labels Awo(A.labels.begin() + PA, A.labels.end() - 1), Bwo(B.labels.begin() + PB, B.labels.end() - 1),
+      Cd(lC.begin() + PC, lC.end());
+  Labels AB(Awo), BA(Bwo);
+  AB.insert(AB.end(), Bwo.begin(), Bwo.end());
+  BA.insert(BA.end(), Awo.begin(), Awo.end());
+  bool ab;
+  if (Cd == AB) ab = true;
+  else if (Cd == BA) ab = false;
+  else fail(SB_ERR_UNSUPPORTED_LAYOUT, "C dense tail must be [A_dense..., B_dense...] or [B_dense..., A_dense...]");
+  std::vector<int> srcA(PC, 0), srcB(PC, 0);
+  for (int j = 0; j < PC; ++j) {
+    int ia = find(A.labels, lC[j]);
+    if (ia >= 0) { require(ia < PA, SB_ERR_LABEL, "C prefix label must come from A prefix"); srcA[j] = ia + 1; }
+    else { int ib = find(B.labels, lC[j]); require(ib >= 0 && ib < PB, SB_ERR_LABEL, "C prefix label must come from B prefix"); srcB[j] = ib + 1; }
+  }
+  const int64_t nA = A->nkeys, nB = B->nkeys, blkA = A->blksize(), blkB = B->blksize();
+  std::vector<int64_t> offA(nA), offB(nB);
+  for (int64_t i = 0; i < nA; ++i) offA[i] = i * blkA;
+  for (int64_t i = 0; i < nB; ++i) offB[i] = i * blkB;
+  auto fA = slice_flags(ctx, A->data.d(), offA, R, chunkA);
+  auto fB = slice_flags(ctx, B->data.d(), offB, R, chunkB);
+  CKeys ck(C);
+  std::vector<std::pair<int64_t, int64_t>> pr;
+  std::vector<int64_t> k(PC);
+  for (int64_t a = 0; a < nA; ++a)
+    for (int64_t b = 0; b < nB; ++b) {
+      bool any = false;
+      for (int64_t s = 0; s < R && !any; ++s) any = fA[a * R + s] && fB[b * R + s];
+      if (!any) continue;  // block created only if some r-slice of both is nonzero
+      for (int q = 0; q < PC; ++q) k[q] = srcA[q] ? A->key(a)[srcA[q] - 1] : B->key(b)[srcB[q] - 1];
+      ck.touch(k);
+      pr.emplace_back(a, b);
+    }
+  auto ord = ck.order();
+  const int64_t blkC = C.blksize();
+  reset_output(ctx, C, static_cast<int64_t>(ord.size()), static_cast<int64_t>(ord.size()) * blkC);
+  ck.commit_keys(C, ord);
+  GemmPlan gp;
+  for (size_t c = 0; c < ord.size(); ++c) {
+    if (ab) gp.add_cblock(static_cast<int64_t>(c) * blkC, chunkA, chunkB);
+    else gp.add_cblock(static_cast<int64_t>(c) * blkC, chunkB, chunkA);
+    for (int ci : ck.contribs[ord[c]]) {
+      // AB: C(chunkA x chunkB) = A(chunkA x R) * B(chunkB x R)^T
+      if (ab) gp.add_pair(pr[ci].first * blkA, pr[ci].second * blkB, R, chunkA, chunkB);
+      else gp.add_pair(pr[ci].second * blkB, pr[ci].first * blkA, R, chunkB, chunkA);
+    }
+  }
+  if (ab) gp.launch(ctx, A->data.d(), B->data.d(), C.data.d(), false, true);
+  else gp.launch(ctx, B->data.d(), A->data.d(), C.data.d(), false, true);
+}
+
+// Shared-label classification and permutation plan common to the BS and
+// aliased multi-label kernels (contract_bs_bs.jl:584-667).
+struct SharedPlan {
+  Labels shared_prefix, red_dense, dkA, dkB;
+  Mode mode;
+  std::vector<int> permA, permB;
+};
+
+std::vector<int> perm_A_join_dense(const Labels& lA, int PA, const Labels& sp, const Labels& dkA, const Labels& red) {
+  std::vector<int> spax, perm;
+  for (auto& l : sp) spax.push_back(find(lA, l) + 1);
+  for (int a = 1; a <= PA; ++a)
+    if (std::find(spax.begin(), spax.end(), a) == spax.end()) perm.push_back(a);
+  perm.insert(perm.end(), spax.begin(), spax.end());
+  for (auto& l : dkA) perm.push_back(find(lA, l) + 1);
+  for (auto& l : red) perm.push_back(find(lA, l) + 1);
+  require(static_cast<int>(perm.size()) == static_cast<int>(lA.size()), SB_ERR_ASSERTION, "A perm length mismatch");
+  return perm;
+}
+std::vector<int> perm_B_join_redfirst(const Labels& lB, int PB, const Labels& sp, const Labels& red, const Labels& dkB) {
+  std::vector<int> spax, perm;
+  for (auto& l : sp) spax.push_back(find(lB, l) + 1);
+  for (int a = 1; a <= PB; ++a)
+    if (std::find(spax.begin(), spax.end(), a) == spax.end()) perm.push_back(a);
+  perm.insert(perm.end(), spax.begin(), spax.end());
+  for (auto& l : red) perm.push_back(find(lB, l) + 1);
+  for (auto& l : dkB) perm.push_back(find(lB, l) + 1);
+  require(static_cast<int>(perm.size()) == static_cast<int>(lB.size()), SB_ERR_ASSERTION, "B perm length mismatch");
+  return perm;
+}
+
+SharedPlan plan_shared(const Labels& lC, int PC, const Op& A, const Op& B, const Labels& shared, bool B_dense) {
+  SharedPlan sp;
+  for (auto& l : shared)
+    require(!has(lC, l), SB_ERR_LABEL, "shared label " + lab_str(l) + " must be reduced (must not appear in labelsC)");
+  const int PA = A->P(), PB = B_dense ? 0 : B->P();
+  Labels shared_dense;
+  for (auto& l : shared) {
+    const int ia = find(A.labels, l), ib = find(B.labels, l);
+    require(ia >= 0 && ib >= 0, SB_ERR_LABEL, "shared label must exist in both A and B");
+    const bool ap = ia < PA;
+    if (B_dense) {
+      (ap ? sp.shared_prefix : shared_dense).push_back(l);
+    } else {
+      const bool bp = ib < PB;
+      if (ap && bp) sp.shared_prefix.push_back(l);
+      else if (!ap && !bp) shared_dense.push_back(l);
+      else fail(SB_ERR_LABEL, "shared label " + lab_str(l) + " crosses prefix/dense; not supported");
+    }
+  }
+  Labels keepA0, keepB0;
+  for (int i = PA; i < A->N(); ++i) {
+    if (has(shared_dense, A.labels[i])) sp.red_dense.push_back(A.labels[i]);
+    else keepA0.push_back(A.labels[i]);
+  }
+  for (int i = PB; i < B->N(); ++i)
+    if (B_dense ? !has(shared, B.labels[i]) : !has(shared_dense, B.labels[i])) keepB0.push_back(B.labels[i]);
+  Labels Cd(lC.begin() + PC, lC.end());
+  sp.mode = cdense_grouping(Cd, keepA0, keepB0, &sp.dkA, &sp.dkB);
+  if (sp.mode == Mode::Interleaved)
+    fail(SB_ERR_UNSUPPORTED_LAYOUT, "Cdense interleaves A/B kept dims; would require permuting C (unsupported; sort/fallback)");
+  require(same_set(sp.dkA, keepA0) && same_set(sp.dkB, keepB0), SB_ERR_LABEL,
+          "C dense labels must be exactly the kept dense labels of A and B");
+  sp.permA = perm_A_join_dense(A.labels, PA, sp.shared_prefix, sp.dkA, sp.red_dense);
+  if (!B_dense) sp.permB = perm_B_join_redfirst(B.labels, PB, sp.shared_prefix, sp.red_dense, sp.dkB);
+  return sp;
+}
+
+int cmp_join(const int64_t* a, const int64_t* b, const std::vector<int>& pa, const std::vector<int>& pb) {
+  for (size_t t = 0; t < pa.size(); ++t) {
+    const int64_t x = a[pa[t] - 1], y = b[pb[t] - 1];
+    if (x < y) return -1;
+    if (x > y) return 1;
+  }
+  return 0;
+}
+int64_t advance_run(const Tensor& T, int64_t i0, const std::vector<int>& pos) {
+  const int64_t n = T.nkeys;
+  if (pos.empty()) return n;
+  int64_t i = i0 + 1;
+  while (i < n) {
+    bool eq = true;
+    for (int p : pos) eq = eq && T.key(i0)[p - 1] == T.key(i)[p - 1];
+    if (!eq) break;
+    ++i;
+  }
+  return i;
+}
+
+// Merge-join of two key-sorted operands on join positions; calls f(ia, ib)
+// for every matched pair in the reference's order (contract_bs_bs.jl:684-728).
+template <class F>
+void merge_join(const Tensor& A, const std::vector<int>& jA, const Tensor& B, const std::vector<int>& jB, F f) {
+  int64_t iA = 0, iB = 0;
+  while (iA < A.nkeys && iB < B.nkeys) {
+    const int c = cmp_join(A.key(iA), B.key(iB), jA, jB);
+    if (c < 0) { iA = advance_run(A, iA, jA); continue; }
+    if (c > 0) { iB = advance_run(B, iB, jB); continue; }
+    const int64_t iA2 = advance_run(A, iA, jA), iB2 = advance_run(B, iB, jB);
+    for (int64_t a = iA; a < iA2; ++a)
+      for (int64_t b = iB; b < iB2; ++b) f(a, b);
+    iA = iA2;
+    iB = iB2;
+  }
+}
+
+std::vector<int> csrc_AB(const Labels& lC, int PC, const Op& A, const Op& B, bool b_has_prefix) {
+  std::vector<int> src;
+  for (int j = 0; j < PC; ++j) {
+    const int ia = find(A.labels, lC[j]);
+    const int ib = find(B.labels, lC[j]);
+    if (ia >= 0 && ia < A->P()) src.push_back(ia + 1);
+    else if (b_has_prefix && ib >= 0 && ib < B->P()) src.push_back(-(ib + 1));
+    else fail(SB_ERR_LABEL, "C prefix label " + lab_str(lC[j]) + " must come from A/B prefix");
+  }
+  return src;
+}
+
+void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Labels& shared) {
+  const int PC = C.P();
+  SharedPlan sp = plan_shared(lC, PC, A0, B0, shared, false);
+  Op A = permuted(ctx, A0, sp.permA);
+  Op B = permuted(ctx, B0, sp.permB);
+  const int PA = A->P(), PB = B->P();
+  const int nkA = static_cast<int>(sp.dkA.size()), nkB = static_cast<int>(sp.dkB.size()),
+            nred = static_cast<int>(sp.red_dense.size());
+  const int64_t M = prod(A->dims, PA, PA + nkA), K = prod(A->dims, PA + nkA, A->N()), N = prod(B->dims, PB + nred, B->N());
+  require(K == prod(B->dims, PB, PB + nred), SB_ERR_DIM_MISMATCH, "Reduced dense extents mismatch between A and B");
+  require(C.blksize() == M * N, SB_ERR_DIM_MISMATCH, "C.blksize must equal M*N");
+  auto src = csrc_AB(lC, PC, A, B, true);
+  std::vector<int> jA, jB;
+  for (auto& l : sp.shared_prefix) { jA.push_back(find(A.labels, l) + 1); jB.push_back(find(B.labels, l) + 1); }
+  CKeys ck(C);
+  std::vector<std::pair<int64_t, int64_t>> pr;
+  std::vector<int64_t> k(PC);
+  merge_join(*A, jA, *B, jB, [&](int64_t a, int64_t b) {
+    for (int q = 0; q < PC; ++q) k[q] = src[q] > 0 ? A->key(a)[src[q] - 1] : B->key(b)[-src[q] - 1];
+    ck.touch(k);
+    pr.emplace_back(a, b);
+  });
+  auto ord = ck.order();
+  const int64_t blkA = A->blksize(), blkB = B->blksize(), blkC = C.blksize();
+  reset_output(ctx, C, static_cast<int64_t>(ord.size()), static_cast<int64_t>(ord.size()) * blkC);
+  ck.commit_keys(C, ord);
+  GemmPlan gp;
+  const bool athenb = sp.mode == Mode::AthenB;
+  for (size_t c = 0; c < ord.size(); ++c) {
+    if (athenb) gp.add_cblock(static_cast<int64_t>(c) * blkC, M, N);
+    else gp.add_cblock(static_cast<int64_t>(c) * blkC, N, M);
+    for (int ci : ck.contribs[ord[c]]) {
+      // AthenB: C(MxN) = A(MxK) B(KxN); BthenA: C(NxM) = B^T A^T
+      if (athenb) gp.add_pair(pr[ci].first * blkA, pr[ci].second * blkB, K, M, K);
+      else gp.add_pair(pr[ci].second * blkB, pr[ci].first * blkA, K, K, M);
+    }
+  }
+  if (athenb) gp.launch(ctx, A->data.d(), B->data.d(), C.data.d(), false, false);
+  else gp.launch(ctx, B->data.d(), A->data.d(), C.data.d(), true, true);
+}
+
+// ══════════════════════════ BS × Dense ═══════════════════════════════════
+
+std::vector<int> move_axis_last(int N, int ax) {
+  std::vector<int> p;
+  for (int d = 1; d <= N; ++d)
+    if (d != ax) p.push_back(d);
+  p.push_back(ax);
+  return p;
+}
+
+void prefix_outer_bd(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Label& r) {
+  const int PC = C.P();
+  Op A = r_to_last_prefix(ctx, A0, r);
+  const int PA = A->P();
+  const int NB = B0->N();
+  const int axB = find(B0.labels, r) + 1;
+  require(axB >= 1, SB_ERR_LABEL, "rlab must be a dim of dense B");
+  const int64_t R = B0->dims[axB - 1];
+  Op B = axB == NB ? view(*B0.t, B0.labels) : permuted(ctx, B0, move_axis_last(NB, axB));
+  const int64_t chunkB = B->numel() / R;
+  Labels Ad(A.labels.begin() + PA, A.labels.end()), Bwo(B.labels.begin(), B.labels.end() - 1),
+      Cd(lC.begin() + PC, lC.end());
+  Labels AB(Ad), BA(Bwo);
+  AB.insert(AB.end(), Bwo.begin(), Bwo.end());
+  BA.insert(BA.end(), Ad.begin(), Ad.end());
+  bool ab;
+  if (Cd == AB) ab = true;
+  else if (Cd == BA) ab = false;
+  else fail(SB_ERR_UNSUPPORTED_LAYOUT, "C dense tail must be [A_dense..., B_wo_r...] or [B_wo_r..., A_dense...]");
+  const int64_t chunkA = A->blksize();
+  require(C.blksize() == chunkA * chunkB, SB_ERR_DIM_MISMATCH, "C.blksize must equal A.blksize * (prod(B dims without r))");
+  std::vector<int> src;
+  for (int j = 0; j < PC; ++j) {
+    const int ia = find(A.labels, lC[j]);
+    require(ia >= 0, SB_ERR_LABEL, "C prefix label not in A");
+    require(ia < PA && !(lC[j] == r), SB_ERR_LABEL, "C prefix must be from A prefix excluding rlab");
+    src.push_back(ia + 1);
+  }
+  const int64_t nA = A->nkeys;
+  std::vector<std::vector<int64_t>> ck(nA, std::vector<int64_t>(PC));
+  for (int64_t i = 0; i < nA; ++i)
+    for (int q = 0; q < PC; ++q) ck[i][q] = A->key(i)[src[q] - 1];
+  std::vector<int64_t> perm(nA);
+  std::iota(perm.begin(), perm.end(), 0);
+  std::stable_sort(perm.begin(), perm.end(), [&](int64_t a, int64_t b) { return ck[a] < ck[b]; });  // sortperm(ckeys)
+  CKeys keys(C);
+  std::vector<int64_t> contrib_a;
+  for (int64_t i = 0; i < nA; ++i) {
+    keys.touch(ck[perm[i]]);
+    contrib_a.push_back(perm[i]);
+    const int64_t rv = A->key(perm[i])[PA - 1];
+    require(rv >= 1 && rv <= R, SB_ERR_ASSERTION, "A block key r out of bounds for dense B");
+  }
+  auto ord = keys.order();
+  const int64_t blkC = C.blksize();
+  reset_output(ctx, C, static_cast<int64_t>(ord.size()), static_cast<int64_t>(ord.size()) * blkC);
+  keys.commit_keys(C, ord);
+  OuterPlan op;
+  for (size_t c = 0; c < ord.size(); ++c) {
+    op.add_cblock(static_cast<int64_t>(c) * blkC, ab ? chunkA : chunkB, ab ? chunkB : chunkA);
+    for (int ci : keys.contribs[ord[c]]) {
+      const int64_t a = contrib_a[ci];
+      const int64_t rv = A->key(a)[PA - 1];
+      if (ab) op.add_pair(a * chunkA, (rv - 1) * chunkB);
+      else op.add_pair((rv - 1) * chunkB, a * chunkA);
+    }
+  }
+  if (ab) op.launch(ctx, A->data.d(), B->data.d(), C.data.d(), true);
+  else op.launch(ctx, B->data.d(), A->data.d(), C.data.d(), true);
+}
+
+void dense_bd(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Label& r) {
+  const int PA = A0->P(), PC = C.P();
+  const int axA = find(A0.labels, r) + 1, axB = find(B0.labels, r) + 1;
+  require(axA > PA, SB_ERR_LABEL, "rlab must be in A dense tail");
+  require(axB >= 1, SB_ERR_LABEL, "rlab must be an axis of B");
+  Op A = axA != A0->N() ? permuted(ctx, A0, perm_r_last(PA, A0->N(), axA)) : view(*A0.t, A0.labels);
+  const int NB = B0->N();
+  Op B = axB != NB ? permuted(ctx, B0, move_axis_last(NB, axB)) : view(*B0.t, B0.labels);
+  const int64_t R = A->dims.back();
+  require(B->dims.back() == R, SB_ERR_DIM_MISMATCH, "reduction extents differ");
+  const int64_t chunkA = A->blksize() / R, chunkB = B->numel() / R;
+  require(C.n2 == (A->n2 - 1) + (NB - 1), SB_ERR_ASSERTION, "N2C must equal (N2A-1)+(NB-1)");
+  require(C.blksize() == chunkA * chunkB, SB_ERR_DIM_MISMATCH, "C.blksize must equal chunkA*chunkB");
+  Labels Awo(A.labels.begin() + PA, A.labels.end() - 1), Bwo(B.labels.begin(), B.labels.end() - 1),
+      Cd(lC.begin() + PC, lC.end());
+  Labels AB(Awo), BA(Bwo);
+  AB.insert(AB.end(), Bwo.begin(), Bwo.end());
+  BA.insert(BA.end(), Awo.begin(), Awo.end());
+  bool ab;
+  if (Cd == AB) ab = true;
+  else if (Cd == BA) ab = false;
+  else fail(SB_ERR_UNSUPPORTED_LAYOUT, "C dense tail must be [A_dense..., B_dense...] or [B_dense..., A_dense...]");
+  std::vector<int> srcA;
+  for (int j = 0; j < PC; ++j) {
+    const int ia = find(A.labels, lC[j]);
+    require(ia >= 0 && ia < PA, SB_ERR_LABEL, "C sparse prefix label must come from A sparse head");
+    srcA.push_back(ia + 1);
+  }
+  const int64_t nA = A->nkeys, blkA = A->blksize();
+  std::vector<int64_t> offA(nA);
+  for (int64_t i = 0; i < nA; ++i) offA[i] = i * blkA;
+  auto fA = slice_flags(ctx, A->data.d(), offA, R, chunkA);
+  auto fB = slice_flags(ctx, B->data.d(), {0}, R, chunkB);
+  CKeys ck(C);
+  std::vector<int64_t> contrib_a;
+  std::vector<int64_t> k(PC);
+  for (int64_t a = 0; a < nA; ++a) {
+    bool any = false;
+    for (int64_t s = 0; s < R && !any; ++s) any = fA[a * R + s] && fB[s];
+    if (!any) continue;
+    for (int q = 0; q < PC; ++q) k[q] = A->key(a)[srcA[q] - 1];
+    ck.touch(k);
+    contrib_a.push_back(a);
+  }
+  auto ord = ck.order();
+  const int64_t blkC = C.blksize();
+  reset_output(ctx, C, static_cast<int64_t>(ord.size()), static_cast<int64_t>(ord.size()) * blkC);
+  ck.commit_keys(C, ord);
+  GemmPlan gp;
+  for (size_t c = 0; c < ord.size(); ++c) {
+    gp.add_cblock(static_cast<int64_t>(c) * blkC, ab ? chunkA : chunkB, ab ? chunkB : chunkA);
+    for (int ci : ck.contribs[ord[c]]) {
+      const int64_t a = contrib_a[ci];
+      if (ab) gp.add_pair(a * blkA, 0, R, chunkA, chunkB);
+      else gp.add_pair(0, a * blkA, R, chunkB, chunkA);
+    }
+  }
+  if (ab) gp.launch(ctx, A->data.d(), B->data.d(), C.data.d(), false, true);
+  else gp.launch(ctx, B->data.d(), A->data.d(), C.data.d(), false, true);
+}
+
+// Dense B permuted to [red..., keepB..., shared_prefix...] so that every slice
+// Bp[:, :, sp_vals] is one contiguous K x N column-major matrix (the values of
+// the reference's Bp[sp_vals..., :, ...] view, contract_bs_dense.jl:589-592).
+struct DenseSlices {
+  Op Bp;
+  int64_t K = 1, N = 1, slab = 0;
+  std::vector<int64_t> sp_dims;
+};
+DenseSlices dense_slices(Ctx* ctx, const Op& B0, const Labels& sp, const Labels& red, const Labels& dkB) {
+  std::vector<int> perm;
+  for (auto& l : red) perm.push_back(find(B0.labels, l) + 1);
+  for (auto& l : dkB) perm.push_back(find(B0.labels, l) + 1);
+  for (auto& l : sp) perm.push_back(find(B0.labels, l) + 1);
+  require(static_cast<int>(perm.size()) == B0->N(), SB_ERR_ASSERTION, "B perm length mismatch; labelsB must match B ndims");
+  DenseSlices ds;
+  ds.Bp = permuted(ctx, B0, perm);
+  const int nr = static_cast<int>(red.size()), nk = static_cast<int>(dkB.size());
+  ds.K = prod(ds.Bp->dims, 0, nr);
+  ds.N = prod(ds.Bp->dims, nr, nr + nk);
+  ds.slab = ds.K * ds.N;
+  ds.sp_dims.assign(ds.Bp->dims.begin() + nr + nk, ds.Bp->dims.end());
+  return ds;
+}
+
+void shared_bd(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Labels& shared) {
+  const int PC = C.P();
+  SharedPlan sp = plan_shared(lC, PC, A0, B0, shared, true);
+  Op A = permuted(ctx, A0, sp.permA);
+  const int PA = A->P();
+  const int nkA = static_cast<int>(sp.dkA.size());
+  DenseSlices ds = dense_slices(ctx, B0, sp.shared_prefix, sp.red_dense, sp.dkB);
+  const int64_t M = prod(A->dims, PA, PA + nkA), K = prod(A->dims, PA + nkA, A->N()), N = ds.N;
+  require(K == ds.K, SB_ERR_DIM_MISMATCH, "Reduced dense extents mismatch between A and B");
+  require(C.blksize() == M * N, SB_ERR_DIM_MISMATCH, "C.blksize must equal M*N");
+  std::vector<int> csrc;
+  for (int j = 0; j < PC; ++j) {
+    const int ia = find(A.labels, lC[j]);
+    require(ia >= 0, SB_ERR_LABEL, "C prefix label must exist in A");
+    require(ia < PA && !has(sp.shared_prefix, lC[j]), SB_ERR_LABEL, "C prefix label must come from A prefix");
+    csrc.push_back(ia + 1);
+  }
+  std::vector<int> jA;
+  for (auto& l : sp.shared_prefix) jA.push_back(find(A.labels, l) + 1);
+  CKeys ck(C);
+  std::vector<std::pair<int64_t, int64_t>> pr;  // (a block, B slab offset)
+  std::vector<int64_t> k(PC);
+  for (int64_t iA = 0; iA < A->nkeys;) {
+    const int64_t iA2 = advance_run(*A, iA, jA);
+    int64_t slab = 0, stride = 1;
+    for (size_t t = 0; t < jA.size(); ++t) {
+      slab += (A->key(iA)[jA[t] - 1] - 1) * stride;
+      stride *= ds.sp_dims[t];
+    }
+    for (int64_t a = iA; a < iA2; ++a) {
+      for (int q = 0; q < PC; ++q) k[q] = A->key(a)[csrc[q] - 1];
+      ck.touch(k);
+      pr.emplace_back(a, slab * ds.slab);
+    }
+    iA = iA2;
+  }
+  auto ord = ck.order();
+  const int64_t blkA = A->blksize(), blkC = C.blksize();
+  reset_output(ctx, C, static_cast<int64_t>(ord.size()), static_cast<int64_t>(ord.size()) * blkC);
+  ck.commit_keys(C, ord);
+  GemmPlan gp;
+  const bool athenb = sp.mode == Mode::AthenB;
+  for (size_t c = 0; c < ord.size(); ++c) {
+    if (athenb) gp.add_cblock(static_cast<int64_t>(c) * blkC, M, N);
+    else gp.add_cblock(static_cast<int64_t>(c) * blkC, N, M);
+    for (int ci : ck.contribs[ord[c]]) {
+      if (athenb) gp.add_pair(pr[ci].first * blkA, pr[ci].second, K, M, K);
+      else gp.add_pair(pr[ci].second, pr[ci].first * blkA, K, K, M);
+    }
+  }
+  if (athenb) gp.launch(ctx, A->data.d(), ds.Bp->data.d(), C.data.d(), false, false);
+  else gp.launch(ctx, ds.Bp->data.d(), A->data.d(), C.data.d(), true, true);
+}
+
+// ══════════════════════════ COO kernels ══════════════════════════════════
+
+// ensure_rlab_last_and_sorted (contract_coo.jl:48-82)
+Op coo_r_last_sorted(Ctx* ctx, const Op& A, const Label& r) {
+  if (A.labels.back() == r) return view(*A.t, A.labels);
+  std::vector<int> perm;
+  for (int i = 0; i < A->N(); ++i)
+    if (!(A.labels[i] == r)) perm.push_back(i + 1);
+  perm.push_back(find(A.labels, r) + 1);
+  Op o = permuted(ctx, A, perm);
+  o.owned->dirty = true;
+  coo_sort(ctx, *o.owned);
+  return o;
+}
+
+void coo_coo(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Label& r) {
+  Op A = coo_r_last_sorted(ctx, A0, r), B = coo_r_last_sorted(ctx, B0, r);
+  const int NC = C.N(), NA = A->N(), NB = B->N();
+  std::vector<std::pair<int, int>> src;
+  for (int t = 0; t < NC; ++t) {
+    const int ia = find(A.labels, lC[t]);
+    if (ia >= 0) src.emplace_back(1, ia);
+    else { const int ib = find(B.labels, lC[t]); require(ib >= 0, SB_ERR_LABEL, "C label not in A or B"); src.emplace_back(2, ib); }
+  }
+  std::vector<int64_t> ia_list, ib_list;
+  int64_t i = 0, j = 0;
+  while (i < A->nkeys && j < B->nkeys) {
+    const int64_t ra = A->key(i)[NA - 1], rb = B->key(j)[NB - 1];
+    if (ra < rb) ++i;
+    else if (rb < ra) ++j;
+    else {
+      const int64_t jlo = j;
+      while (j < B->nkeys && B->key(j)[NB - 1] == rb) ++j;
+      for (; i < A->nkeys && A->key(i)[NA - 1] == ra; ++i)
+        for (int64_t jj = jlo; jj < j; ++jj) { ia_list.push_back(i); ib_list.push_back(jj); }
+    }
+  }
+  const int64_t n = static_cast<int64_t>(ia_list.size());
+  // products on the device; exact zeros are dropped (_push_term!, contract_coo.jl:84-91)
+  std::vector<ScalarTerm> terms(n);
+  std::vector<int32_t> seg(n + 1);
+  for (int64_t q = 0; q < n; ++q) { terms[q] = ScalarTerm{ia_list[q], ib_list[q]}; seg[q] = static_cast<int32_t>(q); }
+  seg[n] = static_cast<int32_t>(n);
+  DevBuf prod_buf(ctx, n * sizeof(double));
+  std::vector<uint8_t> nz;
+  if (n) {
+    DevBuf dt = upload(ctx, terms), dsg = upload(ctx, seg);
+    SB_CK(launch_scalar_prog(A->data.d(), B->data.d(), dt.as<ScalarTerm>(), dsg.as<int32_t>(), n, prod_buf.d(), ctx->stream));
+    DevBuf fl(ctx, n);
+    std::vector<int64_t> offs(n);
+    std::iota(offs.begin(), offs.end(), 0);
+    DevBuf doff = upload(ctx, offs);
+    SB_CK(launch_slice_nonzero(prod_buf.d(), doff.as<int64_t>(), n, 1, 1, fl.as<uint8_t>(), ctx->stream));
+    ctx->note_launch(2);
+    nz = download<uint8_t>(ctx, fl.raw(), n);
+  }
+  std::vector<int64_t> keep;
+  C.keys.clear();
+  for (int64_t q = 0; q < n; ++q) {
+    if (!nz[q]) continue;
+    keep.push_back(q);
+    for (int t = 0; t < NC; ++t)
+      C.keys.push_back(src[t].first == 1 ? A->key(ia_list[q])[src[t].second] : B->key(ib_list[q])[src[t].second]);
+  }
+  C.nkeys = static_cast<int64_t>(keep.size());
+  C.dirty = true;
+  C.data = DevBuf(ctx, C.nkeys * sizeof(double));
+  if (C.nkeys) {
+    DevBuf dk = upload(ctx, keep);
+    SB_CK(launch_gather(prod_buf.d(), dk.as<int64_t>(), C.nkeys, C.data.d(), ctx->stream));
+    ctx->note_launch();
+  }
+}
+
+// aligned_A_to_Cprefix (contract_coo_dense.jl:4-18)
+Op coo_align_to_cprefix(Ctx* ctx, const Op& A, const Labels& lC, int PC, const Label& r) {
+  std::vector<int> perm;
+  for (int j = 0; j < PC; ++j) {
+    const int ia = find(A.labels, lC[j]);
+    require(ia >= 0, SB_ERR_LABEL, "C prefix label not in A");
+    perm.push_back(ia + 1);
+  }
+  const int ir = find(A.labels, r);
+  require(ir >= 0, SB_ERR_LABEL, "rlab not in A");
+  perm.push_back(ir + 1);
+  require(static_cast<int>(perm.size()) == A->N(), SB_ERR_ASSERTION, "PC mismatch: C prefix must be A labels without r");
+  Op o;
+  o.owned = coo_permute(ctx, *A.t, perm);
+  coo_sort(ctx, *o.owned);
+  o.t = o.owned.get();
+  for (int p : perm) o.labels.push_back(A.labels[p - 1]);
+  return o;
+}
+
+Op dense_c_tail_r_last(Ctx* ctx, const Op& B, const Labels& lC, int PC, const Label& r) {
+  std::vector<int> perm;
+  for (size_t j = PC; j < lC.size(); ++j) {
+    const int ib = find(B.labels, lC[j]);
+    require(ib >= 0, SB_ERR_LABEL, "label not found in labelsB");
+    perm.push_back(ib + 1);
+  }
+  const int ir = find(B.labels, r);
+  require(ir >= 0, SB_ERR_LABEL, "rlab not found in labelsB");
+  perm.push_back(ir + 1);
+  require(static_cast<int>(perm.size()) == B->N(), SB_ERR_ASSERTION, "N2 mismatch: C dense labels must be B labels without r");
+  return permuted(ctx, B, perm);
+}
+
+void coo_dense(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Label& r) {
+  const int PC = C.P();
+  require(!has(lC, r), SB_ERR_LABEL, "rlab must be reduced (not in labelsC)");
+  Op A = coo_align_to_cprefix(ctx, A0, lC, PC, r);
+  Op B = dense_c_tail_r_last(ctx, B0, lC, PC, r);
+  require(C.n2 == B->N() - 1, SB_ERR_ASSERTION, "N2 mismatch");
+  const int64_t R = B->dims.back(), chunk = B->numel() / R;
+  require(C.blksize() == chunk, SB_ERR_DIM_MISMATCH, "C.blksize must equal prod(B dims without r)");
+  CKeys ck(C);
+  std::vector<int64_t> ca;
+  const int NA = A->N();
+  for (int64_t i = 0; i < A->nkeys; ++i) {
+    const int64_t rv = A->key(i)[NA - 1];
+    if (rv < 1 || rv > R) continue;
+    ck.touch(std::vector<int64_t>(A->key(i), A->key(i) + PC));
+    ca.push_back(i);
+  }
+  auto ord = ck.order();
+  reset_output(ctx, C, static_cast<int64_t>(ord.size()), static_cast<int64_t>(ord.size()) * chunk);
+  ck.commit_keys(C, ord);
+  AxpyPlan ap;
+  for (size_t c = 0; c < ord.size(); ++c) {
+    ap.add_seg(static_cast<int64_t>(c) * chunk, chunk);
+    for (int ci : ck.contribs[ord[c]]) {
+      const int64_t a = ca[ci];
+      ap.add((A->key(a)[NA - 1] - 1) * chunk, a);
+    }
+  }
+  ap.launch(ctx, B->data.d(), A->data.d(), C.data.d());
+}
+
+void coo_bs_prefix(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A, const Op& B, const Label& r) {
+  const int PB = B->P(), PC = C.P(), NA = A->N();
+  require(PC == NA + PB - 2, SB_ERR_ASSERTION, "PC must equal NA + PB - 2");
+  require(C.n2 == B->n2, SB_ERR_ASSERTION, "C tail must equal B tail");
+  const int aR = find(A.labels, r), bR = find(B.labels, r);
+  std::vector<int> src;
+  for (int j = 0; j < PC; ++j) {
+    const int ia = find(A.labels, lC[j]);
+    if (ia >= 0) src.push_back(ia + 1);
+    else { const int ib = find(B.labels, lC[j]); require(ib >= 0 && ib < PB, SB_ERR_LABEL, "C prefix label must come from A or B prefix"); src.push_back(-(ib + 1)); }
+  }
+  CKeys ck(C);
+  std::vector<std::pair<int64_t, int64_t>> pr;
+  std::vector<int64_t> k(PC);
+  int64_t iA = 0, iB = 0;
+  while (iA < A->nkeys && iB < B->nkeys) {
+    const int64_t rA = A->key(iA)[aR], rB = B->key(iB)[bR];
+    if (rA < rB) { while (iA < A->nkeys && A->key(iA)[aR] == rA) ++iA; }
+    else if (rB < rA) { while (iB < B->nkeys && B->key(iB)[bR] == rB) ++iB; }
+    else {
+      const int64_t blo = iB;
+      while (iB < B->nkeys && B->key(iB)[bR] == rA) ++iB;
+      for (; iA < A->nkeys && A->key(iA)[aR] == rA; ++iA)
+        for (int64_t b = blo; b < iB; ++b) {
+          for (int q = 0; q < PC; ++q) k[q] = src[q] > 0 ? A->key(iA)[src[q] - 1] : B->key(b)[-src[q] - 1];
+          ck.touch(k);
+          pr.emplace_back(iA, b);
+        }
+    }
+  }
+  auto ord = ck.order();
+  const int64_t blk = C.blksize();
+  require(blk == B->blksize(), SB_ERR_DIM_MISMATCH, "C.blksize must equal B.blksize");
+  reset_output(ctx, C, static_cast<int64_t>(ord.size()), static_cast<int64_t>(ord.size()) * blk);
+  ck.commit_keys(C, ord);
+  AxpyPlan ap;
+  for (size_t c = 0; c < ord.size(); ++c) {
+    ap.add_seg(static_cast<int64_t>(c) * blk, blk);
+    for (int ci : ck.contribs[ord[c]]) ap.add(pr[ci].second * blk, pr[ci].first);
+  }
+  ap.launch(ctx, B->data.d(), A->data.d(), C.data.d());
+}
+
+void coo_bs_dense_index(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A, const Op& B0, const Label& r) {
+  const int PB = B0->P(), PC = C.P(), NA = A->N();
+  require(!has(lC, r), SB_ERR_LABEL, "rlab must be reduced (not in labelsC)");
+  require(C.n2 == B0->n2 - 1, SB_ERR_ASSERTION, "N2C must equal N2B - 1");
+  const int axB = find(B0.labels, r) + 1;
+  require(axB > PB, SB_ERR_LABEL, "rlab must be in B dense tail");
+  require(find(A.labels, r) + 1 == NA, SB_ERR_ASSERTION, "Expected A to have rlab as last axis");
+  Op B = axB != B0->N() ? permuted(ctx, B0, perm_r_last(PB, B0->N(), axB)) : view(*B0.t, B0.labels);
+  const int64_t dim_r = B->dims.back(), chunk = B->blksize() / dim_r;
+  Labels exp(B.labels.begin() + PB, B.labels.end() - 1), Cd(lC.begin() + PC, lC.end());
+  require(Cd == exp, SB_ERR_LABEL, "C dense tail must be B dense tail without r");
+  require(C.blksize() == chunk, SB_ERR_DIM_MISMATCH, "C.blksize must equal chunk");
+  std::vector<int> srcA(PC, 0), srcB(PC, 0);
+  for (int j = 0; j < PC; ++j) {
+    const int ia = find(A.labels, lC[j]);
+    if (ia >= 0) srcA[j] = ia + 1;
+    else { const int ib = find(B.labels, lC[j]); require(ib >= 0 && ib < PB, SB_ERR_LABEL, "Label in C prefix must come from B prefix"); srcB[j] = ib + 1; }
+  }
+  // candidate (nnz, block) pairs; value-dependent skip of all-zero α·slice
+  const int64_t nA = A->nkeys, nB = B->nkeys, blkB = B->blksize();
+  std::vector<int64_t> offs, ai;
+  offs.reserve(nA * nB);
+  for (int64_t a = 0; a < nA; ++a) {
+    const int64_t rv = A->key(a)[NA - 1];
+    require(rv >= 1 && rv <= dim_r, SB_ERR_ASSERTION, "Reduction index out of bounds");
+    for (int64_t b = 0; b < nB; ++b) { offs.push_back(b * blkB + (rv - 1) * chunk); ai.push_back(a); }
+  }
+  std::vector<uint8_t> nz;
+  const int64_t ncand = static_cast<int64_t>(offs.size());
+  if (ncand) {
+    DevBuf doff = upload(ctx, offs), dai = upload(ctx, ai);
+    DevBuf fl(ctx, ncand);
+    SB_CK(launch_scaled_slice_nonzero(B->data.d(), A->data.d(), doff.as<int64_t>(), dai.as<int64_t>(), ncand, chunk,
+                                      fl.as<uint8_t>(), ctx->stream));
+    ctx->note_launch();
+    nz = download<uint8_t>(ctx, fl.raw(), ncand);
+  }
+  CKeys ck(C);
+  std::vector<int64_t> cq;
+  std::vector<int64_t> k(PC);
+  for (int64_t q = 0; q < ncand; ++q) {
+    if (!nz[q]) continue;
+    const int64_t a = q / nB, b = q % nB;
+    for (int t = 0; t < PC; ++t) k[t] = srcA[t] ? A->key(a)[srcA[t] - 1] : B->key(b)[srcB[t] - 1];
+    ck.touch(k);
+    cq.push_back(q);
+  }
+  auto ord = ck.order();
+  reset_output(ctx, C, static_cast<int64_t>(ord.size()), static_cast<int64_t>(ord.size()) * chunk);
+  ck.commit_keys(C, ord);
+  AxpyPlan ap;
+  for (size_t c = 0; c < ord.size(); ++c) {
+    ap.add_seg(static_cast<int64_t>(c) * chunk, chunk);
+    for (int ci : ck.contribs[ord[c]]) ap.add(offs[cq[ci]], ai[cq[ci]]);
+  }
+  ap.launch(ctx, B->data.d(), A->data.d(), C.data.d());
+}
+
+// ══════════════════════════ aliased kernels ══════════════════════════════
+//
+// Template bookkeeping of _aliased_contribute! / _commit_aliased_dicts!
+// (contract_aliased.jl:75-146) decided on template ids (structure); scalar
+// sums, template products and demoted accumulators computed on the device.
+
+struct AliasBook {
+  struct Contrib {
+    int tid;        // 1-based combined template id
+    ScalarTerm sc;  // scalar = sa[ia] * sb[ib] (ib < 0: sa[ia])
+  };
+  std::vector<std::vector<int64_t>> keys;
+  std::vector<int64_t> lins;
+  std::unordered_map<int64_t, int> index;
+  std::vector<std::vector<Contrib>> contribs;
+  int PC;
+  std::vector<int64_t> cdims;
+  AliasBook(const Tensor& C) : PC(C.P()), cdims(C.dims) {}
+  void contribute(const std::vector<int64_t>& k, int tid, ScalarTerm sc) {
+    const int64_t l = lin0(k.data(), cdims.data(), PC);
+    auto it = index.find(l);
+    int id;
+    if (it == index.end()) {
+      id = static_cast<int>(keys.size());
+      index.emplace(l, id);
+      keys.push_back(k);
+      lins.push_back(l);
+      contribs.emplace_back();
+    } else {
+      id = it->second;
+    }
+    contribs[id].push_back(Contrib{tid, sc});
+  }
+  // templates: device buffer holding n_combined templates; produces C.
+  void commit(Ctx* ctx, Tensor& C, DevBuf&& templates, int64_t n_combined, const double* sa, const double* sb) {
+    const int64_t blk = C.blksize();
+    const int nk = static_cast<int>(keys.size());
+    // Replay the alias/accum state machine on template ids.
+    std::vector<char> demoted(nk, 0);
+    std::vector<int> alias_tid(nk, 0);
+    std::vector<ScalarTerm> terms;
+    std::vector<int32_t> seg{0};
+    std::vector<int64_t> alias_seg(nk, -1);  // scalar segment of an aliased key
+    struct AccEntry { int tid; int64_t seg; };
+    std::vector<std::vector<AccEntry>> acc(nk);
+    for (int id = 0; id < nk; ++id) {
+      const auto& cs = contribs[id];
+      size_t q = 0;
+      const int t0 = cs[0].tid;
+      while (q < cs.size() && cs[q].tid == t0) terms.push_back(cs[q++].sc);
+      seg.push_back(static_cast<int32_t>(terms.size()));
+      const int64_t first_seg = static_cast<int64_t>(seg.size()) - 2;
+      if (q == cs.size()) {
+        alias_tid[id] = t0;
+        alias_seg[id] = first_seg;
+        continue;
+      }
+      demoted[id] = 1;
+      acc[id].push_back(AccEntry{t0, first_seg});
+      for (; q < cs.size(); ++q) {
+        terms.push_back(cs[q].sc);
+        seg.push_back(static_cast<int32_t>(terms.size()));
+        acc[id].push_back(AccEntry{cs[q].tid, static_cast<int64_t>(seg.size()) - 2});
+      }
+    }
+    const int64_t nseg = static_cast<int64_t>(seg.size()) - 1;
+    DevBuf sv(ctx, nseg * sizeof(double));
+    if (nseg) {
+      DevBuf dt = upload(ctx, terms), ds = upload(ctx, seg);
+      SB_CK(launch_scalar_prog(sa, sb, dt.as<ScalarTerm>(), ds.as<int32_t>(), nseg, sv.d(), ctx->stream));
+      ctx->note_launch();
+    }
+    // Commit: aliased keys keep (tid, scalar); demoted keys get new templates.
+    std::vector<int> order_alias, order_acc;
+    for (int id = 0; id < nk; ++id) (demoted[id] ? order_acc : order_alias).push_back(id);
+    const int64_t n_acc = static_cast<int64_t>(order_acc.size());
+    const int64_t ntot = n_combined + n_acc;
+    DevBuf all(ctx, ntot * blk * sizeof(double));
+    if (n_combined)
+      SB_CK(cudaMemcpyAsync(all.raw(), templates.raw(), n_combined * blk * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    AxpyPlan ap;
+    for (int64_t j = 0; j < n_acc; ++j) {
+      ap.add_seg((n_combined + j) * blk, blk);
+      for (auto& e : acc[order_acc[j]]) ap.add((e.tid - 1) * blk, e.seg);
+    }
+    ap.launch(ctx, templates.d(), sv.d(), all.d());
+    // per-key (tid, scalar-segment) in commit order, then sorted by lin
+    std::vector<int> commit_ids(order_alias);
+    commit_ids.insert(commit_ids.end(), order_acc.begin(), order_acc.end());
+    std::vector<int64_t> tids(nk), segidx(nk);
+    for (size_t j = 0; j < order_alias.size(); ++j) {
+      tids[j] = alias_tid[order_alias[j]];
+      segidx[j] = alias_seg[order_alias[j]];
+    }
+    for (int64_t j = 0; j < n_acc; ++j) {
+      tids[order_alias.size() + j] = n_combined + j + 1;
+      segidx[order_alias.size() + j] = -1;  // scalar 1
+    }
+    std::vector<int> p(nk);
+    std::iota(p.begin(), p.end(), 0);
+    std::stable_sort(p.begin(), p.end(), [&](int a, int b) { return lins[commit_ids[a]] < lins[commit_ids[b]]; });
+    C.keys.clear();
+    C.alias_ids.assign(nk, 0);
+    std::vector<int64_t> sidx(nk);
+    for (int i = 0; i < nk; ++i) {
+      const int src = p[i];
+      const auto& k = keys[commit_ids[src]];
+      C.keys.insert(C.keys.end(), k.begin(), k.end());
+      C.alias_ids[i] = tids[src];
+      sidx[i] = segidx[src];
+    }
+    C.nkeys = nk;
+    C.n_templates = ntot;
+    C.data = std::move(all);
+    // scalars: segment sums for aliased keys, 1.0 for demoted keys
+    C.scalars = DevBuf(ctx, nk * sizeof(double));
+    std::vector<int64_t> gidx, gdst;
+    for (int i = 0; i < nk; ++i)
+      if (sidx[i] >= 0) { gidx.push_back(sidx[i]); gdst.push_back(i); }
+    if (nk) {
+      std::vector<double> host_ones(nk, 1.0);
+      SB_CK(cudaMemcpyAsync(C.scalars.raw(), host_ones.data(), nk * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+      if (!gidx.empty()) {
+        DevBuf dg = upload(ctx, gidx), dd = upload(ctx, gdst);
+        DevBuf tmp(ctx, gidx.size() * sizeof(double));
+        SB_CK(launch_gather(sv.d(), dg.as<int64_t>(), static_cast<int64_t>(gidx.size()), tmp.d(), ctx->stream));
+        SB_CK(launch_scatter(tmp.d(), dd.as<int64_t>(), static_cast<int64_t>(gidx.size()), C.scalars.d(), ctx->stream));
+        ctx->note_launch(2);
+      }
+    }
+  }
+};
+
+void reset_aliased(Ctx* ctx, Tensor& C) {
+  C.keys.clear();
+  C.alias_ids.clear();
+  C.nkeys = 0;
+  C.n_templates = 0;
+  C.data = DevBuf();
+  C.scalars = DevBuf();
+  (void)ctx;
+}
+
+void aliased_coo_dense(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Label& r) {
+  const int PC = C.P();
+  Op A = coo_align_to_cprefix(ctx, A0, lC, PC, r);
+  Op B = dense_c_tail_r_last(ctx, B0, lC, PC, r);
+  const int64_t R = B->dims.back(), chunk = B->numel() / R;
+  require(C.blksize() == chunk, SB_ERR_DIM_MISMATCH, "C.blksize must equal prod(B dims without r)");
+  reset_aliased(ctx, C);
+  AliasBook book(C);
+  std::unordered_map<int64_t, int> rv_tid;
+  std::vector<int64_t> tmpl_src;  // B column offsets of the templates
+  const int NA = A->N();
+  for (int64_t i = 0; i < A->nkeys; ++i) {
+    const int64_t rv = A->key(i)[NA - 1];
+    if (rv < 1 || rv > R) continue;
+    auto it = rv_tid.find(rv);
+    int tid;
+    if (it == rv_tid.end()) {
+      tmpl_src.push_back((rv - 1) * chunk);
+      tid = static_cast<int>(tmpl_src.size());
+      rv_tid.emplace(rv, tid);
+    } else {
+      tid = it->second;
+    }
+    book.contribute(std::vector<int64_t>(A->key(i), A->key(i) + PC), tid, ScalarTerm{i, -1});
+  }
+  const int64_t nt = static_cast<int64_t>(tmpl_src.size());
+  DevBuf tmpl(ctx, nt * chunk * sizeof(double));
+  if (nt) {
+    std::vector<int64_t> idx(nt * chunk);
+    for (int64_t t = 0; t < nt; ++t)
+      for (int64_t e = 0; e < chunk; ++e) idx[t * chunk + e] = tmpl_src[t] + e;
+    DevBuf di = upload(ctx, idx);
+    SB_CK(launch_gather(B->data.d(), di.as<int64_t>(), nt * chunk, tmpl.d(), ctx->stream));
+    ctx->note_launch();
+  }
+  book.commit(ctx, C, std::move(tmpl), nt, A->data.d(), nullptr);
+}
+
+Op aliased_r_last_prefix(Ctx* ctx, const Op& A, const Label& r) {
+  const int ax = find(A.labels, r) + 1;
+  require(ax >= 1 && ax <= A->P(), SB_ERR_LABEL, "rlab must be in sparse prefix");
+  if (ax == A->P()) return view(*A.t, A.labels);
+  return permuted(ctx, A, perm_r_last(A->P(), A->N(), ax));
+}
+Op aliased_r_last_dense(Ctx* ctx, const Op& A, const Label& r) {
+  const int ax = find(A.labels, r) + 1;
+  require(ax > A->P(), SB_ERR_LABEL, "rlab must be in dense tail");
+  if (ax == A->N()) return view(*A.t, A.labels);
+  return permuted(ctx, A, perm_r_last(A->P(), A->N(), ax));
+}
+
+void aliased_ad(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Label& r) {
+  require(!has(lC, r), SB_ERR_LABEL, "rlab must be reduced");
+  const int PC = C.P();
+  const int NB = B0->N();
+  const int axB = find(B0.labels, r) + 1;
+  require(axB >= 1, SB_ERR_LABEL, "rlab must be an axis of B");
+  Op B = axB == NB ? view(*B0.t, B0.labels) : permuted(ctx, B0, move_axis_last(NB, axB));
+  const int64_t R = B->dims.back(), chunkB = B->numel() / R;
+  Labels Bwo(B.labels.begin(), B.labels.end() - 1), Cd(lC.begin() + PC, lC.end());
+  const bool r_prefix = find(A0.labels, r) < A0->P();
+  if (r_prefix) {  // _contract_aliased_prefix_outer_ad! (contract_aliased.jl:154-237)
+    Op A = aliased_r_last_prefix(ctx, A0, r);
+    const int PA = A->P();
+    Labels Ad(A.labels.begin() + PA, A.labels.end());
+    Labels AB(Ad), BA(Bwo);
+    AB.insert(AB.end(), Bwo.begin(), Bwo.end());
+    BA.insert(BA.end(), Ad.begin(), Ad.end());
+    bool ab;
+    if (Cd == AB) ab = true;
+    else if (Cd == BA) ab = false;
+    else fail(SB_ERR_UNSUPPORTED_LAYOUT, "C dense tail must be [A_dense...,B_wo_r...] or [B_wo_r...,A_dense...]");
+    const int64_t blkA = A->blksize();
+    require(C.blksize() == blkA * chunkB, SB_ERR_DIM_MISMATCH, "C.blksize must equal A.blksize * chunkB");
+    std::vector<int> src;
+    for (int j = 0; j < PC; ++j) {
+      const int ia = find(A.labels, lC[j]);
+      require(ia >= 0 && ia < PA && !(lC[j] == r), SB_ERR_LABEL, "C prefix label must come from A sparse prefix excluding rlab");
+      src.push_back(ia + 1);
+    }
+    reset_aliased(ctx, C);
+    AliasBook book(C);
+    std::map<std::pair<int64_t, int64_t>, int> ctm;
+    std::vector<std::pair<int64_t, int64_t>> jobs;  // (tidA, rv)
+    std::vector<int64_t> k(PC);
+    for (int64_t i = 0; i < A->nkeys; ++i) {
+      const int64_t rv = A->key(i)[PA - 1];
+      if (rv < 1 || rv > R) continue;
+      const int64_t tA = A->alias_ids[i];
+      auto key = std::make_pair(tA, rv);
+      auto it = ctm.find(key);
+      int ct;
+      if (it == ctm.end()) { jobs.push_back(key); ct = static_cast<int>(jobs.size()); ctm.emplace(key, ct); }
+      else ct = it->second;
+      for (int q = 0; q < PC; ++q) k[q] = A->key(i)[src[q] - 1];
+      book.contribute(k, ct, ScalarTerm{i, -1});
+    }
+    const int64_t blkC = C.blksize(), nt = static_cast<int64_t>(jobs.size());
+    DevBuf tmpl(ctx, nt * blkC * sizeof(double));
+    OuterPlan op;
+    for (int64_t t = 0; t < nt; ++t) {
+      op.add_cblock(t * blkC, ab ? blkA : chunkB, ab ? chunkB : blkA);
+      if (ab) op.add_pair((jobs[t].first - 1) * blkA, (jobs[t].second - 1) * chunkB);
+      else op.add_pair((jobs[t].second - 1) * chunkB, (jobs[t].first - 1) * blkA);
+    }
+    if (ab) op.launch(ctx, A->data.d(), B->data.d(), tmpl.d(), false);
+    else op.launch(ctx, B->data.d(), A->data.d(), tmpl.d(), false);
+    book.commit(ctx, C, std::move(tmpl), nt, A->scalars.d(), nullptr);
+    return;
+  }
+  // _contract_aliased_dense_ad! (contract_aliased.jl:244-365)
+  Op A = aliased_r_last_dense(ctx, A0, r);
+  const int PA = A->P();
+  require(PC == PA, SB_ERR_ASSERTION, "C sparse prefix must equal A sparse prefix for dense-tail reduction");
+  require(A->dims.back() == R, SB_ERR_DIM_MISMATCH, "Reduction size R mismatch between A dense tail and B");
+  const int64_t chunkA = A->blksize() / R;
+  require(C.blksize() == chunkA * chunkB, SB_ERR_DIM_MISMATCH, "C.blksize must equal chunkA*chunkB");
+  Labels Awo(A.labels.begin() + PA, A.labels.end() - 1);
+  Labels AB(Awo), BA(Bwo);
+  AB.insert(AB.end(), Bwo.begin(), Bwo.end());
+  BA.insert(BA.end(), Awo.begin(), Awo.end());
+  bool ab;
+  if (Cd == AB) ab = true;
+  else if (Cd == BA) ab = false;
+  else fail(SB_ERR_UNSUPPORTED_LAYOUT, "C dense tail must be [A_dense_wo_r...,B_wo_r...] or [B_wo_r...,A_dense_wo_r...]");
+  std::vector<int> src;
+  for (int j = 0; j < PC; ++j) {
+    const int ia = find(A.labels, lC[j]);
+    require(ia >= 0 && ia < PA, SB_ERR_LABEL, "C prefix label must come from A sparse prefix");
+    src.push_back(ia + 1);
+  }
+  const int64_t nt = A->n_templates, blkA = A->blksize(), blkC = C.blksize();
+  reset_aliased(ctx, C);
+  C.data = DevBuf(ctx, nt * blkC * sizeof(double));
+  GemmPlan gp;
+  for (int64_t t = 0; t < nt; ++t) {
+    gp.add_cblock(t * blkC, ab ? chunkA : chunkB, ab ? chunkB : chunkA);
+    if (ab) gp.add_pair(t * blkA, 0, R, chunkA, chunkB);
+    else gp.add_pair(0, t * blkA, R, chunkB, chunkA);
+  }
+  if (ab) gp.launch(ctx, A->data.d(), B->data.d(), C.data.d(), false, true);
+  else gp.launch(ctx, B->data.d(), A->data.d(), C.data.d(), false, true);
+  C.n_templates = nt;
+  const int64_t n = A->nkeys;
+  std::vector<std::vector<int64_t>> keys(n, std::vector<int64_t>(PC));
+  std::vector<int64_t> lins(n);
+  for (int64_t i = 0; i < n; ++i) {
+    for (int q = 0; q < PC; ++q) keys[i][q] = A->key(i)[src[q] - 1];
+    lins[i] = lin0(keys[i].data(), C.dims.data(), PC);
+  }
+  std::vector<int64_t> p(n);
+  std::iota(p.begin(), p.end(), 0);
+  std::stable_sort(p.begin(), p.end(), [&](int64_t a, int64_t b) { return lins[a] < lins[b]; });
+  C.keys.clear();
+  C.alias_ids.resize(n);
+  for (int64_t i = 0; i < n; ++i) {
+    C.keys.insert(C.keys.end(), keys[p[i]].begin(), keys[p[i]].end());
+    C.alias_ids[i] = A->alias_ids[p[i]];
+  }
+  C.nkeys = n;
+  C.scalars = DevBuf(ctx, n * sizeof(double));
+  if (n) {
+    DevBuf dp = upload(ctx, p);
+    SB_CK(launch_gather(A->scalars.d(), dp.as<int64_t>(), n, C.scalars.d(), ctx->stream));
+    ctx->note_launch();
+  }
+}
+
+void aliased_aa(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Label& r) {
+  require(!has(lC, r), SB_ERR_LABEL, "rlab must be reduced");
+  const int PC = C.P();
+  const bool r_prefix = find(B0.labels, r) < B0->P();
+  AliasBook book(C);
+  reset_aliased(ctx, C);
+  std::map<std::pair<int64_t, int64_t>, int> ctm;
+  std::vector<std::pair<int64_t, int64_t>> jobs;
+  std::vector<int64_t> k(PC);
+  if (r_prefix) {  // _contract_aliased_prefix_outer_aa! (contract_aliased.jl:417-520)
+    Op A = aliased_r_last_prefix(ctx, A0, r), B = aliased_r_last_prefix(ctx, B0, r);
+    const int PA = A->P(), PB = B->P();
+    require(C.blksize() == A->blksize() * B->blksize(), SB_ERR_DIM_MISMATCH, "C.blksize must equal A.blksize*B.blksize");
+    Labels Ad(A.labels.begin() + PA, A.labels.end()), Bd(B.labels.begin() + PB, B.labels.end()), Cd(lC.begin() + PC, lC.end());
+    Labels AB(Ad), BA(Bd);
+    AB.insert(AB.end(), Bd.begin(), Bd.end());
+    BA.insert(BA.end(), Ad.begin(), Ad.end());
+    int order;
+    if (Cd == AB) order = 1;
+    else if (Cd == BA) order = 2;
+    else fail(SB_ERR_UNSUPPORTED_LAYOUT, "C dense must be [A_dense...,B_dense...] or [B_dense...,A_dense...]");
+    std::vector<int> src;
+    for (int j = 0; j < PC; ++j) {
+      const int ia = find(A.labels, lC[j]);
+      if (ia >= 0 && ia != PA - 1) src.push_back(ia + 1);
+      else { const int ib = find(B.labels, lC[j]); require(ib >= 0 && ib < PB && !(lC[j] == r), SB_ERR_LABEL, "C prefix label not found in A or B"); src.push_back(-(ib + 1)); }
+    }
+    std::vector<int> jA{PA}, jB{PB};
+    merge_join(*A, jA, *B, jB, [&](int64_t a, int64_t b) {
+      auto key = std::make_pair(A->alias_ids[a], B->alias_ids[b]);
+      auto it = ctm.find(key);
+      int ct;
+      if (it == ctm.end()) { jobs.push_back(key); ct = static_cast<int>(jobs.size()); ctm.emplace(key, ct); }
+      else ct = it->second;
+      for (int q = 0; q < PC; ++q) k[q] = src[q] > 0 ? A->key(a)[src[q] - 1] : B->key(b)[-src[q] - 1];
+      book.contribute(k, ct, ScalarTerm{a, b});
+    });
+    const int64_t blkA = A->blksize(), blkB = B->blksize(), blkC = C.blksize(), nt = static_cast<int64_t>(jobs.size());
+    DevBuf tmpl(ctx, nt * blkC * sizeof(double));
+    OuterPlan op;
+    for (int64_t t = 0; t < nt; ++t) {
+      op.add_cblock(t * blkC, order == 1 ? blkA : blkB, order == 1 ? blkB : blkA);
+      if (order == 1) op.add_pair((jobs[t].first - 1) * blkA, (jobs[t].second - 1) * blkB);
+      else op.add_pair((jobs[t].second - 1) * blkB, (jobs[t].first - 1) * blkA);
+    }
+    if (order == 1) op.launch(ctx, A->data.d(), B->data.d(), tmpl.d(), false);
+    else op.launch(ctx, B->data.d(), A->data.d(), tmpl.d(), false);
+    book.commit(ctx, C, std::move(tmpl), nt, A->scalars.d(), B->scalars.d());
+    return;
+  }
+  // _contract_aliased_dense_aa! (contract_aliased.jl:527-643)
+  require(find(A0.labels, r) >= A0->P(), SB_ERR_LABEL, "rlab must be in A dense tail when it is in B dense tail");
+  Op A = aliased_r_last_dense(ctx, A0, r), B = aliased_r_last_dense(ctx, B0, r);
+  const int PA = A->P(), PB = B->P();
+  const int64_t R = A->dims.back();
+  require(B->dims.back() == R, SB_ERR_DIM_MISMATCH, "Reduction size mismatch");
+  const int64_t chunkA = A->blksize() / R, chunkB = B->blksize() / R;
+  require(C.blksize() == chunkA * chunkB, SB_ERR_DIM_MISMATCH, "C.blksize must equal chunkA*chunkB");
+  Labels Awo(A.labels.begin() + PA, A.labels.end() - 1), Bwo(B.labels.begin() + PB, B.labels.end() - 1),
+      Cd(lC.begin() + PC, lC.end());
+  Labels AB(Awo), BA(Bwo);
+  AB.insert(AB.end(), Bwo.begin(), Bwo.end());
+  BA.insert(BA.end(), Awo.begin(), Awo.end());
+  bool ab;
+  if (Cd == AB) ab = true;
+  else if (Cd == BA) ab = false;
+  else fail(SB_ERR_UNSUPPORTED_LAYOUT, "C dense tail must be [A_dense_wo_r...,B_dense_wo_r...] or swapped");
+  std::vector<int> srcA(PC, 0), srcB(PC, 0);
+  for (int j = 0; j < PC; ++j) {
+    const int ia = find(A.labels, lC[j]);
+    if (ia >= 0) { require(ia < PA, SB_ERR_LABEL, "C prefix label must be in A prefix"); srcA[j] = ia + 1; }
+    else { const int ib = find(B.labels, lC[j]); require(ib >= 0 && ib < PB, SB_ERR_LABEL, "C prefix label must be in B prefix"); srcB[j] = ib + 1; }
+  }
+  for (int64_t a = 0; a < A->nkeys; ++a)
+    for (int64_t b = 0; b < B->nkeys; ++b) {
+      auto key = std::make_pair(A->alias_ids[a], B->alias_ids[b]);
+      auto it = ctm.find(key);
+      int ct;
+      if (it == ctm.end()) { jobs.push_back(key); ct = static_cast<int>(jobs.size()); ctm.emplace(key, ct); }
+      else ct = it->second;
+      for (int q = 0; q < PC; ++q) k[q] = srcA[q] ? A->key(a)[srcA[q] - 1] : B->key(b)[srcB[q] - 1];
+      book.contribute(k, ct, ScalarTerm{a, b});
+    }
+  const int64_t blkA = A->blksize(), blkB = B->blksize(), blkC = C.blksize(), nt = static_cast<int64_t>(jobs.size());
+  DevBuf tmpl(ctx, nt * blkC * sizeof(double));
+  GemmPlan gp;
+  for (int64_t t = 0; t < nt; ++t) {
+    gp.add_cblock(t * blkC, ab ? chunkA : chunkB, ab ? chunkB : chunkA);
+    if (ab) gp.add_pair((jobs[t].first - 1) * blkA, (jobs[t].second - 1) * blkB, R, chunkA, chunkB);
+    else gp.add_pair((jobs[t].second - 1) * blkB, (jobs[t].first - 1) * blkA, R, chunkB, chunkA);
+  }
+  if (ab) gp.launch(ctx, A->data.d(), B->data.d(), tmpl.d(), false, true);
+  else gp.launch(ctx, B->data.d(), A->data.d(), tmpl.d(), false, true);
+  book.commit(ctx, C, std::move(tmpl), nt, A->scalars.d(), B->scalars.d());
+}
+
+void shared_aliased(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Labels& shared) {
+  const int PC = C.P();
+  const bool B_dense = B0->kind == DENSE;
+  SharedPlan sp = plan_shared(lC, PC, A0, B0, shared, B_dense);
+  Op A = permuted(ctx, A0, sp.permA);
+  const int PA = A->P();
+  const int nkA = static_cast<int>(sp.dkA.size());
+  const int64_t M = prod(A->dims, PA, PA + nkA), K = prod(A->dims, PA + nkA, A->N());
+  reset_aliased(ctx, C);
+  AliasBook book(C);
+  std::map<std::pair<int64_t, int64_t>, int> ctm;
+  std::vector<std::pair<int64_t, int64_t>> jobs;
+  std::vector<int64_t> k(PC);
+  const bool athenb = sp.mode == Mode::AthenB;
+  if (B_dense) {  // contract_aliased_shared.jl:103-302
+    DenseSlices ds = dense_slices(ctx, B0, sp.shared_prefix, sp.red_dense, sp.dkB);
+    const int64_t N = ds.N;
+    require(K == ds.K, SB_ERR_DIM_MISMATCH, "Reduction extent mismatch between A dense tail and B");
+    require(C.blksize() == M * N, SB_ERR_DIM_MISMATCH, "C.blksize must equal M*N");
+    std::vector<int> csrc;
+    for (int j = 0; j < PC; ++j) {
+      const int ia = find(A.labels, lC[j]);
+      require(ia >= 0 && ia < PA && !has(sp.shared_prefix, lC[j]), SB_ERR_LABEL, "C prefix label must come from A sparse prefix");
+      csrc.push_back(ia + 1);
+    }
+    std::vector<int> jA;
+    for (auto& l : sp.shared_prefix) jA.push_back(find(A.labels, l) + 1);
+    for (int64_t iA = 0; iA < A->nkeys;) {
+      const int64_t iA2 = advance_run(*A, iA, jA);
+      int64_t slab = 0, stride = 1;
+      for (size_t t = 0; t < jA.size(); ++t) {
+        slab += (A->key(iA)[jA[t] - 1] - 1) * stride;
+        stride *= ds.sp_dims[t];
+      }
+      for (int64_t a = iA; a < iA2; ++a) {
+        auto key = std::make_pair(A->alias_ids[a], slab);
+        auto it = ctm.find(key);
+        int ct;
+        if (it == ctm.end()) { jobs.push_back(key); ct = static_cast<int>(jobs.size()); ctm.emplace(key, ct); }
+        else ct = it->second;
+        for (int q = 0; q < PC; ++q) k[q] = A->key(a)[csrc[q] - 1];
+        book.contribute(k, ct, ScalarTerm{a, -1});
+      }
+      iA = iA2;
+    }
+    const int64_t blkA = A->blksize(), blkC = C.blksize(), nt = static_cast<int64_t>(jobs.size());
+    DevBuf tmpl(ctx, nt * blkC * sizeof(double));
+    GemmPlan gp;
+    for (int64_t t = 0; t < nt; ++t) {
+      const int64_t ao = (jobs[t].first - 1) * blkA, bo = jobs[t].second * ds.slab;
+      if (athenb) { gp.add_cblock(t * blkC, M, N); gp.add_pair(ao, bo, K, M, K); }
+      else { gp.add_cblock(t * blkC, N, M); gp.add_pair(bo, ao, K, K, M); }
+    }
+    if (athenb) gp.launch(ctx, A->data.d(), ds.Bp->data.d(), tmpl.d(), false, false);
+    else gp.launch(ctx, ds.Bp->data.d(), A->data.d(), tmpl.d(), true, true);
+    book.commit(ctx, C, std::move(tmpl), nt, A->scalars.d(), nullptr);
+    return;
+  }
+  // contract_aliased_shared.jl:325-523
+  Op B = permuted(ctx, B0, sp.permB);
+  const int PB = B->P();
+  const int nred = static_cast<int>(sp.red_dense.size());
+  const int64_t N = prod(B->dims, PB + nred, B->N());
+  require(K == prod(B->dims, PB, PB + nred), SB_ERR_DIM_MISMATCH, "Reduction extent mismatch between A and B dense tails");
+  require(C.blksize() == M * N, SB_ERR_DIM_MISMATCH, "C.blksize must equal M*N");
+  auto src = csrc_AB(lC, PC, A, B, true);
+  std::vector<int> jA, jB;
+  for (auto& l : sp.shared_prefix) { jA.push_back(find(A.labels, l) + 1); jB.push_back(find(B.labels, l) + 1); }
+  merge_join(*A, jA, *B, jB, [&](int64_t a, int64_t b) {
+    auto key = std::make_pair(A->alias_ids[a], B->alias_ids[b]);
+    auto it = ctm.find(key);
+    int ct;
+    if (it == ctm.end()) { jobs.push_back(key); ct = static_cast<int>(jobs.size()); ctm.emplace(key, ct); }
+    else ct = it->second;
+    for (int q = 0; q < PC; ++q) k[q] = src[q] > 0 ? A->key(a)[src[q] - 1] : B->key(b)[-src[q] - 1];
+    book.contribute(k, ct, ScalarTerm{a, b});
+  });
+  const int64_t blkA = A->blksize(), blkB = B->blksize(), blkC = C.blksize(), nt = static_cast<int64_t>(jobs.size());
+  DevBuf tmpl(ctx, nt * blkC * sizeof(double));
+  GemmPlan gp;
+  for (int64_t t = 0; t < nt; ++t) {
+    const int64_t ao = (jobs[t].first - 1) * blkA, bo = (jobs[t].second - 1) * blkB;
+    if (athenb) { gp.add_cblock(t * blkC, M, N); gp.add_pair(ao, bo, K, M, K); }
+    else { gp.add_cblock(t * blkC, N, M); gp.add_pair(bo, ao, K, K, M); }
+  }
+  if (athenb) gp.launch(ctx, A->data.d(), B->data.d(), tmpl.d(), false, false);
+  else gp.launch(ctx, B->data.d(), A->data.d(), tmpl.d(), true, true);
+  book.commit(ctx, C, std::move(tmpl), nt, A->scalars.d(), B->scalars.d());
+}
+
+}  // namespace
+
+// ══════════════════════════ dispatch ═════════════════════════════════════
+
+void contract(Ctx* ctx, Tensor& C, const Labels& lC, const Tensor& A, const Labels& lA, const Tensor& B,
+              const Labels& lB) {
+  require(static_cast<int>(lA.size()) == A.N(), SB_ERR_ASSERTION, "labelsA length must match A rank");
+  require(static_cast<int>(lB.size()) == B.N(), SB_ERR_ASSERTION, "labelsB length must match B rank");
+  require(static_cast<int>(lC.size()) == C.N(), SB_ERR_ASSERTION, "labelsC length must match C rank");
+  Op oA = view(A, lA), oB = view(B, lB);
+  if (C.kind == DENSE) {
+    // contract_bs_bs_to_dense! (contract_bs_bs.jl:736-754): P_C = 0 sink.
+    require(A.kind == BS && B.kind == BS, SB_ERR_UNSUPPORTED_TYPES, "dense C needs block-sparse A and B");
+    auto sink = make_tensor(ctx, BS, C.dims, C.N());
+    contract(ctx, *sink, lC, A, lA, B, lB);
+    const int64_t n = C.numel();
+    C.data = DevBuf(ctx, n * sizeof(double));
+    if (sink->nkeys) SB_CK(cudaMemcpyAsync(C.data.raw(), sink->data.raw(), n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    else SB_CK(cudaMemsetAsync(C.data.raw(), 0, n * sizeof(double), ctx->stream));
+    return;
+  }
+  check_c_dims(C, lC, oA, oB);
+  Labels shared, reduced;
+  for (auto& l : lA)
+    if (has(lB, l)) shared.push_back(l);
+  for (auto& l : shared)
+    if (!has(lC, l)) reduced.push_back(l);
+  if (reduced.size() == 1) {
+    require(shared.size() == 1, SB_ERR_ASSERTION, "Expected exactly 1 shared label");
+    const Label r = reduced[0];
+    require(A.dims[find(lA, r)] == B.dims[find(lB, r)], SB_ERR_DIM_MISMATCH, "Dim mismatch on shared label " + lab_str(r));
+    const Kind c = C.kind, a = A.kind, b = B.kind;
+    if (c == COO && a == COO && b == COO) return coo_coo(ctx, C, lC, oA, oB, r);
+    if (c == BS && a == BS && b == BS) {
+      if (find(lB, r) < B.P()) {
+        Op A2 = r_to_last_prefix(ctx, oA, r), B2 = r_to_last_prefix(ctx, oB, r);
+        return prefix_outer_bb(ctx, C, lC, A2, B2, r);
+      }
+      return dense_bb(ctx, C, lC, oA, oB, r);
+    }
+    if (c == BS && a == COO && b == BS) {
+      Op A2 = coo_r_last_sorted(ctx, oA, r);
+      if (find(lB, r) < B.P()) {
+        Op B2 = r_to_last_prefix(ctx, oB, r);
+        return coo_bs_prefix(ctx, C, lC, A2, B2, r);
+      }
+      return coo_bs_dense_index(ctx, C, lC, A2, oB, r);
+    }
+    if (c == BS && a == COO && b == DENSE) return coo_dense(ctx, C, lC, oA, oB, r);
+    if (c == BS && a == BS && b == DENSE) {
+      if (find(lA, r) < A.P()) return prefix_outer_bd(ctx, C, lC, oA, oB, r);
+      return dense_bd(ctx, C, lC, oA, oB, r);
+    }
+    if (c == ALIASED && a == ALIASED && b == DENSE) return aliased_ad(ctx, C, lC, oA, oB, r);
+    if (c == ALIASED && a == ALIASED && b == ALIASED) return aliased_aa(ctx, C, lC, oA, oB, r);
+    if (c == ALIASED && a == COO && b == DENSE) return aliased_coo_dense(ctx, C, lC, oA, oB, r);
+    fail(SB_ERR_UNSUPPORTED_TYPES, "no contract! kernel for this (C, A, B) storage combination");
+  }
+  const Kind c = C.kind, a = A.kind, b = B.kind;
+  if (c == BS && a == BS && b == BS) return shared_bb(ctx, C, lC, oA, oB, shared);
+  if (c == BS && a == BS && b == DENSE) return shared_bd(ctx, C, lC, oA, oB, shared);
+  if (c == ALIASED && a == ALIASED && (b == DENSE || b == ALIASED)) return shared_aliased(ctx, C, lC, oA, oB, shared);
+  fail(SB_ERR_UNSUPPORTED_TYPES, "no contract_shared! kernel for this (C, A, B) storage combination");
+}
+
+}  // namespace sb

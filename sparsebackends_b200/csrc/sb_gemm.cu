@@ -1,0 +1,209 @@
+// Grouped FP64 block GEMM for sm_100a with segmented (atomics-free) accumulation.
+//
+// Blackwell's tcgen05.mma has no f64 kind, so the FP64 tensor-core path is the
+// warp-level DMMA instruction (mma.sync.aligned.m8n8k4 .f64).  Tiles of X and
+// Y are staged into shared memory by a 3-stage cp.async pipeline that runs
+// straight across the pairs of one C block (the K loops of all pairs feeding a
+// C tile are concatenated), so one CTA owns one C tile and writes it once.
+#include "sb_kernels.hpp"
+
+namespace sb {
+namespace {
+
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool valid) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  int bytes = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+
+constexpr int kStages = 3;
+constexpr int kBK = 16;
+
+template <int BM, int BN>
+constexpr int smem_bytes() {
+  return kStages * kBK * ((BM + 4) + (BN + 4)) * 8;
+}
+
+template <int BM, int BN, int WM, int WN, bool XT, bool YT>
+__global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
+    k_gemm_f64(const double* __restrict__ X, const double* __restrict__ Y, double* __restrict__ C,
+               const GemmCBlock* __restrict__ cblocks, const GemmPair* __restrict__ pairs,
+               const GemmTile* __restrict__ tiles) {
+  constexpr int NWM = BM / WM;
+  constexpr int NWN = BN / WN;
+  constexpr int NT = NWM * NWN * 32;
+  constexpr int XP = BM + 4;  // padded k-row length: conflict-free fragment loads
+  constexpr int YP = BN + 4;
+  constexpr int MT = WM / 8;
+  constexpr int NTL = WN / 8;
+  constexpr int XLOADS = BM * kBK / NT;
+  constexpr int YLOADS = BN * kBK / NT;
+  static_assert(BM * kBK % NT == 0 && BN * kBK % NT == 0, "tile/threads mismatch");
+
+  extern __shared__ double smem[];
+  double* Xs = smem;                        // [stage][k][m]
+  double* Ys = smem + kStages * kBK * XP;   // [stage][k][n]
+
+  const GemmTile tile = tiles[blockIdx.x];
+  const GemmCBlock cb = cblocks[tile.cblock];
+  const int M = cb.M, N = cb.N;
+  const int m0 = tile.m0, n0 = tile.n0;
+  const int tid = threadIdx.x;
+
+  int total = 0;
+  for (int p = cb.pair_begin; p < cb.pair_end; ++p) total += (pairs[p].K + kBK - 1) / kBK;
+
+  int lp = cb.pair_begin;  // load cursor: pair index and k-tile within it
+  int lkt = 0;
+
+  auto issue_load = [&](int stage) {
+    const GemmPair pr = pairs[lp];
+    const int k0 = lkt * kBK;
+    const double* xb = X + pr.x_off;
+    const double* yb = Y + pr.y_off;
+    double* xs = Xs + stage * kBK * XP;
+    double* ys = Ys + stage * kBK * YP;
+#pragma unroll
+    for (int r = 0; r < XLOADS; ++r) {
+      const int e = tid + r * NT;
+      int i, k;
+      if (!XT) { i = e % BM; k = e / BM; } else { k = e % kBK; i = e / kBK; }
+      const int gi = m0 + i, gk = k0 + k;
+      const bool v = (gi < M) && (gk < pr.K);
+      const double* src = v ? (XT ? xb + gk + (int64_t)gi * pr.ldx : xb + gi + (int64_t)gk * pr.ldx) : xb;
+      cp_async8(xs + k * XP + i, src, v);
+    }
+#pragma unroll
+    for (int r = 0; r < YLOADS; ++r) {
+      const int e = tid + r * NT;
+      int k, j;
+      if (!YT) { k = e % kBK; j = e / kBK; } else { j = e % BN; k = e / BN; }
+      const int gk = k0 + k, gj = n0 + j;
+      const bool v = (gj < N) && (gk < pr.K);
+      const double* src = v ? (YT ? yb + gj + (int64_t)gk * pr.ldy : yb + gk + (int64_t)gj * pr.ldy) : yb;
+      cp_async8(ys + k * YP + j, src, v);
+    }
+    if (++lkt * kBK >= pr.K) { lkt = 0; ++lp; }
+  };
+
+  const int warp = tid >> 5, lane = tid & 31;
+  const int wm = warp % NWM, wn = warp / NWM;
+  const int g = lane >> 2, t = lane & 3;
+
+  double acc[MT][NTL][2];
+#pragma unroll
+  for (int a = 0; a < MT; ++a)
+#pragma unroll
+    for (int b = 0; b < NTL; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < kStages - 1; ++s) {
+    if (s < total) issue_load(s);
+    cp_async_commit();
+  }
+
+  for (int it = 0; it < total; ++it) {
+    cp_async_wait<kStages - 2>();
+    __syncthreads();
+    if (it + kStages - 1 < total) issue_load((it + kStages - 1) % kStages);
+    cp_async_commit();
+    const double* xs = Xs + (it % kStages) * kBK * XP + wm * WM + g;
+    const double* ys = Ys + (it % kStages) * kBK * YP + wn * WN + g;
+#pragma unroll
+    for (int k4 = 0; k4 < kBK; k4 += 4) {
+      double af[MT], bf[NTL];
+#pragma unroll
+      for (int a = 0; a < MT; ++a) af[a] = xs[(k4 + t) * XP + a * 8];
+#pragma unroll
+      for (int b = 0; b < NTL; ++b) bf[b] = ys[(k4 + t) * YP + b * 8];
+#pragma unroll
+      for (int a = 0; a < MT; ++a)
+#pragma unroll
+        for (int b = 0; b < NTL; ++b) dmma_8x8x4(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+    }
+  }
+  cp_async_wait<0>();
+
+  double* cbase = C + cb.c_off;
+#pragma unroll
+  for (int a = 0; a < MT; ++a) {
+    const int row = m0 + wm * WM + a * 8 + g;
+    if (row >= M) continue;
+#pragma unroll
+    for (int b = 0; b < NTL; ++b) {
+      const int col = n0 + wn * WN + b * 8 + 2 * t;
+      if (col < N) cbase[row + (int64_t)col * M] = acc[a][b][0];
+      if (col + 1 < N) cbase[row + (int64_t)(col + 1) * M] = acc[a][b][1];
+    }
+  }
+}
+
+template <int BM, int BN, int WM, int WN, bool XT, bool YT>
+cudaError_t launch_t(const double* X, const double* Y, double* C, const GemmCBlock* cb,
+                     const GemmPair* pr, const GemmTile* tl, int64_t ntiles, cudaStream_t s) {
+  constexpr int threads = (BM / WM) * (BN / WN) * 32;
+  constexpr int smem = smem_bytes<BM, BN>();
+  auto kern = k_gemm_f64<BM, BN, WM, WN, XT, YT>;
+  static unsigned long long configured = 0;  // one bit per device ordinal
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (!(configured & bit)) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    configured |= bit;
+  }
+  if (ntiles <= 0) return cudaSuccess;
+  if (ntiles > 0x7fffffffLL) return cudaErrorInvalidValue;
+  kern<<<static_cast<unsigned>(ntiles), threads, smem, s>>>(X, Y, C, cb, pr, tl);
+  return cudaGetLastError();
+}
+
+template <int BM, int BN, int WM, int WN>
+cudaError_t dispatch_t(bool xT, bool yT, const double* X, const double* Y, double* C,
+                       const GemmCBlock* cb, const GemmPair* pr, const GemmTile* tl, int64_t nt,
+                       cudaStream_t s) {
+  if (!xT && !yT) return launch_t<BM, BN, WM, WN, false, false>(X, Y, C, cb, pr, tl, nt, s);
+  if (!xT && yT) return launch_t<BM, BN, WM, WN, false, true>(X, Y, C, cb, pr, tl, nt, s);
+  if (xT && !yT) return launch_t<BM, BN, WM, WN, true, false>(X, Y, C, cb, pr, tl, nt, s);
+  return launch_t<BM, BN, WM, WN, true, true>(X, Y, C, cb, pr, tl, nt, s);
+}
+
+}  // namespace
+
+void gemm_tile_dims(GemmShape shape, int* bm, int* bn) {
+  switch (shape) {
+    case GemmShape::T128x32: *bm = 128; *bn = 32; break;
+    case GemmShape::T32x128: *bm = 32; *bn = 128; break;
+    default: *bm = 64; *bn = 64; break;
+  }
+}
+
+cudaError_t launch_gemm_f64(const double* X, const double* Y, double* C,
+                            const GemmCBlock* d_cblocks, const GemmPair* d_pairs,
+                            const GemmTile* d_tiles, int64_t ntiles, bool xT, bool yT,
+                            GemmShape shape, cudaStream_t s) {
+  switch (shape) {
+    case GemmShape::T128x32:
+      return dispatch_t<128, 32, 32, 32>(xT, yT, X, Y, C, d_cblocks, d_pairs, d_tiles, ntiles, s);
+    case GemmShape::T32x128:
+      return dispatch_t<32, 128, 32, 32>(xT, yT, X, Y, C, d_cblocks, d_pairs, d_tiles, ntiles, s);
+    default:
+      return dispatch_t<64, 64, 32, 32>(xT, yT, X, Y, C, d_cblocks, d_pairs, d_tiles, ntiles, s);
+  }
+}
+
+}  // namespace sb

@@ -1,0 +1,173 @@
+// Host-side data structures of libsparseb: context, device buffers, tensors.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/sparseb.h"
+#include "sb_kernels.hpp"
+
+namespace sb {
+
+struct Error : std::runtime_error {
+  sb_status code;
+  Error(sb_status c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] inline void fail(sb_status c, const std::string& m) { throw Error(c, m); }
+inline void require(bool cond, sb_status c, const std::string& m) {
+  if (!cond) fail(c, m);
+}
+void check_cuda(cudaError_t e, const char* what);
+#define SB_CK(x) ::sb::check_cuda((x), #x)
+
+struct Ctx;
+
+// Stream-ordered device buffer of doubles (or raw bytes), freed on the
+// owning context's stream.
+class DevBuf {
+ public:
+  DevBuf() = default;
+  DevBuf(Ctx* ctx, size_t bytes);
+  ~DevBuf();
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept { *this = std::move(o); }
+  DevBuf& operator=(DevBuf&& o) noexcept;
+  void reset();
+  void* raw() const { return p_; }
+  double* d() const { return static_cast<double*>(p_); }
+  template <class T>
+  T* as() const { return static_cast<T*>(p_); }
+  size_t bytes() const { return n_; }
+
+ private:
+  Ctx* ctx_ = nullptr;
+  void* p_ = nullptr;
+  size_t n_ = 0;
+};
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string last_error;
+  int64_t launches = 0;
+  // Deferred frees of host staging buffers are not needed: uploads copy from
+  // pageable memory synchronously with respect to the host.
+  void note_launch(int64_t n = 1) { launches += n; }
+  void sync();
+};
+
+// Upload a host vector to a new device buffer (stream-ordered).
+template <class T>
+DevBuf upload(Ctx* ctx, const std::vector<T>& v) {
+  DevBuf b(ctx, v.size() * sizeof(T));
+  if (!v.empty())
+    check_cuda(cudaMemcpyAsync(b.raw(), v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream),
+               "upload");
+  return b;
+}
+template <class T>
+std::vector<T> download(Ctx* ctx, const void* dptr, size_t n) {
+  std::vector<T> v(n);
+  if (n) {
+    check_cuda(cudaMemcpyAsync(v.data(), dptr, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream), "download");
+    check_cuda(cudaStreamSynchronize(ctx->stream), "download sync");
+  }
+  return v;
+}
+
+enum Kind : int { DENSE = SB_KIND_DENSE, COO = SB_KIND_COO, BS = SB_KIND_BLOCKSPARSE, ALIASED = SB_KIND_ALIASED };
+
+struct Tensor {
+  Ctx* ctx = nullptr;
+  Kind kind = DENSE;
+  std::vector<int64_t> dims;
+  int n2 = 0;                 // tail count (BS / aliased); dense: nd; COO: 0
+  std::vector<int64_t> keys;  // row-major: nkeys x P (BS/aliased) or nkeys x N (COO); 1-based
+  int64_t nkeys = 0;
+  DevBuf data;                // dense values | BS blocks (packed, key order) | COO vals | aliased templates
+  // aliased only
+  int64_t n_templates = 0;
+  std::vector<int64_t> alias_ids;  // 1-based, per key
+  DevBuf scalars;                  // per key
+  // COO only
+  bool dirty = false;
+
+  int N() const { return static_cast<int>(dims.size()); }
+  int P() const { return N() - n2; }
+  int64_t blksize() const {
+    int64_t b = 1;
+    for (int i = P(); i < N(); ++i) b *= dims[i];
+    return b;
+  }
+  int64_t numel() const {
+    int64_t b = 1;
+    for (auto d : dims) b *= d;
+    return b;
+  }
+  const int64_t* key(int64_t i) const { return keys.data() + i * (kind == COO ? N() : P()); }
+  int64_t key_len() const { return kind == COO ? N() : P(); }
+  int64_t payload_len() const {
+    switch (kind) {
+      case DENSE: return numel();
+      case BS: return nkeys * blksize();
+      case COO: return nkeys;
+      default: return n_templates * blksize();
+    }
+  }
+};
+
+using TensorPtr = std::unique_ptr<Tensor>;
+
+// Column-major 0-based linear index of a 1-based key over dims[0..len).
+inline int64_t lin0(const int64_t* k, const int64_t* dims, int len) {
+  int64_t idx = 0, stride = 1;
+  for (int d = 0; d < len; ++d) {
+    idx += (k[d] - 1) * stride;
+    stride *= dims[d];
+  }
+  return idx;
+}
+
+// ── tensor utilities (sb_tensor.cpp) ─────────────────────────────────────
+TensorPtr make_tensor(Ctx* ctx, Kind kind, const std::vector<int64_t>& dims, int n2);
+void sort_bs_keys_in_place(Tensor& t);  // keys must already be sorted-able; used at creation
+TensorPtr bs_permute(Ctx* ctx, const Tensor& A, const std::vector<int>& perm1);  // 1-based perm
+TensorPtr aliased_permute(Ctx* ctx, const Tensor& A, const std::vector<int>& perm1);
+TensorPtr dense_permute(Ctx* ctx, const Tensor& A, const std::vector<int>& perm1);
+TensorPtr coo_permute(Ctx* ctx, const Tensor& A, const std::vector<int>& perm1);  // dirty, unsorted
+void coo_sort(Ctx* ctx, Tensor& A);
+TensorPtr copy_tensor(Ctx* ctx, const Tensor& A);
+TensorPtr bs_from_dense(Ctx* ctx, const Tensor& D, int n2, double atol, double rtol, bool dropzeros);
+TensorPtr coo_from_dense(Ctx* ctx, const Tensor& D, double atol, double rtol);
+TensorPtr to_dense(Ctx* ctx, const Tensor& A);
+TensorPtr aliased_to_bs(Ctx* ctx, const Tensor& A);
+void check_no_cross_perm(const std::vector<int>& perm1, int N, int P);
+bool is_identity(const std::vector<int>& perm1);
+
+// ── contraction (sb_contract.cpp) ────────────────────────────────────────
+struct Label {
+  uint64_t id, plev;
+  bool operator==(const Label& o) const { return id == o.id && plev == o.plev; }
+  bool operator!=(const Label& o) const { return !(*this == o); }
+};
+using Labels = std::vector<Label>;
+void contract(Ctx* ctx, Tensor& C, const Labels& lC, const Tensor& A, const Labels& lA, const Tensor& B,
+              const Labels& lB);
+
+}  // namespace sb
+
+struct sb_ctx {
+  sb::Ctx impl;
+};
+struct sb_tensor {
+  sb::TensorPtr impl;
+  sb_ctx* owner = nullptr;
+};

@@ -1,0 +1,381 @@
+// Bandwidth-bound kernels of the block-sparse contraction engine (sm_100a):
+// tail permutes (tiled shared-memory transposes), outer-product and scaled
+// segmented accumulation with the reference's rounding, structure flags,
+// gathers/scatters and the scalar programs of the aliased format.
+#include <algorithm>
+
+#include "sb_kernels.hpp"
+
+namespace sb {
+namespace {
+
+constexpr int kThreads = 256;
+
+inline unsigned grid_for(int64_t n, int per_block = kThreads) {
+  int64_t g = (n + per_block - 1) / per_block;
+  if (g < 1) g = 1;
+  if (g > 148LL * 32) g = 148LL * 32;  // grid-stride loops beyond this
+  return static_cast<unsigned>(g);
+}
+
+// ── outer-product accumulation ────────────────────────────────────────────
+__global__ void k_outer_acc(const double* __restrict__ A, const double* __restrict__ B,
+                            double* __restrict__ C, const OuterCBlock* __restrict__ cbs,
+                            int64_t ncb, const OuterPair* __restrict__ pairs, bool kahan) {
+  for (int64_t c = blockIdx.y; c < ncb; c += gridDim.y) {
+    const OuterCBlock cb = cbs[c];
+    const int64_t n = (int64_t)cb.M * cb.N;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+         e += (int64_t)gridDim.x * blockDim.x) {
+      const int64_t i = e % cb.M, j = e / cb.M;
+      double acc = 0.0, comp = 0.0;
+      if (kahan) {
+        for (int p = cb.pair_begin; p < cb.pair_end; ++p) {
+          const double prod = __dmul_rn(A[pairs[p].a_off + i], B[pairs[p].b_off + j]);
+          const double y = __dsub_rn(prod, comp);
+          const double t = __dadd_rn(acc, y);
+          comp = __dsub_rn(__dsub_rn(t, acc), y);
+          acc = t;
+        }
+      } else {
+        for (int p = cb.pair_begin; p < cb.pair_end; ++p)
+          acc = __dadd_rn(acc, __dmul_rn(A[pairs[p].a_off + i], B[pairs[p].b_off + j]));
+      }
+      C[cb.c_off + e] = acc;
+    }
+  }
+}
+
+// ── segmented scaled accumulation ─────────────────────────────────────────
+__global__ void k_axpy_seg(const double* __restrict__ src, const double* __restrict__ alpha,
+                           double* __restrict__ C, const AxpySeg* __restrict__ segs, int64_t nsegs,
+                           const AxpyEntry* __restrict__ ents) {
+  for (int64_t g = blockIdx.y; g < nsegs; g += gridDim.y) {
+    const AxpySeg sg = segs[g];
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < sg.len;
+         t += (int64_t)gridDim.x * blockDim.x) {
+      double acc = 0.0;
+      for (int e = sg.e_begin; e < sg.e_end; ++e) {
+        const AxpyEntry en = ents[e];
+        const double a = en.alpha_idx >= 0 ? alpha[en.alpha_idx] : 1.0;
+        acc = __dadd_rn(acc, __dmul_rn(a, src[en.src_off + t]));
+      }
+      C[sg.c_off + t] = acc;
+    }
+  }
+}
+
+// ── permutes ──────────────────────────────────────────────────────────────
+// General gather: consecutive threads write consecutive output elements.
+__global__ void k_permute_general(const double* __restrict__ src, double* __restrict__ dst,
+                                  const int64_t* __restrict__ src_off, int64_t nblocks, int64_t blk,
+                                  PermDesc d) {
+  const int64_t total = nblocks * blk;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = idx / blk;
+    int64_t e = idx - b * blk;
+    int64_t so = 0;
+    for (int r = 0; r < d.rank; ++r) {
+      const int64_t c = e % d.out_dims[r];
+      e /= d.out_dims[r];
+      so += c * d.in_strides[r];
+    }
+    dst[idx] = src[src_off[b] + so];
+  }
+}
+
+// Tiled transpose: output axis 0 (unit output stride) is read with source
+// stride sv; output axis q has unit source stride.  A 32x32 tile is read
+// coalesced along q and written coalesced along axis 0; the remaining axes
+// are a batch.
+struct TileDesc {
+  int64_t dv, du;        // extents of output axis 0 and output axis q
+  int64_t sv;            // source stride of output axis 0
+  int64_t ou;            // output stride of output axis q
+  int nb;                // number of batch axes
+  int64_t bdims[kMaxRank];
+  int64_t bsrc[kMaxRank];
+  int64_t bdst[kMaxRank];
+  int64_t nbatch, tiles_u, tiles_v;
+};
+
+__global__ void k_permute_tiled(const double* __restrict__ src, double* __restrict__ dst,
+                                const int64_t* __restrict__ src_off, int64_t blk, TileDesc d,
+                                int64_t total_ctas) {
+  __shared__ double tile[32][33];
+  for (int64_t cta = blockIdx.x; cta < total_ctas; cta += gridDim.x) {
+    int64_t t = cta;
+    const int64_t tu = t % d.tiles_u; t /= d.tiles_u;
+    const int64_t tv = t % d.tiles_v; t /= d.tiles_v;
+    int64_t bt = t % d.nbatch;
+    const int64_t b = t / d.nbatch;
+    int64_t sb = src_off[b], db = b * blk;
+    for (int r = 0; r < d.nb; ++r) {
+      const int64_t c = bt % d.bdims[r];
+      bt /= d.bdims[r];
+      sb += c * d.bsrc[r];
+      db += c * d.bdst[r];
+    }
+    const int64_t u0 = tu * 32, v0 = tv * 32;
+    // load: threadIdx.x runs along u (unit source stride)
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+      const int64_t v = v0 + yy, u = u0 + threadIdx.x;
+      if (v < d.dv && u < d.du) tile[yy][threadIdx.x] = src[sb + u + v * d.sv];
+    }
+    __syncthreads();
+    // store: threadIdx.x runs along v (unit output stride)
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+      const int64_t u = u0 + yy, v = v0 + threadIdx.x;
+      if (v < d.dv && u < d.du) dst[db + v + u * d.ou] = tile[threadIdx.x][yy];
+    }
+    __syncthreads();
+  }
+}
+
+// ── structure flags ───────────────────────────────────────────────────────
+__global__ void k_slice_nonzero(const double* __restrict__ src, const int64_t* __restrict__ off,
+                                int64_t nslices, int64_t chunk, uint8_t* __restrict__ flags,
+                                int64_t nseg) {
+  for (int64_t sgi = blockIdx.x; sgi < nseg; sgi += gridDim.x) {
+    const int64_t b = sgi / nslices, s = sgi % nslices;
+    const double* p = src + off[b] + s * chunk;
+    int any = 0;
+    for (int64_t t = threadIdx.x; t < chunk && !any; t += blockDim.x) any = (p[t] != 0.0);
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) flags[sgi] = any ? 1 : 0;
+  }
+}
+
+__global__ void k_scaled_slice_nonzero(const double* __restrict__ src, const double* __restrict__ alpha,
+                                       const int64_t* __restrict__ off, const int64_t* __restrict__ ai,
+                                       int64_t n, int64_t chunk, uint8_t* __restrict__ flags) {
+  for (int64_t q = blockIdx.x; q < n; q += gridDim.x) {
+    const double a = alpha[ai[q]];
+    const double* p = src + off[q];
+    int any = 0;
+    for (int64_t t = threadIdx.x; t < chunk && !any; t += blockDim.x) any = (__dmul_rn(a, p[t]) != 0.0);
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) flags[q] = any ? 1 : 0;
+  }
+}
+
+__global__ void k_block_max_gt(const double* __restrict__ src, int64_t nblocks, int64_t blk, double tol,
+                               uint8_t* __restrict__ flags) {
+  __shared__ double red[kThreads];
+  for (int64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
+    double m = 0.0;
+    for (int64_t t = threadIdx.x; t < blk; t += blockDim.x) {
+      const double a = fabs(src[b * blk + t]);
+      if (a > m) m = a;  // NaN never compares greater, as in the reference loop
+    }
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s && red[threadIdx.x + s] > red[threadIdx.x]) red[threadIdx.x] = red[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) flags[b] = red[0] > tol ? 1 : 0;
+    __syncthreads();
+  }
+}
+
+__global__ void k_elem_keep(const double* __restrict__ src, int64_t n, double atol, double rtol,
+                            uint8_t* __restrict__ flags) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double a = fabs(src[i]);
+    flags[i] = (a > atol + rtol * a) ? 1 : 0;
+  }
+}
+
+__global__ void k_maxabs(const double* __restrict__ src, int64_t n, double* __restrict__ out) {
+  __shared__ double red[kThreads];
+  double m = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, fabs(src[i]));
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = red[0];
+}
+
+// ── gathers / scatters ────────────────────────────────────────────────────
+__global__ void k_gather(const double* __restrict__ src, const int64_t* __restrict__ idx, int64_t n,
+                         double* __restrict__ dst) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = src[idx[i]];
+}
+__global__ void k_scatter(const double* __restrict__ src, const int64_t* __restrict__ idx, int64_t n,
+                          double* __restrict__ dst) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[idx[i]] = src[i];
+}
+__global__ void k_scale_blocks(const double* __restrict__ src, const int64_t* __restrict__ toff,
+                               const double* __restrict__ scal, int64_t nblocks, int64_t blk,
+                               double* __restrict__ dst) {
+  const int64_t total = nblocks * blk;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = i / blk, t = i - b * blk;
+    dst[i] = __dmul_rn(scal[b], src[toff[b] + t]);
+  }
+}
+__global__ void k_blocks_to_strided(const double* __restrict__ data, const int64_t* __restrict__ lin,
+                                    int64_t nblocks, int64_t blk, int64_t stride, double* __restrict__ dense) {
+  const int64_t total = nblocks * blk;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = i / blk, t = i - b * blk;
+    dense[lin[b] + stride * t] = data[i];
+  }
+}
+
+// ── scalar programs ───────────────────────────────────────────────────────
+__global__ void k_scalar_prog(const double* __restrict__ sa, const double* __restrict__ sb,
+                              const ScalarTerm* __restrict__ terms, const int32_t* __restrict__ seg,
+                              int64_t nsegs, double* __restrict__ out) {
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < nsegs; g += (int64_t)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    bool first = true;
+    for (int e = seg[g]; e < seg[g + 1]; ++e) {
+      const ScalarTerm tm = terms[e];
+      const double v = tm.ib >= 0 ? __dmul_rn(sa[tm.ia], sb[tm.ib]) : sa[tm.ia];
+      acc = first ? v : __dadd_rn(acc, v);
+      first = false;
+    }
+    out[g] = acc;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_outer_acc(const double* A, const double* B, double* C, const OuterCBlock* d_cb,
+                             int64_t ncb, const OuterPair* d_pairs, int64_t max_elems, bool kahan,
+                             cudaStream_t s) {
+  if (ncb <= 0 || max_elems <= 0) return cudaSuccess;
+  dim3 grid(grid_for(max_elems), static_cast<unsigned>(ncb < 65535 ? ncb : 65535));
+  if ((int64_t)grid.x * grid.y > 148LL * 64) grid.x = static_cast<unsigned>(std::max<int64_t>(1, 148LL * 64 / grid.y));
+  k_outer_acc<<<grid, kThreads, 0, s>>>(A, B, C, d_cb, ncb, d_pairs, kahan);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_axpy_seg(const double* src, const double* d_alpha, double* C, const AxpySeg* d_segs,
+                            int64_t nsegs, const AxpyEntry* d_entries, int64_t max_len, cudaStream_t s) {
+  if (nsegs <= 0 || max_len <= 0) return cudaSuccess;
+  dim3 grid(grid_for(max_len), static_cast<unsigned>(nsegs < 65535 ? nsegs : 65535));
+  if ((int64_t)grid.x * grid.y > 148LL * 64) grid.x = static_cast<unsigned>(std::max<int64_t>(1, 148LL * 64 / grid.y));
+  k_axpy_seg<<<grid, kThreads, 0, s>>>(src, d_alpha, C, d_segs, nsegs, d_entries);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_permute_blocks(const double* src, double* dst, const int64_t* d_src_off, int64_t nblocks,
+                                  int64_t blk, const PermDesc& desc, cudaStream_t s) {
+  if (nblocks <= 0 || blk <= 0) return cudaSuccess;
+  // Find the output axis with unit source stride (q) and decide the kernel.
+  int q = -1;
+  for (int r = 0; r < desc.rank; ++r)
+    if (desc.in_strides[r] == 1 && desc.out_dims[r] > 1) { q = r; break; }
+  const bool first_unit = desc.rank == 0 || desc.in_strides[0] == 1 || desc.out_dims[0] == 1;
+  if (first_unit || q <= 0 || desc.out_dims[0] < 4 || desc.out_dims[q] < 4) {
+    k_permute_general<<<grid_for(nblocks * blk), kThreads, 0, s>>>(src, dst, d_src_off, nblocks, blk, desc);
+    return cudaGetLastError();
+  }
+  TileDesc td{};
+  td.dv = desc.out_dims[0];
+  td.du = desc.out_dims[q];
+  td.sv = desc.in_strides[0];
+  int64_t ostride = 1;
+  int nb = 0;
+  for (int r = 0; r < desc.rank; ++r) {
+    if (r == q) td.ou = ostride;
+    if (r != 0 && r != q) {
+      td.bdims[nb] = desc.out_dims[r];
+      td.bsrc[nb] = desc.in_strides[r];
+      td.bdst[nb] = ostride;
+      ++nb;
+    }
+    ostride *= desc.out_dims[r];
+  }
+  td.nb = nb;
+  td.nbatch = 1;
+  for (int r = 0; r < nb; ++r) td.nbatch *= td.bdims[r];
+  td.tiles_u = (td.du + 31) / 32;
+  td.tiles_v = (td.dv + 31) / 32;
+  const int64_t total = nblocks * td.nbatch * td.tiles_u * td.tiles_v;
+  const unsigned g = static_cast<unsigned>(total < 148LL * 64 ? total : 148LL * 64);
+  k_permute_tiled<<<g, dim3(32, 8), 0, s>>>(src, dst, d_src_off, blk, td, total);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_slice_nonzero(const double* src, const int64_t* d_off, int64_t nblocks, int64_t nslices,
+                                 int64_t chunk, uint8_t* flags, cudaStream_t s) {
+  const int64_t nseg = nblocks * nslices;
+  if (nseg <= 0) return cudaSuccess;
+  const unsigned g = static_cast<unsigned>(nseg < 148LL * 32 ? nseg : 148LL * 32);
+  k_slice_nonzero<<<g, 128, 0, s>>>(src, d_off, nslices, chunk, flags, nseg);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scaled_slice_nonzero(const double* src, const double* alpha, const int64_t* d_off,
+                                        const int64_t* d_ai, int64_t n, int64_t chunk, uint8_t* flags,
+                                        cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const unsigned g = static_cast<unsigned>(n < 148LL * 32 ? n : 148LL * 32);
+  k_scaled_slice_nonzero<<<g, 128, 0, s>>>(src, alpha, d_off, d_ai, n, chunk, flags);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_block_max_gt(const double* src, int64_t nblocks, int64_t blk, double tol, uint8_t* flags,
+                                cudaStream_t s) {
+  if (nblocks <= 0) return cudaSuccess;
+  const unsigned g = static_cast<unsigned>(nblocks < 148LL * 32 ? nblocks : 148LL * 32);
+  k_block_max_gt<<<g, kThreads, 0, s>>>(src, nblocks, blk, tol, flags);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_elem_keep(const double* src, int64_t n, double atol, double rtol, uint8_t* flags,
+                             cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_elem_keep<<<grid_for(n), kThreads, 0, s>>>(src, n, atol, rtol, flags);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_maxabs(const double* src, int64_t n, double* d_out, cudaStream_t s) {
+  k_maxabs<<<1, kThreads, 0, s>>>(src, n, d_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather(const double* src, const int64_t* d_idx, int64_t n, double* dst, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_gather<<<grid_for(n), kThreads, 0, s>>>(src, d_idx, n, dst);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter(const double* src, const int64_t* d_idx, int64_t n, double* dst, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_scatter<<<grid_for(n), kThreads, 0, s>>>(src, d_idx, n, dst);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scale_blocks(const double* src, const int64_t* d_tmpl_off, const double* d_scal,
+                                int64_t nblocks, int64_t blk, double* dst, cudaStream_t s) {
+  if (nblocks <= 0 || blk <= 0) return cudaSuccess;
+  k_scale_blocks<<<grid_for(nblocks * blk), kThreads, 0, s>>>(src, d_tmpl_off, d_scal, nblocks, blk, dst);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_blocks_to_strided(const double* data, const int64_t* d_lin, int64_t nblocks, int64_t blk,
+                                     int64_t stride, double* dense, cudaStream_t s) {
+  if (nblocks <= 0 || blk <= 0) return cudaSuccess;
+  k_blocks_to_strided<<<grid_for(nblocks * blk), kThreads, 0, s>>>(data, d_lin, nblocks, blk, stride, dense);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scalar_prog(const double* sa, const double* sb, const ScalarTerm* d_terms,
+                               const int32_t* d_seg_begin, int64_t nsegs, double* out, cudaStream_t s) {
+  if (nsegs <= 0) return cudaSuccess;
+  k_scalar_prog<<<grid_for(nsegs), kThreads, 0, s>>>(sa, sb, d_terms, d_seg_begin, nsegs, out);
+  return cudaGetLastError();
+}
+
+}  // namespace sb

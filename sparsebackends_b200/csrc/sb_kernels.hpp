@@ -1,0 +1,132 @@
+// Device kernel launchers for the block-sparse contraction engine (sm_100a).
+//
+// Every launcher enqueues work on the given stream and returns immediately.
+// Offsets are in elements (doubles) relative to the base pointers passed.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sb {
+
+// ── grouped FP64 GEMM with segmented accumulation ──────────────────────────
+//
+// For every C block c:  C_c = sum_{p in [pair_begin_c, pair_end_c)} X_p * Y_p
+// where X_p is M_c x K_p and Y_p is K_p x N_c, C_c is column-major M_c x N_c
+// (leading dimension M_c).  X is read "N" (element (i,k) at x + i + k*ldx) or
+// "T" (element (i,k) at x + k + i*ldx); Y likewise ((k,j) at y + k + j*ldy or
+// y + j + k*ldy).  Each C tile is produced by exactly one CTA: no atomics, C
+// is written once (no zero-init needed), accumulation order over pairs is the
+// pair order.
+struct GemmCBlock {
+  int64_t c_off;
+  int32_t M, N;
+  int32_t pair_begin, pair_end;
+};
+struct GemmPair {
+  int64_t x_off, y_off;
+  int32_t K, ldx, ldy, pad;
+};
+struct GemmTile {
+  int32_t cblock, m0, n0, pad;
+};
+
+enum class GemmShape : int { T64x64 = 0, T128x32 = 1, T32x128 = 2 };
+
+cudaError_t launch_gemm_f64(const double* X, const double* Y, double* C,
+                            const GemmCBlock* d_cblocks, const GemmPair* d_pairs,
+                            const GemmTile* d_tiles, int64_t ntiles,
+                            bool xT, bool yT, GemmShape shape, cudaStream_t s);
+
+// Number of tiles of a (M, N) C block for the given tile shape.
+void gemm_tile_dims(GemmShape shape, int* bm, int* bn);
+
+// ── outer-product accumulation (K = 1 pairs) on CUDA cores ─────────────────
+//
+// For every C block c: C_c[i + j*M] = sum_p a_p[i] * b_p[j] in pair order, with
+// the reference's rounding (c = c + a*b, no fusion) or Kahan compensation.
+struct OuterCBlock {
+  int64_t c_off;
+  int32_t M, N;
+  int32_t pair_begin, pair_end;
+};
+struct OuterPair {
+  int64_t a_off, b_off;
+};
+cudaError_t launch_outer_acc(const double* Abase, const double* Bbase, double* C,
+                             const OuterCBlock* d_cblocks, int64_t ncblocks,
+                             const OuterPair* d_pairs, int64_t max_elems, bool kahan,
+                             cudaStream_t s);
+
+// ── segmented scaled accumulation (axpy) ───────────────────────────────────
+//
+// For every segment g: C[c_off_g + t] = sum_{e in seg g} alpha_e * src[src_off_e + t]
+// for t < len_g, rounding as c = c + alpha*src (alpha from d_alpha[alpha_idx_e],
+// or 1.0 when alpha_idx_e < 0).
+struct AxpySeg {
+  int64_t c_off;
+  int64_t len;
+  int32_t e_begin, e_end;
+};
+struct AxpyEntry {
+  int64_t src_off;
+  int64_t alpha_idx;
+};
+cudaError_t launch_axpy_seg(const double* src, const double* d_alpha, double* C,
+                            const AxpySeg* d_segs, int64_t nsegs, const AxpyEntry* d_entries,
+                            int64_t max_len, cudaStream_t s);
+
+// ── permutes ───────────────────────────────────────────────────────────────
+//
+// dst block b (packed at b*blk) = tail-permute of src block at src_off[b].
+// out_dims[r]: output tail dims (fastest first); in_strides[r]: stride in the
+// source block of output axis r.
+constexpr int kMaxRank = 12;
+struct PermDesc {
+  int rank;
+  int64_t out_dims[kMaxRank];
+  int64_t in_strides[kMaxRank];
+};
+cudaError_t launch_permute_blocks(const double* src, double* dst, const int64_t* d_src_off,
+                                  int64_t nblocks, int64_t blk, const PermDesc& desc,
+                                  cudaStream_t s);
+
+// ── value-dependent structure helpers ──────────────────────────────────────
+// flags[b*nslices + s] = any(src[off_b + s*chunk + t] != 0, t < chunk)
+cudaError_t launch_slice_nonzero(const double* src, const int64_t* d_off, int64_t nblocks,
+                                 int64_t nslices, int64_t chunk, uint8_t* flags, cudaStream_t s);
+// flags[q] = any(alpha[ai_q] * src[off_q + t] != 0, t < chunk)
+cudaError_t launch_scaled_slice_nonzero(const double* src, const double* alpha,
+                                        const int64_t* d_off, const int64_t* d_ai, int64_t n,
+                                        int64_t chunk, uint8_t* flags, cudaStream_t s);
+// flags[b] = max_t |src[b*blk + t]| > tol
+cudaError_t launch_block_max_gt(const double* src, int64_t nblocks, int64_t blk, double tol,
+                                uint8_t* flags, cudaStream_t s);
+// flags[i] = |src[i]| > atol + rtol*|src[i]|
+cudaError_t launch_elem_keep(const double* src, int64_t n, double atol, double rtol,
+                             uint8_t* flags, cudaStream_t s);
+// max |src[i]| into *d_out (single value)
+cudaError_t launch_maxabs(const double* src, int64_t n, double* d_out, cudaStream_t s);
+
+// ── gathers / scatters ─────────────────────────────────────────────────────
+cudaError_t launch_gather(const double* src, const int64_t* d_idx, int64_t n, double* dst,
+                          cudaStream_t s);
+cudaError_t launch_scatter(const double* src, const int64_t* d_idx, int64_t n, double* dst,
+                           cudaStream_t s);
+// dst[b*blk + t] = scal[b] * src[tmpl_off[b] + t]
+cudaError_t launch_scale_blocks(const double* src, const int64_t* d_tmpl_off,
+                                const double* d_scal, int64_t nblocks, int64_t blk,
+                                double* dst, cudaStream_t s);
+// dense[lin_b + stride*t] = data[b*blk + t]
+cudaError_t launch_blocks_to_strided(const double* data, const int64_t* d_lin, int64_t nblocks,
+                                     int64_t blk, int64_t stride, double* dense, cudaStream_t s);
+
+// ── scalar programs (aliased bookkeeping) ──────────────────────────────────
+// out[g] = sum_{e in seg g} (sa[ia_e] * (ib_e >= 0 ? sb[ib_e] : 1)), left to right.
+struct ScalarTerm {
+  int64_t ia, ib;
+};
+cudaError_t launch_scalar_prog(const double* sa, const double* sb, const ScalarTerm* d_terms,
+                               const int32_t* d_seg_begin, int64_t nsegs, double* out,
+                               cudaStream_t s);
+
+}  // namespace sb

@@ -1,0 +1,397 @@
+// Tensor storage on the device: creation helpers, permutes and conversions.
+//
+// Reference: SparseBackends/src/blocksparse/{storage,conversions}.jl,
+// src/coo/{storage,conversions}.jl, src/aliased/{storage,conversions}.jl.
+// Keys (integer metadata) live on the host; every payload value lives on and
+// is produced by the device.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "sb_internal.hpp"
+
+namespace sb {
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    fail(SB_ERR_OOM, std::string("device allocation failed: ") + what);
+  }
+  fail(SB_ERR_CUDA, std::string(cudaGetErrorString(e)) + " at " + what);
+}
+
+void Ctx::sync() { SB_CK(cudaStreamSynchronize(stream)); }
+
+DevBuf::DevBuf(Ctx* ctx, size_t bytes) : ctx_(ctx), n_(bytes) {
+  if (bytes) SB_CK(cudaMallocAsync(&p_, bytes, ctx->stream));
+}
+DevBuf::~DevBuf() { reset(); }
+void DevBuf::reset() {
+  if (p_) cudaFreeAsync(p_, ctx_->stream);
+  p_ = nullptr;
+  n_ = 0;
+}
+DevBuf& DevBuf::operator=(DevBuf&& o) noexcept {
+  if (this != &o) {
+    reset();
+    ctx_ = o.ctx_;
+    p_ = o.p_;
+    n_ = o.n_;
+    o.p_ = nullptr;
+    o.n_ = 0;
+  }
+  return *this;
+}
+
+TensorPtr make_tensor(Ctx* ctx, Kind kind, const std::vector<int64_t>& dims, int n2) {
+  auto t = std::make_unique<Tensor>();
+  t->ctx = ctx;
+  t->kind = kind;
+  t->dims = dims;
+  t->n2 = n2;
+  return t;
+}
+
+bool is_identity(const std::vector<int>& p) {
+  for (size_t i = 0; i < p.size(); ++i)
+    if (p[i] != static_cast<int>(i) + 1) return false;
+  return true;
+}
+
+void check_no_cross_perm(const std::vector<int>& perm, int N, int P) {
+  require(static_cast<int>(perm.size()) == N, SB_ERR_ASSERTION, "perm length must equal rank");
+  std::vector<int> s(perm);
+  std::sort(s.begin(), s.end());
+  for (int i = 0; i < N; ++i) require(s[i] == i + 1, SB_ERR_ASSERTION, "perm must be a permutation of 1:N");
+  for (int i = 0; i < P; ++i)
+    require(perm[i] <= P, SB_ERR_ASSERTION, "No-cross reorder violated: output prefix axis uses old block axis");
+  for (int i = P; i < N; ++i)
+    require(perm[i] > P, SB_ERR_ASSERTION, "No-cross reorder violated: output block axis uses old prefix axis");
+}
+
+// Column-major strides of dims[lo..hi).
+static std::vector<int64_t> cm_strides(const std::vector<int64_t>& dims, int lo, int hi) {
+  std::vector<int64_t> s(hi - lo);
+  int64_t acc = 1;
+  for (int i = lo; i < hi; ++i) {
+    s[i - lo] = acc;
+    acc *= dims[i];
+  }
+  return s;
+}
+
+// dst block b = tail permutation of src block at src_off[b].
+static void permute_blocks(Ctx* ctx, const double* src, double* dst, const std::vector<int64_t>& src_off,
+                           int64_t blk, const std::vector<int64_t>& out_dims, const std::vector<int64_t>& in_strides) {
+  if (src_off.empty() || blk == 0) return;
+  require(out_dims.size() <= static_cast<size_t>(kMaxRank), SB_ERR_INVALID_ARG, "tail rank too large");
+  PermDesc d{};
+  // Drop unit axes; they do not move data.
+  int r = 0;
+  for (size_t i = 0; i < out_dims.size(); ++i) {
+    if (out_dims[i] == 1) continue;
+    d.out_dims[r] = out_dims[i];
+    d.in_strides[r] = in_strides[i];
+    ++r;
+  }
+  d.rank = r;
+  DevBuf doff = upload(ctx, src_off);
+  SB_CK(launch_permute_blocks(src, dst, doff.as<int64_t>(), static_cast<int64_t>(src_off.size()), blk, d, ctx->stream));
+  ctx->note_launch();
+}
+
+void sort_bs_keys_in_place(Tensor& t) {
+  (void)t;  // keys are kept sorted by construction
+}
+
+TensorPtr bs_permute(Ctx* ctx, const Tensor& A, const std::vector<int>& perm) {
+  const int N = A.N(), P = A.P();
+  check_no_cross_perm(perm, N, P);
+  std::vector<int64_t> dimsB(N);
+  for (int j = 0; j < N; ++j) dimsB[j] = A.dims[perm[j] - 1];
+  auto out = make_tensor(ctx, BS, dimsB, A.n2);
+  const int64_t n = A.nkeys, blk = A.blksize();
+  std::vector<int64_t> nk(n * P);
+  std::vector<int64_t> lin(n);
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t* k = A.key(i);
+    for (int j = 0; j < P; ++j) nk[i * P + j] = k[perm[j] - 1];
+    lin[i] = lin0(&nk[i * P], dimsB.data(), P);
+  }
+  std::vector<int64_t> p(n);
+  std::iota(p.begin(), p.end(), 0);
+  std::stable_sort(p.begin(), p.end(), [&](int64_t a, int64_t b) { return lin[a] < lin[b]; });
+  out->keys.resize(n * P);
+  for (int64_t i = 0; i < n; ++i)
+    std::copy(&nk[p[i] * P], &nk[p[i] * P] + P, &out->keys[i * P]);
+  out->nkeys = n;
+  out->data = DevBuf(ctx, n * blk * sizeof(double));
+  std::vector<int64_t> soff(n);
+  for (int64_t i = 0; i < n; ++i) soff[i] = p[i] * blk;
+  auto so = cm_strides(A.dims, P, N);
+  std::vector<int64_t> od(A.n2), is(A.n2);
+  for (int r = 0; r < A.n2; ++r) {
+    od[r] = dimsB[P + r];
+    is[r] = so[perm[P + r] - 1 - P];
+  }
+  permute_blocks(ctx, A.data.d(), out->data.d(), soff, blk, od, is);
+  return out;
+}
+
+TensorPtr aliased_permute(Ctx* ctx, const Tensor& A, const std::vector<int>& perm) {
+  const int N = A.N(), P = A.P();
+  check_no_cross_perm(perm, N, P);
+  std::vector<int64_t> dimsB(N);
+  for (int j = 0; j < N; ++j) dimsB[j] = A.dims[perm[j] - 1];
+  auto out = make_tensor(ctx, ALIASED, dimsB, A.n2);
+  const int64_t blk = A.blksize();
+  out->n_templates = A.n_templates;
+  out->data = DevBuf(ctx, A.n_templates * blk * sizeof(double));
+  std::vector<int64_t> soff(A.n_templates);
+  for (int64_t t = 0; t < A.n_templates; ++t) soff[t] = t * blk;
+  auto so = cm_strides(A.dims, P, N);
+  std::vector<int64_t> od(A.n2), is(A.n2);
+  for (int r = 0; r < A.n2; ++r) {
+    od[r] = dimsB[P + r];
+    is[r] = so[perm[P + r] - 1 - P];
+  }
+  permute_blocks(ctx, A.data.d(), out->data.d(), soff, blk, od, is);
+  const int64_t n = A.nkeys;
+  std::vector<int64_t> nk(n * P), lin(n);
+  for (int64_t i = 0; i < n; ++i) {
+    for (int j = 0; j < P; ++j) nk[i * P + j] = A.key(i)[perm[j] - 1];
+    lin[i] = lin0(&nk[i * P], dimsB.data(), P);
+  }
+  std::vector<int64_t> p(n);
+  std::iota(p.begin(), p.end(), 0);
+  std::stable_sort(p.begin(), p.end(), [&](int64_t a, int64_t b) { return lin[a] < lin[b]; });
+  out->keys.resize(n * P);
+  out->alias_ids.resize(n);
+  for (int64_t i = 0; i < n; ++i) {
+    std::copy(&nk[p[i] * P], &nk[p[i] * P] + P, &out->keys[i * P]);
+    out->alias_ids[i] = A.alias_ids[p[i]];
+  }
+  out->nkeys = n;
+  out->scalars = DevBuf(ctx, n * sizeof(double));
+  if (n) {
+    DevBuf dp = upload(ctx, p);
+    SB_CK(launch_gather(A.scalars.d(), dp.as<int64_t>(), n, out->scalars.d(), ctx->stream));
+    ctx->note_launch();
+  }
+  return out;
+}
+
+TensorPtr dense_permute(Ctx* ctx, const Tensor& A, const std::vector<int>& perm) {
+  const int N = A.N();
+  require(static_cast<int>(perm.size()) == N, SB_ERR_ASSERTION, "perm length must equal rank");
+  std::vector<int64_t> dimsB(N);
+  for (int j = 0; j < N; ++j) dimsB[j] = A.dims[perm[j] - 1];
+  auto out = make_tensor(ctx, DENSE, dimsB, N);
+  const int64_t n = A.numel();
+  out->data = DevBuf(ctx, n * sizeof(double));
+  auto so = cm_strides(A.dims, 0, N);
+  std::vector<int64_t> is(N);
+  for (int r = 0; r < N; ++r) is[r] = so[perm[r] - 1];
+  permute_blocks(ctx, A.data.d(), out->data.d(), {0}, n, dimsB, is);
+  return out;
+}
+
+TensorPtr copy_tensor(Ctx* ctx, const Tensor& A) {
+  auto out = make_tensor(ctx, A.kind, A.dims, A.n2);
+  out->keys = A.keys;
+  out->nkeys = A.nkeys;
+  out->n_templates = A.n_templates;
+  out->alias_ids = A.alias_ids;
+  out->dirty = A.dirty;
+  const int64_t len = A.payload_len();
+  out->data = DevBuf(ctx, len * sizeof(double));
+  if (len) SB_CK(cudaMemcpyAsync(out->data.raw(), A.data.raw(), len * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  if (A.kind == ALIASED) {
+    out->scalars = DevBuf(ctx, A.nkeys * sizeof(double));
+    if (A.nkeys)
+      SB_CK(cudaMemcpyAsync(out->scalars.raw(), A.scalars.raw(), A.nkeys * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  return out;
+}
+
+TensorPtr coo_permute(Ctx* ctx, const Tensor& A, const std::vector<int>& perm) {
+  const int N = A.N();
+  require(static_cast<int>(perm.size()) == N, SB_ERR_ASSERTION, "perm length must equal rank");
+  std::vector<int> s(perm);
+  std::sort(s.begin(), s.end());
+  for (int i = 0; i < N; ++i) require(s[i] == i + 1, SB_ERR_INVALID_ARG, "perm must be a permutation of 1:N");
+  auto out = copy_tensor(ctx, A);
+  for (int j = 0; j < N; ++j) out->dims[j] = A.dims[perm[j] - 1];
+  for (int64_t i = 0; i < A.nkeys; ++i)
+    for (int j = 0; j < N; ++j) out->keys[i * N + j] = A.keys[i * N + perm[j] - 1];
+  out->dirty = true;
+  return out;
+}
+
+void coo_sort(Ctx* ctx, Tensor& A) {
+  if (!A.dirty) return;
+  const int N = A.N();
+  const int64_t n = A.nkeys;
+  std::vector<int64_t> p(n);
+  std::iota(p.begin(), p.end(), 0);
+  // sortperm(keys; by = reverse): lexicographic on the reversed tuple.
+  std::stable_sort(p.begin(), p.end(), [&](int64_t a, int64_t b) {
+    for (int d = N - 1; d >= 0; --d) {
+      const int64_t x = A.keys[a * N + d], y = A.keys[b * N + d];
+      if (x != y) return x < y;
+    }
+    return false;
+  });
+  std::vector<int64_t> nk(n * N);
+  for (int64_t i = 0; i < n; ++i) std::copy(&A.keys[p[i] * N], &A.keys[p[i] * N] + N, &nk[i * N]);
+  A.keys.swap(nk);
+  if (n) {
+    DevBuf nv(ctx, n * sizeof(double));
+    DevBuf dp = upload(ctx, p);
+    SB_CK(launch_gather(A.data.d(), dp.as<int64_t>(), n, nv.d(), ctx->stream));
+    ctx->note_launch();
+    A.data = std::move(nv);
+  }
+  A.dirty = false;
+}
+
+TensorPtr bs_from_dense(Ctx* ctx, const Tensor& D, int n2, double atol, double rtol, bool dropzeros) {
+  require(D.kind == DENSE, SB_ERR_INVALID_ARG, "blocksparse_from_dense needs a dense tensor");
+  const int N = D.N();
+  require(n2 >= 0 && n2 <= N, SB_ERR_ASSERTION, "0 <= N2 <= N required");
+  const int P = N - n2;
+  int64_t Ptot = 1, blk = 1;
+  for (int i = 0; i < P; ++i) Ptot *= D.dims[i];
+  for (int i = P; i < N; ++i) blk *= D.dims[i];
+  auto out = make_tensor(ctx, BS, D.dims, n2);
+  // Block-major copy: blocks[p*blk + t] = dense[p + Ptot*t].
+  DevBuf blocks(ctx, Ptot * blk * sizeof(double));
+  permute_blocks(ctx, D.data.d(), blocks.d(), {0}, Ptot * blk, {blk, Ptot}, {Ptot, 1});
+  double gmax = 0.0;
+  if (rtol != 0.0 && Ptot * blk > 0) {
+    DevBuf dm(ctx, sizeof(double));
+    SB_CK(launch_maxabs(D.data.d(), Ptot * blk, dm.d(), ctx->stream));
+    ctx->note_launch();
+    gmax = download<double>(ctx, dm.raw(), 1)[0];
+  }
+  const double tol = std::max(atol, rtol * gmax);
+  std::vector<uint8_t> keep(Ptot, 1);
+  if (dropzeros && Ptot > 0) {
+    DevBuf fl(ctx, Ptot);
+    SB_CK(launch_block_max_gt(blocks.d(), Ptot, blk, tol, fl.as<uint8_t>(), ctx->stream));
+    ctx->note_launch();
+    keep = download<uint8_t>(ctx, fl.raw(), Ptot);
+  }
+  std::vector<int64_t> soff;
+  for (int64_t p = 0; p < Ptot; ++p) {
+    if (!keep[p]) continue;
+    soff.push_back(p * blk);
+    int64_t r = p;
+    for (int d = 0; d < P; ++d) {
+      out->keys.push_back(r % D.dims[d] + 1);
+      r /= D.dims[d];
+    }
+  }
+  out->nkeys = static_cast<int64_t>(soff.size());
+  out->data = DevBuf(ctx, out->nkeys * blk * sizeof(double));
+  permute_blocks(ctx, blocks.d(), out->data.d(), soff, blk, {blk}, {1});
+  return out;
+}
+
+TensorPtr coo_from_dense(Ctx* ctx, const Tensor& D, double atol, double rtol) {
+  require(D.kind == DENSE, SB_ERR_INVALID_ARG, "coo_from_dense needs a dense tensor");
+  const int N = D.N();
+  const int64_t n = D.numel();
+  auto out = make_tensor(ctx, COO, D.dims, 0);
+  std::vector<uint8_t> keep;
+  if (n) {
+    DevBuf fl(ctx, n);
+    SB_CK(launch_elem_keep(D.data.d(), n, atol, rtol, fl.as<uint8_t>(), ctx->stream));
+    ctx->note_launch();
+    keep = download<uint8_t>(ctx, fl.raw(), n);
+  }
+  std::vector<int64_t> idx;
+  for (int64_t i = 0; i < n; ++i) {
+    if (!keep[i]) continue;
+    idx.push_back(i);
+    int64_t r = i;
+    for (int d = 0; d < N; ++d) {
+      out->keys.push_back(r % D.dims[d] + 1);
+      r /= D.dims[d];
+    }
+  }
+  out->nkeys = static_cast<int64_t>(idx.size());
+  out->data = DevBuf(ctx, out->nkeys * sizeof(double));
+  if (out->nkeys) {
+    DevBuf di = upload(ctx, idx);
+    SB_CK(launch_gather(D.data.d(), di.as<int64_t>(), out->nkeys, out->data.d(), ctx->stream));
+    ctx->note_launch();
+  }
+  out->dirty = false;
+  return out;
+}
+
+TensorPtr aliased_to_bs(Ctx* ctx, const Tensor& A) {
+  require(A.kind == ALIASED, SB_ERR_INVALID_ARG, "to_blocksparse needs an aliased tensor");
+  auto out = make_tensor(ctx, BS, A.dims, A.n2);
+  out->keys = A.keys;
+  out->nkeys = A.nkeys;
+  const int64_t blk = A.blksize();
+  out->data = DevBuf(ctx, A.nkeys * blk * sizeof(double));
+  if (A.nkeys) {
+    std::vector<int64_t> toff(A.nkeys);
+    for (int64_t i = 0; i < A.nkeys; ++i) toff[i] = (A.alias_ids[i] - 1) * blk;
+    DevBuf dt = upload(ctx, toff);
+    SB_CK(launch_scale_blocks(A.data.d(), dt.as<int64_t>(), A.scalars.d(), A.nkeys, blk, out->data.d(), ctx->stream));
+    ctx->note_launch();
+  }
+  return out;
+}
+
+TensorPtr to_dense(Ctx* ctx, const Tensor& A) {
+  if (A.kind == DENSE) return copy_tensor(ctx, A);
+  if (A.kind == ALIASED) {
+    auto b = aliased_to_bs(ctx, A);
+    return to_dense(ctx, *b);
+  }
+  const int N = A.N();
+  auto out = make_tensor(ctx, DENSE, A.dims, N);
+  const int64_t n = A.numel();
+  out->data = DevBuf(ctx, n * sizeof(double));
+  if (n) SB_CK(cudaMemsetAsync(out->data.raw(), 0, n * sizeof(double), ctx->stream));
+  if (A.kind == BS) {
+    const int P = A.P();
+    int64_t Ptot = 1;
+    for (int i = 0; i < P; ++i) Ptot *= A.dims[i];
+    std::vector<int64_t> lin(A.nkeys);
+    for (int64_t i = 0; i < A.nkeys; ++i) lin[i] = lin0(A.key(i), A.dims.data(), P);
+    if (A.nkeys) {
+      DevBuf dl = upload(ctx, lin);
+      SB_CK(launch_blocks_to_strided(A.data.d(), dl.as<int64_t>(), A.nkeys, A.blksize(), Ptot, out->data.d(), ctx->stream));
+      ctx->note_launch();
+    }
+  } else {  // COO: later duplicates overwrite earlier ones, as `out[coord...] = v` in order
+    std::vector<int64_t> lin(A.nkeys);
+    for (int64_t i = 0; i < A.nkeys; ++i) lin[i] = lin0(A.key(i), A.dims.data(), N);
+    std::vector<int64_t> last_src, dst;
+    std::vector<int64_t> order(A.nkeys);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return lin[a] < lin[b]; });
+    for (size_t j = 0; j < order.size(); ++j) {
+      if (j + 1 < order.size() && lin[order[j + 1]] == lin[order[j]]) continue;
+      last_src.push_back(order[j]);
+      dst.push_back(lin[order[j]]);
+    }
+    if (!dst.empty()) {
+      DevBuf ds = upload(ctx, last_src), dd = upload(ctx, dst);
+      DevBuf tmp(ctx, dst.size() * sizeof(double));
+      SB_CK(launch_gather(A.data.d(), ds.as<int64_t>(), static_cast<int64_t>(dst.size()), tmp.d(), ctx->stream));
+      SB_CK(launch_scatter(tmp.d(), dd.as<int64_t>(), static_cast<int64_t>(dst.size()), out->data.d(), ctx->stream));
+      ctx->note_launch(2);
+    }
+  }
+  return out;
+}
+
+}  // namespace sb
