@@ -74,6 +74,15 @@ SB_API void* sb_ctx_get_stream(const sb_ctx* ctx);
 SB_API sb_status sb_ctx_synchronize(sb_ctx* ctx);
 /* Number of kernels this context has launched so far.                        */
 SB_API int64_t sb_ctx_launch_count(const sb_ctx* ctx);
+/* Per-launch kernel timing (CUDA events on the context stream), the
+ * replacement of the reference's SB_TRACE stage timers
+ * (ta/contract_bs_dense.jl:46-202).  Enabling clears earlier records.       */
+SB_API sb_status sb_ctx_set_profiling(sb_ctx* ctx, int enable);
+/* Totals for one kernel class since profiling was enabled:
+ * kind 0 = block GEMM, 1 = permute, 2 = outer-product accumulation,
+ * 3 = segmented axpy, 4 = other.  Synchronises the context stream.          */
+SB_API sb_status sb_ctx_profile_summary(sb_ctx* ctx, int kind, int64_t* launches, double* total_ms,
+                                        double* flops, double* bytes);
 
 /* ── tensor creation (host arrays are copied to the device) ──────────────── */
 /* Dense tensor; data may be NULL (zeros).  Replaces the Array operands of

@@ -76,15 +76,31 @@ def _sortperm(keys: Sequence[Any], by) -> List[int]:
 # ───────────────────────────── storage types ──────────────────────────────
 
 
-@dataclass
 class BS:
-    """``NewBlockSparseSorted`` (src/blocksparse/storage.jl:3-9)."""
+    """``NewBlockSparseSorted`` (src/blocksparse/storage.jl:3-9).
 
-    dims: Tuple[int, ...]
-    n2: int
-    keys: List[Key] = field(default_factory=list)
-    ids: List[int] = field(default_factory=list)
-    data: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    Payload slots are kept as a list of per-id arrays so that appending a
+    block is O(blksize), like Julia's amortised ``append!`` (storage.jl:67-71);
+    ``data`` concatenates them on demand."""
+
+    def __init__(self, dims, n2, keys=None, ids=None, data=None):
+        self.dims = tuple(int(d) for d in dims)
+        self.n2 = int(n2)
+        self.keys: List[Key] = list(keys or [])
+        self.ids: List[int] = list(ids or [])
+        self.data = np.zeros(0) if data is None else data
+
+    @property
+    def data(self) -> np.ndarray:
+        if not self._slots:
+            return np.zeros(0)
+        return np.concatenate(self._slots)
+
+    @data.setter
+    def data(self, value) -> None:
+        v = np.asarray(value, dtype=np.float64).reshape(-1)
+        b = self.blksize
+        self._slots = [v[i * b:(i + 1) * b].copy() for i in range(len(v) // b)] if b else []
 
     @property
     def N(self) -> int:
@@ -103,12 +119,11 @@ class BS:
         dims = tuple(int(d) for d in dims)
         _assert((len(dims) == 0 and n2 == 0) or (0 < n2 <= len(dims)))
         _assert(all(d >= 1 for d in dims))
-        return BS(dims, n2, [], [], np.zeros(0))
+        return BS(dims, n2)
 
     def block(self, id_: int) -> np.ndarray:
-        """``_block_view`` (storage.jl:138-141); id is 1-based."""
-        b = self.blksize
-        return self.data[(id_ - 1) * b: id_ * b]
+        """``_block_view`` (storage.jl:138-141); id is 1-based; writes go through."""
+        return self._slots[id_ - 1]
 
     def find_key(self, k: Key) -> Tuple[int, bool]:
         """``_find_key`` (storage.jl:49-65) → (0-based insert position, found)."""
@@ -129,14 +144,14 @@ class BS:
         i, found = self.find_key(k)
         if found:
             return self.ids[i]
-        id_ = len(self.data) // self.blksize + 1
-        self.data = np.concatenate([self.data, np.zeros(self.blksize)])
+        self._slots.append(np.zeros(self.blksize))
+        id_ = len(self._slots)
         self.keys.insert(i, k)
         self.ids.insert(i, id_)
         return id_
 
     def clear(self) -> None:
-        self.keys, self.ids, self.data = [], [], np.zeros(0)
+        self.keys, self.ids, self._slots = [], [], []
 
     def blocks_by_key(self) -> Dict[Key, np.ndarray]:
         return {k: self.block(i).copy() for k, i in zip(self.keys, self.ids)}
@@ -162,7 +177,7 @@ class BS:
         for j in range(self.n2):
             lin += (I[P + j] - 1) * stride
             stride *= self.dims[P + j]
-        self.data[(id_ - 1) * self.blksize + lin] = v
+        self.block(id_)[lin] = v
 
 
 @dataclass

@@ -112,6 +112,19 @@ class Context:
     def launch_count(self) -> int:
         return int(self._lib.sb_ctx_launch_count(self._h))
 
+    PROFILE_KINDS = {"gemm": 0, "permute": 1, "outer": 2, "axpy": 3, "other": 4}
+
+    def set_profiling(self, enable: bool) -> None:
+        """Time every kernel launch with CUDA events on the context stream."""
+        _check(self, self._lib.sb_ctx_set_profiling(self._h, int(bool(enable))))
+
+    def profile(self, kind: str = "gemm") -> dict:
+        """Launch count, total ms, algorithmic FLOPs and bytes of one kernel class."""
+        n, ms, fl, by = C.c_int64(), C.c_double(), C.c_double(), C.c_double()
+        _check(self, self._lib.sb_ctx_profile_summary(self._h, self.PROFILE_KINDS[kind], C.byref(n), C.byref(ms),
+                                                      C.byref(fl), C.byref(by)))
+        return dict(launches=n.value, ms=ms.value, flops=fl.value, bytes=by.value)
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:

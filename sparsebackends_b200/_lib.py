@@ -29,6 +29,8 @@ SIGNATURES = {
     "sb_ctx_get_stream": (vp, [vp]),
     "sb_ctx_synchronize": (C.c_int, [vp]),
     "sb_ctx_launch_count": (i64, [vp]),
+    "sb_ctx_set_profiling": (C.c_int, [vp, C.c_int]),
+    "sb_ctx_profile_summary": (C.c_int, [vp, C.c_int, P_i64, P_f64, P_f64, P_f64]),
     "sb_tensor_create_dense": (C.c_int, [vp, C.c_int, P_i64, P_f64, C.POINTER(vp)]),
     "sb_tensor_create_dense_device": (C.c_int, [vp, C.c_int, P_i64, vp, C.POINTER(vp)]),
     "sb_tensor_create_bs": (C.c_int, [vp, C.c_int, P_i64, C.c_int, i64, P_i64, P_i64, P_f64, C.POINTER(vp)]),

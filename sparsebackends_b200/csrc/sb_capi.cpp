@@ -2,6 +2,9 @@
 // No C++ exception crosses this boundary: every failure becomes an
 // sb_status and a message retrievable with sb_last_error().
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 
@@ -81,6 +84,16 @@ sb_status sb_ctx_create(int device, unsigned flags, sb_ctx** out) {
       check_cuda(e, "cudaStreamCreateWithFlags");
     }
     c->impl.own_stream = true;
+    const char* tr = std::getenv("SPARSEB_TRACE");
+    c->impl.trace = tr && tr[0] && tr[0] != '0';
+    if (const char* gt = std::getenv("SPARSEB_GEMM_TILE")) {
+      const std::string v(gt);
+      if (v == "64x64") c->impl.gemm_tile = 0;
+      else if (v == "128x32") c->impl.gemm_tile = 1;
+      else if (v == "32x128") c->impl.gemm_tile = 2;
+      else if (v == "128x64") c->impl.gemm_tile = 3;
+      else if (v == "64x128") c->impl.gemm_tile = 4;
+    }
     // Keep freed device memory cached in the stream-ordered pool.
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -94,6 +107,8 @@ sb_status sb_ctx_create(int device, unsigned flags, sb_ctx** out) {
 sb_status sb_ctx_destroy(sb_ctx* ctx) {
   if (!ctx) return SB_OK;
   cudaStreamSynchronize(ctx->impl.stream);
+  ctx->impl.clear_profile();
+  ctx->impl.release_staging();
   if (ctx->impl.own_stream) cudaStreamDestroy(ctx->impl.stream);
   delete ctx;
   return SB_OK;
@@ -106,6 +121,7 @@ sb_status sb_ctx_set_stream(sb_ctx* ctx, void* stream) {
     check_ctx(ctx);
     SB_CK(cudaSetDevice(ctx->impl.device));
     SB_CK(cudaStreamSynchronize(ctx->impl.stream));
+    ctx->impl.release_staging();
     if (ctx->impl.own_stream) cudaStreamDestroy(ctx->impl.stream);
     ctx->impl.stream = static_cast<cudaStream_t>(stream);
     ctx->impl.own_stream = false;
@@ -122,6 +138,41 @@ sb_status sb_ctx_synchronize(sb_ctx* ctx) {
 }
 
 int64_t sb_ctx_launch_count(const sb_ctx* ctx) { return ctx ? ctx->impl.launches : 0; }
+
+sb_status sb_ctx_set_profiling(sb_ctx* ctx, int enable) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    ctx->impl.sync();
+    ctx->impl.clear_profile();
+    ctx->impl.profiling = enable != 0;
+  });
+}
+
+sb_status sb_ctx_profile_summary(sb_ctx* ctx, int kind, int64_t* launches, double* total_ms, double* flops,
+                                 double* bytes) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    require(kind >= 0 && kind < PROF_NKINDS, SB_ERR_INVALID_ARG, "unknown kernel class");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    ctx->impl.sync();
+    int64_t n = 0;
+    double ms = 0.0, f = 0.0, b = 0.0;
+    for (auto& r : ctx->impl.prof) {
+      if (r.kind != kind) continue;
+      float e = 0.f;
+      SB_CK(cudaEventElapsedTime(&e, r.a, r.b));
+      ++n;
+      ms += e;
+      f += r.flops;
+      b += r.bytes;
+    }
+    if (launches) *launches = n;
+    if (total_ms) *total_ms = ms;
+    if (flops) *flops = f;
+    if (bytes) *bytes = b;
+  });
+}
 
 sb_status sb_tensor_create_dense(sb_ctx* ctx, int nd, const int64_t* dims, const double* data, sb_tensor** out) {
   return guard(ctx, [&] {
@@ -368,8 +419,15 @@ sb_status sb_contract(sb_ctx* ctx, sb_tensor* C, const uint64_t* labelsC, int nC
     check_t(A);
     check_t(B);
     SB_CK(cudaSetDevice(ctx->impl.device));
+    const auto t0 = std::chrono::steady_clock::now();
     contract(&ctx->impl, *C->impl, read_labels(labelsC, nC), *A->impl, read_labels(labelsA, nA), *B->impl,
              read_labels(labelsB, nB));
+    if (ctx->impl.trace) {
+      const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      std::fprintf(stderr, "[sparseb] %s  A(kind=%d, keys=%lld) x B(kind=%d, keys=%lld) -> C(keys=%lld)  host %.3f ms\n",
+                   ctx->impl.kernel_name, A->impl->kind, static_cast<long long>(A->impl->nkeys), B->impl->kind,
+                   static_cast<long long>(B->impl->nkeys), static_cast<long long>(C->impl->nkeys), ms);
+    }
   });
 }
 

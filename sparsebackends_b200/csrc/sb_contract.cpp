@@ -181,12 +181,15 @@ struct CKeys {
   }
 };
 
+// Overwrite semantics of contract! (every kernel empties C first).  The
+// payload buffer is kept when its size does not change: every element of it
+// is rewritten by the kernel that follows.
 void reset_output(Ctx* ctx, Tensor& C, int64_t nkeys, int64_t payload) {
   C.keys.clear();
   C.alias_ids.clear();
   C.nkeys = nkeys;
   C.n_templates = 0;
-  C.data = DevBuf(ctx, payload * sizeof(double));
+  if (C.data.bytes() != static_cast<size_t>(payload) * sizeof(double)) C.data = DevBuf(ctx, payload * sizeof(double));
   C.scalars.reset();
 }
 
@@ -198,7 +201,7 @@ struct GemmPlan {
   void add_cblock(int64_t c_off, int64_t M, int64_t N) {
     require(M < (1LL << 31) && N < (1LL << 31), SB_ERR_INVALID_ARG, "block matrix extent exceeds 2^31");
     cbs.push_back(GemmCBlock{c_off, static_cast<int32_t>(M), static_cast<int32_t>(N),
-                             static_cast<int32_t>(pairs.size()), static_cast<int32_t>(pairs.size())});
+                             static_cast<int32_t>(pairs.size()), static_cast<int32_t>(pairs.size()), 0, 1});
   }
   void add_pair(int64_t x_off, int64_t y_off, int64_t K, int64_t ldx, int64_t ldy) {
     require(K < (1LL << 31) && ldx < (1LL << 31) && ldy < (1LL << 31), SB_ERR_INVALID_ARG,
@@ -215,16 +218,30 @@ struct GemmPlan {
     GemmShape shape = GemmShape::T64x64;
     if (N <= 32 && M >= 128) shape = GemmShape::T128x32;
     else if (M <= 32 && N >= 128) shape = GemmShape::T32x128;
+    else if (M >= 256 && N >= 128) shape = M >= N ? GemmShape::T128x64 : GemmShape::T64x128;
+    if (ctx->gemm_tile >= 0) shape = static_cast<GemmShape>(ctx->gemm_tile);
     int bm, bn;
     gemm_tile_dims(shape, &bm, &bn);
-    std::vector<GemmTile> tiles;
-    for (size_t c = 0; c < cbs.size(); ++c)
-      for (int n0 = 0; n0 < cbs[c].N; n0 += bn)
-        for (int m0 = 0; m0 < cbs[c].M; m0 += bm)
-          tiles.push_back(GemmTile{static_cast<int32_t>(c), m0, n0, 0});
-    DevBuf dc = upload(ctx, cbs), dp = upload(ctx, pairs), dt = upload(ctx, tiles);
-    SB_CK(launch_gemm_f64(X, Y, C, dc.as<GemmCBlock>(), dp.as<GemmPair>(), dt.as<GemmTile>(),
-                          static_cast<int64_t>(tiles.size()), xT, yT, shape, ctx->stream));
+    int64_t ntiles = 0;
+    double flops = 0.0, bytes = 0.0;
+    for (auto& c : cbs) {
+      const int64_t mt = (c.M + bm - 1) / bm, nt = (c.N + bn - 1) / bn;
+      require(ntiles + mt * nt < (1LL << 31), SB_ERR_INVALID_ARG, "too many GEMM tiles in one launch");
+      c.tile_begin = static_cast<int32_t>(ntiles);
+      c.mtiles = static_cast<int32_t>(mt);
+      ntiles += mt * nt;
+      bytes += 8.0 * c.M * c.N;
+      for (int p = c.pair_begin; p < c.pair_end; ++p) {
+        flops += 2.0 * c.M * c.N * pairs[p].K;
+        bytes += 8.0 * (static_cast<double>(c.M) + c.N) * pairs[p].K;
+      }
+    }
+    DevBuf dc = upload(ctx, cbs), dp = upload(ctx, pairs);
+    {
+      ProfScope ps(ctx, PROF_GEMM, flops, bytes);
+      SB_CK(launch_gemm_f64(X, Y, C, dc.as<GemmCBlock>(), static_cast<int32_t>(cbs.size()), dp.as<GemmPair>(), ntiles,
+                            xT, yT, shape, ctx->stream));
+    }
     ctx->note_launch();
   }
 };
@@ -245,8 +262,17 @@ struct OuterPlan {
   void launch(Ctx* ctx, const double* A, const double* B, double* C, bool kahan) {
     if (cbs.empty()) return;
     DevBuf dc = upload(ctx, cbs), dp = upload(ctx, pairs);
-    SB_CK(launch_outer_acc(A, B, C, dc.as<OuterCBlock>(), static_cast<int64_t>(cbs.size()), dp.as<OuterPair>(),
-                           max_elems, kahan, ctx->stream));
+    double flops = 0.0, bytes = 0.0;
+    for (auto& c : cbs) {
+      const double np = c.pair_end - c.pair_begin;
+      flops += 2.0 * c.M * c.N * np;
+      bytes += 8.0 * (static_cast<double>(c.M) * c.N + np * (c.M + c.N));
+    }
+    {
+      ProfScope ps(ctx, PROF_OUTER, flops, bytes);
+      SB_CK(launch_outer_acc(A, B, C, dc.as<OuterCBlock>(), static_cast<int64_t>(cbs.size()), dp.as<OuterPair>(),
+                             max_elems, kahan, ctx->stream));
+    }
     ctx->note_launch();
   }
 };
@@ -266,8 +292,17 @@ struct AxpyPlan {
   void launch(Ctx* ctx, const double* src, const double* alpha, double* C) {
     if (segs.empty()) return;
     DevBuf ds = upload(ctx, segs), de = upload(ctx, ents);
-    SB_CK(launch_axpy_seg(src, alpha, C, ds.as<AxpySeg>(), static_cast<int64_t>(segs.size()), de.as<AxpyEntry>(),
-                          max_len, ctx->stream));
+    double flops = 0.0, bytes = 0.0;
+    for (auto& g : segs) {
+      const double ne = g.e_end - g.e_begin;
+      flops += 2.0 * g.len * ne;
+      bytes += 8.0 * g.len * (1.0 + ne);
+    }
+    {
+      ProfScope ps(ctx, PROF_AXPY, flops, bytes);
+      SB_CK(launch_axpy_seg(src, alpha, C, ds.as<AxpySeg>(), static_cast<int64_t>(segs.size()), de.as<AxpyEntry>(),
+                            max_len, ctx->stream));
+    }
     ctx->note_launch();
   }
 };
@@ -297,6 +332,7 @@ void check_c_dims(const Tensor& C, const Labels& lC, const Op& A, const Op& B) {
 // ══════════════════════════ BS × BS ══════════════════════════════════════
 
 void prefix_outer_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A, const Op& B, const Label& r) {
+  ctx->kernel_name = "contract_prefix_outer_bb!";
   const int PA = A->P(), PB = B->P(), PC = C.P();
   Labels Ad(A.labels.begin() + PA, A.labels.end()), Bd(B.labels.begin() + PB, B.labels.end()),
       Cd(lC.begin() + PC, lC.end());
@@ -351,6 +387,7 @@ void prefix_outer_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A, const O
 }
 
 void dense_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Label& r) {
+  ctx->kernel_name = "contract_dense_bb!";
   const int PA = A0->P(), PB = B0->P(), PC = C.P();
   const int axA = find(A0.labels, r) + 1, axB = find(B0.labels, r) + 1;
   require(axA > PA, SB_ERR_LABEL, "rlab must be in A dense tail");
@@ -532,6 +569,7 @@ std::vector<int> csrc_AB(const Labels& lC, int PC, const Op& A, const Op& B, boo
 }
 
 void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Labels& shared) {
+  ctx->kernel_name = "contract_shared! (BS x BS)";
   const int PC = C.P();
   SharedPlan sp = plan_shared(lC, PC, A0, B0, shared, false);
   Op A = permuted(ctx, A0, sp.permA);
@@ -583,6 +621,7 @@ std::vector<int> move_axis_last(int N, int ax) {
 }
 
 void prefix_outer_bd(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Label& r) {
+  ctx->kernel_name = "contract_prefix_outer_bd!";
   const int PC = C.P();
   Op A = r_to_last_prefix(ctx, A0, r);
   const int PA = A->P();
@@ -644,6 +683,7 @@ void prefix_outer_bd(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const 
 }
 
 void dense_bd(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Label& r) {
+  ctx->kernel_name = "contract_dense_bd!";
   const int PA = A0->P(), PC = C.P();
   const int axA = find(A0.labels, r) + 1, axB = find(B0.labels, r) + 1;
   require(axA > PA, SB_ERR_LABEL, "rlab must be in A dense tail");
@@ -729,6 +769,7 @@ DenseSlices dense_slices(Ctx* ctx, const Op& B0, const Labels& sp, const Labels&
 }
 
 void shared_bd(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Labels& shared) {
+  ctx->kernel_name = "contract_shared! (BS x Dense)";
   const int PC = C.P();
   SharedPlan sp = plan_shared(lC, PC, A0, B0, shared, true);
   Op A = permuted(ctx, A0, sp.permA);
@@ -798,6 +839,7 @@ Op coo_r_last_sorted(Ctx* ctx, const Op& A, const Label& r) {
 }
 
 void coo_coo(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Label& r) {
+  ctx->kernel_name = "contract! (COO x COO)";
   Op A = coo_r_last_sorted(ctx, A0, r), B = coo_r_last_sorted(ctx, B0, r);
   const int NC = C.N(), NA = A->N(), NB = B->N();
   std::vector<std::pair<int, int>> src;
@@ -891,6 +933,7 @@ Op dense_c_tail_r_last(Ctx* ctx, const Op& B, const Labels& lC, int PC, const La
 }
 
 void coo_dense(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Label& r) {
+  ctx->kernel_name = "contract! (COO x Dense)";
   const int PC = C.P();
   require(!has(lC, r), SB_ERR_LABEL, "rlab must be reduced (not in labelsC)");
   Op A = coo_align_to_cprefix(ctx, A0, lC, PC, r);
@@ -922,6 +965,7 @@ void coo_dense(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0
 }
 
 void coo_bs_prefix(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A, const Op& B, const Label& r) {
+  ctx->kernel_name = "contract_prefix! (COO x BS)";
   const int PB = B->P(), PC = C.P(), NA = A->N();
   require(PC == NA + PB - 2, SB_ERR_ASSERTION, "PC must equal NA + PB - 2");
   require(C.n2 == B->n2, SB_ERR_ASSERTION, "C tail must equal B tail");
@@ -965,6 +1009,7 @@ void coo_bs_prefix(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A, const Op&
 }
 
 void coo_bs_dense_index(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A, const Op& B0, const Label& r) {
+  ctx->kernel_name = "contract_dense_index! (COO x BS)";
   const int PB = B0->P(), PC = C.P(), NA = A->N();
   require(!has(lC, r), SB_ERR_LABEL, "rlab must be reduced (not in labelsC)");
   require(C.n2 == B0->n2 - 1, SB_ERR_ASSERTION, "N2C must equal N2B - 1");
@@ -1166,6 +1211,7 @@ void reset_aliased(Ctx* ctx, Tensor& C) {
 }
 
 void aliased_coo_dense(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Label& r) {
+  ctx->kernel_name = "contract_aliased! (COO x Dense)";
   const int PC = C.P();
   Op A = coo_align_to_cprefix(ctx, A0, lC, PC, r);
   Op B = dense_c_tail_r_last(ctx, B0, lC, PC, r);
@@ -1217,6 +1263,7 @@ Op aliased_r_last_dense(Ctx* ctx, const Op& A, const Label& r) {
 }
 
 void aliased_ad(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Label& r) {
+  ctx->kernel_name = "contract_aliased! (Aliased x Dense)";
   require(!has(lC, r), SB_ERR_LABEL, "rlab must be reduced");
   const int PC = C.P();
   const int NB = B0->N();
@@ -1334,6 +1381,7 @@ void aliased_ad(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B
 }
 
 void aliased_aa(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Label& r) {
+  ctx->kernel_name = "contract_aliased! (Aliased x Aliased)";
   require(!has(lC, r), SB_ERR_LABEL, "rlab must be reduced");
   const int PC = C.P();
   const bool r_prefix = find(B0.labels, r) < B0->P();
@@ -1430,6 +1478,7 @@ void aliased_aa(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B
 }
 
 void shared_aliased(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Labels& shared) {
+  ctx->kernel_name = "contract_shared! (Aliased)";
   const int PC = C.P();
   const bool B_dense = B0->kind == DENSE;
   SharedPlan sp = plan_shared(lC, PC, A0, B0, shared, B_dense);

@@ -30,22 +30,29 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
 
 constexpr int kStages = 3;
 constexpr int kBK = 16;
+constexpr int kKP = kBK + 4;  // padded k-run length of k-contiguous tiles
 
-template <int BM, int BN>
-constexpr int smem_bytes() {
-  return kStages * kBK * ((BM + 4) + (BN + 4)) * 8;
-}
+// Shared-memory layout of one operand tile: the dimension that is contiguous
+// in global memory stays contiguous in shared memory (conflict-free cp.async
+// writes); the padding (rows of BM+4 or BK+4 doubles) makes the DMMA fragment
+// reads conflict-free as well.
+template <int BM, int BN, bool XT, bool YT>
+struct TileLayout {
+  static constexpr int XSZ = XT ? BM * kKP : kBK * (BM + 4);  // X: [i][k] if XT else [k][i]
+  static constexpr int YSZ = YT ? kBK * (BN + 4) : BN * kKP;  // Y: [k][j] if YT else [j][k]
+  static constexpr int bytes() { return kStages * (XSZ + YSZ) * 8; }
+  __device__ static int xidx(int i, int k) { return XT ? i * kKP + k : k * (BM + 4) + i; }
+  __device__ static int yidx(int k, int j) { return YT ? k * (BN + 4) + j : j * kKP + k; }
+};
 
 template <int BM, int BN, int WM, int WN, bool XT, bool YT>
 __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
     k_gemm_f64(const double* __restrict__ X, const double* __restrict__ Y, double* __restrict__ C,
-               const GemmCBlock* __restrict__ cblocks, const GemmPair* __restrict__ pairs,
-               const GemmTile* __restrict__ tiles) {
+               const GemmCBlock* __restrict__ cblocks, int32_t ncb, const GemmPair* __restrict__ pairs) {
+  using TL = TileLayout<BM, BN, XT, YT>;
   constexpr int NWM = BM / WM;
   constexpr int NWN = BN / WN;
   constexpr int NT = NWM * NWN * 32;
-  constexpr int XP = BM + 4;  // padded k-row length: conflict-free fragment loads
-  constexpr int YP = BN + 4;
   constexpr int MT = WM / 8;
   constexpr int NTL = WN / 8;
   constexpr int XLOADS = BM * kBK / NT;
@@ -53,13 +60,20 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
   static_assert(BM * kBK % NT == 0 && BN * kBK % NT == 0, "tile/threads mismatch");
 
   extern __shared__ double smem[];
-  double* Xs = smem;                        // [stage][k][m]
-  double* Ys = smem + kStages * kBK * XP;   // [stage][k][n]
+  double* Xs = smem;                    // kStages tiles of TL::XSZ
+  double* Ys = smem + kStages * TL::XSZ;  // kStages tiles of TL::YSZ
 
-  const GemmTile tile = tiles[blockIdx.x];
-  const GemmCBlock cb = cblocks[tile.cblock];
+  // C block of this CTA: last c with tile_begin <= blockIdx.x
+  int lo = 0, hi = ncb - 1;
+  const int bid = static_cast<int>(blockIdx.x);
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (cblocks[mid].tile_begin <= bid) lo = mid; else hi = mid - 1;
+  }
+  const GemmCBlock cb = cblocks[lo];
   const int M = cb.M, N = cb.N;
-  const int m0 = tile.m0, n0 = tile.n0;
+  const int lt = bid - cb.tile_begin;
+  const int m0 = (lt % cb.mtiles) * BM, n0 = (lt / cb.mtiles) * BN;
   const int tid = threadIdx.x;
 
   int total = 0;
@@ -73,8 +87,8 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
     const int k0 = lkt * kBK;
     const double* xb = X + pr.x_off;
     const double* yb = Y + pr.y_off;
-    double* xs = Xs + stage * kBK * XP;
-    double* ys = Ys + stage * kBK * YP;
+    double* xs = Xs + stage * TL::XSZ;
+    double* ys = Ys + stage * TL::YSZ;
 #pragma unroll
     for (int r = 0; r < XLOADS; ++r) {
       const int e = tid + r * NT;
@@ -83,7 +97,7 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
       const int gi = m0 + i, gk = k0 + k;
       const bool v = (gi < M) && (gk < pr.K);
       const double* src = v ? (XT ? xb + gk + (int64_t)gi * pr.ldx : xb + gi + (int64_t)gk * pr.ldx) : xb;
-      cp_async8(xs + k * XP + i, src, v);
+      cp_async8(xs + TL::xidx(i, k), src, v);
     }
 #pragma unroll
     for (int r = 0; r < YLOADS; ++r) {
@@ -93,7 +107,7 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
       const int gk = k0 + k, gj = n0 + j;
       const bool v = (gj < N) && (gk < pr.K);
       const double* src = v ? (YT ? yb + gj + (int64_t)gk * pr.ldy : yb + gk + (int64_t)gj * pr.ldy) : yb;
-      cp_async8(ys + k * YP + j, src, v);
+      cp_async8(ys + TL::yidx(k, j), src, v);
     }
     if (++lkt * kBK >= pr.K) { lkt = 0; ++lp; }
   };
@@ -119,15 +133,15 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
     __syncthreads();
     if (it + kStages - 1 < total) issue_load((it + kStages - 1) % kStages);
     cp_async_commit();
-    const double* xs = Xs + (it % kStages) * kBK * XP + wm * WM + g;
-    const double* ys = Ys + (it % kStages) * kBK * YP + wn * WN + g;
+    const double* xs = Xs + (it % kStages) * TL::XSZ;
+    const double* ys = Ys + (it % kStages) * TL::YSZ;
 #pragma unroll
     for (int k4 = 0; k4 < kBK; k4 += 4) {
       double af[MT], bf[NTL];
 #pragma unroll
-      for (int a = 0; a < MT; ++a) af[a] = xs[(k4 + t) * XP + a * 8];
+      for (int a = 0; a < MT; ++a) af[a] = xs[TL::xidx(wm * WM + a * 8 + g, k4 + t)];
 #pragma unroll
-      for (int b = 0; b < NTL; ++b) bf[b] = ys[(k4 + t) * YP + b * 8];
+      for (int b = 0; b < NTL; ++b) bf[b] = ys[TL::yidx(k4 + t, wn * WN + b * 8 + g)];
 #pragma unroll
       for (int a = 0; a < MT; ++a)
 #pragma unroll
@@ -151,10 +165,10 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
 }
 
 template <int BM, int BN, int WM, int WN, bool XT, bool YT>
-cudaError_t launch_t(const double* X, const double* Y, double* C, const GemmCBlock* cb,
-                     const GemmPair* pr, const GemmTile* tl, int64_t ntiles, cudaStream_t s) {
+cudaError_t launch_t(const double* X, const double* Y, double* C, const GemmCBlock* cb, int32_t ncb,
+                     const GemmPair* pr, int64_t ntiles, cudaStream_t s) {
   constexpr int threads = (BM / WM) * (BN / WN) * 32;
-  constexpr int smem = smem_bytes<BM, BN>();
+  constexpr int smem = TileLayout<BM, BN, XT, YT>::bytes();
   auto kern = k_gemm_f64<BM, BN, WM, WN, XT, YT>;
   static unsigned long long configured = 0;  // one bit per device ordinal
   int dev = 0;
@@ -168,18 +182,17 @@ cudaError_t launch_t(const double* X, const double* Y, double* C, const GemmCBlo
   }
   if (ntiles <= 0) return cudaSuccess;
   if (ntiles > 0x7fffffffLL) return cudaErrorInvalidValue;
-  kern<<<static_cast<unsigned>(ntiles), threads, smem, s>>>(X, Y, C, cb, pr, tl);
+  kern<<<static_cast<unsigned>(ntiles), threads, smem, s>>>(X, Y, C, cb, ncb, pr);
   return cudaGetLastError();
 }
 
 template <int BM, int BN, int WM, int WN>
 cudaError_t dispatch_t(bool xT, bool yT, const double* X, const double* Y, double* C,
-                       const GemmCBlock* cb, const GemmPair* pr, const GemmTile* tl, int64_t nt,
-                       cudaStream_t s) {
-  if (!xT && !yT) return launch_t<BM, BN, WM, WN, false, false>(X, Y, C, cb, pr, tl, nt, s);
-  if (!xT && yT) return launch_t<BM, BN, WM, WN, false, true>(X, Y, C, cb, pr, tl, nt, s);
-  if (xT && !yT) return launch_t<BM, BN, WM, WN, true, false>(X, Y, C, cb, pr, tl, nt, s);
-  return launch_t<BM, BN, WM, WN, true, true>(X, Y, C, cb, pr, tl, nt, s);
+                       const GemmCBlock* cb, int32_t ncb, const GemmPair* pr, int64_t nt, cudaStream_t s) {
+  if (!xT && !yT) return launch_t<BM, BN, WM, WN, false, false>(X, Y, C, cb, ncb, pr, nt, s);
+  if (!xT && yT) return launch_t<BM, BN, WM, WN, false, true>(X, Y, C, cb, ncb, pr, nt, s);
+  if (xT && !yT) return launch_t<BM, BN, WM, WN, true, false>(X, Y, C, cb, ncb, pr, nt, s);
+  return launch_t<BM, BN, WM, WN, true, true>(X, Y, C, cb, ncb, pr, nt, s);
 }
 
 }  // namespace
@@ -188,21 +201,26 @@ void gemm_tile_dims(GemmShape shape, int* bm, int* bn) {
   switch (shape) {
     case GemmShape::T128x32: *bm = 128; *bn = 32; break;
     case GemmShape::T32x128: *bm = 32; *bn = 128; break;
+    case GemmShape::T128x64: *bm = 128; *bn = 64; break;
+    case GemmShape::T64x128: *bm = 64; *bn = 128; break;
     default: *bm = 64; *bn = 64; break;
   }
 }
 
 cudaError_t launch_gemm_f64(const double* X, const double* Y, double* C,
-                            const GemmCBlock* d_cblocks, const GemmPair* d_pairs,
-                            const GemmTile* d_tiles, int64_t ntiles, bool xT, bool yT,
-                            GemmShape shape, cudaStream_t s) {
+                            const GemmCBlock* d_cblocks, int32_t ncb, const GemmPair* d_pairs,
+                            int64_t ntiles, bool xT, bool yT, GemmShape shape, cudaStream_t s) {
   switch (shape) {
     case GemmShape::T128x32:
-      return dispatch_t<128, 32, 32, 32>(xT, yT, X, Y, C, d_cblocks, d_pairs, d_tiles, ntiles, s);
+      return dispatch_t<128, 32, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, s);
     case GemmShape::T32x128:
-      return dispatch_t<32, 128, 32, 32>(xT, yT, X, Y, C, d_cblocks, d_pairs, d_tiles, ntiles, s);
+      return dispatch_t<32, 128, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, s);
+    case GemmShape::T128x64:
+      return dispatch_t<128, 64, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, s);
+    case GemmShape::T64x128:
+      return dispatch_t<64, 128, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, s);
     default:
-      return dispatch_t<64, 64, 32, 32>(xT, yT, X, Y, C, d_cblocks, d_pairs, d_tiles, ntiles, s);
+      return dispatch_t<64, 64, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, s);
   }
 }
 

@@ -52,25 +52,67 @@ class DevBuf {
   size_t n_ = 0;
 };
 
+// Kernel classes reported by the in-library profiler.
+enum ProfKind : int { PROF_GEMM = 0, PROF_PERMUTE = 1, PROF_OUTER = 2, PROF_AXPY = 3, PROF_OTHER = 4, PROF_NKINDS = 5 };
+
 struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   std::string last_error;
   int64_t launches = 0;
-  // Deferred frees of host staging buffers are not needed: uploads copy from
-  // pageable memory synchronously with respect to the host.
+  // Optional per-launch timing: a pair of CUDA events on the context stream
+  // around every kernel, with the launch's algorithmic FLOPs and bytes.
+  struct ProfRec {
+    int kind;
+    cudaEvent_t a, b;
+    double flops, bytes;
+  };
+  bool profiling = false;
+  std::vector<ProfRec> prof;
+  // SPARSEB_TRACE=1 (read once at context creation): one line per contract!
+  // call on stderr with the kernel chosen, block counts and host time.
+  bool trace = false;
+  const char* kernel_name = "";
+  // SPARSEB_GEMM_TILE=<BM>x<BN> forces one GEMM tile shape (tuning); -1 = auto.
+  int gemm_tile = -1;
+  // Pinned staging ring for host-to-device plan uploads: a copy from pinned
+  // memory does not synchronise the stream, so host planning of the next
+  // contraction overlaps the device work of the current one.  A slot is
+  // reused once the event recorded after its copy has completed.
+  struct Slot {
+    void* host = nullptr;
+    size_t cap = 0;
+    cudaEvent_t ev = nullptr;
+    bool pending = false;
+  };
+  std::vector<Slot> slots;
+  size_t next_slot = 0;
+  void stage_copy(void* dst, const void* src, size_t bytes);
+  void release_staging();
   void note_launch(int64_t n = 1) { launches += n; }
   void sync();
+  void clear_profile();
+};
+
+// Records events around one kernel launch when the context is profiling.
+class ProfScope {
+ public:
+  ProfScope(Ctx* c, int kind, double flops, double bytes);
+  ~ProfScope();
+
+ private:
+  Ctx* c_;
+  int kind_;
+  double flops_, bytes_;
+  cudaEvent_t a_ = nullptr;
 };
 
 // Upload a host vector to a new device buffer (stream-ordered).
 template <class T>
 DevBuf upload(Ctx* ctx, const std::vector<T>& v) {
   DevBuf b(ctx, v.size() * sizeof(T));
-  if (!v.empty())
-    check_cuda(cudaMemcpyAsync(b.raw(), v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream),
-               "upload");
+  if (!v.empty()) ctx->stage_copy(b.raw(), v.data(), v.size() * sizeof(T));
   return b;
 }
 template <class T>

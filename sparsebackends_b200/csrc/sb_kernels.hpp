@@ -17,25 +17,25 @@ namespace sb {
 // y + j + k*ldy).  Each C tile is produced by exactly one CTA: no atomics, C
 // is written once (no zero-init needed), accumulation order over pairs is the
 // pair order.
+// Tiles of C block c are CTAs [tile_begin, tile_begin + mtiles*ntiles); the
+// kernel finds its C block by binary search over tile_begin, so no per-tile
+// descriptor list is built or uploaded.
 struct GemmCBlock {
   int64_t c_off;
   int32_t M, N;
   int32_t pair_begin, pair_end;
+  int32_t tile_begin, mtiles;
 };
 struct GemmPair {
   int64_t x_off, y_off;
   int32_t K, ldx, ldy, pad;
 };
-struct GemmTile {
-  int32_t cblock, m0, n0, pad;
-};
 
-enum class GemmShape : int { T64x64 = 0, T128x32 = 1, T32x128 = 2 };
+enum class GemmShape : int { T64x64 = 0, T128x32 = 1, T32x128 = 2, T128x64 = 3, T64x128 = 4 };
 
 cudaError_t launch_gemm_f64(const double* X, const double* Y, double* C,
-                            const GemmCBlock* d_cblocks, const GemmPair* d_pairs,
-                            const GemmTile* d_tiles, int64_t ntiles,
-                            bool xT, bool yT, GemmShape shape, cudaStream_t s);
+                            const GemmCBlock* d_cblocks, int32_t ncblocks, const GemmPair* d_pairs,
+                            int64_t ntiles, bool xT, bool yT, GemmShape shape, cudaStream_t s);
 
 // Number of tiles of a (M, N) C block for the given tile shape.
 void gemm_tile_dims(GemmShape shape, int* bm, int* bn);

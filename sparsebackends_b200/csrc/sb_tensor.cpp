@@ -23,6 +23,65 @@ void check_cuda(cudaError_t e, const char* what) {
 
 void Ctx::sync() { SB_CK(cudaStreamSynchronize(stream)); }
 
+void Ctx::stage_copy(void* dst, const void* src, size_t bytes) {
+  if (slots.empty()) slots.resize(32);
+  Slot& s = slots[next_slot];
+  next_slot = (next_slot + 1) % slots.size();
+  if (s.pending) {
+    SB_CK(cudaEventSynchronize(s.ev));
+    s.pending = false;
+  }
+  if (!s.ev) SB_CK(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming));
+  if (s.cap < bytes) {
+    if (s.host) SB_CK(cudaFreeHost(s.host));
+    s.host = nullptr;
+    s.cap = 0;
+    const size_t cap = std::max<size_t>(bytes, std::max<size_t>(64 << 10, 2 * s.cap));
+    SB_CK(cudaHostAlloc(&s.host, cap, cudaHostAllocDefault));
+    s.cap = cap;
+  }
+  std::memcpy(s.host, src, bytes);
+  SB_CK(cudaMemcpyAsync(dst, s.host, bytes, cudaMemcpyHostToDevice, stream));
+  SB_CK(cudaEventRecord(s.ev, stream));
+  s.pending = true;
+}
+
+void Ctx::release_staging() {
+  for (auto& s : slots) {
+    if (s.ev) {
+      cudaEventSynchronize(s.ev);
+      cudaEventDestroy(s.ev);
+    }
+    if (s.host) cudaFreeHost(s.host);
+  }
+  slots.clear();
+  next_slot = 0;
+}
+
+void Ctx::clear_profile() {
+  for (auto& r : prof) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  prof.clear();
+}
+
+ProfScope::ProfScope(Ctx* c, int kind, double flops, double bytes) : c_(c), kind_(kind), flops_(flops), bytes_(bytes) {
+  if (!c_->profiling) return;
+  SB_CK(cudaEventCreate(&a_));
+  SB_CK(cudaEventRecord(a_, c_->stream));
+}
+ProfScope::~ProfScope() {
+  if (!a_) return;
+  cudaEvent_t b = nullptr;
+  if (cudaEventCreate(&b) != cudaSuccess || cudaEventRecord(b, c_->stream) != cudaSuccess) {
+    cudaEventDestroy(a_);
+    if (b) cudaEventDestroy(b);
+    return;
+  }
+  c_->prof.push_back(Ctx::ProfRec{kind_, a_, b, flops_, bytes_});
+}
+
 DevBuf::DevBuf(Ctx* ctx, size_t bytes) : ctx_(ctx), n_(bytes) {
   if (bytes) SB_CK(cudaMallocAsync(&p_, bytes, ctx->stream));
 }
@@ -97,7 +156,10 @@ static void permute_blocks(Ctx* ctx, const double* src, double* dst, const std::
   }
   d.rank = r;
   DevBuf doff = upload(ctx, src_off);
-  SB_CK(launch_permute_blocks(src, dst, doff.as<int64_t>(), static_cast<int64_t>(src_off.size()), blk, d, ctx->stream));
+  {
+    ProfScope ps(ctx, PROF_PERMUTE, 0.0, 16.0 * static_cast<double>(src_off.size()) * static_cast<double>(blk));
+    SB_CK(launch_permute_blocks(src, dst, doff.as<int64_t>(), static_cast<int64_t>(src_off.size()), blk, d, ctx->stream));
+  }
   ctx->note_launch();
 }
 

@@ -1,0 +1,277 @@
+"""U(1) sectors on the reference's block-sparse format, and the two-site H_eff apply.
+
+The reference stores every tensor as ``NewBlockSparseSorted`` (prefix-sparse,
+tail-dense, uniform block size).  A U(1)-graded link becomes two axes:
+
+* a prefix axis ``q`` over its charge sectors (keys = allowed sector tuples);
+* a tail axis ``m`` over the states inside a sector, zero-padded to the
+  largest sector dimension ``D``.
+
+Blocks exist only for charge-conserving sector tuples.  The MPO link is graded
+the same way (its channels grouped by the charge they carry: -2, 0, +2), which
+keeps the H_eff chain at the MPS' block sparsity.
+
+``HeffChain`` applies the two-site effective Hamiltonian in the order of
+ITensorMPS ``product(::ProjMPO, v)`` (ψ·L, ·W₁, ·W₂, ·R), as four
+``contract!`` calls (``src/tensoralgebra/contract_bs_bs.jl:572-730``).  Label
+orders are chosen so that each call's operand permutations are key reorders
+only: every dense tail already sits in the [kept..., reduced...] order the
+kernel wants.
+"""
+from __future__ import annotations
+
+import itertools
+from dataclasses import dataclass, field
+from typing import Dict, List, Sequence, Tuple
+
+import numpy as np
+
+
+@dataclass
+class U1Link:
+    """Charge sectors of one link: ``charges[i]`` with ``dims[i]`` states."""
+
+    charges: List[int]
+    dims: List[int]
+
+    @property
+    def S(self) -> int:
+        return len(self.charges)
+
+    @property
+    def D(self) -> int:
+        return max(self.dims)
+
+    @property
+    def total(self) -> int:
+        return int(sum(self.dims))
+
+    def index(self, q: int) -> int:
+        return self.charges.index(q)
+
+
+PHYS = [+1, -1]  # 2Sz of the spin-1/2 states s = 1, 2
+
+
+def gaussian_sectors(chi: int, charges: Sequence[int], width: float, min_dim: int = 1) -> U1Link:
+    """Sector dims ∝ exp(-(q/2)²/(2 width²)) summing to ``chi`` (a DMRG-like profile)."""
+    w = np.exp(-((np.asarray(charges) / 2.0) ** 2) / (2 * width ** 2))
+    raw = w / w.sum() * chi
+    dims = np.maximum(min_dim, np.floor(raw)).astype(int)
+    # distribute the remainder to the largest fractional parts
+    rem = chi - int(dims.sum())
+    order = np.argsort(-(raw - np.floor(raw)))
+    i = 0
+    while rem > 0:
+        dims[order[i % len(dims)]] += 1
+        rem -= 1
+        i += 1
+    while rem < 0:
+        j = int(np.argmax(dims))
+        dims[j] -= 1
+        rem += 1
+    return U1Link(list(charges), [int(d) for d in dims])
+
+
+def mpo_link(channels_per_charge: Dict[int, int]) -> U1Link:
+    """MPO link graded by channel charge, e.g. {-2: k, 0: 2+k, 2: k}."""
+    qs = sorted(channels_per_charge)
+    return U1Link(qs, [channels_per_charge[q] for q in qs])
+
+
+@dataclass
+class HeffLayout:
+    """Dims, tail counts, labels and charge-allowed keys of every tensor in the chain."""
+
+    left: U1Link
+    right: U1Link
+    mpo: U1Link
+    d: int = 2
+    labels: Dict[str, List[str]] = field(default_factory=dict)
+    dims: Dict[str, Tuple[int, ...]] = field(default_factory=dict)
+    n2: Dict[str, int] = field(default_factory=dict)
+    keys: Dict[str, List[Tuple[int, ...]]] = field(default_factory=dict)
+
+    def __post_init__(self):
+        l, r, w, d = self.left, self.right, self.mpo, self.d
+        S_l, S_r, S_w, D_l, D_r, D_w = l.S, r.S, w.S, l.D, r.D, w.D
+        ext = {"ql": S_l, "qlp": S_l, "qr": S_r, "qrp": S_r, "qwl": S_w, "qwm": S_w, "qwr": S_w,
+               "s1": d, "s2": d, "s1p": d, "s2p": d,
+               "ml": D_l, "mlp": D_l, "mr": D_r, "mrp": D_r, "mwl": D_w, "mwm": D_w, "mwr": D_w}
+        lab = {
+            "psi": ["ql", "s1", "s2", "qr", "ml", "mr"],
+            "L": ["qlp", "qwl", "ql", "mlp", "mwl", "ml"],
+            "W1": ["qwl", "s1p", "s1", "qwm", "mwl", "mwm"],
+            "W2": ["qwm", "s2p", "s2", "qwr", "mwm", "mwr"],
+            "R": ["qrp", "qwr", "qr", "mrp", "mwr", "mr"],
+            # intermediates: orders chosen so that no dense tail needs a permute
+            "T1": ["qlp", "s2", "qr", "qwl", "s1", "mr", "mlp", "mwl"],
+            "T2": ["qlp", "qr", "s1p", "qwm", "s2", "mr", "mlp", "mwm"],
+            "T3": ["qlp", "s1p", "s2p", "qwr", "qr", "mwr", "mr", "mlp"],
+            "T4": ["qlp", "s1p", "s2p", "qrp", "mlp", "mrp"],
+        }
+        n2 = {"psi": 2, "L": 3, "W1": 2, "W2": 2, "R": 3, "T1": 3, "T2": 3, "T3": 3, "T4": 2}
+        self.labels = lab
+        self.n2 = n2
+        self.dims = {k: tuple(ext[x] for x in v) for k, v in lab.items()}
+        self.ext = ext
+        self.keys = {
+            "psi": self._psi_keys(),
+            "L": self._env_keys(l),
+            "W1": self._mpo_keys(),
+            "W2": self._mpo_keys(),
+            "R": self._env_keys(r),
+        }
+
+    # ψ(ql, s1, s2, qr): Q(ql) + σ1 + σ2 = Q(qr)
+    def _psi_keys(self):
+        out = []
+        for ql, s1, s2, qr in itertools.product(range(self.left.S), range(self.d), range(self.d), range(self.right.S)):
+            if self.left.charges[ql] + PHYS[s1] + PHYS[s2] == self.right.charges[qr]:
+                out.append((ql + 1, s1 + 1, s2 + 1, qr + 1))
+        return out
+
+    # L(q', qw, q) / R(q', qw, q): Q(q') - Q(q) = c(qw)
+    def _env_keys(self, link: U1Link):
+        out = []
+        for qp, qw, q in itertools.product(range(link.S), range(self.mpo.S), range(link.S)):
+            if link.charges[qp] - link.charges[q] == self.mpo.charges[qw]:
+                out.append((qp + 1, qw + 1, q + 1))
+        return out
+
+    # W(qwl, s', s, qwr): c(qwr) = c(qwl) + σ(s') - σ(s)
+    def _mpo_keys(self):
+        out = []
+        w = self.mpo
+        for a, sp, s, b in itertools.product(range(w.S), range(self.d), range(self.d), range(w.S)):
+            if w.charges[b] == w.charges[a] + PHYS[sp] - PHYS[s]:
+                out.append((a + 1, sp + 1, s + 1, b + 1))
+        return out
+
+    def valid_extent(self, name: str, key: Tuple[int, ...]) -> Tuple[int, ...]:
+        """Unpadded extents of a block's tail axes (the rest is zero padding)."""
+        lab = self.labels[name]
+        P = len(lab) - self.n2[name]
+        kv = {l: key[i] for i, l in enumerate(lab[:P])}
+        grade = {"ml": ("ql", self.left), "mlp": ("qlp", self.left), "mr": ("qr", self.right),
+                 "mrp": ("qrp", self.right), "mwl": ("qwl", self.mpo), "mwm": ("qwm", self.mpo),
+                 "mwr": ("qwr", self.mpo)}
+        out = []
+        for t in lab[P:]:
+            q, link = grade[t]
+            out.append(link.dims[kv[q] - 1] if q in kv else link.D)
+        return tuple(out)
+
+
+def random_block_tensor(layout: HeffLayout, name: str, rng: np.random.Generator, scale: float = 1.0):
+    """Gaussian entries inside each block's sector extents, zero padding outside.
+
+    Returns (keys, data) in the reference layout (keys sorted column-major,
+    blocks packed in that order)."""
+    lab = layout.labels[name]
+    dims = layout.dims[name]
+    n2 = layout.n2[name]
+    P = len(dims) - n2
+    tail = dims[P:]
+    blk = int(np.prod(tail))
+    keys = layout.keys[name]
+    pd = dims[:P]
+
+    def lin(k):
+        idx, st = 0, 1
+        for a in range(P):
+            idx += (k[a] - 1) * st
+            st *= pd[a]
+        return idx
+
+    keys = sorted(keys, key=lin)
+    data = np.zeros(len(keys) * blk)
+    for i, k in enumerate(keys):
+        ext = layout.valid_extent(name, k)
+        blkarr = np.zeros(tail)
+        blkarr[tuple(slice(0, e) for e in ext)] = rng.standard_normal(ext) * scale
+        data[i * blk:(i + 1) * blk] = blkarr.reshape(-1, order="F")
+    return keys, data
+
+
+class HeffChain:
+    """Two-site H_eff · ψ through four ``contract!`` calls on the device.
+
+    The intermediate and output tensors are allocated once and overwritten by
+    every apply (``contract!`` semantics)."""
+
+    STEPS = (("T1", "L", "psi"), ("T2", "T1", "W1"), ("T3", "T2", "W2"), ("T4", "R", "T3"))
+
+    def __init__(self, layout: HeffLayout, ctx=None):
+        import sparsebackends_b200 as sb
+        self.sb = sb
+        self.layout = layout
+        self.out = {n: sb.NewBlockSparseSorted.empty(layout.dims[n], layout.n2[n], ctx=ctx)
+                    for n in ("T1", "T2", "T3", "T4")}
+
+    def apply(self, psi, L, W1, W2, R):
+        t = {"psi": psi, "L": L, "W1": W1, "W2": W2, "R": R, **self.out}
+        lab = self.layout.labels
+        for c, a, b in self.STEPS:
+            self.sb.contract_(t[c], lab[c], t[a], lab[a], t[b], lab[b])
+        return self.out["T4"]
+
+
+GRADE = {"ml": "ql", "mlp": "qlp", "mr": "qr", "mrp": "qrp", "mwl": "qwl", "mwm": "qwm", "mwr": "qwr"}
+
+
+def _link_of(layout: HeffLayout, qlabel: str) -> U1Link:
+    if qlabel in ("ql", "qlp"):
+        return layout.left
+    if qlabel in ("qr", "qrp"):
+        return layout.right
+    return layout.mpo
+
+
+def chain_structure(layout: HeffLayout):
+    """Key-level simulation of the four steps: per step the matched block pairs
+    (as label->value dicts) and the output key set.  Pure integer work on the
+    host; used for FLOP accounting only."""
+    lab = layout.labels
+    keys = {n: [dict(zip(lab[n][: len(lab[n]) - layout.n2[n]], k)) for k in layout.keys[n]]
+            for n in ("psi", "L", "W1", "W2", "R")}
+    steps = []
+    for c, a, b in HeffChain.STEPS:
+        la, lb, lc = lab[a], lab[b], lab[c]
+        Pa, Pb, Pc = (len(x) - layout.n2[n] for x, n in ((la, a), (lb, b), (lc, c)))
+        shared_pref = [x for x in la[:Pa] if x in lb[:Pb]]
+        groups = {}
+        for kb in keys[b]:
+            groups.setdefault(tuple(kb[x] for x in shared_pref), []).append(kb)
+        pairs, ckeys = [], {}
+        for ka in keys[a]:
+            for kb in groups.get(tuple(ka[x] for x in shared_pref), []):
+                kv = {**ka, **kb}
+                pairs.append(kv)
+                ckeys[tuple(kv[x] for x in lc[:Pc])] = {x: kv[x] for x in lc[:Pc]}
+        keys[c] = list(ckeys.values())
+        red = [x for x in la[Pa:] if x in lb[Pb:]]
+        keepA = [x for x in la[Pa:] if x not in red]
+        keepB = [x for x in lb[Pb:] if x not in red]
+        steps.append(dict(C=c, A=a, B=b, pairs=pairs, nC=len(keys[c]), red=red, keepA=keepA, keepB=keepB))
+    return steps
+
+
+def chain_flops(layout: HeffLayout, padded: bool = True) -> float:
+    """FLOPs of one H_eff apply: the sum over matched block pairs of 2·m·n·k.
+
+    ``padded=True`` counts the executed (zero-padded) GEMM shapes;
+    ``padded=False`` counts the unpadded sector extents, the algorithmic work."""
+    total = 0.0
+    for st in chain_structure(layout):
+        for kv in st["pairs"]:
+            def ext(x):
+                if padded:
+                    return layout.ext[x]
+                q = GRADE[x]
+                return _link_of(layout, q).dims[kv[q] - 1]
+            m = np.prod([ext(x) for x in st["keepA"]]) if st["keepA"] else 1
+            n = np.prod([ext(x) for x in st["keepB"]]) if st["keepB"] else 1
+            k = np.prod([ext(x) for x in st["red"]]) if st["red"] else 1
+            total += 2.0 * m * n * k
+    return total
