@@ -164,6 +164,33 @@ SB_API sb_status sb_to_dense(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out);
 /* to_blocksparse(::AliasedBlockSparse) (aliased/conversions.jl:18-32).       */
 SB_API sb_status sb_aliased_to_blocksparse(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out);
 
+/* ── allocation-free grouped block GEMM ──────────────────────────────────────
+ * No counterpart in the reference: an extra entry point of this library.
+ *
+ * For callers that cannot allocate device memory during a solve (a fixed
+ * memory budget or pre-sized pool, or a host runtime that forbids cudaMalloc
+ * while it owns the device): runs the block GEMM that sb_contract uses,
+ *     C[c_off[c] + i + j*c_rows[c]] = sum_{p in [c_pair_begin[c], c_pair_begin[c+1])} X_p(i,:) . Y_p(:,j)
+ * with X_p at d_X + x_off[p] (element (i,k) at i + k*ldx[p], or k + i*ldx[p]
+ * when x_trans) and Y_p at d_Y + y_off[p] (element (k,j) at k + j*ldy[p], or
+ * j + k*ldy[p] when y_trans), K[p] the reduced extent.  Every C block is
+ * written exactly once (no accumulation into prior C contents).
+ * The caller passes device pointers for inputs and outputs and the plan in
+ * host arrays; the function calls no cudaMalloc/cudaFree or any allocating
+ * routine: the plan is copied into a static device array of 640 KiB that
+ * every GPU loading the library holds until exit.
+ * Limits: n_cblocks <= 4096 and c_pair_begin[n_cblocks] <= 16384; larger
+ * plans are rejected with SB_ERR_INVALID_ARG and a message in err (if given).
+ * The first call on a device resolves the array's device address (set-up);
+ * make that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (e.g. on different streams) race.            */
+SB_API sb_status sb_block_gemm_f64_noalloc(void* stream, const double* d_X, const double* d_Y, double* d_C,
+                                           int32_t n_cblocks, const int64_t* c_off, const int32_t* c_rows,
+                                           const int32_t* c_cols, const int32_t* c_pair_begin,
+                                           const int64_t* x_off, const int64_t* y_off, const int32_t* K,
+                                           const int32_t* ldx, const int32_t* ldy, int x_trans, int y_trans,
+                                           char* err, int32_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

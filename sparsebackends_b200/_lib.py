@@ -51,6 +51,10 @@ SIGNATURES = {
     "sb_coo_from_dense": (C.c_int, [vp, vp, C.c_double, C.c_double, C.POINTER(vp)]),
     "sb_to_dense": (C.c_int, [vp, vp, C.POINTER(vp)]),
     "sb_aliased_to_blocksparse": (C.c_int, [vp, vp, C.POINTER(vp)]),
+    "sb_block_gemm_f64_noalloc": (C.c_int, [vp, vp, vp, vp, C.c_int32, P_i64, C.POINTER(C.c_int32),
+                                            C.POINTER(C.c_int32), C.POINTER(C.c_int32), P_i64, P_i64,
+                                            C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                            C.c_int, C.c_int, C.c_char_p, C.c_int32]),
 }
 
 STATUS = {

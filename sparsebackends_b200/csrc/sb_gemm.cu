@@ -5,6 +5,9 @@
 // Y are staged into shared memory by a 3-stage cp.async pipeline that runs
 // straight across the pairs of one C block (the K loops of all pairs feeding a
 // C tile are concatenated), so one CTA owns one C tile and writes it once.
+#include <cstdio>
+
+#include "../../include/sparseb.h"
 #include "sb_kernels.hpp"
 
 namespace sb {
@@ -225,3 +228,123 @@ cudaError_t launch_gemm_f64(const double* X, const double* Y, double* C,
 }
 
 }  // namespace sb
+
+// ── allocation-free grouped GEMM (sb_block_gemm_f64_noalloc) ───────────────
+//
+// For callers that cannot allocate device memory themselves or let a library
+// do it: code running under a strict memory budget or a pre-sized pool, or
+// hosts (e.g. a Julia CUDA.jl or embedded runtime) that forbid cudaMalloc
+// during a solve.  The plan descriptors that sb_contract keeps in allocated
+// device buffers live instead in this file-scope device array, which every GPU
+// that loads the library holds until process exit.  Limits: at most
+// kNoAllocMaxCBlocks output blocks and kNoAllocMaxPairs block pairs per call
+// (640 KiB of scratch).
+namespace {
+
+constexpr int kNoAllocMaxCBlocks = 4096;
+constexpr int kNoAllocMaxPairs = 16384;
+constexpr size_t kNoAllocScratchBytes =
+    kNoAllocMaxCBlocks * sizeof(sb::GemmCBlock) + kNoAllocMaxPairs * sizeof(sb::GemmPair);
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch per device ordinal, resolved once per
+// device (with that device current) by cudaGetSymbolAddress.
+constexpr int kMaxDevices = 64;
+void* g_scratch_addr[kMaxDevices] = {};
+
+// Host staging of the plan; per thread so concurrent host threads do not share it.
+thread_local sb::GemmCBlock t_cblocks[kNoAllocMaxCBlocks];
+thread_local sb::GemmPair t_pairs[kNoAllocMaxPairs];
+thread_local char* t_err = nullptr;
+thread_local int32_t t_err_len = 0;
+
+sb_status noalloc_fail(sb_status code, const char* msg) {
+  if (t_err && t_err_len > 0) std::snprintf(t_err, static_cast<size_t>(t_err_len), "sb_block_gemm_f64_noalloc: %s", msg);
+  return code;
+}
+
+}  // namespace
+
+extern "C" SB_API sb_status sb_block_gemm_f64_noalloc(void* stream, const double* d_X, const double* d_Y, double* d_C,
+                                                      int32_t n_cblocks, const int64_t* c_off, const int32_t* c_rows,
+                                                      const int32_t* c_cols, const int32_t* c_pair_begin,
+                                                      const int64_t* x_off, const int64_t* y_off, const int32_t* K,
+                                                      const int32_t* ldx, const int32_t* ldy, int x_trans,
+                                                      int y_trans, char* err, int32_t err_len) {
+  t_err = err;
+  t_err_len = err_len;
+  if (err && err_len > 0) err[0] = '\0';
+  if (n_cblocks < 0) return noalloc_fail(SB_ERR_INVALID_ARG, "n_cblocks < 0");
+  if (n_cblocks == 0) return SB_OK;
+  if (!d_X || !d_Y || !d_C || !c_off || !c_rows || !c_cols || !c_pair_begin)
+    return noalloc_fail(SB_ERR_INVALID_ARG, "NULL pointer argument");
+  if (n_cblocks > kNoAllocMaxCBlocks) {
+    char m[160];
+    std::snprintf(m, sizeof(m), "%d output blocks exceed the static scratch limit of %d", n_cblocks, kNoAllocMaxCBlocks);
+    return noalloc_fail(SB_ERR_INVALID_ARG, m);
+  }
+  const int32_t n_pairs = c_pair_begin[n_cblocks];
+  if (c_pair_begin[0] != 0 || n_pairs < 0) return noalloc_fail(SB_ERR_INVALID_ARG, "c_pair_begin must start at 0");
+  if (n_pairs > kNoAllocMaxPairs) {
+    char m[160];
+    std::snprintf(m, sizeof(m), "%d block pairs exceed the static scratch limit of %d", n_pairs, kNoAllocMaxPairs);
+    return noalloc_fail(SB_ERR_INVALID_ARG, m);
+  }
+  if (n_pairs > 0 && (!x_off || !y_off || !K || !ldx || !ldy))
+    return noalloc_fail(SB_ERR_INVALID_ARG, "NULL pair array");
+
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+    return noalloc_fail(SB_ERR_CUDA, "no usable current CUDA device");
+  // One-time set-up on this device (the first call on a device must not be
+  // inside a stream capture).
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) return noalloc_fail(SB_ERR_CUDA, cudaGetErrorString(e));
+    g_scratch_addr[dev] = p;
+  }
+  auto* d_cb = static_cast<sb::GemmCBlock*>(g_scratch_addr[dev]);
+  auto* d_pr = reinterpret_cast<sb::GemmPair*>(static_cast<unsigned char*>(g_scratch_addr[dev]) +
+                                               kNoAllocMaxCBlocks * sizeof(sb::GemmCBlock));
+
+  // Tile shape: same rule as the library's allocating path.
+  int32_t Mx = 0, Nx = 0;
+  for (int32_t c = 0; c < n_cblocks; ++c) {
+    if (c_rows[c] < 1 || c_cols[c] < 1) return noalloc_fail(SB_ERR_INVALID_ARG, "C block extents must be >= 1");
+    if (c_pair_begin[c + 1] < c_pair_begin[c]) return noalloc_fail(SB_ERR_INVALID_ARG, "c_pair_begin not monotone");
+    Mx = c_rows[c] > Mx ? c_rows[c] : Mx;
+    Nx = c_cols[c] > Nx ? c_cols[c] : Nx;
+  }
+  sb::GemmShape shape = sb::GemmShape::T64x64;
+  if (Nx <= 32 && Mx >= 128) shape = sb::GemmShape::T128x32;
+  else if (Mx <= 32 && Nx >= 128) shape = sb::GemmShape::T32x128;
+  else if (Mx >= 256 && Nx >= 128) shape = Mx >= Nx ? sb::GemmShape::T128x64 : sb::GemmShape::T64x128;
+  int bm = 64, bn = 64;
+  sb::gemm_tile_dims(shape, &bm, &bn);
+
+  int64_t ntiles = 0;
+  for (int32_t c = 0; c < n_cblocks; ++c) {
+    const int64_t mt = (c_rows[c] + bm - 1) / bm, nt = (c_cols[c] + bn - 1) / bn;
+    if (ntiles + mt * nt >= (1LL << 31)) return noalloc_fail(SB_ERR_INVALID_ARG, "too many GEMM tiles");
+    t_cblocks[c] = sb::GemmCBlock{c_off[c], c_rows[c], c_cols[c], c_pair_begin[c], c_pair_begin[c + 1],
+                                  static_cast<int32_t>(ntiles), static_cast<int32_t>(mt)};
+    ntiles += mt * nt;
+  }
+  for (int32_t p = 0; p < n_pairs; ++p) {
+    if (K[p] < 1) return noalloc_fail(SB_ERR_INVALID_ARG, "pair K must be >= 1");
+    t_pairs[p] = sb::GemmPair{x_off[p], y_off[p], K[p], ldx[p], ldy[p], 0};
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // Every call rewrites the descriptors it uses; nothing in the scratch has to
+  // start at zero.  Copies from pageable host memory return once the data is
+  // staged, so the thread-local host arrays may be reused on the next call.
+  cudaError_t e = cudaMemcpyAsync(d_cb, t_cblocks, n_cblocks * sizeof(sb::GemmCBlock), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && n_pairs)
+    e = cudaMemcpyAsync(d_pr, t_pairs, n_pairs * sizeof(sb::GemmPair), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = sb::launch_gemm_f64(d_X, d_Y, d_C, d_cb, n_cblocks, d_pr, ntiles, x_trans != 0, y_trans != 0, shape, s);
+  if (e != cudaSuccess) return noalloc_fail(SB_ERR_CUDA, cudaGetErrorString(e));
+  return SB_OK;
+}
