@@ -3,9 +3,10 @@
 One step = one application of the two-site effective Hamiltonian
 (psi·L, ·W1, ·W2, ·R: four contract! calls) on synthetic, seeded inputs with
 the shapes of the chi = 2048 J1-J2 6x6-cylinder workload: 11 U(1) sectors with
-a Gaussian dimension profile summing to 2048 (padded to 411 per sector in the
-reference's uniform block format) and an MPO link of 38 channels graded by
-charge {-2: 12, 0: 14, +2: 12}.
+a Gaussian dimension profile summing to 2048 and an MPO link of 38 channels
+graded by charge {-2: 12, 0: 14, +2: 12}.  The headline runs the ragged block
+format (every block at its sector extents); the reference's uniform format
+(every sector zero-padded to 411) is timed beside it on the same entries.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -57,16 +58,19 @@ def workload(chi: int):
     return qn.HeffLayout(left, left, mpo)
 
 
-def host_tensors(layout, seed: int):
+def host_tensors(layout, seed: int, with_ragged: bool = False):
+    """Seeded operands.  Uniform (reference layout, zero-padded sectors) always;
+    with ``with_ragged`` also the same entries stored unpadded per block."""
     from sparsebackends_b200 import qn
     rng = np.random.Generator(np.random.PCG64(seed))
-    out = {}
+    out, rag = {}, {}
     for name, scale in (("psi", 1.0), ("L", 0.05), ("W1", 0.3), ("W2", 0.3), ("R", 0.05)):
-        keys, data = qn.random_block_tensor(layout, name, rng, scale)
+        keys, data, exts = qn.random_block_tensor(layout, name, rng, scale, ragged=True)
         if name == "psi":
             data /= np.linalg.norm(data)
-        out[name] = (keys, data)
-    return out
+        out[name] = (keys, qn.pad_ragged(layout, name, keys, data, exts))
+        rag[name] = (keys, data, exts)
+    return (out, rag) if with_ragged else out
 
 
 # ── clocks during the timed region ───────────────────────────────────────
@@ -239,118 +243,147 @@ def run_ours(args, world, rank, local):
 
     torch.cuda.set_device(local)
     layout = workload(args.chi)
-    host = host_tensors(layout, args.seed)
+    host, host_r = host_tensors(layout, args.seed, with_ragged=True)
     ctx = sb.Context(local)
-    dev = {n: sb.NewBlockSparseSorted(layout.dims[n], layout.n2[n], k, None, d, ctx=ctx) for n, (k, d) in host.items()}
-    chain = qn.HeffChain(layout, ctx)
+    # ragged (unpadded sectors): the headline form; uniform: the reference layout
+    dev_r = {n: sb.NewBlockSparseSorted(layout.dims[n], layout.n2[n], k, None, d, ctx=ctx, block_dims=e)
+             for n, (k, d, e) in host_r.items()}
+    dev_u = {n: sb.NewBlockSparseSorted(layout.dims[n], layout.n2[n], k, None, d, ctx=ctx) for n, (k, d) in host.items()}
+    chain_r, chain_u = qn.HeffChain(layout, ctx), qn.HeffChain(layout, ctx)
     stream = torch.cuda.ExternalStream(ctx.stream)
     flops_alg = qn.chain_flops(layout, padded=False)
-    flops_exec = qn.chain_flops(layout, padded=True)
+    flops_pad = qn.chain_flops(layout, padded=True)
 
-    def apply_once():
-        return chain.apply(dev["psi"], dev["L"], dev["W1"], dev["W2"], dev["R"])
+    def apply_r():
+        return chain_r.apply(dev_r["psi"], dev_r["L"], dev_r["W1"], dev_r["W2"], dev_r["R"])
+
+    def apply_u():
+        return chain_u.apply(dev_u["psi"], dev_u["L"], dev_u["W1"], dev_u["W2"], dev_u["R"])
 
     for _ in range(max(args.warmup, 3)):
-        apply_once()
+        apply_r()
+        apply_u()
     ctx.synchronize()
+    # the two forms agree (same keys; unpadded blocks equal the padded result)
+    ur, uu = sb.to_uniform(chain_r.out["T4"]), chain_u.out["T4"]
+    assert ur.keys == uu.keys
+    d_r, d_u = ur.data, uu.data
+    agree = float(np.linalg.norm(d_r - d_u) / max(np.linalg.norm(d_u), 1e-300))
+    assert agree < 1e-12, agree
     peak = fp64_peak_tflops() if rank == 0 else 0.0
     torch.cuda.synchronize()
 
-    # ── device-resident throughput (value) ──
-    barrier(world)
-    ctx.synchronize()
+    def timed(fn, steps, profile=False):
+        barrier(world)
+        ctx.synchronize()
+        if profile:
+            ctx.set_profiling(True)
+        l0 = ctx.launch_count
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(steps):
+            fn()
+        e.record(stream)
+        ctx.synchronize()
+        prof = {k: ctx.profile(k) for k in ("gemm", "permute", "outer", "axpy")} if profile else None
+        if profile:
+            ctx.set_profiling(False)
+        barrier(world)
+        return reduce_max(s.elapsed_time(e), world), ctx.launch_count - l0, prof
+
+    # ── device-resident throughput (value): ragged form ──
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
-    ctx.set_profiling(True)
-    l0 = ctx.launch_count
-    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s.record(stream)
-    for _ in range(args.steps):
-        apply_once()
-    e.record(stream)
-    ctx.synchronize()
-    ms = s.elapsed_time(e)
-    launches = ctx.launch_count - l0
+    ms, launches, prof = timed(apply_r, args.steps, profile=True)
     clocks = sampler.stop()
-    prof = {k: ctx.profile(k) for k in ("gemm", "permute", "outer", "axpy")}
-    ctx.set_profiling(False)
-    barrier(world)
-    ms_max = reduce_max(ms, world)
-    value = world * args.steps / (ms_max / 1e3)
+    value = world * args.steps / (ms / 1e3)
+    # uniform (reference layout) for comparison
+    ms_u, _, prof_u = timed(apply_u, args.steps, profile=True)
+    value_u = world * args.steps / (ms_u / 1e3)
 
     # ── end to end through the public API (pinned host psi in, H·psi out) ──
-    psi_keys, psi_data = host["psi"]
-    pin_in = torch.empty(psi_data.size, dtype=torch.float64, pin_memory=True)
-    pin_in.numpy()[:] = psi_data
-    t4_blocks = chain.out["T4"]._info()["nkeys"]
-    t4_len = t4_blocks * chain.out["T4"].blksize
-    pin_out = torch.empty(max(t4_len, 1), dtype=torch.float64, pin_memory=True)
     lib = ctx._lib
-    in_ptr = C.cast(C.c_void_p(pin_in.data_ptr()), C.POINTER(C.c_double))
-    out_ptr = C.cast(C.c_void_p(pin_out.data_ptr()), C.POINTER(C.c_double))
 
-    def e2e_once():
-        p = sb.NewBlockSparseSorted.__new__(sb.NewBlockSparseSorted)
-        h = C.c_void_p()
+    def make_e2e(ragged):
+        keys = host_r["psi"][0] if ragged else host["psi"][0]
+        data = host_r["psi"][1] if ragged else host["psi"][1]
+        exts = host_r["psi"][2]
+        pin_in = torch.empty(max(data.size, 1), dtype=torch.float64, pin_memory=True)
+        pin_in.numpy()[: data.size] = data
+        chain = chain_r if ragged else chain_u
+        out_len = chain.out["T4"]._layout()[2]
+        pin_out = torch.empty(max(out_len, 1), dtype=torch.float64, pin_memory=True)
+        in_ptr = C.cast(C.c_void_p(pin_in.data_ptr()), C.POINTER(C.c_double))
+        out_ptr = C.cast(C.c_void_p(pin_out.data_ptr()), C.POINTER(C.c_double))
         dims = layout.dims["psi"]
-        flat = [x for k in psi_keys for x in k]
-        st = lib.sb_tensor_create_bs(ctx._h, len(dims), sb._i64(dims), layout.n2["psi"], len(psi_keys),
-                                     sb._i64(flat), None, in_ptr, C.byref(h))
-        sb._check(ctx, st)
-        sb._Tensor.__init__(p, ctx, h)
-        out = chain.apply(p, dev["L"], dev["W1"], dev["W2"], dev["R"])
-        sb._check(ctx, lib.sb_tensor_export_bs(ctx._h, out._h, None, None, out_ptr))
+        kflat = sb._i64([x for k in keys for x in k])
+        bflat = sb._i64([x for e in exts for x in e])
+        devs = dev_r if ragged else dev_u
 
+        def once():
+            p = sb.NewBlockSparseSorted.__new__(sb.NewBlockSparseSorted)
+            h = C.c_void_p()
+            if ragged:
+                st = lib.sb_tensor_create_bs_ragged(ctx._h, len(dims), sb._i64(dims), layout.n2["psi"], len(keys),
+                                                    kflat, bflat, in_ptr, C.byref(h))
+            else:
+                st = lib.sb_tensor_create_bs(ctx._h, len(dims), sb._i64(dims), layout.n2["psi"], len(keys), kflat,
+                                             None, in_ptr, C.byref(h))
+            sb._check(ctx, st)
+            sb._Tensor.__init__(p, ctx, h)
+            out = chain.apply(p, devs["L"], devs["W1"], devs["W2"], devs["R"])
+            sb._check(ctx, lib.sb_tensor_export_bs(ctx._h, out._h, None, None, out_ptr))
+
+        return once, int(data.size * 8), int(out_len * 8)
+
+    e2e_r, h2d_r, d2h_r = make_e2e(True)
+    e2e_u, h2d_u, d2h_u = make_e2e(False)
     for _ in range(2):
-        e2e_once()
-    barrier(world)
-    ctx.synchronize()
-    s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s2.record(stream)
-    for _ in range(args.steps):
-        e2e_once()
-    e2.record(stream)
-    ctx.synchronize()
-    ms_e2e = reduce_max(s2.elapsed_time(e2), world)
+        e2e_r()
+        e2e_u()
+    ms_e2e, _, _ = timed(e2e_r, args.steps)
+    ms_e2e_u, _, _ = timed(e2e_u, args.steps)
     e2e_value = world * args.steps / (ms_e2e / 1e3)
-
-    # parity spot check of the benchmarked output against a fresh apply
-    if rank == 0:
-        got = pin_out.numpy()[:t4_len].copy()
-        ref_keys = chain.out["T4"].keys
-        assert len(ref_keys) == t4_blocks
-        assert np.all(np.isfinite(got))
+    e2e_value_u = world * args.steps / (ms_e2e_u / 1e3)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, runs, el = cpu_matvec_rate(layout, host, args.cpu_budget_s, 8)
         cpu = {"value": rate, "unit": UNIT, "cores": blas_threads(), "kind": "port",
                "sample": f"{runs} full matvec(s) of the same workload in {el:.1f} s, oracle (numpy + OpenBLAS) "
-                         f"restatement of contract_shared! (contract_bs_bs.jl:572-730)"}
+                         f"restatement of contract_shared! (contract_bs_bs.jl:572-730) on the reference's "
+                         f"uniform (zero-padded) blocks"}
 
     if rank != 0:
         return
     g = prof["gemm"]
     achieved = g["flops"] / (g["ms"] * 1e-3) / 1e12 if g["ms"] > 0 else 0.0
+    gu = prof_u["gemm"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"two-site H_eff matvec, U(1) chi={args.chi}, MPO w=38 (J1-J2 6x6 sized)",
                    "chi": args.chi, "sectors": layout.left.dims, "mpo_channels": layout.mpo.dims,
+                   "format": "ragged block extents (unpadded U(1) sectors); uniform reference layout reported "
+                             "in uniform_format",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (operators ~0.6 GB, intermediates ~2.3 GB each)"},
         "gflops_algorithmic": flops_alg * value / 1e9,
-        "gflops_executed": flops_exec * value / 1e9,
         "roofline": {"bound": "tensor", "kernel": "k_gemm_f64 (DMMA m8n8k4)", "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                      "peak_source": "measured live: torch.matmul float64 8192^3, best of 10 (cuBLAS DGEMM)",
                      "traffic": None, "launches": g["launches"], "kernel_ms_per_step": g["ms"] / args.steps},
         "kernel_time_share": {k: v["ms"] / max(1e-9, sum(x["ms"] for x in prof.values())) for k, v in prof.items()},
+        "uniform_format": {"value": value_u, "ms_per_step": ms_u / args.steps,
+                           "gflops_executed": flops_pad * value_u / 1e9,
+                           "gemm_tflops": gu["flops"] / (gu["ms"] * 1e-3) / 1e12 if gu["ms"] > 0 else 0.0,
+                           "e2e": {"value": e2e_value_u, "unit": UNIT, "h2d_bytes_per_step": h2d_u,
+                                   "d2h_bytes_per_step": d2h_u}},
+        "ragged_vs_uniform_rel_diff": agree,
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(psi_data.size * 8),
-                "d2h_bytes_per_step": int(t4_len * 8)},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_r, "d2h_bytes_per_step": d2h_r},
         "gpu_launches": launches,
         "clocks": clocks,
     }

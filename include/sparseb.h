@@ -63,7 +63,9 @@ typedef struct sb_ctx sb_ctx;
 typedef struct sb_tensor sb_tensor;
 
 /* ── context ─────────────────────────────────────────────────────────────── */
-/* Creates a context on `device` with its own non-blocking stream.            */
+/* Creates a context on `device` with its own non-blocking stream.  Tensors
+ * keep their context alive: destroying a context that still owns tensors
+ * is deferred until the last of them is freed.                              */
 SB_API sb_status sb_ctx_create(int device, unsigned flags, sb_ctx** out);
 SB_API sb_status sb_ctx_destroy(sb_ctx* ctx);
 /* Message of the last failing call on this context ("" if none).            */
@@ -101,6 +103,16 @@ SB_API sb_status sb_tensor_create_dense_device(sb_ctx* ctx, int nd, const int64_
 SB_API sb_status sb_tensor_create_bs(sb_ctx* ctx, int nd, const int64_t* dims, int n_tail, int64_t nblocks,
                               const int64_t* keys, const int64_t* ids, const double* data,
                               sb_tensor** out);
+/* Ragged block-sparse tensor: the reference's NewBlockSparseSorted
+ * (src/blocksparse/storage.jl:3-9) extended with per-block tail extents, for
+ * U(1)-graded links whose sectors differ in size (the reference pads every
+ * block to the largest sector).  block_dims: nblocks x n_tail extents, each
+ * in 1:dims of its tail axis; data: the blocks in the order of keys, each
+ * column-major over its own extents.  Logically equal to the uniform tensor
+ * obtained by zero padding (sb_tensor_to_uniform).                           */
+SB_API sb_status sb_tensor_create_bs_ragged(sb_ctx* ctx, int nd, const int64_t* dims, int n_tail,
+                                            int64_t nblocks, const int64_t* keys, const int64_t* block_dims,
+                                            const double* data, sb_tensor** out);
 /* COOTensor{T,N}(dims, keys, vals, dirty) (src/coo/storage.jl:1-15).        */
 SB_API sb_status sb_tensor_create_coo(sb_ctx* ctx, int nd, const int64_t* dims, int64_t nnz,
                                const int64_t* keys, const double* vals, int dirty, sb_tensor** out);
@@ -124,6 +136,16 @@ SB_API sb_status sb_tensor_export_coo(sb_ctx* ctx, const sb_tensor* t, int64_t* 
 SB_API sb_status sb_tensor_export_aliased(sb_ctx* ctx, const sb_tensor* t, double* templates,
                                    int64_t* keys, int64_t* alias_ids, double* scalars);
 SB_API sb_status sb_tensor_export_dense(sb_ctx* ctx, const sb_tensor* t, double* data);
+/* Block layout: ragged flag, per-block tail extents (nkeys x n_tail, in key
+ * order) and payload length in doubles.  Any pointer may be NULL.           */
+SB_API sb_status sb_tensor_block_dims(const sb_tensor* t, int* ragged, int64_t* block_dims,
+                                      int64_t* payload_len);
+/* Ragged -> uniform by zero padding (the reference layout, for a Julia
+ * caller), and uniform -> ragged by cropping each block to block_dims; with
+ * check_zero, cropping a nonzero entry is an SB_ERR_ASSERTION.              */
+SB_API sb_status sb_tensor_to_uniform(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out);
+SB_API sb_status sb_tensor_to_ragged(sb_ctx* ctx, const sb_tensor* A, const int64_t* block_dims,
+                                     int check_zero, sb_tensor** out);
 /* Device pointer and length (doubles) of the payload (dense data, block data,
  * COO values or aliased templates), for zero-copy interop.                   */
 SB_API sb_status sb_tensor_device_data(const sb_tensor* t, double** d_ptr, int64_t* len);

@@ -40,6 +40,7 @@ __all__ = [
     "SparseBackendsError", "Context", "default_context", "DenseTensor", "NewBlockSparseSorted", "COOTensor",
     "AliasedBlockSparse", "contract_", "contract_bs_bs_to_dense", "blocksparse_from_dense", "coo_from_dense",
     "to_dense", "to_blocksparse", "permutedims", "sort_", "compression_ratio", "output_inds", "label_key",
+    "to_uniform", "to_ragged",
 ]
 
 
@@ -127,8 +128,9 @@ class Context:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            self._lib.sb_ctx_destroy(h)
+        lib = getattr(self, "_lib", None)
+        if h is not None and h.value and lib is not None:
+            lib.sb_ctx_destroy(h)  # deferred by the library while tensors are alive
             self._h = None
 
 
@@ -151,8 +153,9 @@ class _Tensor:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            self.ctx._lib.sb_tensor_free(h)
+        ctx = getattr(self, "ctx", None)
+        if h is not None and h.value and ctx is not None and getattr(ctx, "_lib", None) is not None:
+            ctx._lib.sb_tensor_free(h)
             self._h = None
 
     def _info(self):
@@ -233,7 +236,10 @@ class NewBlockSparseSorted(_Tensor):
 
     def __init__(self, dims: Sequence[int], n2: int, keys: Optional[Sequence[Sequence[int]]] = None,
                  ids: Optional[Sequence[int]] = None, data: Optional[np.ndarray] = None,
-                 ctx: Optional[Context] = None, _handle=None):
+                 ctx: Optional[Context] = None, _handle=None, block_dims: Optional[Sequence[Sequence[int]]] = None):
+        """With ``block_dims`` (one tail-extent tuple per key, same order as
+        ``keys``) the tensor is ragged: each block is stored unpadded, column-
+        major over its own extents, concatenated in ``keys`` order."""
         ctx = ctx or default_context()
         if _handle is not None:
             super().__init__(ctx, _handle)
@@ -247,9 +253,31 @@ class NewBlockSparseSorted(_Tensor):
         flat = [int(x) for k in keys for x in k]
         d = None if data is None else np.ascontiguousarray(np.asarray(data, dtype=np.float64).reshape(-1))
         h = C.c_void_p()
-        _check(ctx, ctx._lib.sb_tensor_create_bs(ctx._h, len(dims), _i64(dims), int(n2), n, _i64(flat),
-                                                 _i64(ids) if ids is not None else None, _f64ptr(d), C.byref(h)))
+        if block_dims is not None:
+            bd = [int(x) for b in block_dims for x in b]
+            _check(ctx, ctx._lib.sb_tensor_create_bs_ragged(ctx._h, len(dims), _i64(dims), int(n2), n, _i64(flat),
+                                                            _i64(bd), _f64ptr(d), C.byref(h)))
+        else:
+            _check(ctx, ctx._lib.sb_tensor_create_bs(ctx._h, len(dims), _i64(dims), int(n2), n, _i64(flat),
+                                                     _i64(ids) if ids is not None else None, _f64ptr(d), C.byref(h)))
         super().__init__(ctx, h)
+
+    def _layout(self):
+        i = self._info()
+        n, n2 = i["nkeys"], i["n2"]
+        rg, ln = C.c_int(), C.c_int64()
+        bd = (C.c_int64 * max(n * n2, 1))()
+        _check(self.ctx, self.ctx._lib.sb_tensor_block_dims(self._h, C.byref(rg), bd, C.byref(ln)))
+        return bool(rg.value), [tuple(bd[j * n2 + t] for t in range(n2)) for j in range(n)], ln.value
+
+    @property
+    def is_ragged(self) -> bool:
+        return self._layout()[0]
+
+    @property
+    def block_dims(self) -> List[Tuple[int, ...]]:
+        """Tail extents of every block in key order (the full tail dims when uniform)."""
+        return self._layout()[1]
 
     @property
     def n2(self) -> int:
@@ -267,9 +295,10 @@ class NewBlockSparseSorted(_Tensor):
     def _export(self):
         i = self._info()
         P, n, blk = len(i["dims"]) - i["n2"], i["nkeys"], i["blksize"]
+        _, _, plen = self._layout()
         keys = (C.c_int64 * max(n * P, 1))()
         ids = (C.c_int64 * max(n, 1))()
-        data = np.empty(n * blk, dtype=np.float64)
+        data = np.empty(plen, dtype=np.float64)
         _check(self.ctx, self.ctx._lib.sb_tensor_export_bs(self.ctx._h, self._h, keys, ids, _f64ptr(data)))
         klist = [tuple(keys[j * P + t] for t in range(P)) for j in range(n)]
         return klist, [ids[j] for j in range(n)], data
@@ -287,9 +316,15 @@ class NewBlockSparseSorted(_Tensor):
         return self._export()[2]
 
     def blocks_by_key(self) -> dict:
+        """Flat column-major payload of every block (unpadded when ragged)."""
         keys, ids, data = self._export()
-        blk = self.blksize
-        return {k: data[(i - 1) * blk: i * blk].copy() for k, i in zip(keys, ids)}
+        _, bd, _ = self._layout()
+        out, off = {}, 0
+        for k, e in zip(keys, bd):
+            ln = int(np.prod(e)) if e else 1
+            out[k] = data[off: off + ln].copy()
+            off += ln
+        return out
 
     @staticmethod
     def empty(dims: Sequence[int], n2: int, ctx: Optional[Context] = None) -> "NewBlockSparseSorted":
@@ -396,6 +431,21 @@ class AliasedBlockSparse(_Tensor):
     @staticmethod
     def empty(dims: Sequence[int], n2: int, ctx: Optional[Context] = None) -> "AliasedBlockSparse":
         return AliasedBlockSparse(dims, n2, ctx=ctx)
+
+
+def to_uniform(A: NewBlockSparseSorted) -> NewBlockSparseSorted:
+    """Zero-pad a ragged tensor to the reference's uniform block format."""
+    h = C.c_void_p()
+    _check(A.ctx, A.ctx._lib.sb_tensor_to_uniform(A.ctx._h, A._h, C.byref(h)))
+    return _from_handle(A.ctx, h)
+
+
+def to_ragged(A: NewBlockSparseSorted, block_dims: Sequence[Sequence[int]], check_zero: bool = True):
+    """Crop every block of a uniform tensor to ``block_dims`` (key order)."""
+    bd = [int(x) for b in block_dims for x in b]
+    h = C.c_void_p()
+    _check(A.ctx, A.ctx._lib.sb_tensor_to_ragged(A.ctx._h, A._h, _i64(bd), int(check_zero), C.byref(h)))
+    return _from_handle(A.ctx, h)
 
 
 def compression_ratio(A: AliasedBlockSparse) -> float:

@@ -53,7 +53,17 @@ sb_tensor* wrap(sb_ctx* ctx, TensorPtr t) {
   auto* h = new sb_tensor;
   h->impl = std::move(t);
   h->owner = ctx;
+  if (ctx) ++ctx->impl.live_tensors;
   return h;
+}
+
+void destroy_ctx_now(sb_ctx* ctx) {
+  cudaSetDevice(ctx->impl.device);
+  cudaStreamSynchronize(ctx->impl.stream);
+  ctx->impl.clear_profile();
+  ctx->impl.release_staging();
+  if (ctx->impl.own_stream) cudaStreamDestroy(ctx->impl.stream);
+  delete ctx;
 }
 
 void check_keys_in_range(const std::vector<int64_t>& keys, int64_t n, int klen, const std::vector<int64_t>& dims) {
@@ -106,11 +116,11 @@ sb_status sb_ctx_create(int device, unsigned flags, sb_ctx** out) {
 
 sb_status sb_ctx_destroy(sb_ctx* ctx) {
   if (!ctx) return SB_OK;
-  cudaStreamSynchronize(ctx->impl.stream);
-  ctx->impl.clear_profile();
-  ctx->impl.release_staging();
-  if (ctx->impl.own_stream) cudaStreamDestroy(ctx->impl.stream);
-  delete ctx;
+  if (ctx->impl.live_tensors > 0) {
+    ctx->impl.destroy_pending = true;  // the last sb_tensor_free finishes the job
+    return SB_OK;
+  }
+  destroy_ctx_now(ctx);
   return SB_OK;
 }
 
@@ -241,15 +251,109 @@ sb_status sb_tensor_create_bs(sb_ctx* ctx, int nd, const int64_t* dims, int n_ta
       if (packed) {
         t->data = std::move(raw);
       } else {
-        std::vector<int64_t> idx(nblocks * blk);
-        for (int64_t i = 0; i < nblocks; ++i)
-          for (int64_t e = 0; e < blk; ++e) idx[i * blk + e] = src_off[i] + e;
-        DevBuf di = upload(c, idx);
-        SB_CK(launch_gather(raw.d(), di.as<int64_t>(), nblocks * blk, t->data.d(), c->stream));
-        c->note_launch();
+        std::vector<int64_t> dof(nblocks), len(nblocks, blk);
+        for (int64_t i = 0; i < nblocks; ++i) dof[i] = i * blk;
+        copy_blocks(c, raw.d(), t->data.d(), src_off, dof, len);
       }
     }
     *out = wrap(ctx, std::move(t));
+  });
+}
+
+sb_status sb_tensor_create_bs_ragged(sb_ctx* ctx, int nd, const int64_t* dims, int n_tail, int64_t nblocks,
+                                     const int64_t* keys, const int64_t* block_dims, const double* data,
+                                     sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    auto d = read_dims(nd, dims);
+    require(n_tail > 0 && n_tail <= nd, SB_ERR_ASSERTION, "0 < N2 <= N required");
+    require(nblocks >= 0, SB_ERR_INVALID_ARG, "nblocks < 0");
+    require(nblocks == 0 || (block_dims && data && (keys || nd == n_tail)), SB_ERR_INVALID_ARG,
+            "keys/block_dims/data NULL");
+    Ctx* c = &ctx->impl;
+    auto t = make_tensor(c, BS, d, n_tail);
+    const int P = t->P();
+    std::vector<int64_t> k(nblocks * P);
+    if (P) std::copy(keys, keys + nblocks * P, k.begin());
+    check_keys_in_range(k, nblocks, P, d);
+    std::vector<int64_t> lin(nblocks), p(nblocks), in_off(nblocks + 1, 0);
+    for (int64_t i = 0; i < nblocks; ++i) {
+      lin[i] = lin0(&k[i * P], d.data(), P);
+      int64_t len = 1;
+      for (int r = 0; r < n_tail; ++r) {
+        const int64_t e = block_dims[i * n_tail + r];
+        require(e >= 1 && e <= d[P + r], SB_ERR_ASSERTION, "block extent must be in 1:dims of its tail axis");
+        len *= e;
+      }
+      in_off[i + 1] = in_off[i] + len;
+    }
+    std::iota(p.begin(), p.end(), 0);
+    std::stable_sort(p.begin(), p.end(), [&](int64_t a, int64_t b) { return lin[a] < lin[b]; });
+    for (int64_t i = 1; i < nblocks; ++i) require(lin[p[i]] != lin[p[i - 1]], SB_ERR_ASSERTION, "duplicate block key");
+    t->ragged = true;
+    t->keys.resize(nblocks * P);
+    t->bdims.resize(nblocks * n_tail);
+    t->boff.assign(nblocks + 1, 0);
+    std::vector<int64_t> so(nblocks), dof(nblocks), len(nblocks);
+    for (int64_t i = 0; i < nblocks; ++i) {
+      std::copy(&k[p[i] * P], &k[p[i] * P] + P, &t->keys[i * P]);
+      std::copy(block_dims + p[i] * n_tail, block_dims + (p[i] + 1) * n_tail, &t->bdims[i * n_tail]);
+      len[i] = in_off[p[i] + 1] - in_off[p[i]];
+      so[i] = in_off[p[i]];
+      t->boff[i + 1] = t->boff[i] + len[i];
+      dof[i] = t->boff[i];
+    }
+    t->nkeys = nblocks;
+    const int64_t total = in_off[nblocks];
+    if (total) {
+      DevBuf raw(c, total * sizeof(double));
+      SB_CK(cudaMemcpyAsync(raw.raw(), data, total * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      bool sorted = true;
+      for (int64_t i = 0; i < nblocks; ++i) sorted = sorted && p[i] == i;
+      if (sorted) {
+        t->data = std::move(raw);
+      } else {
+        t->data = DevBuf(c, total * sizeof(double));
+        copy_blocks(c, raw.d(), t->data.d(), so, dof, len);
+      }
+    }
+    *out = wrap(ctx, std::move(t));
+  });
+}
+
+sb_status sb_tensor_block_dims(const sb_tensor* t, int* ragged, int64_t* block_dims, int64_t* payload_len) {
+  return guard(t ? t->owner : nullptr, [&] {
+    check_t(t);
+    const Tensor& x = *t->impl;
+    if (ragged) *ragged = x.ragged ? 1 : 0;
+    if (payload_len) *payload_len = x.payload_len();
+    if (block_dims && x.kind == BS)
+      for (int64_t i = 0; i < x.nkeys; ++i)
+        for (int r = 0; r < x.n2; ++r) block_dims[i * x.n2 + r] = x.block_dim(i, r);
+  });
+}
+
+sb_status sb_tensor_to_uniform(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    *out = wrap(ctx, bs_to_uniform(&ctx->impl, *A->impl));
+  });
+}
+
+sb_status sb_tensor_to_ragged(sb_ctx* ctx, const sb_tensor* A, const int64_t* block_dims, int check_zero, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    require(out != nullptr && (block_dims || A->impl->nkeys == 0), SB_ERR_INVALID_ARG, "out/block_dims NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    const Tensor& x = *A->impl;
+    std::vector<int64_t> bd(block_dims, block_dims + x.nkeys * x.n2);
+    *out = wrap(ctx, bs_to_ragged(&ctx->impl, x, bd, check_zero != 0));
   });
 }
 
@@ -317,10 +421,12 @@ sb_status sb_tensor_create_aliased(sb_ctx* ctx, int nd, const int64_t* dims, int
 sb_status sb_tensor_free(sb_tensor* t) {
   if (!t) return SB_OK;
   sb_ctx* ctx = t->owner;
-  return guard(ctx, [&] {
+  const sb_status st = guard(ctx, [&] {
     if (ctx) SB_CK(cudaSetDevice(ctx->impl.device));
     delete t;
   });
+  if (ctx && --ctx->impl.live_tensors == 0 && ctx->impl.destroy_pending) destroy_ctx_now(ctx);
+  return st;
 }
 
 sb_status sb_tensor_info(const sb_tensor* t, int* kind, int* nd, int64_t* dims, int* n_tail, int64_t* nkeys,
@@ -350,7 +456,7 @@ sb_status sb_tensor_export_bs(sb_ctx* ctx, const sb_tensor* t, int64_t* keys, in
     if (ids)
       for (int64_t i = 0; i < x.nkeys; ++i) ids[i] = i + 1;
     if (data && x.nkeys) {
-      SB_CK(cudaMemcpyAsync(data, x.data.raw(), x.nkeys * x.blksize() * sizeof(double), cudaMemcpyDeviceToHost, ctx->impl.stream));
+      SB_CK(cudaMemcpyAsync(data, x.data.raw(), x.payload_len() * sizeof(double), cudaMemcpyDeviceToHost, ctx->impl.stream));
       ctx->impl.sync();
     }
   });

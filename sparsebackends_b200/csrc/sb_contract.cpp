@@ -191,6 +191,9 @@ void reset_output(Ctx* ctx, Tensor& C, int64_t nkeys, int64_t payload) {
   C.n_templates = 0;
   if (C.data.bytes() != static_cast<size_t>(payload) * sizeof(double)) C.data = DevBuf(ctx, payload * sizeof(double));
   C.scalars.reset();
+  C.ragged = false;
+  C.bdims.clear();
+  C.boff.clear();
 }
 
 // ── launch helpers ────────────────────────────────────────────────────────
@@ -592,18 +595,73 @@ void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0
     pr.emplace_back(a, b);
   });
   auto ord = ck.order();
-  const int64_t blkA = A->blksize(), blkB = B->blksize(), blkC = C.blksize();
-  reset_output(ctx, C, static_cast<int64_t>(ord.size()), static_cast<int64_t>(ord.size()) * blkC);
-  ck.commit_keys(C, ord);
-  GemmPlan gp;
   const bool athenb = sp.mode == Mode::AthenB;
+  const bool ragged = A->ragged || B->ragged;
+  const int n2C = C.n2;
+  // Per-pair GEMM extents from the blocks' own tail extents (uniform tensors:
+  // the full dims).  Ragged operands must agree on every reduced extent, and
+  // all pairs feeding one C block must agree on its extents.
+  struct PairDims { int64_t m, k, n; };
+  std::vector<PairDims> pd(pr.size());
+  std::vector<int64_t> cbd(ragged ? ord.size() * n2C : 0);
   for (size_t c = 0; c < ord.size(); ++c) {
-    if (athenb) gp.add_cblock(static_cast<int64_t>(c) * blkC, M, N);
-    else gp.add_cblock(static_cast<int64_t>(c) * blkC, N, M);
+    bool first = true;
     for (int ci : ck.contribs[ord[c]]) {
+      const int64_t a = pr[ci].first, b = pr[ci].second;
+      int64_t m = 1, kk = 1, n = 1;
+      for (int t = 0; t < nkA; ++t) m *= A->block_dim(a, t);
+      for (int t = 0; t < nred; ++t) {
+        const int64_t ea = A->block_dim(a, nkA + t), eb = B->block_dim(b, t);
+        require(ea == eb, SB_ERR_DIM_MISMATCH, "ragged reduced extents differ within a matched block pair");
+        kk *= ea;
+      }
+      for (int t = 0; t < nkB; ++t) n *= B->block_dim(b, nred + t);
+      pd[ci] = PairDims{m, kk, n};
+      if (ragged) {
+        std::vector<int64_t> e;
+        if (athenb) {
+          for (int t = 0; t < nkA; ++t) e.push_back(A->block_dim(a, t));
+          for (int t = 0; t < nkB; ++t) e.push_back(B->block_dim(b, nred + t));
+        } else {
+          for (int t = 0; t < nkB; ++t) e.push_back(B->block_dim(b, nred + t));
+          for (int t = 0; t < nkA; ++t) e.push_back(A->block_dim(a, t));
+        }
+        if (first) std::copy(e.begin(), e.end(), cbd.begin() + c * n2C);
+        else
+          require(std::equal(e.begin(), e.end(), cbd.begin() + c * n2C), SB_ERR_DIM_MISMATCH,
+                  "ragged extents of one output block differ between contributing pairs");
+      }
+      first = false;
+    }
+  }
+  const int64_t blkC = C.blksize();
+  std::vector<int64_t> cboff(ord.size() + 1, 0);
+  for (size_t c = 0; c < ord.size(); ++c) {
+    int64_t len = blkC;
+    if (ragged) {
+      len = 1;
+      for (int t = 0; t < n2C; ++t) len *= cbd[c * n2C + t];
+    }
+    cboff[c + 1] = cboff[c] + len;
+  }
+  reset_output(ctx, C, static_cast<int64_t>(ord.size()), cboff.back());
+  ck.commit_keys(C, ord);
+  if (ragged) {
+    C.ragged = true;
+    C.bdims = std::move(cbd);
+    C.boff = cboff;
+  }
+  GemmPlan gp;
+  for (size_t c = 0; c < ord.size(); ++c) {
+    const auto& c0 = pd[ck.contribs[ord[c]][0]];
+    if (athenb) gp.add_cblock(cboff[c], c0.m, c0.n);
+    else gp.add_cblock(cboff[c], c0.n, c0.m);
+    for (int ci : ck.contribs[ord[c]]) {
+      const int64_t xa = A->block_off(pr[ci].first), yb = B->block_off(pr[ci].second);
+      const auto& d = pd[ci];
       // AthenB: C(MxN) = A(MxK) B(KxN); BthenA: C(NxM) = B^T A^T
-      if (athenb) gp.add_pair(pr[ci].first * blkA, pr[ci].second * blkB, K, M, K);
-      else gp.add_pair(pr[ci].second * blkB, pr[ci].first * blkA, K, K, M);
+      if (athenb) gp.add_pair(xa, yb, d.k, d.m, d.k);
+      else gp.add_pair(yb, xa, d.k, d.k, d.m);
     }
   }
   if (athenb) gp.launch(ctx, A->data.d(), B->data.d(), C.data.d(), false, false);
@@ -1581,6 +1639,7 @@ void contract(Ctx* ctx, Tensor& C, const Labels& lC, const Tensor& A, const Labe
   if (C.kind == DENSE) {
     // contract_bs_bs_to_dense! (contract_bs_bs.jl:736-754): P_C = 0 sink.
     require(A.kind == BS && B.kind == BS, SB_ERR_UNSUPPORTED_TYPES, "dense C needs block-sparse A and B");
+    require_uniform(A.ragged ? A : B, "contract_bs_bs_to_dense!");
     auto sink = make_tensor(ctx, BS, C.dims, C.N());
     contract(ctx, *sink, lC, A, lA, B, lB);
     const int64_t n = C.numel();
@@ -1590,6 +1649,7 @@ void contract(Ctx* ctx, Tensor& C, const Labels& lC, const Tensor& A, const Labe
     return;
   }
   check_c_dims(C, lC, oA, oB);
+  const bool ragged_in = (A.kind == BS && A.ragged) || (B.kind == BS && B.ragged);
   Labels shared, reduced;
   for (auto& l : lA)
     if (has(lB, l)) shared.push_back(l);
@@ -1599,6 +1659,7 @@ void contract(Ctx* ctx, Tensor& C, const Labels& lC, const Tensor& A, const Labe
     require(shared.size() == 1, SB_ERR_ASSERTION, "Expected exactly 1 shared label");
     const Label r = reduced[0];
     require(A.dims[find(lA, r)] == B.dims[find(lB, r)], SB_ERR_DIM_MISMATCH, "Dim mismatch on shared label " + lab_str(r));
+    if (ragged_in) require_uniform(A.ragged ? A : B, "single-label contract!");
     const Kind c = C.kind, a = A.kind, b = B.kind;
     if (c == COO && a == COO && b == COO) return coo_coo(ctx, C, lC, oA, oB, r);
     if (c == BS && a == BS && b == BS) {
@@ -1628,6 +1689,7 @@ void contract(Ctx* ctx, Tensor& C, const Labels& lC, const Tensor& A, const Labe
   }
   const Kind c = C.kind, a = A.kind, b = B.kind;
   if (c == BS && a == BS && b == BS) return shared_bb(ctx, C, lC, oA, oB, shared);
+  if (ragged_in) require_uniform(A.ragged ? A : B, "contract_shared!");
   if (c == BS && a == BS && b == DENSE) return shared_bd(ctx, C, lC, oA, oB, shared);
   if (c == ALIASED && a == ALIASED && (b == DENSE || b == ALIASED)) return shared_aliased(ctx, C, lC, oA, oB, shared);
   fail(SB_ERR_UNSUPPORTED_TYPES, "no contract_shared! kernel for this (C, A, B) storage combination");

@@ -90,6 +90,10 @@ struct Ctx {
   size_t next_slot = 0;
   void stage_copy(void* dst, const void* src, size_t bytes);
   void release_staging();
+  // Tensors keep their context alive: sb_ctx_destroy with live tensors only
+  // marks the context, and the last sb_tensor_free destroys it.
+  int64_t live_tensors = 0;
+  bool destroy_pending = false;
   void note_launch(int64_t n = 1) { launches += n; }
   void sync();
   void clear_profile();
@@ -141,6 +145,13 @@ struct Tensor {
   DevBuf scalars;                  // per key
   // COO only
   bool dirty = false;
+  // Ragged block-sparse (extension of the reference format): every block has
+  // its own tail extents (bdims, nkeys x n2) and offset (boff, nkeys + 1);
+  // block i is column-major over bdims[i].  A uniform tensor is the special
+  // case bdims[i] = dims[P:], boff[i] = i * blksize (left implicit).
+  bool ragged = false;
+  std::vector<int64_t> bdims;
+  std::vector<int64_t> boff;
 
   int N() const { return static_cast<int>(dims.size()); }
   int P() const { return N() - n2; }
@@ -156,10 +167,14 @@ struct Tensor {
   }
   const int64_t* key(int64_t i) const { return keys.data() + i * (kind == COO ? N() : P()); }
   int64_t key_len() const { return kind == COO ? N() : P(); }
+  // Per-block layout, valid for uniform and ragged tensors.
+  int64_t block_off(int64_t i) const { return ragged ? boff[i] : i * blksize(); }
+  int64_t block_len(int64_t i) const { return ragged ? boff[i + 1] - boff[i] : blksize(); }
+  int64_t block_dim(int64_t i, int t) const { return ragged ? bdims[i * n2 + t] : dims[P() + t]; }
   int64_t payload_len() const {
     switch (kind) {
       case DENSE: return numel();
-      case BS: return nkeys * blksize();
+      case BS: return ragged ? (nkeys ? boff[nkeys] : 0) : nkeys * blksize();
       case COO: return nkeys;
       default: return n_templates * blksize();
     }
@@ -191,6 +206,13 @@ TensorPtr bs_from_dense(Ctx* ctx, const Tensor& D, int n2, double atol, double r
 TensorPtr coo_from_dense(Ctx* ctx, const Tensor& D, double atol, double rtol);
 TensorPtr to_dense(Ctx* ctx, const Tensor& A);
 TensorPtr aliased_to_bs(Ctx* ctx, const Tensor& A);
+// Ragged <-> uniform adapters (zero padding / cropping).
+TensorPtr bs_to_uniform(Ctx* ctx, const Tensor& A);
+TensorPtr bs_to_ragged(Ctx* ctx, const Tensor& A, const std::vector<int64_t>& bdims, bool check_zero);
+// Copies variable-size blocks: dst[dst_off[i] + e] = src[src_off[i] + e], e < len[i].
+void copy_blocks(Ctx* ctx, const double* src, double* dst, const std::vector<int64_t>& src_off,
+                 const std::vector<int64_t>& dst_off, const std::vector<int64_t>& len);
+void require_uniform(const Tensor& t, const char* what);
 void check_no_cross_perm(const std::vector<int>& perm1, int N, int P);
 bool is_identity(const std::vector<int>& perm1);
 

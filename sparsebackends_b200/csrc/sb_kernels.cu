@@ -133,6 +133,55 @@ __global__ void k_permute_tiled(const double* __restrict__ src, double* __restri
   }
 }
 
+// ── variable-size block copies / permutes ─────────────────────────────────
+__global__ void k_copy_blocks(const double* __restrict__ src, double* __restrict__ dst,
+                              const BlockCopy* __restrict__ items, int64_t n) {
+  for (int64_t b = blockIdx.y; b < n; b += gridDim.y) {
+    const BlockCopy it = items[b];
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < it.len; e += (int64_t)gridDim.x * blockDim.x)
+      dst[it.dst_off + e] = src[it.src_off + e];
+  }
+}
+
+__global__ void k_perm_blocks(const double* __restrict__ src, double* __restrict__ dst,
+                              const BlockPerm* __restrict__ items, int64_t n) {
+  for (int64_t b = blockIdx.y; b < n; b += gridDim.y) {
+    const BlockPerm& it = items[b];
+    for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < it.len;
+         e0 += (int64_t)gridDim.x * blockDim.x) {
+      int64_t e = e0, so = 0;
+      bool in = true;
+      for (int r = 0; r < it.rank; ++r) {
+        const int64_t c = e % it.out_dims[r];
+        e /= it.out_dims[r];
+        in = in && c < it.in_lim[r];
+        so += c * it.in_strides[r];
+      }
+      dst[it.dst_off + e0] = in ? src[it.src_off + so] : 0.0;
+    }
+  }
+}
+
+__global__ void k_outside_nonzero(const double* __restrict__ src, const BlockPerm* __restrict__ items, int64_t n,
+                                  uint8_t* __restrict__ flags) {
+  for (int64_t b = blockIdx.x; b < n; b += gridDim.x) {
+    const BlockPerm& it = items[b];
+    int any = 0;
+    for (int64_t e0 = threadIdx.x; e0 < it.len && !any; e0 += blockDim.x) {
+      int64_t e = e0;
+      bool in = true;
+      for (int r = 0; r < it.rank; ++r) {
+        const int64_t c = e % it.out_dims[r];
+        e /= it.out_dims[r];
+        in = in && c < it.in_lim[r];
+      }
+      any = !in && src[it.src_off + e0] != 0.0;
+    }
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) flags[b] = any ? 1 : 0;
+  }
+}
+
 // ── structure flags ───────────────────────────────────────────────────────
 __global__ void k_slice_nonzero(const double* __restrict__ src, const int64_t* __restrict__ off,
                                 int64_t nslices, int64_t chunk, uint8_t* __restrict__ flags,
@@ -304,6 +353,33 @@ cudaError_t launch_permute_blocks(const double* src, double* dst, const int64_t*
   const int64_t total = nblocks * td.nbatch * td.tiles_u * td.tiles_v;
   const unsigned g = static_cast<unsigned>(total < 148LL * 64 ? total : 148LL * 64);
   k_permute_tiled<<<g, dim3(32, 8), 0, s>>>(src, dst, d_src_off, blk, td, total);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_copy_blocks(const double* src, double* dst, const BlockCopy* d_items, int64_t n, int64_t max_len,
+                               cudaStream_t s) {
+  if (n <= 0 || max_len <= 0) return cudaSuccess;
+  dim3 grid(grid_for(max_len), static_cast<unsigned>(n < 65535 ? n : 65535));
+  if ((int64_t)grid.x * grid.y > 148LL * 64) grid.x = static_cast<unsigned>(std::max<int64_t>(1, 148LL * 64 / grid.y));
+  k_copy_blocks<<<grid, kThreads, 0, s>>>(src, dst, d_items, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_perm_blocks(const double* src, double* dst, const BlockPerm* d_items, int64_t n, int64_t max_len,
+                               cudaStream_t s) {
+  if (n <= 0 || max_len <= 0) return cudaSuccess;
+  dim3 grid(grid_for(max_len), static_cast<unsigned>(n < 65535 ? n : 65535));
+  if ((int64_t)grid.x * grid.y > 148LL * 64) grid.x = static_cast<unsigned>(std::max<int64_t>(1, 148LL * 64 / grid.y));
+  k_perm_blocks<<<grid, kThreads, 0, s>>>(src, dst, d_items, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_outside_nonzero(const double* src, const BlockPerm* d_items, int64_t n, int64_t max_len,
+                                   uint8_t* flags, cudaStream_t s) {
+  (void)max_len;
+  if (n <= 0) return cudaSuccess;
+  const unsigned g = static_cast<unsigned>(n < 148LL * 32 ? n : 148LL * 32);
+  k_outside_nonzero<<<g, 128, 0, s>>>(src, d_items, n, flags);
   return cudaGetLastError();
 }
 

@@ -90,6 +90,29 @@ cudaError_t launch_permute_blocks(const double* src, double* dst, const int64_t*
                                   int64_t nblocks, int64_t blk, const PermDesc& desc,
                                   cudaStream_t s);
 
+// Variable-size block copy: dst[dst_off[i] + e] = src[src_off[i] + e] for e < len[i].
+struct BlockCopy {
+  int64_t src_off, dst_off, len;
+};
+cudaError_t launch_copy_blocks(const double* src, double* dst, const BlockCopy* d_items, int64_t n,
+                               int64_t max_len, cudaStream_t s);
+// Per-block tail permute / pad / crop: output block i (dst_off, out_dims) element
+// e reads src[src_off + sum_r c_r * in_strides[r]] when every coordinate c_r is
+// below in_lim[r], and writes 0 otherwise (zero padding).
+struct BlockPerm {
+  int64_t src_off, dst_off, len;
+  int rank;
+  int64_t out_dims[kMaxRank];
+  int64_t in_strides[kMaxRank];
+  int64_t in_lim[kMaxRank];
+};
+cudaError_t launch_perm_blocks(const double* src, double* dst, const BlockPerm* d_items, int64_t n,
+                               int64_t max_len, cudaStream_t s);
+// flags[i] = 1 if block i of src holds a nonzero outside its box in_lim
+// (used to check that cropping a padded block loses nothing).
+cudaError_t launch_outside_nonzero(const double* src, const BlockPerm* d_items, int64_t n, int64_t max_len,
+                                   uint8_t* flags, cudaStream_t s);
+
 // ── value-dependent structure helpers ──────────────────────────────────────
 // flags[b*nslices + s] = any(src[off_b + s*chunk + t] != 0, t < chunk)
 cudaError_t launch_slice_nonzero(const double* src, const int64_t* d_off, int64_t nblocks,

@@ -167,6 +167,141 @@ void sort_bs_keys_in_place(Tensor& t) {
   (void)t;  // keys are kept sorted by construction
 }
 
+void require_uniform(const Tensor& t, const char* what) {
+  if (t.ragged)
+    fail(SB_ERR_UNSUPPORTED_LAYOUT,
+         std::string(what) + ": ragged block-sparse operands are supported by contract_shared! (BS x BS), "
+                             "permutedims and the uniform/ragged adapters; convert with sb_tensor_to_uniform");
+}
+
+void copy_blocks(Ctx* ctx, const double* src, double* dst, const std::vector<int64_t>& src_off,
+                 const std::vector<int64_t>& dst_off, const std::vector<int64_t>& len) {
+  if (src_off.empty()) return;
+  std::vector<BlockCopy> items(src_off.size());
+  int64_t mx = 0;
+  double bytes = 0.0;
+  for (size_t i = 0; i < items.size(); ++i) {
+    items[i] = BlockCopy{src_off[i], dst_off[i], len[i]};
+    mx = std::max(mx, len[i]);
+    bytes += 16.0 * len[i];
+  }
+  DevBuf d = upload(ctx, items);
+  ProfScope ps(ctx, PROF_PERMUTE, 0.0, bytes);
+  SB_CK(launch_copy_blocks(src, dst, d.as<BlockCopy>(), static_cast<int64_t>(items.size()), mx, ctx->stream));
+  ctx->note_launch();
+}
+
+// Per-block permute/pad/crop through BlockPerm descriptors.
+static void perm_blocks(Ctx* ctx, const double* src, double* dst, std::vector<BlockPerm>& items) {
+  if (items.empty()) return;
+  int64_t mx = 0;
+  double bytes = 0.0;
+  for (auto& it : items) {
+    mx = std::max(mx, it.len);
+    bytes += 16.0 * it.len;
+  }
+  DevBuf d = upload(ctx, items);
+  ProfScope ps(ctx, PROF_PERMUTE, 0.0, bytes);
+  SB_CK(launch_perm_blocks(src, dst, d.as<BlockPerm>(), static_cast<int64_t>(items.size()), mx, ctx->stream));
+  ctx->note_launch();
+}
+
+static BlockPerm make_block_perm(int64_t src_off, int64_t dst_off, const std::vector<int64_t>& out_dims,
+                                 const std::vector<int64_t>& in_strides, const std::vector<int64_t>& in_lim) {
+  require(out_dims.size() <= static_cast<size_t>(kMaxRank), SB_ERR_INVALID_ARG, "tail rank too large");
+  BlockPerm b{};
+  b.src_off = src_off;
+  b.dst_off = dst_off;
+  b.len = 1;
+  b.rank = static_cast<int>(out_dims.size());
+  for (size_t r = 0; r < out_dims.size(); ++r) {
+    b.out_dims[r] = out_dims[r];
+    b.in_strides[r] = in_strides[r];
+    b.in_lim[r] = in_lim[r];
+    b.len *= out_dims[r];
+  }
+  return b;
+}
+
+TensorPtr bs_to_uniform(Ctx* ctx, const Tensor& A) {
+  require(A.kind == BS, SB_ERR_INVALID_ARG, "to_uniform needs a block-sparse tensor");
+  auto out = make_tensor(ctx, BS, A.dims, A.n2);
+  out->keys = A.keys;
+  out->nkeys = A.nkeys;
+  const int64_t blk = A.blksize();
+  out->data = DevBuf(ctx, A.nkeys * blk * sizeof(double));
+  if (!A.ragged) {
+    if (A.nkeys)
+      SB_CK(cudaMemcpyAsync(out->data.raw(), A.data.raw(), A.nkeys * blk * sizeof(double), cudaMemcpyDeviceToDevice,
+                            ctx->stream));
+    return out;
+  }
+  const int P = A.P();
+  std::vector<int64_t> od(A.dims.begin() + P, A.dims.end());
+  std::vector<BlockPerm> items;
+  for (int64_t i = 0; i < A.nkeys; ++i) {
+    std::vector<int64_t> st(A.n2), lim(A.n2);
+    int64_t acc = 1;
+    for (int t = 0; t < A.n2; ++t) {
+      st[t] = acc;
+      lim[t] = A.block_dim(i, t);
+      acc *= lim[t];
+    }
+    items.push_back(make_block_perm(A.block_off(i), i * blk, od, st, lim));
+  }
+  perm_blocks(ctx, A.data.d(), out->data.d(), items);
+  return out;
+}
+
+TensorPtr bs_to_ragged(Ctx* ctx, const Tensor& A, const std::vector<int64_t>& bd, bool check_zero) {
+  require(A.kind == BS, SB_ERR_INVALID_ARG, "to_ragged needs a block-sparse tensor");
+  require(static_cast<int64_t>(bd.size()) == A.nkeys * A.n2, SB_ERR_INVALID_ARG, "block_dims must be nkeys x n_tail");
+  const int P = A.P();
+  auto out = make_tensor(ctx, BS, A.dims, A.n2);
+  out->keys = A.keys;
+  out->nkeys = A.nkeys;
+  out->ragged = true;
+  out->bdims = bd;
+  out->boff.assign(A.nkeys + 1, 0);
+  for (int64_t i = 0; i < A.nkeys; ++i) {
+    int64_t len = 1;
+    for (int t = 0; t < A.n2; ++t) {
+      const int64_t e = bd[i * A.n2 + t];
+      require(e >= 1 && e <= A.block_dim(i, t), SB_ERR_ASSERTION, "block extent out of range");
+      len *= e;
+    }
+    out->boff[i + 1] = out->boff[i] + len;
+  }
+  out->data = DevBuf(ctx, out->boff[A.nkeys] * sizeof(double));
+  std::vector<BlockPerm> items, checks;
+  for (int64_t i = 0; i < A.nkeys; ++i) {
+    std::vector<int64_t> od(A.n2), st(A.n2), full(A.n2);
+    int64_t acc = 1;
+    for (int t = 0; t < A.n2; ++t) {
+      od[t] = bd[i * A.n2 + t];
+      full[t] = A.block_dim(i, t);
+      st[t] = acc;
+      acc *= full[t];
+    }
+    items.push_back(make_block_perm(A.block_off(i), out->boff[i], od, st, od));
+    if (check_zero) checks.push_back(make_block_perm(A.block_off(i), 0, full, st, od));
+  }
+  if (check_zero && !checks.empty()) {
+    int64_t mx = 0;
+    for (auto& c : checks) mx = std::max(mx, c.len);
+    DevBuf dc = upload(ctx, checks);
+    DevBuf fl(ctx, checks.size());
+    SB_CK(launch_outside_nonzero(A.data.d(), dc.as<BlockPerm>(), static_cast<int64_t>(checks.size()), mx,
+                                 fl.as<uint8_t>(), ctx->stream));
+    ctx->note_launch();
+    auto f = download<uint8_t>(ctx, fl.raw(), checks.size());
+    for (size_t i = 0; i < f.size(); ++i)
+      require(!f[i], SB_ERR_ASSERTION, "cropping would drop nonzero entries of block " + std::to_string(i + 1));
+  }
+  perm_blocks(ctx, A.data.d(), out->data.d(), items);
+  return out;
+}
+
 TensorPtr bs_permute(Ctx* ctx, const Tensor& A, const std::vector<int>& perm) {
   const int N = A.N(), P = A.P();
   check_no_cross_perm(perm, N, P);
@@ -188,6 +323,45 @@ TensorPtr bs_permute(Ctx* ctx, const Tensor& A, const std::vector<int>& perm) {
   for (int64_t i = 0; i < n; ++i)
     std::copy(&nk[p[i] * P], &nk[p[i] * P] + P, &out->keys[i * P]);
   out->nkeys = n;
+  bool tail_identity = true;
+  for (int r = 0; r < A.n2; ++r) tail_identity = tail_identity && perm[P + r] == P + r + 1;
+  if (A.ragged) {
+    // per-block extents travel with their blocks, permuted like the tail axes
+    out->ragged = true;
+    out->bdims.resize(n * A.n2);
+    out->boff.assign(n + 1, 0);
+    for (int64_t i = 0; i < n; ++i) {
+      for (int r = 0; r < A.n2; ++r) out->bdims[i * A.n2 + r] = A.block_dim(p[i], perm[P + r] - 1 - P);
+      out->boff[i + 1] = out->boff[i] + A.block_len(p[i]);
+    }
+    out->data = DevBuf(ctx, out->boff[n] * sizeof(double));
+    if (tail_identity) {
+      std::vector<int64_t> so(n), dof(n), len(n);
+      for (int64_t i = 0; i < n; ++i) {
+        so[i] = A.block_off(p[i]);
+        dof[i] = out->boff[i];
+        len[i] = A.block_len(p[i]);
+      }
+      copy_blocks(ctx, A.data.d(), out->data.d(), so, dof, len);
+    } else {
+      std::vector<BlockPerm> items;
+      for (int64_t i = 0; i < n; ++i) {
+        std::vector<int64_t> sst(A.n2), od(A.n2), is(A.n2);
+        int64_t acc = 1;
+        for (int t = 0; t < A.n2; ++t) {
+          sst[t] = acc;
+          acc *= A.block_dim(p[i], t);
+        }
+        for (int r = 0; r < A.n2; ++r) {
+          od[r] = out->bdims[i * A.n2 + r];
+          is[r] = sst[perm[P + r] - 1 - P];
+        }
+        items.push_back(make_block_perm(A.block_off(p[i]), out->boff[i], od, is, od));
+      }
+      perm_blocks(ctx, A.data.d(), out->data.d(), items);
+    }
+    return out;
+  }
   out->data = DevBuf(ctx, n * blk * sizeof(double));
   std::vector<int64_t> soff(n);
   for (int64_t i = 0; i < n; ++i) soff[i] = p[i] * blk;
@@ -266,6 +440,9 @@ TensorPtr copy_tensor(Ctx* ctx, const Tensor& A) {
   out->n_templates = A.n_templates;
   out->alias_ids = A.alias_ids;
   out->dirty = A.dirty;
+  out->ragged = A.ragged;
+  out->bdims = A.bdims;
+  out->boff = A.boff;
   const int64_t len = A.payload_len();
   out->data = DevBuf(ctx, len * sizeof(double));
   if (len) SB_CK(cudaMemcpyAsync(out->data.raw(), A.data.raw(), len * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
@@ -413,6 +590,10 @@ TensorPtr aliased_to_bs(Ctx* ctx, const Tensor& A) {
 
 TensorPtr to_dense(Ctx* ctx, const Tensor& A) {
   if (A.kind == DENSE) return copy_tensor(ctx, A);
+  if (A.kind == BS && A.ragged) {
+    auto u = bs_to_uniform(ctx, A);
+    return to_dense(ctx, *u);
+  }
   if (A.kind == ALIASED) {
     auto b = aliased_to_bs(ctx, A);
     return to_dense(ctx, *b);

@@ -163,11 +163,13 @@ class HeffLayout:
         return tuple(out)
 
 
-def random_block_tensor(layout: HeffLayout, name: str, rng: np.random.Generator, scale: float = 1.0):
+def random_block_tensor(layout: HeffLayout, name: str, rng: np.random.Generator, scale: float = 1.0,
+                        ragged: bool = False):
     """Gaussian entries inside each block's sector extents, zero padding outside.
 
     Returns (keys, data) in the reference layout (keys sorted column-major,
-    blocks packed in that order)."""
+    blocks packed in that order).  With ``ragged=True`` returns
+    (keys, data, block_dims): the same entries stored unpadded, block by block."""
     lab = layout.labels[name]
     dims = layout.dims[name]
     n2 = layout.n2[name]
@@ -185,6 +187,10 @@ def random_block_tensor(layout: HeffLayout, name: str, rng: np.random.Generator,
         return idx
 
     keys = sorted(keys, key=lin)
+    if ragged:
+        exts = [layout.valid_extent(name, k) for k in keys]
+        parts = [(rng.standard_normal(e) * scale).reshape(-1, order="F") for e in exts]
+        return keys, (np.concatenate(parts) if parts else np.zeros(0)), exts
     data = np.zeros(len(keys) * blk)
     for i, k in enumerate(keys):
         ext = layout.valid_extent(name, k)
@@ -192,6 +198,23 @@ def random_block_tensor(layout: HeffLayout, name: str, rng: np.random.Generator,
         blkarr[tuple(slice(0, e) for e in ext)] = rng.standard_normal(ext) * scale
         data[i * blk:(i + 1) * blk] = blkarr.reshape(-1, order="F")
     return keys, data
+
+
+def pad_ragged(layout: HeffLayout, name: str, keys, data, exts):
+    """Zero-pad ragged blocks into the uniform reference layout (host arrays)."""
+    dims = layout.dims[name]
+    P = len(dims) - layout.n2[name]
+    tail = dims[P:]
+    blk = int(np.prod(tail))
+    out = np.zeros(len(keys) * blk)
+    off = 0
+    for i, e in enumerate(exts):
+        n = int(np.prod(e))
+        b = np.zeros(tail)
+        b[tuple(slice(0, x) for x in e)] = data[off: off + n].reshape(e, order="F")
+        out[i * blk:(i + 1) * blk] = b.reshape(-1, order="F")
+        off += n
+    return out
 
 
 class HeffChain:

@@ -328,3 +328,19 @@ def test_error_statuses(sb):
     with pytest.raises(sb.SparseBackendsError) as ei:
         sb.contract_(Cc, ["i", "y"], A, ["i", "r"], sb.DenseTensor(np.zeros((4, 2))), ["r", "y"])
     assert ei.value.status == "SB_ERR_UNSUPPORTED_TYPES"
+
+
+def test_context_destroy_is_deferred_while_tensors_live(sb):
+    """sb_ctx_destroy with live tensors is deferred to the last sb_tensor_free
+    (Python finalizers can run in any order, e.g. at interpreter exit)."""
+    import ctypes as C
+    ctx = sb.Context(0)
+    lib = ctx._lib
+    t = sb.NewBlockSparseSorted((2, 3), 1, [(1,)], None, np.arange(3.0), ctx=ctx)
+    u = sb.DenseTensor(np.ones((2, 2)), ctx)
+    h = ctx._h
+    assert lib.sb_ctx_destroy(h) == 0           # deferred: two tensors alive
+    assert np.array_equal(t.data, np.arange(3.0))  # the context still works for them
+    del u
+    ctx._h = C.c_void_p()                       # Python must not destroy it again
+    del t                                       # the last free destroys the context
