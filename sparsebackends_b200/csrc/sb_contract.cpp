@@ -21,6 +21,7 @@
 //                              contract_aliased_shared.jl
 //   bs_bs_to_dense()           contract_bs_bs.jl:736-754
 #include <algorithm>
+#include <climits>
 #include <map>
 #include <numeric>
 #include <unordered_map>
@@ -215,29 +216,69 @@ struct GemmPlan {
   }
   void launch(Ctx* ctx, const double* X, const double* Y, double* C, bool xT, bool yT) {
     if (cbs.empty()) return;
-    // Tile shape from the (uniform) C block shape.
-    int64_t M = 0, N = 0;
-    for (auto& c : cbs) { M = std::max<int64_t>(M, c.M); N = std::max<int64_t>(N, c.N); }
+    int64_t M = 0, N = 0, Kmax = 0, Mmin = INT64_MAX, Nmin = INT64_MAX;
+    double flops = 0.0, bytes = 0.0;
+    for (auto& c : cbs) {
+      M = std::max<int64_t>(M, c.M);
+      N = std::max<int64_t>(N, c.N);
+      Mmin = std::min<int64_t>(Mmin, c.M);
+      Nmin = std::min<int64_t>(Nmin, c.N);
+      bytes += 8.0 * c.M * c.N;
+      for (int p = c.pair_begin; p < c.pair_end; ++p) {
+        Kmax = std::max<int64_t>(Kmax, pairs[p].K);
+        flops += 2.0 * c.M * c.N * pairs[p].K;
+        bytes += 8.0 * (static_cast<double>(c.M) + c.N) * pairs[p].K;
+      }
+    }
+    // Skinny streaming kernel: every pair K <= 32, one side <= 32 everywhere,
+    // the other side long (HBM-bound outer-product-like GEMMs).
+    const bool skinny_n = Kmax <= 32 && N <= 32 && Mmin >= 256;
+    const bool skinny_m = Kmax <= 32 && M <= 32 && Nmin >= 256;
+    if ((skinny_n || skinny_m) && ctx->gemm_tile < 0) {
+      const bool small_rows = skinny_m;
+      int64_t nctas = 0;
+      for (auto& c : cbs) {
+        const int64_t bigx = small_rows ? c.N : c.M;
+        c.tile_begin = static_cast<int32_t>(nctas);
+        c.mtiles = 1;
+        nctas += (bigx + 255) / 256;
+      }
+      DevBuf dc = upload(ctx, cbs), dp = upload(ctx, pairs);
+      {
+        ProfScope ps(ctx, PROF_GEMM, flops, bytes);
+        SB_CK(launch_gemm_f64_skinny(X, Y, C, dc.as<GemmCBlock>(), static_cast<int32_t>(cbs.size()), dp.as<GemmPair>(),
+                                     nctas, xT, yT, small_rows, static_cast<int>(small_rows ? M : N),
+                                     static_cast<int>(Kmax), ctx->stream));
+      }
+      ctx->note_launch();
+      return;
+    }
+    // Tile shape from the FLOP-weighted block shape (ragged launches mix
+    // large and small blocks; the heavy ones decide).
+    double wm = 0.0, wn = 0.0, wsum = 0.0;
+    for (auto& c : cbs) {
+      double w = 0.0;
+      for (int p = c.pair_begin; p < c.pair_end; ++p) w += static_cast<double>(pairs[p].K);
+      w *= static_cast<double>(c.M) * c.N;
+      wm += w * c.M;
+      wn += w * c.N;
+      wsum += w;
+    }
+    const double am = wsum > 0 ? wm / wsum : static_cast<double>(M), an = wsum > 0 ? wn / wsum : static_cast<double>(N);
     GemmShape shape = GemmShape::T64x64;
-    if (N <= 32 && M >= 128) shape = GemmShape::T128x32;
-    else if (M <= 32 && N >= 128) shape = GemmShape::T32x128;
-    else if (M >= 256 && N >= 128) shape = M >= N ? GemmShape::T128x64 : GemmShape::T64x128;
+    if (an <= 32 && am >= 128) shape = GemmShape::T128x32;
+    else if (am <= 32 && an >= 128) shape = GemmShape::T32x128;
+    else if (am >= 1024 && an >= 512) shape = am >= an ? GemmShape::T128x64 : GemmShape::T64x128;
     if (ctx->gemm_tile >= 0) shape = static_cast<GemmShape>(ctx->gemm_tile);
     int bm, bn;
     gemm_tile_dims(shape, &bm, &bn);
     int64_t ntiles = 0;
-    double flops = 0.0, bytes = 0.0;
     for (auto& c : cbs) {
       const int64_t mt = (c.M + bm - 1) / bm, nt = (c.N + bn - 1) / bn;
       require(ntiles + mt * nt < (1LL << 31), SB_ERR_INVALID_ARG, "too many GEMM tiles in one launch");
       c.tile_begin = static_cast<int32_t>(ntiles);
       c.mtiles = static_cast<int32_t>(mt);
       ntiles += mt * nt;
-      bytes += 8.0 * c.M * c.N;
-      for (int p = c.pair_begin; p < c.pair_end; ++p) {
-        flops += 2.0 * c.M * c.N * pairs[p].K;
-        bytes += 8.0 * (static_cast<double>(c.M) + c.N) * pairs[p].K;
-      }
     }
     DevBuf dc = upload(ctx, cbs), dp = upload(ctx, pairs);
     {

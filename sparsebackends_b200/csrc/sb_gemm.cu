@@ -198,6 +198,94 @@ cudaError_t dispatch_t(bool xT, bool yT, const double* X, const double* Y, doubl
   return launch_t<BM, BN, WM, WN, true, true>(X, Y, C, cb, ncb, pr, nt, s);
 }
 
+// ── skinny streaming GEMM (K <= 32, one of M/N <= 32) ─────────────────────
+constexpr int kSkinnyThreads = 256;
+
+template <int SM, int KM, bool SMALL_ROWS, bool XT, bool YT>
+__global__ void __launch_bounds__(kSkinnyThreads)
+    k_gemm_skinny(const double* __restrict__ X, const double* __restrict__ Y, double* __restrict__ C,
+                  const GemmCBlock* __restrict__ cblocks, int32_t ncb, const GemmPair* __restrict__ pairs) {
+  __shared__ double small[32 * 33];
+  int lo = 0, hi = ncb - 1;
+  const int bid = static_cast<int>(blockIdx.x);
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (cblocks[mid].tile_begin <= bid) lo = mid; else hi = mid - 1;
+  }
+  const GemmCBlock cb = cblocks[lo];
+  const int M = cb.M, N = cb.N;
+  const int big = SMALL_ROWS ? N : M;
+  const int ns = SMALL_ROWS ? M : N;  // small extent (<= SM)
+  const int idx = (bid - cb.tile_begin) * kSkinnyThreads + static_cast<int>(threadIdx.x);
+  double acc[SM];
+#pragma unroll
+  for (int j = 0; j < SM; ++j) acc[j] = 0.0;
+  for (int p = cb.pair_begin; p < cb.pair_end; ++p) {
+    const GemmPair pr = pairs[p];
+    const int K = pr.K;
+    __syncthreads();
+    // stage the small operand as small[k * 33 + s]
+    for (int e = threadIdx.x; e < K * ns; e += kSkinnyThreads) {
+      const int k = e % K, sidx = e / K;
+      double v;
+      if (SMALL_ROWS)  // X(i = sidx, k)
+        v = XT ? X[pr.x_off + k + (int64_t)sidx * pr.ldx] : X[pr.x_off + sidx + (int64_t)k * pr.ldx];
+      else  // Y(k, j = sidx)
+        v = YT ? Y[pr.y_off + sidx + (int64_t)k * pr.ldy] : Y[pr.y_off + k + (int64_t)sidx * pr.ldy];
+      small[k * 33 + sidx] = v;
+    }
+    __syncthreads();
+    if (idx < big) {
+      // issue all K loads of this row/column before using them
+      double v[KM];
+#pragma unroll
+      for (int k = 0; k < KM; ++k) {
+        if (k < K) {
+          if (SMALL_ROWS)  // Y(k, j = idx)
+            v[k] = YT ? Y[pr.y_off + idx + (int64_t)k * pr.ldy] : Y[pr.y_off + k + (int64_t)idx * pr.ldy];
+          else  // X(i = idx, k)
+            v[k] = XT ? X[pr.x_off + k + (int64_t)idx * pr.ldx] : X[pr.x_off + idx + (int64_t)k * pr.ldx];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < KM; ++k) {
+        if (k < K) {
+          const double* srow = small + k * 33;
+#pragma unroll
+          for (int j = 0; j < SM; ++j)
+            if (j < ns) acc[j] = fma(v[k], srow[j], acc[j]);
+        }
+      }
+    }
+  }
+  if (idx >= big) return;
+  double* cbase = C + cb.c_off;
+#pragma unroll
+  for (int j = 0; j < SM; ++j) {
+    if (j >= ns) break;
+    if (SMALL_ROWS) cbase[j + (int64_t)idx * M] = acc[j];  // C(j, idx)
+    else cbase[idx + (int64_t)j * M] = acc[j];             // C(idx, j)
+  }
+}
+
+template <int SM, int KM, bool SR>
+cudaError_t skinny_t(bool xT, bool yT, const double* X, const double* Y, double* C, const GemmCBlock* cb, int32_t ncb,
+                     const GemmPair* pr, int64_t nctas, cudaStream_t s) {
+  const unsigned g = static_cast<unsigned>(nctas);
+  if (!xT && !yT) k_gemm_skinny<SM, KM, SR, false, false><<<g, kSkinnyThreads, 0, s>>>(X, Y, C, cb, ncb, pr);
+  else if (!xT && yT) k_gemm_skinny<SM, KM, SR, false, true><<<g, kSkinnyThreads, 0, s>>>(X, Y, C, cb, ncb, pr);
+  else if (xT && !yT) k_gemm_skinny<SM, KM, SR, true, false><<<g, kSkinnyThreads, 0, s>>>(X, Y, C, cb, ncb, pr);
+  else k_gemm_skinny<SM, KM, SR, true, true><<<g, kSkinnyThreads, 0, s>>>(X, Y, C, cb, ncb, pr);
+  return cudaGetLastError();
+}
+
+template <int SM, int KM>
+cudaError_t skinny_sr(bool sr, bool xT, bool yT, const double* X, const double* Y, double* C, const GemmCBlock* cb,
+                      int32_t ncb, const GemmPair* pr, int64_t nctas, cudaStream_t s) {
+  return sr ? skinny_t<SM, KM, true>(xT, yT, X, Y, C, cb, ncb, pr, nctas, s)
+            : skinny_t<SM, KM, false>(xT, yT, X, Y, C, cb, ncb, pr, nctas, s);
+}
+
 }  // namespace
 
 void gemm_tile_dims(GemmShape shape, int* bm, int* bn) {
@@ -208,6 +296,18 @@ void gemm_tile_dims(GemmShape shape, int* bm, int* bn) {
     case GemmShape::T64x128: *bm = 64; *bn = 128; break;
     default: *bm = 64; *bn = 64; break;
   }
+}
+
+cudaError_t launch_gemm_f64_skinny(const double* X, const double* Y, double* C, const GemmCBlock* d_cblocks,
+                                   int32_t ncb, const GemmPair* d_pairs, int64_t nctas, bool xT, bool yT,
+                                   bool small_rows, int small_max, int k_max, cudaStream_t s) {
+  if (nctas <= 0) return cudaSuccess;
+  if (nctas > 0x7fffffffLL || small_max > 32 || k_max > 32) return cudaErrorInvalidValue;
+  const bool s16 = small_max <= 16, k16 = k_max <= 16;
+  if (s16 && k16) return skinny_sr<16, 16>(small_rows, xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, s);
+  if (s16) return skinny_sr<16, 32>(small_rows, xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, s);
+  if (k16) return skinny_sr<32, 16>(small_rows, xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, s);
+  return skinny_sr<32, 32>(small_rows, xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, s);
 }
 
 cudaError_t launch_gemm_f64(const double* X, const double* Y, double* C,

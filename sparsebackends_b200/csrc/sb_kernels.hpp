@@ -37,6 +37,16 @@ cudaError_t launch_gemm_f64(const double* X, const double* Y, double* C,
                             const GemmCBlock* d_cblocks, int32_t ncblocks, const GemmPair* d_pairs,
                             int64_t ntiles, bool xT, bool yT, GemmShape shape, cudaStream_t s);
 
+// Skinny variant (streaming, CUDA cores) for launches whose every pair has
+// K <= 32 and whose C blocks have min(M, N) <= 32: one thread per row (when
+// N is the small side) or per column (when M is), the small operand of each
+// pair staged in shared memory, partial sums over the pairs in registers.
+// CTAs of C block c: [tile_begin, tile_begin + ceil(big/256)) (mtiles unused).
+cudaError_t launch_gemm_f64_skinny(const double* X, const double* Y, double* C,
+                                   const GemmCBlock* d_cblocks, int32_t ncblocks, const GemmPair* d_pairs,
+                                   int64_t nctas, bool xT, bool yT, bool small_rows, int small_max,
+                                   int k_max, cudaStream_t s);
+
 // Number of tiles of a (M, N) C block for the given tile shape.
 void gemm_tile_dims(GemmShape shape, int* bm, int* bn);
 

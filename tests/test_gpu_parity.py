@@ -344,3 +344,17 @@ def test_context_destroy_is_deferred_while_tensors_live(sb):
     del u
     ctx._h = C.c_void_p()                       # Python must not destroy it again
     del t                                       # the last free destroys the context
+
+
+@pytest.mark.parametrize("seed", [51, 52])
+def test_random_skinny_streaming_gemm(sb, seed):
+    """Small K and one small output side route to the streaming GEMM kernel
+    (both orientations, several pairs accumulated per output block)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    # A[(i, q) | (m, k)] x B[(q, j) | (k, n)]: M=700 rows, K=13, N=11
+    _, A = rand_bs(rng, (2, 3, 700, 13), 2, density=0.9)
+    _, B = rand_bs(rng, (3, 2, 13, 11), 2, density=0.9)
+    lA, lB = ["i", "q", "m", "k"], ["q", "j", "k", "n"]
+    for lC, dims in ((["i", "j", "m", "n"], (2, 2, 700, 11)), (["i", "j", "n", "m"], (2, 2, 11, 700))):
+        Cg, Cref = run_both(sb, so.BS.empty(dims, 2), lC, A, lA, B, lB)
+        assert_bs_equal(Cg, Cref)
