@@ -104,6 +104,7 @@ sb_status sb_ctx_create(int device, unsigned flags, sb_ctx** out) {
       else if (v == "128x64") c->impl.gemm_tile = 3;
       else if (v == "64x128") c->impl.gemm_tile = 4;
     }
+    if (const char* sk = std::getenv("SPARSEB_GEMM_SPLITK")) c->impl.gemm_splitk = std::max(0, std::atoi(sk));
     // Keep freed device memory cached in the stream-ordered pool.
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {

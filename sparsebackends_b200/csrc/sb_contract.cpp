@@ -230,10 +230,10 @@ struct GemmPlan {
         bytes += 8.0 * (static_cast<double>(c.M) + c.N) * pairs[p].K;
       }
     }
-    // Skinny streaming kernel: every pair K <= 32, one side <= 32 everywhere,
-    // the other side long (HBM-bound outer-product-like GEMMs).
-    const bool skinny_n = Kmax <= 32 && N <= 32 && Mmin >= 256;
-    const bool skinny_m = Kmax <= 32 && M <= 32 && Nmin >= 256;
+    // Thin kernel: every pair K <= 16, one side <= 16 everywhere, the other
+    // side long (HBM-bound outer-product-like GEMMs).
+    const bool skinny_n = Kmax <= 16 && N <= 16 && Mmin >= 128;
+    const bool skinny_m = Kmax <= 16 && M <= 16 && Nmin >= 128;
     if ((skinny_n || skinny_m) && ctx->gemm_tile < 0) {
       const bool small_rows = skinny_m;
       int64_t nctas = 0;
@@ -241,7 +241,7 @@ struct GemmPlan {
         const int64_t bigx = small_rows ? c.N : c.M;
         c.tile_begin = static_cast<int32_t>(nctas);
         c.mtiles = 1;
-        nctas += (bigx + 255) / 256;
+        nctas += (bigx + 127) / 128;
       }
       DevBuf dc = upload(ctx, cbs), dp = upload(ctx, pairs);
       {
@@ -280,13 +280,28 @@ struct GemmPlan {
       c.mtiles = static_cast<int32_t>(mt);
       ntiles += mt * nt;
     }
+    // Split-K when the tiles fill less than ~3 waves of the 148 SMs and each
+    // tile has a long K loop (segments of >= 32 k-tiles).
+    int64_t kt_avg = 0;
+    for (auto& c : cbs) {
+      int64_t kt = 0;
+      for (int p = c.pair_begin; p < c.pair_end; ++p) kt += (pairs[p].K + 15) / 16;
+      kt_avg += kt * ((c.M + bm - 1) / bm) * ((c.N + bn - 1) / bn);
+    }
+    kt_avg = ntiles ? kt_avg / ntiles : 0;
+    int splitk = 1;
+    const int64_t wave = 148 * 4;
+    while (splitk < 16 && ntiles * splitk < 3 * wave && kt_avg / (2 * splitk) >= 32) splitk *= 2;
+    if (ctx->gemm_splitk > 0) splitk = ctx->gemm_splitk;
     DevBuf dc = upload(ctx, cbs), dp = upload(ctx, pairs);
+    DevBuf part;
+    if (splitk > 1) part = DevBuf(ctx, static_cast<size_t>(splitk) * ntiles * bm * bn * sizeof(double));
     {
       ProfScope ps(ctx, PROF_GEMM, flops, bytes);
       SB_CK(launch_gemm_f64(X, Y, C, dc.as<GemmCBlock>(), static_cast<int32_t>(cbs.size()), dp.as<GemmPair>(), ntiles,
-                            xT, yT, shape, ctx->stream));
+                            xT, yT, shape, ctx->stream, splitk, part.d()));
     }
-    ctx->note_launch();
+    ctx->note_launch(splitk > 1 ? 2 : 1);
   }
 };
 

@@ -51,7 +51,8 @@ struct TileLayout {
 template <int BM, int BN, int WM, int WN, bool XT, bool YT>
 __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
     k_gemm_f64(const double* __restrict__ X, const double* __restrict__ Y, double* __restrict__ C,
-               const GemmCBlock* __restrict__ cblocks, int32_t ncb, const GemmPair* __restrict__ pairs) {
+               const GemmCBlock* __restrict__ cblocks, int32_t ncb, const GemmPair* __restrict__ pairs,
+               int32_t splitk, int32_t ntiles, double* __restrict__ partial) {
   using TL = TileLayout<BM, BN, XT, YT>;
   constexpr int NWM = BM / WM;
   constexpr int NWN = BN / WN;
@@ -66,9 +67,12 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
   double* Xs = smem;                    // kStages tiles of TL::XSZ
   double* Ys = smem + kStages * TL::XSZ;  // kStages tiles of TL::YSZ
 
-  // C block of this CTA: last c with tile_begin <= blockIdx.x
+  // Split-K: CTA = (segment, tile), segments outermost so that concurrently
+  // running CTAs work on the same K range of neighbouring tiles.
+  const int seg = static_cast<int>(blockIdx.x) / ntiles;
+  const int bid = static_cast<int>(blockIdx.x) % ntiles;
+  // C block of this CTA: last c with tile_begin <= bid
   int lo = 0, hi = ncb - 1;
-  const int bid = static_cast<int>(blockIdx.x);
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
     if (cblocks[mid].tile_begin <= bid) lo = mid; else hi = mid - 1;
@@ -79,11 +83,19 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
   const int m0 = (lt % cb.mtiles) * BM, n0 = (lt / cb.mtiles) * BN;
   const int tid = threadIdx.x;
 
-  int total = 0;
-  for (int p = cb.pair_begin; p < cb.pair_end; ++p) total += (pairs[p].K + kBK - 1) / kBK;
+  int ktot = 0;
+  for (int p = cb.pair_begin; p < cb.pair_end; ++p) ktot += (pairs[p].K + kBK - 1) / kBK;
+  // this segment's range of the concatenated k-tiles
+  const int kb = static_cast<int>(static_cast<int64_t>(ktot) * seg / splitk);
+  const int ke = static_cast<int>(static_cast<int64_t>(ktot) * (seg + 1) / splitk);
+  const int total = ke - kb;
 
   int lp = cb.pair_begin;  // load cursor: pair index and k-tile within it
-  int lkt = 0;
+  int lkt = kb;
+  while (lp < cb.pair_end && lkt >= (pairs[lp].K + kBK - 1) / kBK) {
+    lkt -= (pairs[lp].K + kBK - 1) / kBK;
+    ++lp;
+  }
 
   auto issue_load = [&](int stage) {
     const GemmPair pr = pairs[lp];
@@ -153,6 +165,21 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
   }
   cp_async_wait<0>();
 
+  if (splitk > 1) {
+    // partial tile, column-major BM x BN, reduced by k_splitk_reduce
+    double* pt = partial + (static_cast<int64_t>(seg) * ntiles + bid) * (BM * BN);
+#pragma unroll
+    for (int a = 0; a < MT; ++a) {
+      const int rl = wm * WM + a * 8 + g;
+#pragma unroll
+      for (int b = 0; b < NTL; ++b) {
+        const int cl = wn * WN + b * 8 + 2 * t;
+        pt[rl + cl * BM] = acc[a][b][0];
+        pt[rl + (cl + 1) * BM] = acc[a][b][1];
+      }
+    }
+    return;
+  }
   double* cbase = C + cb.c_off;
 #pragma unroll
   for (int a = 0; a < MT; ++a) {
@@ -167,9 +194,34 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
   }
 }
 
+// Deterministic split-K reduction: C tile = sum over segments in order.
+template <int BM, int BN>
+__global__ void k_splitk_reduce(double* __restrict__ C, const GemmCBlock* __restrict__ cblocks, int32_t ncb,
+                                int32_t splitk, int32_t ntiles, const double* __restrict__ partial) {
+  const int64_t total = static_cast<int64_t>(ntiles) * BM * BN;
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int bid = static_cast<int>(e / (BM * BN));
+    const int w = static_cast<int>(e % (BM * BN));
+    const int rl = w % BM, cl = w / BM;
+    int lo = 0, hi = ncb - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (cblocks[mid].tile_begin <= bid) lo = mid; else hi = mid - 1;
+    }
+    const GemmCBlock cb = cblocks[lo];
+    const int lt = bid - cb.tile_begin;
+    const int row = (lt % cb.mtiles) * BM + rl, col = (lt / cb.mtiles) * BN + cl;
+    if (row >= cb.M || col >= cb.N) continue;
+    double acc = 0.0;
+    for (int sg = 0; sg < splitk; ++sg) acc += partial[(static_cast<int64_t>(sg) * ntiles + bid) * (BM * BN) + w];
+    C[cb.c_off + row + static_cast<int64_t>(col) * cb.M] = acc;
+  }
+}
+
 template <int BM, int BN, int WM, int WN, bool XT, bool YT>
 cudaError_t launch_t(const double* X, const double* Y, double* C, const GemmCBlock* cb, int32_t ncb,
-                     const GemmPair* pr, int64_t ntiles, cudaStream_t s) {
+                     const GemmPair* pr, int64_t ntiles, int splitk, double* partial, cudaStream_t s) {
   constexpr int threads = (BM / WM) * (BN / WN) * 32;
   constexpr int smem = TileLayout<BM, BN, XT, YT>::bytes();
   auto kern = k_gemm_f64<BM, BN, WM, WN, XT, YT>;
@@ -184,28 +236,58 @@ cudaError_t launch_t(const double* X, const double* Y, double* C, const GemmCBlo
     configured |= bit;
   }
   if (ntiles <= 0) return cudaSuccess;
-  if (ntiles > 0x7fffffffLL) return cudaErrorInvalidValue;
-  kern<<<static_cast<unsigned>(ntiles), threads, smem, s>>>(X, Y, C, cb, ncb, pr);
+  if (splitk < 1 || ntiles * splitk > 0x7fffffffLL || (splitk > 1 && !partial)) return cudaErrorInvalidValue;
+  kern<<<static_cast<unsigned>(ntiles * splitk), threads, smem, s>>>(X, Y, C, cb, ncb, pr, splitk,
+                                                                     static_cast<int32_t>(ntiles), partial);
+  e = cudaGetLastError();
+  if (e != cudaSuccess || splitk == 1) return e;
+  const int64_t elems = ntiles * BM * BN;
+  const unsigned g = static_cast<unsigned>(std::min<int64_t>((elems + 255) / 256, 148LL * 64));
+  k_splitk_reduce<BM, BN><<<g, 256, 0, s>>>(C, cb, ncb, splitk, static_cast<int32_t>(ntiles), partial);
   return cudaGetLastError();
 }
 
 template <int BM, int BN, int WM, int WN>
 cudaError_t dispatch_t(bool xT, bool yT, const double* X, const double* Y, double* C,
-                       const GemmCBlock* cb, int32_t ncb, const GemmPair* pr, int64_t nt, cudaStream_t s) {
-  if (!xT && !yT) return launch_t<BM, BN, WM, WN, false, false>(X, Y, C, cb, ncb, pr, nt, s);
-  if (!xT && yT) return launch_t<BM, BN, WM, WN, false, true>(X, Y, C, cb, ncb, pr, nt, s);
-  if (xT && !yT) return launch_t<BM, BN, WM, WN, true, false>(X, Y, C, cb, ncb, pr, nt, s);
-  return launch_t<BM, BN, WM, WN, true, true>(X, Y, C, cb, ncb, pr, nt, s);
+                       const GemmCBlock* cb, int32_t ncb, const GemmPair* pr, int64_t nt, int sk, double* part,
+                       cudaStream_t s) {
+  if (!xT && !yT) return launch_t<BM, BN, WM, WN, false, false>(X, Y, C, cb, ncb, pr, nt, sk, part, s);
+  if (!xT && yT) return launch_t<BM, BN, WM, WN, false, true>(X, Y, C, cb, ncb, pr, nt, sk, part, s);
+  if (xT && !yT) return launch_t<BM, BN, WM, WN, true, false>(X, Y, C, cb, ncb, pr, nt, sk, part, s);
+  return launch_t<BM, BN, WM, WN, true, true>(X, Y, C, cb, ncb, pr, nt, sk, part, s);
 }
 
-// ── skinny streaming GEMM (K <= 32, one of M/N <= 32) ─────────────────────
-constexpr int kSkinnyThreads = 256;
+// ── thin GEMM (K <= 16, one of M/N <= 16, the other long) ─────────────────
+// One CTA covers kThinBig elements of the long dimension of one C block; the
+// long operand tile (kThinBig x 16) and the small one (16 x 16) of each pair
+// are staged by cp.async with the next pair prefetched while DMMA runs on the
+// current one; the C tile goes through shared memory so that its stores are
+// fully coalesced (C columns of the long side, or the contiguous run of short
+// columns).
+constexpr int kThinBig = 128;
+constexpr int kThinThreads = 128;
+constexpr int kThinKP = 20;            // padded k-run / small-side stride
+constexpr int kThinBP = kThinBig + 4;  // padded long-side stride
 
-template <int SM, int KM, bool SMALL_ROWS, bool XT, bool YT>
-__global__ void __launch_bounds__(kSkinnyThreads)
-    k_gemm_skinny(const double* __restrict__ X, const double* __restrict__ Y, double* __restrict__ C,
-                  const GemmCBlock* __restrict__ cblocks, int32_t ncb, const GemmPair* __restrict__ pairs) {
-  __shared__ double small[32 * 33];
+template <bool SR, bool XT, bool YT>
+struct ThinLayout {
+  // long operand: X when !SR (rows), Y when SR (columns); small operand the other.
+  static constexpr bool LONG_KCONTIG = SR ? !YT : XT;  // long tile stored [l][k] when k is contiguous
+  static constexpr int LSZ = LONG_KCONTIG ? kThinBig * kThinKP : 16 * kThinBP;
+  static constexpr int SSZ = 16 * kThinKP;  // small tile [k][s]
+  __device__ static int lidx(int l, int k) { return LONG_KCONTIG ? l * kThinKP + k : k * kThinBP + l; }
+  __device__ static int sidx(int k, int s) { return k * kThinKP + s; }
+};
+
+template <bool SR, bool XT, bool YT>
+__global__ void __launch_bounds__(kThinThreads)
+    k_gemm_thin(const double* __restrict__ X, const double* __restrict__ Y, double* __restrict__ C,
+                const GemmCBlock* __restrict__ cblocks, int32_t ncb, const GemmPair* __restrict__ pairs) {
+  using TL = ThinLayout<SR, XT, YT>;
+  static_assert(2 * TL::LSZ >= kThinBig * 17, "C staging must fit in the long-operand buffers");
+  __shared__ double Ls[2][TL::LSZ];
+  __shared__ double Ss[2][TL::SSZ];
+  double* Cs = &Ls[0][0];  // reused for the C tile after the last pair
   int lo = 0, hi = ncb - 1;
   const int bid = static_cast<int>(blockIdx.x);
   while (lo < hi) {
@@ -214,76 +296,132 @@ __global__ void __launch_bounds__(kSkinnyThreads)
   }
   const GemmCBlock cb = cblocks[lo];
   const int M = cb.M, N = cb.N;
-  const int big = SMALL_ROWS ? N : M;
-  const int ns = SMALL_ROWS ? M : N;  // small extent (<= SM)
-  const int idx = (bid - cb.tile_begin) * kSkinnyThreads + static_cast<int>(threadIdx.x);
-  double acc[SM];
-#pragma unroll
-  for (int j = 0; j < SM; ++j) acc[j] = 0.0;
-  for (int p = cb.pair_begin; p < cb.pair_end; ++p) {
+  const int L = SR ? N : M;   // long extent
+  const int ns = SR ? M : N;  // short extent (<= 16)
+  const int l0 = (bid - cb.tile_begin) * kThinBig;
+  const int tid = threadIdx.x;
+
+  auto load = [&](int stage, int p) {
     const GemmPair pr = pairs[p];
     const int K = pr.K;
+    // long tile: kThinBig x 16
+#pragma unroll
+    for (int r = 0; r < kThinBig * 16 / kThinThreads; ++r) {
+      const int e = tid + r * kThinThreads;
+      int l, k;
+      if (TL::LONG_KCONTIG) { k = e % 16; l = e / 16; } else { l = e % kThinBig; k = e / kThinBig; }
+      const int gl = l0 + l;
+      const bool v = gl < L && k < K;
+      const double* src;
+      if (!SR) src = XT ? X + pr.x_off + k + (int64_t)gl * pr.ldx : X + pr.x_off + gl + (int64_t)k * pr.ldx;
+      else src = YT ? Y + pr.y_off + gl + (int64_t)k * pr.ldy : Y + pr.y_off + k + (int64_t)gl * pr.ldy;
+      cp_async8(&Ls[stage][TL::lidx(l, k)], v ? src : (SR ? Y : X), v);
+    }
+    // small tile: 16 x 16 as [k][s]
+#pragma unroll
+    for (int r = 0; r < 256 / kThinThreads; ++r) {
+      const int e = tid + r * kThinThreads;
+      const int k = e % 16, sI = e / 16;
+      const bool v = sI < ns && k < K;
+      const double* src;
+      if (!SR) src = YT ? Y + pr.y_off + sI + (int64_t)k * pr.ldy : Y + pr.y_off + k + (int64_t)sI * pr.ldy;
+      else src = XT ? X + pr.x_off + k + (int64_t)sI * pr.ldx : X + pr.x_off + sI + (int64_t)k * pr.ldx;
+      cp_async8(&Ss[stage][TL::sidx(k, sI)], v ? src : (SR ? X : Y), v);
+    }
+  };
+
+  const int warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;
+  // !SR: warp owns long rows [warp*32, +32) x 16 short columns: 4 x 2 m8n8 tiles
+  //  SR: warp owns long columns [warp*32, +32) x 16 short rows: 2 x 4 tiles
+  double acc[8][2];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) acc[a][0] = acc[a][1] = 0.0;
+
+  const int p0 = cb.pair_begin, p1 = cb.pair_end;
+  if (p0 < p1) load(0, p0);
+  cp_async_commit();
+  for (int p = p0; p < p1; ++p) {
+    const int st = (p - p0) & 1;
+    if (p + 1 < p1) load(st ^ 1, p + 1);
+    cp_async_commit();
+    cp_async_wait<1>();
     __syncthreads();
-    // stage the small operand as small[k * 33 + s]
-    for (int e = threadIdx.x; e < K * ns; e += kSkinnyThreads) {
-      const int k = e % K, sidx = e / K;
-      double v;
-      if (SMALL_ROWS)  // X(i = sidx, k)
-        v = XT ? X[pr.x_off + k + (int64_t)sidx * pr.ldx] : X[pr.x_off + sidx + (int64_t)k * pr.ldx];
-      else  // Y(k, j = sidx)
-        v = YT ? Y[pr.y_off + sidx + (int64_t)k * pr.ldy] : Y[pr.y_off + k + (int64_t)sidx * pr.ldy];
-      small[k * 33 + sidx] = v;
+    const double* ls = Ls[st];
+    const double* ss = Ss[st];
+#pragma unroll
+    for (int k4 = 0; k4 < 16; k4 += 4) {
+      if (!SR) {
+        double af[4], bf[2];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) af[a] = ls[TL::lidx(warp * 32 + a * 8 + g, k4 + t)];
+#pragma unroll
+        for (int b = 0; b < 2; ++b) bf[b] = ss[TL::sidx(k4 + t, b * 8 + g)];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 2; ++b) dmma_8x8x4(acc[a * 2 + b][0], acc[a * 2 + b][1], af[a], bf[b]);
+      } else {
+        double af[2], bf[4];
+#pragma unroll
+        for (int a = 0; a < 2; ++a) af[a] = ss[TL::sidx(k4 + t, a * 8 + g)];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) bf[b] = ls[TL::lidx(warp * 32 + b * 8 + g, k4 + t)];
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) dmma_8x8x4(acc[a * 4 + b][0], acc[a * 4 + b][1], af[a], bf[b]);
+      }
     }
     __syncthreads();
-    if (idx < big) {
-      // issue all K loads of this row/column before using them
-      double v[KM];
-#pragma unroll
-      for (int k = 0; k < KM; ++k) {
-        if (k < K) {
-          if (SMALL_ROWS)  // Y(k, j = idx)
-            v[k] = YT ? Y[pr.y_off + idx + (int64_t)k * pr.ldy] : Y[pr.y_off + k + (int64_t)idx * pr.ldy];
-          else  // X(i = idx, k)
-            v[k] = XT ? X[pr.x_off + k + (int64_t)idx * pr.ldx] : X[pr.x_off + idx + (int64_t)k * pr.ldx];
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < KM; ++k) {
-        if (k < K) {
-          const double* srow = small + k * 33;
-#pragma unroll
-          for (int j = 0; j < SM; ++j)
-            if (j < ns) acc[j] = fma(v[k], srow[j], acc[j]);
-        }
-      }
-    }
   }
-  if (idx >= big) return;
+  cp_async_wait<0>();
+  __syncthreads();
+  // stage C tile as Cs[l * 17 + s] (long index l, short index s)
+  if (!SR) {
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const int l = warp * 32 + a * 8 + g, s0 = b * 8 + 2 * t;
+        Cs[l * 17 + s0] = acc[a * 2 + b][0];
+        Cs[l * 17 + s0 + 1] = acc[a * 2 + b][1];
+      }
+  } else {
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int s = a * 8 + g, l0c = warp * 32 + b * 8 + 2 * t;
+        Cs[l0c * 17 + s] = acc[a * 4 + b][0];
+        Cs[(l0c + 1) * 17 + s] = acc[a * 4 + b][1];
+      }
+  }
+  __syncthreads();
   double* cbase = C + cb.c_off;
-#pragma unroll
-  for (int j = 0; j < SM; ++j) {
-    if (j >= ns) break;
-    if (SMALL_ROWS) cbase[j + (int64_t)idx * M] = acc[j];  // C(j, idx)
-    else cbase[idx + (int64_t)j * M] = acc[j];             // C(idx, j)
+  const int nl = min(kThinBig, L - l0);
+  if (!SR) {
+    // C(i = l0 + l, j = s) at i + j*M: coalesced along l for each s
+    for (int e = tid; e < nl * ns; e += kThinThreads) {
+      const int l = e % nl, s = e / nl;
+      cbase[(l0 + l) + (int64_t)s * M] = Cs[l * 17 + s];
+    }
+  } else {
+    // C(i = s, j = l0 + l) at s + (l0 + l)*M with M = ns: one contiguous run
+    double* run = cbase + (int64_t)l0 * M;
+    for (int e = tid; e < nl * ns; e += kThinThreads) run[e] = Cs[(e / ns) * 17 + (e % ns)];
   }
 }
 
-template <int SM, int KM, bool SR>
-cudaError_t skinny_t(bool xT, bool yT, const double* X, const double* Y, double* C, const GemmCBlock* cb, int32_t ncb,
-                     const GemmPair* pr, int64_t nctas, cudaStream_t s) {
+template <bool SR>
+cudaError_t thin_t(bool xT, bool yT, const double* X, const double* Y, double* C, const GemmCBlock* cb, int32_t ncb,
+                   const GemmPair* pr, int64_t nctas, cudaStream_t s) {
   const unsigned g = static_cast<unsigned>(nctas);
-  if (!xT && !yT) k_gemm_skinny<SM, KM, SR, false, false><<<g, kSkinnyThreads, 0, s>>>(X, Y, C, cb, ncb, pr);
-  else if (!xT && yT) k_gemm_skinny<SM, KM, SR, false, true><<<g, kSkinnyThreads, 0, s>>>(X, Y, C, cb, ncb, pr);
-  else if (xT && !yT) k_gemm_skinny<SM, KM, SR, true, false><<<g, kSkinnyThreads, 0, s>>>(X, Y, C, cb, ncb, pr);
-  else k_gemm_skinny<SM, KM, SR, true, true><<<g, kSkinnyThreads, 0, s>>>(X, Y, C, cb, ncb, pr);
+  if (!xT && !yT) k_gemm_thin<SR, false, false><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr);
+  else if (!xT && yT) k_gemm_thin<SR, false, true><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr);
+  else if (xT && !yT) k_gemm_thin<SR, true, false><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr);
+  else k_gemm_thin<SR, true, true><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr);
   return cudaGetLastError();
-}
-
-template <int SM, int KM>
-cudaError_t skinny_sr(bool sr, bool xT, bool yT, const double* X, const double* Y, double* C, const GemmCBlock* cb,
-                      int32_t ncb, const GemmPair* pr, int64_t nctas, cudaStream_t s) {
-  return sr ? skinny_t<SM, KM, true>(xT, yT, X, Y, C, cb, ncb, pr, nctas, s)
-            : skinny_t<SM, KM, false>(xT, yT, X, Y, C, cb, ncb, pr, nctas, s);
 }
 
 }  // namespace
@@ -302,28 +440,26 @@ cudaError_t launch_gemm_f64_skinny(const double* X, const double* Y, double* C, 
                                    int32_t ncb, const GemmPair* d_pairs, int64_t nctas, bool xT, bool yT,
                                    bool small_rows, int small_max, int k_max, cudaStream_t s) {
   if (nctas <= 0) return cudaSuccess;
-  if (nctas > 0x7fffffffLL || small_max > 32 || k_max > 32) return cudaErrorInvalidValue;
-  const bool s16 = small_max <= 16, k16 = k_max <= 16;
-  if (s16 && k16) return skinny_sr<16, 16>(small_rows, xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, s);
-  if (s16) return skinny_sr<16, 32>(small_rows, xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, s);
-  if (k16) return skinny_sr<32, 16>(small_rows, xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, s);
-  return skinny_sr<32, 32>(small_rows, xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, s);
+  if (nctas > 0x7fffffffLL || small_max > 16 || k_max > 16) return cudaErrorInvalidValue;
+  return small_rows ? thin_t<true>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, s)
+                    : thin_t<false>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, s);
 }
 
 cudaError_t launch_gemm_f64(const double* X, const double* Y, double* C,
                             const GemmCBlock* d_cblocks, int32_t ncb, const GemmPair* d_pairs,
-                            int64_t ntiles, bool xT, bool yT, GemmShape shape, cudaStream_t s) {
+                            int64_t ntiles, bool xT, bool yT, GemmShape shape, cudaStream_t s,
+                            int splitk, double* partial) {
   switch (shape) {
     case GemmShape::T128x32:
-      return dispatch_t<128, 32, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, s);
+      return dispatch_t<128, 32, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, splitk, partial, s);
     case GemmShape::T32x128:
-      return dispatch_t<32, 128, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, s);
+      return dispatch_t<32, 128, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, splitk, partial, s);
     case GemmShape::T128x64:
-      return dispatch_t<128, 64, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, s);
+      return dispatch_t<128, 64, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, splitk, partial, s);
     case GemmShape::T64x128:
-      return dispatch_t<64, 128, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, s);
+      return dispatch_t<64, 128, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, splitk, partial, s);
     default:
-      return dispatch_t<64, 64, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, s);
+      return dispatch_t<64, 64, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, splitk, partial, s);
   }
 }
 

@@ -76,6 +76,8 @@ struct Ctx {
   const char* kernel_name = "";
   // SPARSEB_GEMM_TILE=<BM>x<BN> forces one GEMM tile shape (tuning); -1 = auto.
   int gemm_tile = -1;
+  // SPARSEB_GEMM_SPLITK=<n> forces the split-K factor (tuning); 0 = auto.
+  int gemm_splitk = 0;
   // Pinned staging ring for host-to-device plan uploads: a copy from pinned
   // memory does not synchronise the stream, so host planning of the next
   // contraction overlaps the device work of the current one.  A slot is

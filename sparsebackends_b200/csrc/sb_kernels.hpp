@@ -33,15 +33,18 @@ struct GemmPair {
 
 enum class GemmShape : int { T64x64 = 0, T128x32 = 1, T32x128 = 2, T128x64 = 3, T64x128 = 4 };
 
+// splitk > 1: the concatenated K range of every C tile is cut into splitk
+// segments computed by separate CTAs into partial (splitk * ntiles * BM*BN
+// doubles), then summed in segment order by a second kernel (deterministic).
 cudaError_t launch_gemm_f64(const double* X, const double* Y, double* C,
                             const GemmCBlock* d_cblocks, int32_t ncblocks, const GemmPair* d_pairs,
-                            int64_t ntiles, bool xT, bool yT, GemmShape shape, cudaStream_t s);
+                            int64_t ntiles, bool xT, bool yT, GemmShape shape, cudaStream_t s,
+                            int splitk = 1, double* partial = nullptr);
 
-// Skinny variant (streaming, CUDA cores) for launches whose every pair has
-// K <= 32 and whose C blocks have min(M, N) <= 32: one thread per row (when
-// N is the small side) or per column (when M is), the small operand of each
-// pair staged in shared memory, partial sums over the pairs in registers.
-// CTAs of C block c: [tile_begin, tile_begin + ceil(big/256)) (mtiles unused).
+// Thin variant for launches whose every pair has K <= 16 and whose C blocks
+// have min(M, N) <= 16 (HBM-bound): DMMA on 128 x 16 tiles of the long side,
+// cp.async double buffering across pairs, shared-memory staged stores.
+// CTAs of C block c: [tile_begin, tile_begin + ceil(long/128)) (mtiles unused).
 cudaError_t launch_gemm_f64_skinny(const double* X, const double* Y, double* C,
                                    const GemmCBlock* d_cblocks, int32_t ncblocks, const GemmPair* d_pairs,
                                    int64_t nctas, bool xT, bool yT, bool small_rows, int small_max,

@@ -358,3 +358,16 @@ def test_random_skinny_streaming_gemm(sb, seed):
     for lC, dims in ((["i", "j", "m", "n"], (2, 2, 700, 11)), (["i", "j", "n", "m"], (2, 2, 11, 700))):
         Cg, Cref = run_both(sb, so.BS.empty(dims, 2), lC, A, lA, B, lB)
         assert_bs_equal(Cg, Cref)
+
+
+@pytest.mark.parametrize("seed", [61, 62])
+def test_random_splitk_gemm(sb, seed):
+    """Few output tiles with long reductions take the split-K path (partial
+    tiles summed in a fixed order by a second kernel)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    _, A = rand_bs(rng, (2, 3, 70, 1100), 2, density=1.0)
+    _, B = rand_bs(rng, (3, 2, 1100, 50), 2, density=1.0)
+    lA, lB = ["i", "q", "m", "k"], ["q", "j", "k", "n"]
+    for lC, dims in ((["i", "j", "m", "n"], (2, 2, 70, 50)), (["i", "j", "n", "m"], (2, 2, 50, 70))):
+        Cg, Cref = run_both(sb, so.BS.empty(dims, 2), lC, A, lA, B, lB)
+        assert_bs_equal(Cg, Cref)
