@@ -186,6 +186,50 @@ SB_API sb_status sb_to_dense(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out);
 /* to_blocksparse(::AliasedBlockSparse) (aliased/conversions.jl:18-32).       */
 SB_API sb_status sb_aliased_to_blocksparse(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out);
 
+/* ── vector-space operations (Krylov solvers) ────────────────────────────────
+ * The hooks KrylovKit's Lanczos needs from stored tensors
+ * (SparseBackends/src/tensor_wrappers.jl:793-923; aliased variants
+ * src/tensor_wrappers_aliased.jl:524-551).  All values stay on the device;
+ * sb_tensor_dot and sb_tensor_norm synchronise the context stream to return
+ * their scalar.  Reductions run in a fixed order (identical bits run to run). */
+
+/* Elementwise ops of map!(f, R, R, A): R[i] = f(R[i], A[i]) over the stored
+ * values by position (tensor_wrappers.jl:854-868), rounded as written.       */
+typedef enum {
+  SB_MAP_AXPY = 0,  /* r = r + alpha*a            */
+  SB_MAP_AXPBY = 1, /* r = beta*r + alpha*a       */
+  SB_MAP_COPY = 2,  /* r = a                      */
+  SB_MAP_MUL = 3    /* r = r*a                    */
+} sb_map_op;
+
+/* LinearAlgebra.norm(w) (tensor_wrappers.jl:796-799): 2-norm of the stored
+ * values; aliased: sqrt(sum_i sum_j (scalars[i]*template[alias_i][j])^2)
+ * (tensor_wrappers_aliased.jl:524-536).                                      */
+SB_API sb_status sb_tensor_norm(sb_ctx* ctx, const sb_tensor* A, double* out);
+/* dot(x, y) = (dag(x) * y)[]: the full contraction of contract_bs_bs_to_dense!
+ * with every label shared (ta/contract_bs_bs.jl:736-754) = sum over keys in
+ * both operands of the block dot products.  Block-sparse x block-sparse
+ * (uniform or ragged; equal extents per shared key) or dense x dense.        */
+SB_API sb_status sb_tensor_dot(sb_ctx* ctx, const sb_tensor* A, const sb_tensor* B, double* out);
+/* copy(w) (tensor_wrappers.jl:816-822): deep copy, any kind.                 */
+SB_API sb_status sb_tensor_copy(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out);
+/* similar(w) (tensor_wrappers.jl:897-918): same structure, zero values.      */
+SB_API sb_status sb_tensor_similar(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out);
+/* In-place scale, the value part of alpha * w (tensor_wrappers.jl:803-810):
+ * stored values (aliased: the per-block scalars) multiplied by alpha.        */
+SB_API sb_status sb_tensor_scale(sb_ctx* ctx, sb_tensor* A, double alpha);
+/* fill!(w, x) (tensor_wrappers.jl:848-851): every stored value set to x
+ * (block-sparse, COO, dense).                                                */
+SB_API sb_status sb_tensor_fill(sb_ctx* ctx, sb_tensor* A, double x);
+/* map!(f, R, R, A) for f in sb_map_op (tensor_wrappers.jl:854-868,
+ * tensor_wrappers_aliased.jl:538-551 on the scalars).  Same kind and the same
+ * number of stored values, else SB_ERR_DIM_MISMATCH ("Mismatched sparsity
+ * patterns").                                                                */
+SB_API sb_status sb_tensor_map(sb_ctx* ctx, sb_tensor* R, const sb_tensor* A, int op, double alpha, double beta);
+/* x + y (tensor_wrappers.jl:825-838): union of block keys; a key in both gets
+ * a + b.  Block-sparse + block-sparse (uniform or ragged) or dense + dense.  */
+SB_API sb_status sb_tensor_add(sb_ctx* ctx, const sb_tensor* A, const sb_tensor* B, sb_tensor** out);
+
 /* ── allocation-free grouped block GEMM ──────────────────────────────────────
  * No counterpart in the reference: an extra entry point of this library.
  *

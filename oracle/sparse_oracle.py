@@ -1675,3 +1675,78 @@ def contract_bs_bs_to_dense(dimsC, labelsC, A: BS, labelsA, B: BS, labelsB) -> n
         blk = Cbs.block(Cbs.ids[0])
         out = blk.reshape(dimsC, order="F").copy() if NC else np.array(blk[0])
     return out
+
+
+# ── vector-space hooks used by Krylov solvers (src/tensor_wrappers.jl:793-923) ──
+
+def bs_norm(A: BS) -> float:
+    """``norm(w) = norm(w.blocksparse.data)`` (tensor_wrappers.jl:796)."""
+    return float(np.linalg.norm(A.data))
+
+
+def bs_scale(alpha: float, A: BS) -> BS:
+    """``alpha * w``: same keys and ids, ``T(alpha) .* data`` (tensor_wrappers.jl:803-810)."""
+    return BS(A.dims, A.n2, list(A.keys), list(A.ids), float(alpha) * A.data)
+
+
+def bs_copy(A: BS) -> BS:
+    """``copy(w)`` (tensor_wrappers.jl:816-822)."""
+    return BS(A.dims, A.n2, list(A.keys), list(A.ids), A.data.copy())
+
+
+def bs_add(A: BS, B: BS) -> BS:
+    """``wA + wB`` (tensor_wrappers.jl:825-838): C = copy(A); for each B block,
+    ``_ensure_block!`` in C (new blocks start at zero) and ``c[i] += b[i]``."""
+    _assert(A.dims == B.dims and A.n2 == B.n2, "dims differ")
+    Cb = bs_copy(A)
+    for k, ib in zip(B.keys, B.ids):
+        ic = Cb.ensure_block(k)
+        blk = Cb.block(ic)
+        blk += B.block(ib)
+    return Cb
+
+
+def bs_fill(A: BS, x: float) -> BS:
+    """``fill!(storage.blocksparse.data, x)`` (tensor_wrappers.jl:848-851)."""
+    for s in A._slots:
+        s[:] = x
+    return A
+
+
+def map_values(op: str, r: np.ndarray, a: np.ndarray, alpha: float = 1.0, beta: float = 1.0) -> np.ndarray:
+    """``_apply_elementwise!(f, R, A)`` (tensor_wrappers.jl:854-868): f over the
+    stored values by position; lengths must agree.  ``op`` names the f."""
+    if len(r) != len(a):
+        raise ValueError("Mismatched sparsity patterns in _external_map!")
+    if op == "axpy":
+        return r + alpha * a
+    if op == "axpby":
+        return beta * r + alpha * a
+    if op == "copy":
+        return a.copy()
+    if op == "mul":
+        return r * a
+    raise ValueError(op)
+
+
+def bs_dot(A: BS, B: BS) -> float:
+    """``dot(x, y) = (dag(x) * y)[]`` for real block-sparse tensors: the full
+    contraction (contract_bs_bs_to_dense!, contract_bs_bs.jl:736-754, every
+    label shared) = sum over keys present in both of the block dot products."""
+    _assert(A.dims == B.dims and A.n2 == B.n2, "dims differ")
+    bb = B.blocks_by_key()
+    s = 0.0
+    for k, ia in zip(A.keys, A.ids):
+        if k in bb:
+            s += float(np.dot(A.block(ia), bb[k]))
+    return s
+
+
+def aliased_norm(A: "Aliased") -> float:
+    """``norm`` of an aliased tensor (tensor_wrappers_aliased.jl:524-536):
+    sqrt(sum_i sum_j abs2(scalars[i] * templates[alias_ids[i]][j]))."""
+    s = 0.0
+    for i in range(len(A.keys)):
+        t = A.template(A.alias_ids[i])
+        s += float(np.sum((A.scalars[i] * t) ** 2))
+    return float(np.sqrt(s))

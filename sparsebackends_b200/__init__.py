@@ -40,7 +40,8 @@ __all__ = [
     "SparseBackendsError", "Context", "default_context", "DenseTensor", "NewBlockSparseSorted", "COOTensor",
     "AliasedBlockSparse", "contract_", "contract_bs_bs_to_dense", "blocksparse_from_dense", "coo_from_dense",
     "to_dense", "to_blocksparse", "permutedims", "sort_", "compression_ratio", "output_inds", "label_key",
-    "to_uniform", "to_ragged",
+    "to_uniform", "to_ragged", "norm", "dot", "inner", "copy", "similar", "scale_", "fill_", "map_", "axpy_",
+    "axpby_", "add", "MAP_AXPY", "MAP_AXPBY", "MAP_COPY", "MAP_MUL",
 ]
 
 
@@ -113,7 +114,7 @@ class Context:
     def launch_count(self) -> int:
         return int(self._lib.sb_ctx_launch_count(self._h))
 
-    PROFILE_KINDS = {"gemm": 0, "permute": 1, "outer": 2, "axpy": 3, "other": 4}
+    PROFILE_KINDS = {"gemm": 0, "permute": 1, "outer": 2, "axpy": 3, "other": 4, "vector": 5}
 
     def set_profiling(self, enable: bool) -> None:
         """Time every kernel launch with CUDA events on the context stream."""
@@ -184,6 +185,26 @@ class _Tensor:
         p, n = C.c_void_p(), C.c_int64()
         _check(self.ctx, self.ctx._lib.sb_tensor_device_data(self._h, C.byref(p), C.byref(n)))
         return p.value or 0, n.value
+
+    # vector-space hooks (src/tensor_wrappers.jl:793-923): alpha*x, -x, x/alpha, x+y, x-y
+    def __rmul__(self, alpha: float) -> "_Tensor":
+        out = copy(self)
+        return scale_(out, alpha)
+
+    def __mul__(self, alpha: float) -> "_Tensor":
+        return self.__rmul__(alpha)
+
+    def __neg__(self) -> "_Tensor":
+        return (-1.0) * self
+
+    def __truediv__(self, alpha: float) -> "_Tensor":
+        return (1.0 / alpha) * self
+
+    def __add__(self, other: "_Tensor") -> "_Tensor":
+        return add(self, other)
+
+    def __sub__(self, other: "_Tensor") -> "_Tensor":
+        return add(self, (-1.0) * other)
 
 
 class DenseTensor(_Tensor):
@@ -471,6 +492,81 @@ def _as_operand(x, ctx: Context) -> _Tensor:
     if isinstance(x, _Tensor):
         return x
     return DenseTensor(np.asarray(x, dtype=np.float64), ctx)
+
+
+# ── vector-space operations (KrylovKit hooks, src/tensor_wrappers.jl:793-923) ──
+
+MAP_AXPY, MAP_AXPBY, MAP_COPY, MAP_MUL = 0, 1, 2, 3
+
+
+def norm(A: _Tensor) -> float:
+    """``LinearAlgebra.norm(w)``: 2-norm of the stored values (aliased: of the
+    logical blocks, tensor_wrappers_aliased.jl:524-536)."""
+    out = C.c_double()
+    _check(A.ctx, A.ctx._lib.sb_tensor_norm(A.ctx._h, A._h, C.byref(out)))
+    return out.value
+
+
+def dot(A: _Tensor, B: _Tensor) -> float:
+    """``dot(x, y) = (dag(x) * y)[]`` for real tensors: the sum over keys in
+    both operands of the block dot products (contract_bs_bs_to_dense! with every
+    label shared)."""
+    out = C.c_double()
+    _check(A.ctx, A.ctx._lib.sb_tensor_dot(A.ctx._h, A._h, B._h, C.byref(out)))
+    return out.value
+
+
+inner = dot
+
+
+def copy(A: _Tensor) -> _Tensor:
+    """``copy(w)``: deep copy on the device."""
+    h = C.c_void_p()
+    _check(A.ctx, A.ctx._lib.sb_tensor_copy(A.ctx._h, A._h, C.byref(h)))
+    return _from_handle(A.ctx, h)
+
+
+def similar(A: _Tensor) -> _Tensor:
+    """``similar(w)``: same keys and layout, zero values."""
+    h = C.c_void_p()
+    _check(A.ctx, A.ctx._lib.sb_tensor_similar(A.ctx._h, A._h, C.byref(h)))
+    return _from_handle(A.ctx, h)
+
+
+def scale_(A: _Tensor, alpha: float) -> _Tensor:
+    """In place: stored values (aliased: scalars) times ``alpha``."""
+    _check(A.ctx, A.ctx._lib.sb_tensor_scale(A.ctx._h, A._h, float(alpha)))
+    return A
+
+
+def fill_(A: _Tensor, x: float) -> _Tensor:
+    """``fill!(w, x)`` on the stored values."""
+    _check(A.ctx, A.ctx._lib.sb_tensor_fill(A.ctx._h, A._h, float(x)))
+    return A
+
+
+def map_(R: _Tensor, A: _Tensor, op: int, alpha: float = 1.0, beta: float = 1.0) -> _Tensor:
+    """``map!(f, R, R, A)`` by stored position for f in MAP_AXPY (r + alpha*a),
+    MAP_AXPBY (beta*r + alpha*a), MAP_COPY (a), MAP_MUL (r*a)."""
+    _check(R.ctx, R.ctx._lib.sb_tensor_map(R.ctx._h, R._h, A._h, int(op), float(alpha), float(beta)))
+    return R
+
+
+def axpy_(alpha: float, x: _Tensor, y: _Tensor) -> _Tensor:
+    """``y .= y .+ alpha .* x`` (same sparsity pattern)."""
+    return map_(y, x, MAP_AXPY, alpha)
+
+
+def axpby_(alpha: float, x: _Tensor, beta: float, y: _Tensor) -> _Tensor:
+    """``y .= beta .* y .+ alpha .* x`` (same sparsity pattern)."""
+    return map_(y, x, MAP_AXPBY, alpha, beta)
+
+
+def add(A: _Tensor, B: _Tensor) -> _Tensor:
+    """``x + y``: union of the block keys; shared keys add."""
+    h = C.c_void_p()
+    _check(A.ctx, A.ctx._lib.sb_tensor_add(A.ctx._h, A._h, B._h, C.byref(h)))
+    return _from_handle(A.ctx, h)
 
 
 def contract_(C_: _Tensor, labelsC: Sequence[Any], A, labelsA: Sequence[Any], B, labelsB: Sequence[Any]) -> _Tensor:

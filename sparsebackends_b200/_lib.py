@@ -56,6 +56,14 @@ SIGNATURES = {
     "sb_coo_from_dense": (C.c_int, [vp, vp, C.c_double, C.c_double, C.POINTER(vp)]),
     "sb_to_dense": (C.c_int, [vp, vp, C.POINTER(vp)]),
     "sb_aliased_to_blocksparse": (C.c_int, [vp, vp, C.POINTER(vp)]),
+    "sb_tensor_norm": (C.c_int, [vp, vp, P_f64]),
+    "sb_tensor_dot": (C.c_int, [vp, vp, vp, P_f64]),
+    "sb_tensor_copy": (C.c_int, [vp, vp, C.POINTER(vp)]),
+    "sb_tensor_similar": (C.c_int, [vp, vp, C.POINTER(vp)]),
+    "sb_tensor_scale": (C.c_int, [vp, vp, C.c_double]),
+    "sb_tensor_fill": (C.c_int, [vp, vp, C.c_double]),
+    "sb_tensor_map": (C.c_int, [vp, vp, vp, C.c_int, C.c_double, C.c_double]),
+    "sb_tensor_add": (C.c_int, [vp, vp, vp, C.POINTER(vp)]),
     "sb_block_gemm_f64_noalloc": (C.c_int, [vp, vp, vp, vp, C.c_int32, P_i64, C.POINTER(C.c_int32),
                                             C.POINTER(C.c_int32), C.POINTER(C.c_int32), P_i64, P_i64,
                                             C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),

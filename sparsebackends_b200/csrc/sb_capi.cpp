@@ -104,6 +104,7 @@ sb_status sb_ctx_create(int device, unsigned flags, sb_ctx** out) {
       else if (v == "128x64") c->impl.gemm_tile = 3;
       else if (v == "64x128") c->impl.gemm_tile = 4;
     }
+    if (const char* th = std::getenv("SPARSEB_GEMM_THIN")) c->impl.gemm_thin = std::atoi(th);
     if (const char* sk = std::getenv("SPARSEB_GEMM_SPLITK")) c->impl.gemm_splitk = std::max(0, std::atoi(sk));
     // Keep freed device memory cached in the stream-ordered pool.
     cudaMemPool_t pool;
@@ -610,6 +611,88 @@ sb_status sb_aliased_to_blocksparse(sb_ctx* ctx, const sb_tensor* A, sb_tensor**
     require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
     SB_CK(cudaSetDevice(ctx->impl.device));
     *out = wrap(ctx, aliased_to_bs(&ctx->impl, *A->impl));
+  });
+}
+
+// ── vector-space operations ────────────────────────────────────────────────
+
+sb_status sb_tensor_norm(sb_ctx* ctx, const sb_tensor* A, double* out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    *out = tensor_norm(&ctx->impl, *A->impl);
+  });
+}
+
+sb_status sb_tensor_dot(sb_ctx* ctx, const sb_tensor* A, const sb_tensor* B, double* out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    check_t(B);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    *out = tensor_dot(&ctx->impl, *A->impl, *B->impl);
+  });
+}
+
+sb_status sb_tensor_copy(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    *out = wrap(ctx, copy_tensor(&ctx->impl, *A->impl));
+  });
+}
+
+sb_status sb_tensor_similar(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    *out = wrap(ctx, tensor_similar(&ctx->impl, *A->impl));
+  });
+}
+
+sb_status sb_tensor_scale(sb_ctx* ctx, sb_tensor* A, double alpha) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    tensor_scale(&ctx->impl, *A->impl, alpha);
+  });
+}
+
+sb_status sb_tensor_fill(sb_ctx* ctx, sb_tensor* A, double x) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    tensor_fill(&ctx->impl, *A->impl, x);
+  });
+}
+
+sb_status sb_tensor_map(sb_ctx* ctx, sb_tensor* R, const sb_tensor* A, int op, double alpha, double beta) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(R);
+    check_t(A);
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    tensor_map(&ctx->impl, *R->impl, *A->impl, op, alpha, beta);
+  });
+}
+
+sb_status sb_tensor_add(sb_ctx* ctx, const sb_tensor* A, const sb_tensor* B, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    check_t(B);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    *out = wrap(ctx, tensor_add(&ctx->impl, *A->impl, *B->impl));
   });
 }
 

@@ -96,9 +96,12 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
     lkt -= (pairs[lp].K + kBK - 1) / kBK;
     ++lp;
   }
+  // descriptor of the pair being loaded, kept in registers; the next one is
+  // fetched when the cursor moves on, a k-tile before it is needed
+  GemmPair pr{};
+  if (lp < cb.pair_end) pr = pairs[lp];
 
   auto issue_load = [&](int stage) {
-    const GemmPair pr = pairs[lp];
     const int k0 = lkt * kBK;
     const double* xb = X + pr.x_off;
     const double* yb = Y + pr.y_off;
@@ -124,7 +127,10 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
       const double* src = v ? (YT ? yb + gj + (int64_t)gk * pr.ldy : yb + gk + (int64_t)gj * pr.ldy) : yb;
       cp_async8(ys + TL::yidx(k, j), src, v);
     }
-    if (++lkt * kBK >= pr.K) { lkt = 0; ++lp; }
+    if (++lkt * kBK >= pr.K) {
+      lkt = 0;
+      if (++lp < cb.pair_end) pr = pairs[lp];
+    }
   };
 
   const int warp = tid >> 5, lane = tid & 31;

@@ -53,7 +53,9 @@ class DevBuf {
 };
 
 // Kernel classes reported by the in-library profiler.
-enum ProfKind : int { PROF_GEMM = 0, PROF_PERMUTE = 1, PROF_OUTER = 2, PROF_AXPY = 3, PROF_OTHER = 4, PROF_NKINDS = 5 };
+enum ProfKind : int {
+  PROF_GEMM = 0, PROF_PERMUTE = 1, PROF_OUTER = 2, PROF_AXPY = 3, PROF_OTHER = 4, PROF_VECTOR = 5, PROF_NKINDS = 6
+};
 
 struct Ctx {
   int device = 0;
@@ -78,6 +80,9 @@ struct Ctx {
   int gemm_tile = -1;
   // SPARSEB_GEMM_SPLITK=<n> forces the split-K factor (tuning); 0 = auto.
   int gemm_splitk = 0;
+  // SPARSEB_GEMM_THIN=0 keeps K<=16 launches on the tiled kernel (tuning);
+  // -1 = auto (the thin kernel for every launch it can serve).
+  int gemm_thin = -1;
   // Pinned staging ring for host-to-device plan uploads: a copy from pinned
   // memory does not synchronise the stream, so host planning of the next
   // contraction overlaps the device work of the current one.  A slot is
@@ -217,6 +222,15 @@ void copy_blocks(Ctx* ctx, const double* src, double* dst, const std::vector<int
 void require_uniform(const Tensor& t, const char* what);
 void check_no_cross_perm(const std::vector<int>& perm1, int N, int P);
 bool is_identity(const std::vector<int>& perm1);
+
+// ── vector-space operations (sb_vector.cpp) ──────────────────────────────
+double tensor_dot(Ctx* ctx, const Tensor& A, const Tensor& B);
+double tensor_norm(Ctx* ctx, const Tensor& A);
+void tensor_scale(Ctx* ctx, Tensor& A, double alpha);
+void tensor_fill(Ctx* ctx, Tensor& A, double x);
+void tensor_map(Ctx* ctx, Tensor& R, const Tensor& A, int op, double alpha, double beta);
+TensorPtr tensor_similar(Ctx* ctx, const Tensor& A);
+TensorPtr tensor_add(Ctx* ctx, const Tensor& A, const Tensor& B);
 
 // ── contraction (sb_contract.cpp) ────────────────────────────────────────
 struct Label {

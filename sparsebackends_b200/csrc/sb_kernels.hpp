@@ -31,6 +31,9 @@ struct GemmPair {
   int32_t K, ldx, ldy, pad;
 };
 
+// CTA tile shapes, all with 32x32 warp tiles.  (Measured on the H_eff steps:
+// 32x64 / 64x32 warp tiles need 190-250 registers, halve the resident CTAs and
+// run 4-16% slower.)
 enum class GemmShape : int { T64x64 = 0, T128x32 = 1, T32x128 = 2, T128x64 = 3, T64x128 = 4 };
 
 // splitk > 1: the concatenated K range of every C tile is cut into splitk
@@ -155,6 +158,30 @@ cudaError_t launch_scale_blocks(const double* src, const int64_t* d_tmpl_off,
 // dense[lin_b + stride*t] = data[b*blk + t]
 cudaError_t launch_blocks_to_strided(const double* data, const int64_t* d_lin, int64_t nblocks,
                                      int64_t blk, int64_t stride, double* dense, cudaStream_t s);
+
+// ── vector-space operations (Krylov solvers) ───────────────────────────────
+// Dot product over chunks of at most kDotChunk elements: *d_out = sum over
+// chunks of sum_t (s*X[x_off+t]) * (s*Y[y_off+t]) with s = S[s_idx] (s = 1
+// when s_idx < 0); d_partial holds nchunks doubles.  Fixed reduction order:
+// identical bits on every call.
+constexpr int kDotChunk = 4096;
+struct DotChunk {
+  int64_t x_off, y_off;
+  int64_t s_idx;
+  int32_t len, pad;
+};
+cudaError_t launch_dot_chunks(const double* X, const double* Y, const double* S, const DotChunk* d_chunks,
+                              int64_t nchunks, double* d_partial, double* d_out, cudaStream_t s);
+// Elementwise R[i] = f(R[i], A[i]) for i < n.
+enum MapOp : int { kMapAxpy = 0, kMapAxpby = 1, kMapCopy = 2, kMapMul = 3, kMapScale = 4, kMapFill = 5 };
+cudaError_t launch_map(double* R, const double* A, int64_t n, int op, double alpha, double beta, cudaStream_t s);
+// Key-union add: C[c_off + e] = A-block, 0 + B-block, or A-block + B-block
+// (a_off / b_off < 0 marks a missing operand block).
+struct AddBlock {
+  int64_t a_off, b_off, c_off, len;
+};
+cudaError_t launch_add_blocks(const double* A, const double* B, double* C, const AddBlock* d_items, int64_t n,
+                              int64_t max_len, cudaStream_t s);
 
 // ── scalar programs (aliased bookkeeping) ──────────────────────────────────
 // out[g] = sum_{e in seg g} (sa[ia_e] * (ib_e >= 0 ? sb[ib_e] : 1)), left to right.

@@ -217,6 +217,66 @@ def pad_ragged(layout: HeffLayout, name: str, keys, data, exts):
     return out
 
 
+def _channel_conj(layout: HeffLayout, qw: int) -> int:
+    """1-based sector index of the conjugate MPO channel sector (charge -c)."""
+    w = layout.mpo
+    return w.index(-w.charges[qw - 1]) + 1
+
+
+def hermitian_operators(layout: HeffLayout, rng: np.random.Generator, scales=None):
+    """Seeded L, W1, W2, R (ragged host triples (keys, data, block_dims)) for
+    which the two-site H_eff is a real symmetric operator.
+
+    With the channel involution w -> w' (charge c -> -c, same index inside the
+    sector) it suffices that L[a', w, a] = L[a, w', a'], R likewise and
+    W[wl, s', s, wr] = W[wl', s, s', wr']: substituting w -> w' in the sum over
+    channels then swaps bra and ket.  Each operator is the average of a random
+    one and its transpose under that map; the charge rules map allowed keys to
+    allowed keys.  Requires a charge-symmetric MPO link."""
+    w = layout.mpo
+    for q, dq in zip(w.charges, w.dims):
+        if -q not in w.charges or w.dims[w.index(-q)] != dq:
+            raise ValueError("hermitian_operators needs an MPO link symmetric under c -> -c")
+    scales = scales or {"L": 0.05, "W1": 0.3, "W2": 0.3, "R": 0.05}
+    out = {}
+    for name in ("L", "W1", "W2", "R"):
+        keys, data, exts = random_block_tensor(layout, name, rng, scales[name], ragged=True)
+        blocks, off = {}, 0
+        for k, e in zip(keys, exts):
+            n = int(np.prod(e))
+            blocks[k] = data[off: off + n].reshape(e, order="F")
+            off += n
+        sym = []
+        for k, e in zip(keys, exts):
+            if name in ("L", "R"):
+                kt = (k[2], _channel_conj(layout, k[1]), k[0])
+                bt = np.transpose(blocks[kt], (2, 1, 0))
+            else:
+                kt = (_channel_conj(layout, k[0]), k[2], k[1], _channel_conj(layout, k[3]))
+                bt = blocks[kt]
+            sym.append((0.5 * (blocks[k] + bt)).reshape(-1, order="F"))
+        out[name] = (keys, np.concatenate(sym) if sym else np.zeros(0), exts)
+    return out
+
+
+class HeffOperator:
+    """x -> H_eff x as a new device tensor (the operator KrylovKit's eigsolve
+    applies: ITensorMPS ``product(::ProjMPO, v)``).  Operands stay resident;
+    each call runs the four-contraction chain and copies the result out of the
+    chain's reused output buffer."""
+
+    def __init__(self, layout: HeffLayout, L, W1, W2, R, ctx=None):
+        import sparsebackends_b200 as sb
+        self.sb = sb
+        self.chain = HeffChain(layout, ctx)
+        self.ops = (L, W1, W2, R)
+        self.calls = 0
+
+    def __call__(self, psi):
+        self.calls += 1
+        return self.sb.copy(self.chain.apply(psi, *self.ops))
+
+
 class HeffChain:
     """Two-site H_eff · ψ through four ``contract!`` calls on the device.
 
