@@ -230,6 +230,34 @@ SB_API sb_status sb_tensor_map(sb_ctx* ctx, sb_tensor* R, const sb_tensor* A, in
  * a + b.  Block-sparse + block-sparse (uniform or ragged) or dense + dense.  */
 SB_API sb_status sb_tensor_add(sb_ctx* ctx, const sb_tensor* A, const sb_tensor* B, sb_tensor** out);
 
+/* ── block factorisations (src/ops_factorize.jl) ─────────────────────────────
+ * Values on the device (Householder QR; batched one-sided Jacobi SVD); index
+ * bookkeeping and the truncation decision on the host, as in the reference.  */
+
+/* blocksparse_left_qr(A) (ops_factorize.jl:8-43) for A with prefix (l, r) and
+ * dense tail (s) (N = 3, n_tail = 1, uniform).  M[(li-1)*d_s + s, ri] =
+ * A[l_vals[li], r_vals[ri]][s] over the sorted distinct l and r values of the
+ * keys; thin QR M = Q R, k = min(n_l*d_s, n_r), Householder reflectors with
+ * LAPACK's sign convention.  *Q: block-sparse, dims (dims[0], d_s, k), prefix
+ * (l), one block per l value (d_s x k); *R: dense k x n_r.  l_vals (capacity
+ * dims[0]) and r_vals (capacity dims[1]) receive the distinct values when not
+ * NULL; their counts go to *n_l and *n_r.                                    */
+SB_API sb_status sb_blocksparse_left_qr(sb_ctx* ctx, const sb_tensor* A, sb_tensor** Q, sb_tensor** R,
+                                        int64_t* l_vals, int64_t* n_l, int64_t* r_vals, int64_t* n_r);
+/* blocksparse_svd(A; ortho, maxdim, mindim, cutoff) (ops_factorize.jl:50-148)
+ * for A with prefix (L, R) and dense tail (s1, s2) (N = 4, n_tail = 2,
+ * uniform, s1 <= 32).  One SVD per L group of d_s1 x (n_R(L)*d_s2), global
+ * truncation: keep min(maxdim, total), then drop the smallest while the count
+ * is above mindim and sv < cutoff * max sv.  *U: dims (dims[0], new_bond,
+ * d_s1), prefix (L, b); *SV: dims (new_bond, dims[1], d_s2), prefix (b, R);
+ * the singular values go to U when ortho_right, to SV otherwise.  svs gets
+ * the kept singular values in bond order (min(capacity, *n_kept) of them;
+ * dims[0]*d_s1 always suffices); *truncerr = sum of the dropped sv^2 (the
+ * Spectrum of the reference is (svs.^2, truncerr)).                          */
+SB_API sb_status sb_blocksparse_svd(sb_ctx* ctx, const sb_tensor* A, int ortho_right, int64_t maxdim,
+                                    int64_t mindim, double cutoff, sb_tensor** U, sb_tensor** SV, double* svs,
+                                    int64_t svs_capacity, int64_t* n_kept, double* truncerr);
+
 /* ── allocation-free grouped block GEMM ──────────────────────────────────────
  * No counterpart in the reference: an extra entry point of this library.
  *

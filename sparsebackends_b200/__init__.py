@@ -41,7 +41,7 @@ __all__ = [
     "AliasedBlockSparse", "contract_", "contract_bs_bs_to_dense", "blocksparse_from_dense", "coo_from_dense",
     "to_dense", "to_blocksparse", "permutedims", "sort_", "compression_ratio", "output_inds", "label_key",
     "to_uniform", "to_ragged", "norm", "dot", "inner", "copy", "similar", "scale_", "fill_", "map_", "axpy_",
-    "axpby_", "add", "MAP_AXPY", "MAP_AXPBY", "MAP_COPY", "MAP_MUL",
+    "axpby_", "add", "MAP_AXPY", "MAP_AXPBY", "MAP_COPY", "MAP_MUL", "blocksparse_left_qr", "blocksparse_svd",
 ]
 
 
@@ -567,6 +567,44 @@ def add(A: _Tensor, B: _Tensor) -> _Tensor:
     h = C.c_void_p()
     _check(A.ctx, A.ctx._lib.sb_tensor_add(A.ctx._h, A._h, B._h, C.byref(h)))
     return _from_handle(A.ctx, h)
+
+
+# ── block factorisations (src/ops_factorize.jl) ────────────────────────────
+
+def blocksparse_left_qr(A: NewBlockSparseSorted):
+    """``blocksparse_left_qr(A)`` (ops_factorize.jl:8-43) for A with prefix
+    (l, r) and dense tail (s).  Returns (Q, R, l_vals, r_vals): Q block-sparse
+    (l | s, b), R a DenseTensor k x n_r, the sorted distinct l and r values."""
+    ctx = A.ctx
+    dims = A.dims
+    q, r = C.c_void_p(), C.c_void_p()
+    lv = (C.c_int64 * max(dims[0], 1))()
+    rv = (C.c_int64 * max(dims[1], 1))()
+    nl, nr = C.c_int64(), C.c_int64()
+    _check(ctx, ctx._lib.sb_blocksparse_left_qr(ctx._h, A._h, C.byref(q), C.byref(r), lv, C.byref(nl), rv,
+                                                C.byref(nr)))
+    return (_from_handle(ctx, q), _from_handle(ctx, r), [lv[i] for i in range(nl.value)],
+            [rv[i] for i in range(nr.value)])
+
+
+def blocksparse_svd(A: NewBlockSparseSorted, ortho: str = "left", maxdim: int = 2 ** 62, mindim: int = 1,
+                    cutoff: float = 0.0):
+    """``blocksparse_svd(A; ortho, maxdim, mindim, cutoff)`` (ops_factorize.jl:50-148)
+    for A with prefix (L, R) and dense tail (s1, s2).  Returns
+    (U, SV, svs_kept, spectrum) with spectrum = {"eigs": svs^2, "truncerr": ...}."""
+    if ortho not in ("left", "right"):
+        raise ValueError("ortho must be 'left' or 'right'")
+    ctx = A.ctx
+    dims = A.dims
+    cap = max(dims[0] * dims[2], 1)
+    u, sv = C.c_void_p(), C.c_void_p()
+    svs = np.zeros(cap)
+    nk, te = C.c_int64(), C.c_double()
+    _check(ctx, ctx._lib.sb_blocksparse_svd(ctx._h, A._h, int(ortho == "right"), int(maxdim), int(mindim),
+                                            float(cutoff), C.byref(u), C.byref(sv), _f64ptr(svs), cap,
+                                            C.byref(nk), C.byref(te)))
+    kept = svs[: nk.value].copy()
+    return _from_handle(ctx, u), _from_handle(ctx, sv), kept, {"eigs": kept ** 2, "truncerr": te.value}
 
 
 def contract_(C_: _Tensor, labelsC: Sequence[Any], A, labelsA: Sequence[Any], B, labelsB: Sequence[Any]) -> _Tensor:

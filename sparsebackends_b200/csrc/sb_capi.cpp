@@ -696,4 +696,41 @@ sb_status sb_tensor_add(sb_ctx* ctx, const sb_tensor* A, const sb_tensor* B, sb_
   });
 }
 
+// ── block factorisations ───────────────────────────────────────────────────
+
+sb_status sb_blocksparse_left_qr(sb_ctx* ctx, const sb_tensor* A, sb_tensor** Q, sb_tensor** R, int64_t* l_vals,
+                                 int64_t* n_l, int64_t* r_vals, int64_t* n_r) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    require(Q != nullptr && R != nullptr, SB_ERR_INVALID_ARG, "Q/R out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    QrResult r = blocksparse_left_qr(&ctx->impl, *A->impl);
+    if (l_vals) std::copy(r.l_vals.begin(), r.l_vals.end(), l_vals);
+    if (r_vals) std::copy(r.r_vals.begin(), r.r_vals.end(), r_vals);
+    if (n_l) *n_l = static_cast<int64_t>(r.l_vals.size());
+    if (n_r) *n_r = static_cast<int64_t>(r.r_vals.size());
+    *Q = wrap(ctx, std::move(r.Q));
+    *R = wrap(ctx, std::move(r.R));
+  });
+}
+
+sb_status sb_blocksparse_svd(sb_ctx* ctx, const sb_tensor* A, int ortho_right, int64_t maxdim, int64_t mindim,
+                             double cutoff, sb_tensor** U, sb_tensor** SV, double* svs, int64_t svs_capacity,
+                             int64_t* n_kept, double* truncerr) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    require(U != nullptr && SV != nullptr, SB_ERR_INVALID_ARG, "U/SV out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    SvdResult r = blocksparse_svd(&ctx->impl, *A->impl, ortho_right != 0, maxdim, mindim, cutoff);
+    const int64_t nk = static_cast<int64_t>(r.svs.size());
+    if (svs) std::copy(r.svs.begin(), r.svs.begin() + std::min(nk, std::max<int64_t>(svs_capacity, 0)), svs);
+    if (n_kept) *n_kept = nk;
+    if (truncerr) *truncerr = r.truncerr;
+    *U = wrap(ctx, std::move(r.U));
+    *SV = wrap(ctx, std::move(r.SV));
+  });
+}
+
 }  // extern "C"

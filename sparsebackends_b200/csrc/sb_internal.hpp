@@ -232,6 +232,20 @@ void tensor_map(Ctx* ctx, Tensor& R, const Tensor& A, int op, double alpha, doub
 TensorPtr tensor_similar(Ctx* ctx, const Tensor& A);
 TensorPtr tensor_add(Ctx* ctx, const Tensor& A, const Tensor& B);
 
+// ── block factorisations (sb_factorize.cpp) ──────────────────────────────
+struct QrResult {
+  TensorPtr Q, R;
+  std::vector<int64_t> l_vals, r_vals;
+};
+struct SvdResult {
+  TensorPtr U, SV;
+  std::vector<double> svs;
+  double truncerr = 0.0;
+};
+QrResult blocksparse_left_qr(Ctx* ctx, const Tensor& A);
+SvdResult blocksparse_svd(Ctx* ctx, const Tensor& A, bool ortho_right, int64_t maxdim, int64_t mindim,
+                          double cutoff);
+
 // ── contraction (sb_contract.cpp) ────────────────────────────────────────
 struct Label {
   uint64_t id, plev;

@@ -183,6 +183,38 @@ struct AddBlock {
 cudaError_t launch_add_blocks(const double* A, const double* B, double* C, const AddBlock* d_items, int64_t n,
                               int64_t max_len, cudaStream_t s);
 
+// ── block factorisations (QR, SVD truncation) ──────────────────────────────
+// In-place Householder QR of the column-major m x n matrix M (LAPACK dlarfg
+// convention): R in the upper triangle, reflector j below the diagonal of
+// column j with scale tau[j]; *launches counts the kernels issued.
+cudaError_t launch_householder_qr(double* M, int64_t m, int64_t n, double* tau, cudaStream_t s, int64_t* launches);
+// Thin Q (m x k, column-major) from the reflectors in M.
+cudaError_t launch_householder_form_q(const double* M, int64_t m, int64_t k, const double* tau, double* Q,
+                                      cudaStream_t s, int64_t* launches);
+// R (k x n, column-major) = upper triangle of the first k rows of M.
+cudaError_t launch_upper(const double* M, int64_t m, int64_t k, int64_t n, double* R, cudaStream_t s);
+// Strided 2-D copies: dst[dst_off + r*dst_rs + c*dst_cs] = src[src_off + r*src_rs + c*src_cs]
+// (times scale[s_idx] when s_idx >= 0) for r < rows, c < cols.
+struct Gather2D {
+  int64_t src_off, dst_off, rows, cols, src_rs, src_cs, dst_rs, dst_cs, s_idx;
+};
+cudaError_t launch_gather_2d(const double* src, double* dst, const double* scale, const Gather2D* d_items, int64_t n,
+                             int64_t max_elems, cudaStream_t s);
+// One-sided Jacobi SVD of row-major m x n matrices (m <= kSvdMaxRows) at
+// A + a_off: on return Vt + a_off holds the right singular vectors as rows,
+// U + u_off the left ones (column-major m x m) and S + s_off the m singular
+// values, all sorted by decreasing singular value.  A is overwritten.
+// *d_status is set to 1 when some matrix has not converged in max_sweeps.
+constexpr int kSvdMaxRows = 32;
+struct SvdGroup {
+  int64_t a_off;
+  int64_t n;
+  int64_t u_off, s_off;
+  int32_t m, pad;
+};
+cudaError_t launch_svd_rows(double* A, double* Vt, double* U, double* S, const SvdGroup* d_groups, int64_t ngroups,
+                            int max_sweeps, int* d_status, cudaStream_t s);
+
 // ── scalar programs (aliased bookkeeping) ──────────────────────────────────
 // out[g] = sum_{e in seg g} (sa[ia_e] * (ib_e >= 0 ? sb[ib_e] : 1)), left to right.
 struct ScalarTerm {
