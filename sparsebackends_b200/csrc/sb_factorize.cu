@@ -119,7 +119,17 @@ __global__ void __launch_bounds__(kFacThreads)
   double* a = A + g.a_off;
   for (int e = threadIdx.x; e < m * m; e += kFacThreads) Us[e] = (e % m == e / m) ? 1.0 : 0.0;
   __syncthreads();
+  // Rotation threshold |gamma| > tol * sqrt(alpha * beta) with tol = n * eps,
+  // the rounding bound of the length-n dot products: below it the rows are
+  // orthogonal to working accuracy.  (A tighter threshold makes rank-deficient
+  // groups rotate rounding-level rows forever.)
   const double eps = 2.220446049250313e-16;
+  const double tol = eps * static_cast<double>(n > 1 ? n : 1);
+  // Rows with norm below eps * ||A||_F are rounding noise: they take part in
+  // no rotation (rotating them against each other never settles).
+  double fro = 0.0;
+  for (int64_t i = threadIdx.x; i < static_cast<int64_t>(m) * n; i += kFacThreads) fro = __fma_rn(a[i], a[i], fro);
+  const double tiny = eps * eps * block_sum(fro, red);
   bool rotated = true;
   int sweep = 0;
   for (; sweep < max_sweeps && rotated; ++sweep) {
@@ -138,10 +148,11 @@ __global__ void __launch_bounds__(kFacThreads)
         const double alpha = block_sum(sa, red);
         const double beta = block_sum(sb2, red);
         const double gamma = block_sum(sc, red);
-        if (gamma == 0.0 || fabs(gamma) <= eps * sqrt(alpha * beta)) continue;  // uniform across the CTA
+        // uniform across the CTA (reduced values)
+        if (alpha <= tiny || beta <= tiny || gamma == 0.0 || fabs(gamma) <= tol * sqrt(alpha) * sqrt(beta)) continue;
         rotated = true;
         const double zeta = (beta - alpha) / (2.0 * gamma);
-        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + hypot(1.0, zeta));
         const double cs = 1.0 / sqrt(1.0 + t * t);
         const double sn = cs * t;
         for (int64_t i = threadIdx.x; i < n; i += kFacThreads) {
