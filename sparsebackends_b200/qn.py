@@ -109,8 +109,10 @@ class HeffLayout:
             "T2": ["qlp", "qr", "s1p", "qwm", "s2", "mr", "mlp", "mwm"],
             "T3": ["qlp", "s1p", "s2p", "qwr", "qr", "mwr", "mr", "mlp"],
             "T4": ["qlp", "s1p", "s2p", "qrp", "mlp", "mrp"],
+            # one-site MPS tensor (environment updates)
+            "A": ["ql", "s1", "qr", "ml", "mr"],
         }
-        n2 = {"psi": 2, "L": 3, "W1": 2, "W2": 2, "R": 3, "T1": 3, "T2": 3, "T3": 3, "T4": 2}
+        n2 = {"psi": 2, "L": 3, "W1": 2, "W2": 2, "R": 3, "T1": 3, "T2": 3, "T3": 3, "T4": 2, "A": 2}
         self.labels = lab
         self.n2 = n2
         self.dims = {k: tuple(ext[x] for x in v) for k, v in lab.items()}
@@ -121,6 +123,7 @@ class HeffLayout:
             "W1": self._mpo_keys(),
             "W2": self._mpo_keys(),
             "R": self._env_keys(r),
+            "A": self._site_keys(),
         }
 
     # ψ(ql, s1, s2, qr): Q(ql) + σ1 + σ2 = Q(qr)
@@ -129,6 +132,14 @@ class HeffLayout:
         for ql, s1, s2, qr in itertools.product(range(self.left.S), range(self.d), range(self.d), range(self.right.S)):
             if self.left.charges[ql] + PHYS[s1] + PHYS[s2] == self.right.charges[qr]:
                 out.append((ql + 1, s1 + 1, s2 + 1, qr + 1))
+        return out
+
+    # A(ql, s, qr): Q(ql) + σ = Q(qr)
+    def _site_keys(self):
+        out = []
+        for ql, s, qr in itertools.product(range(self.left.S), range(self.d), range(self.right.S)):
+            if self.left.charges[ql] + PHYS[s] == self.right.charges[qr]:
+                out.append((ql + 1, s + 1, qr + 1))
         return out
 
     # L(q', qw, q) / R(q', qw, q): Q(q') - Q(q) = c(qw)
@@ -275,6 +286,47 @@ class HeffOperator:
     def __call__(self, psi):
         self.calls += 1
         return self.sb.copy(self.chain.apply(psi, *self.ops))
+
+
+def contract_new(labelsC, n2C, A, labelsA, B, labelsB):
+    """``contract!`` into a freshly allocated block-sparse C whose dims follow
+    from the operands' dims by label (the caller's allocation in
+    tensor_wrappers.jl:654)."""
+    import sparsebackends_b200 as sb
+    ext = dict(zip(labelsA, A.dims))
+    ext.update(zip(labelsB, B.dims))
+    C = sb.NewBlockSparseSorted.empty(tuple(ext[x] for x in labelsC), n2C, ctx=A.ctx)
+    return sb.contract_(C, labelsC, A, labelsA, B, labelsB)
+
+
+def make_L(L, A, W):
+    """Left environment update, ITensorMPS ``makeL!``: L' = L · A · W · Ā.
+
+    L'[(qr', mr'), (qw', mw'), (qr, mr)] = sum L[(ql', ml'), (qw, mw), (ql, ml)]
+    A[(ql, ml), s, (qr, mr)] W[(qw, mw), s', s, (qw', mw')] A[(ql', ml'), s', (qr', mr')]
+    as three ``contract!`` calls on the device (real tensors: Ā = A).  The
+    result has the layout of the environments (labels q', qw, q | m', mw, m)."""
+    E1 = contract_new(["qlp", "qwl", "s1", "qr", "mr", "mlp", "mwl"], 3,
+                      L, ["qlp", "qwl", "ql", "mlp", "mwl", "ml"], A, ["ql", "s1", "qr", "ml", "mr"])
+    E2 = contract_new(["qlp", "qr", "s1p", "qwm", "mr", "mlp", "mwm"], 3,
+                      E1, ["qlp", "qwl", "s1", "qr", "mr", "mlp", "mwl"], W,
+                      ["qwl", "s1p", "s1", "qwm", "mwl", "mwm"])
+    return contract_new(["qrp", "qwm", "qr", "mrp", "mwm", "mr"], 3,
+                        E2, ["qlp", "qr", "s1p", "qwm", "mr", "mlp", "mwm"], A, ["qlp", "s1p", "qrp", "mlp", "mrp"])
+
+
+def make_R(R, B, W):
+    """Right environment update, ITensorMPS ``makeR!``: R' = R · B · W · B̄.
+
+    R'[(ql', ml'), (qw, mw), (ql, ml)] = sum R[(qr', mr'), (qw', mw'), (qr, mr)]
+    B[(ql, ml), s, (qr, mr)] W[(qw, mw), s', s, (qw', mw')] B[(ql', ml'), s', (qr', mr')]."""
+    F1 = contract_new(["qrp", "qwm", "ql", "s1", "ml", "mrp", "mwm"], 3,
+                      R, ["qrp", "qwm", "qr", "mrp", "mwm", "mr"], B, ["ql", "s1", "qr", "ml", "mr"])
+    F2 = contract_new(["qrp", "ql", "s1p", "qwl", "ml", "mrp", "mwl"], 3,
+                      F1, ["qrp", "qwm", "ql", "s1", "ml", "mrp", "mwm"], W,
+                      ["qwl", "s1p", "s1", "qwm", "mwl", "mwm"])
+    return contract_new(["qlp", "qwl", "ql", "mlp", "mwl", "ml"], 3,
+                        F2, ["qrp", "ql", "s1p", "qwl", "ml", "mrp", "mwl"], B, ["qlp", "s1p", "qrp", "mlp", "mrp"])
 
 
 class HeffChain:
