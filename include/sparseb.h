@@ -230,6 +230,15 @@ SB_API sb_status sb_tensor_map(sb_ctx* ctx, sb_tensor* R, const sb_tensor* A, in
  * a + b.  Block-sparse + block-sparse (uniform or ragged) or dense + dense.  */
 SB_API sb_status sb_tensor_add(sb_ctx* ctx, const sb_tensor* A, const sb_tensor* B, sb_tensor** out);
 
+/* Axis fusion, axes 1-based.  Block-sparse: fuse_two_axes!
+ * (src/blocksparse/conversions.jl:228-314): two prefix axes a1 < a2 fold into
+ * a1 with key (k[a2]-1)*d[a1] + k[a1] (keys re-sorted); two tail axes fold
+ * after moving the later one next to the earlier one (uniform tensors only);
+ * mixed prefix/tail is SB_ERR_INVALID_ARG.  COO: fuse_axes_coo
+ * (src/coo/conversions.jl:174-222): adjacent axes only (else
+ * SB_ERR_ASSERTION), ax1 kept as the fast index, result sorted.              */
+SB_API sb_status sb_fuse_axes(sb_ctx* ctx, const sb_tensor* A, int ax1, int ax2, sb_tensor** out);
+
 /* ── block factorisations (src/ops_factorize.jl) ─────────────────────────────
  * Values on the device (Householder QR; batched one-sided Jacobi SVD); index
  * bookkeeping and the truncation decision on the host, as in the reference.  */

@@ -1750,3 +1750,59 @@ def aliased_norm(A: "Aliased") -> float:
         t = A.template(A.alias_ids[i])
         s += float(np.sum((A.scalars[i] * t) ** 2))
     return float(np.sqrt(s))
+
+
+# ── axis fusion (link fusion after MPO x MPO) ─────────────────────────────────
+
+def fuse_two_axes(A: BS, ax1: int, ax2: int) -> BS:
+    """``fuse_two_axes!`` (src/blocksparse/conversions.jl:228-314), axes 1-based.
+
+    Prefix pair: fused key (k[a2]-1)*d[a1] + k[a1] at a1, a2 dropped, blocks and
+    key order kept as in the reference (fuse_sparse_axes does not re-sort).
+    Tail pair: move the later tail axis right after the earlier one (stable),
+    then fold the two adjacent axes."""
+    N, P = A.N, A.P
+    if not (1 <= ax1 <= N and 1 <= ax2 <= N) or ax1 == ax2:
+        raise ValueError("axes must be distinct and in 1:N")
+    s1, s2 = ax1 <= P, ax2 <= P
+    if s1 != s2:
+        raise ValueError("Cannot fuse across sparse-head and dense-tail axes")
+    a1, a2 = min(ax1, ax2), max(ax1, ax2)
+    if s1:
+        d1, d2 = A.dims[a1 - 1], A.dims[a2 - 1]
+        nd = tuple(d1 * d2 if i == a1 else A.dims[i - 1] for i in range(1, N + 1) if i != a2)
+        keys = []
+        for k in A.keys:
+            f = (k[a2 - 1] - 1) * d1 + k[a1 - 1]
+            keys.append(tuple(f if j == a1 else k[j - 1] for j in range(1, P + 1) if j != a2))
+        out = BS(nd, A.n2)
+        out.keys, out.ids, out._slots = keys, list(A.ids), [s.copy() for s in A._slots]
+        return out
+    p1, p2 = a1 - P, a2 - P
+    B = A
+    if p2 != p1 + 1:
+        pb = list(range(1, A.n2 + 1))
+        x = pb.pop(p2 - 1)
+        pb.insert(p1, x)
+        B = bs_permutedims(A, list(range(1, P + 1)) + [P + q for q in pb])
+    nd = tuple(B.dims[a1 - 1] * B.dims[a1] if i == a1 else B.dims[i - 1] for i in range(1, N + 1) if i != a1 + 1)
+    out = BS(nd, A.n2 - 1)
+    out.keys, out.ids, out._slots = list(B.keys), list(B.ids), [s.copy() for s in B._slots]
+    return out
+
+
+def fuse_axes_coo(A: "COO", ax1: int, ax2: int) -> "COO":
+    """``fuse_axes_coo`` (src/coo/conversions.jl:174-222): adjacent axes, ax1
+    kept as the fast index at ax1 - (ax2 < ax1); the result is sorted."""
+    N = len(A.dims)
+    if ax1 == ax2 or not (1 <= ax1 <= N and 1 <= ax2 <= N):
+        raise ValueError("axes must be distinct and in 1:N")
+    _assert(abs(ax1 - ax2) == 1, "Currently only adjacent axes can be fused")
+    dkeep, ddrop = A.dims[ax1 - 1], A.dims[ax2 - 1]
+    out_ax = ax1 - (1 if ax2 < ax1 else 0)
+    old = lambda j: j if j < ax2 else j + 1  # noqa: E731
+    nd = tuple(dkeep * ddrop if j == out_ax else A.dims[old(j) - 1] for j in range(1, N))
+    keys = [tuple((c[ax2 - 1] - 1) * dkeep + c[ax1 - 1] if j == out_ax else c[old(j) - 1] for j in range(1, N))
+            for c in A.keys]
+    C = COO(nd, keys, list(A.vals), True)
+    return coo_sort(C)

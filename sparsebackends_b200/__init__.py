@@ -42,6 +42,7 @@ __all__ = [
     "to_dense", "to_blocksparse", "permutedims", "sort_", "compression_ratio", "output_inds", "label_key",
     "to_uniform", "to_ragged", "norm", "dot", "inner", "copy", "similar", "scale_", "fill_", "map_", "axpy_",
     "axpby_", "add", "MAP_AXPY", "MAP_AXPBY", "MAP_COPY", "MAP_MUL", "blocksparse_left_qr", "blocksparse_svd",
+    "fuse_axes",
 ]
 
 
@@ -566,6 +567,14 @@ def add(A: _Tensor, B: _Tensor) -> _Tensor:
     """``x + y``: union of the block keys; shared keys add."""
     h = C.c_void_p()
     _check(A.ctx, A.ctx._lib.sb_tensor_add(A.ctx._h, A._h, B._h, C.byref(h)))
+    return _from_handle(A.ctx, h)
+
+
+def fuse_axes(A: _Tensor, ax1: int, ax2: int) -> _Tensor:
+    """``fuse_two_axes!`` (block-sparse, conversions.jl:228-314) or
+    ``fuse_axes_coo`` (COO, coo/conversions.jl:174-222); axes 1-based."""
+    h = C.c_void_p()
+    _check(A.ctx, A.ctx._lib.sb_fuse_axes(A.ctx._h, A._h, int(ax1), int(ax2), C.byref(h)))
     return _from_handle(A.ctx, h)
 
 

@@ -64,6 +64,7 @@ SIGNATURES = {
     "sb_tensor_fill": (C.c_int, [vp, vp, C.c_double]),
     "sb_tensor_map": (C.c_int, [vp, vp, vp, C.c_int, C.c_double, C.c_double]),
     "sb_tensor_add": (C.c_int, [vp, vp, vp, C.POINTER(vp)]),
+    "sb_fuse_axes": (C.c_int, [vp, vp, C.c_int, C.c_int, C.POINTER(vp)]),
     "sb_blocksparse_left_qr": (C.c_int, [vp, vp, C.POINTER(vp), C.POINTER(vp), P_i64, P_i64, P_i64, P_i64]),
     "sb_blocksparse_svd": (C.c_int, [vp, vp, C.c_int, i64, i64, C.c_double, C.POINTER(vp), C.POINTER(vp), P_f64,
                                      i64, P_i64, P_f64]),

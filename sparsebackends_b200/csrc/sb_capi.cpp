@@ -733,4 +733,16 @@ sb_status sb_blocksparse_svd(sb_ctx* ctx, const sb_tensor* A, int ortho_right, i
   });
 }
 
+sb_status sb_fuse_axes(sb_ctx* ctx, const sb_tensor* A, int ax1, int ax2, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    const Tensor& x = *A->impl;
+    require(x.kind == BS || x.kind == COO, SB_ERR_UNSUPPORTED_TYPES, "fuse: block-sparse or COO tensor expected");
+    *out = wrap(ctx, x.kind == BS ? bs_fuse_axes(&ctx->impl, x, ax1, ax2) : coo_fuse_axes(&ctx->impl, x, ax1, ax2));
+  });
+}
+
 }  // extern "C"

@@ -232,6 +232,10 @@ void tensor_map(Ctx* ctx, Tensor& R, const Tensor& A, int op, double alpha, doub
 TensorPtr tensor_similar(Ctx* ctx, const Tensor& A);
 TensorPtr tensor_add(Ctx* ctx, const Tensor& A, const Tensor& B);
 
+// ── axis fusion (sb_fuse.cpp); axes 1-based ──────────────────────────────
+TensorPtr bs_fuse_axes(Ctx* ctx, const Tensor& A, int ax1, int ax2);
+TensorPtr coo_fuse_axes(Ctx* ctx, const Tensor& A, int ax1, int ax2);
+
 // ── block factorisations (sb_factorize.cpp) ──────────────────────────────
 struct QrResult {
   TensorPtr Q, R;
