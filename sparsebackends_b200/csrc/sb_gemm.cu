@@ -31,29 +31,31 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
       : "d"(a), "d"(b));
 }
 
-constexpr int kStages = 3;
-constexpr int kBK = 16;
-constexpr int kKP = kBK + 4;  // padded k-run length of k-contiguous tiles
+constexpr int kBK = 16;       // default k-tile
+constexpr int kStages = 3;    // default pipeline depth
 
-// Shared-memory layout of one operand tile: the dimension that is contiguous
-// in global memory stays contiguous in shared memory (conflict-free cp.async
-// writes); the padding (rows of BM+4 or BK+4 doubles) makes the DMMA fragment
-// reads conflict-free as well.
-template <int BM, int BN, bool XT, bool YT>
+// Shared-memory layout of one operand tile (BK-deep, ST pipeline stages): the
+// dimension that is contiguous in global memory stays contiguous in shared
+// memory (conflict-free cp.async writes); the padding (rows of BM+4 or BK+4
+// doubles) makes the DMMA fragment reads conflict-free within each half-warp.
+template <int BM, int BN, bool XT, bool YT, int BK = kBK, int ST = kStages>
 struct TileLayout {
-  static constexpr int XSZ = XT ? BM * kKP : kBK * (BM + 4);  // X: [i][k] if XT else [k][i]
-  static constexpr int YSZ = YT ? kBK * (BN + 4) : BN * kKP;  // Y: [k][j] if YT else [j][k]
-  static constexpr int bytes() { return kStages * (XSZ + YSZ) * 8; }
-  __device__ static int xidx(int i, int k) { return XT ? i * kKP + k : k * (BM + 4) + i; }
-  __device__ static int yidx(int k, int j) { return YT ? k * (BN + 4) + j : j * kKP + k; }
+  static constexpr int KP = BK + 4;  // padded k-run length of k-contiguous tiles
+  static constexpr int XSZ = XT ? BM * KP : BK * (BM + 4);  // X: [i][k] if XT else [k][i]
+  static constexpr int YSZ = YT ? BK * (BN + 4) : BN * KP;  // Y: [k][j] if YT else [j][k]
+  static constexpr int bytes() { return ST * (XSZ + YSZ) * 8; }
+  __device__ static int xidx(int i, int k) { return XT ? i * KP + k : k * (BM + 4) + i; }
+  __device__ static int yidx(int k, int j) { return YT ? k * (BN + 4) + j : j * KP + k; }
 };
 
-template <int BM, int BN, int WM, int WN, bool XT, bool YT>
+template <int BM, int BN, int WM, int WN, bool XT, bool YT, int BK = kBK, int ST = kStages>
 __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
     k_gemm_f64(const double* __restrict__ X, const double* __restrict__ Y, double* __restrict__ C,
                const GemmCBlock* __restrict__ cblocks, int32_t ncb, const GemmPair* __restrict__ pairs,
                int32_t splitk, int32_t ntiles, double* __restrict__ partial) {
-  using TL = TileLayout<BM, BN, XT, YT>;
+  constexpr int kBK = BK;
+  constexpr int kStages = ST;
+  using TL = TileLayout<BM, BN, XT, YT, BK, ST>;
   constexpr int NWM = BM / WM;
   constexpr int NWN = BN / WN;
   constexpr int NT = NWM * NWN * 32;
@@ -225,12 +227,12 @@ __global__ void k_splitk_reduce(double* __restrict__ C, const GemmCBlock* __rest
   }
 }
 
-template <int BM, int BN, int WM, int WN, bool XT, bool YT>
+template <int BM, int BN, int WM, int WN, bool XT, bool YT, int BK = kBK, int ST = kStages>
 cudaError_t launch_t(const double* X, const double* Y, double* C, const GemmCBlock* cb, int32_t ncb,
                      const GemmPair* pr, int64_t ntiles, int splitk, double* partial, cudaStream_t s) {
   constexpr int threads = (BM / WM) * (BN / WN) * 32;
-  constexpr int smem = TileLayout<BM, BN, XT, YT>::bytes();
-  auto kern = k_gemm_f64<BM, BN, WM, WN, XT, YT>;
+  constexpr int smem = TileLayout<BM, BN, XT, YT, BK, ST>::bytes();
+  auto kern = k_gemm_f64<BM, BN, WM, WN, XT, YT, BK, ST>;
   static unsigned long long configured = 0;  // one bit per device ordinal
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -253,14 +255,14 @@ cudaError_t launch_t(const double* X, const double* Y, double* C, const GemmCBlo
   return cudaGetLastError();
 }
 
-template <int BM, int BN, int WM, int WN>
+template <int BM, int BN, int WM, int WN, int BK = kBK, int ST = kStages>
 cudaError_t dispatch_t(bool xT, bool yT, const double* X, const double* Y, double* C,
                        const GemmCBlock* cb, int32_t ncb, const GemmPair* pr, int64_t nt, int sk, double* part,
                        cudaStream_t s) {
-  if (!xT && !yT) return launch_t<BM, BN, WM, WN, false, false>(X, Y, C, cb, ncb, pr, nt, sk, part, s);
-  if (!xT && yT) return launch_t<BM, BN, WM, WN, false, true>(X, Y, C, cb, ncb, pr, nt, sk, part, s);
-  if (xT && !yT) return launch_t<BM, BN, WM, WN, true, false>(X, Y, C, cb, ncb, pr, nt, sk, part, s);
-  return launch_t<BM, BN, WM, WN, true, true>(X, Y, C, cb, ncb, pr, nt, sk, part, s);
+  if (!xT && !yT) return launch_t<BM, BN, WM, WN, false, false, BK, ST>(X, Y, C, cb, ncb, pr, nt, sk, part, s);
+  if (!xT && yT) return launch_t<BM, BN, WM, WN, false, true, BK, ST>(X, Y, C, cb, ncb, pr, nt, sk, part, s);
+  if (xT && !yT) return launch_t<BM, BN, WM, WN, true, false, BK, ST>(X, Y, C, cb, ncb, pr, nt, sk, part, s);
+  return launch_t<BM, BN, WM, WN, true, true, BK, ST>(X, Y, C, cb, ncb, pr, nt, sk, part, s);
 }
 
 // ── thin GEMM (K <= 16, one of M/N <= 16, the other long) ─────────────────

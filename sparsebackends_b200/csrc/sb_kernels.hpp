@@ -31,9 +31,10 @@ struct GemmPair {
   int32_t K, ldx, ldy, pad;
 };
 
-// CTA tile shapes, all with 32x32 warp tiles.  (Measured on the H_eff steps:
-// 32x64 / 64x32 warp tiles need 190-250 registers, halve the resident CTAs and
-// run 4-16% slower.)
+// CTA tile shapes, all with 32x32 warp tiles, k-tile 16, 3 stages.  Measured
+// on the H_eff steps (64x64 tiles, chi = 2048): 32x64 / 64x32 warp tiles need
+// 190-250 registers, halve the resident CTAs and run 4-16% slower; 4 stages,
+// k-tile 32 (2 or 3 stages) and eight 32x16 warps run 0-18% slower.
 enum class GemmShape : int { T64x64 = 0, T128x32 = 1, T32x128 = 2, T128x64 = 3, T64x128 = 4 };
 
 // splitk > 1: the concatenated K range of every C tile is cut into splitk
