@@ -193,13 +193,21 @@ def dist_setup(args):
 
 
 def reduce_max(x: float, world: int) -> float:
+    """Max over ranks (device time of the slowest replica)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_rate(world: int, steps: int, ms_max: float) -> float:
+    """Whole-job matvec/s of `world` independent replicas that each ran
+    `steps` matvecs, timed by the slowest one (ms_max)."""
+    return world * steps / (ms_max / 1e3)
 
 
 def barrier(world: int):
@@ -297,10 +305,10 @@ def run_ours(args, world, rank, local):
     time.sleep(0.3)
     ms, launches, prof = timed(apply_r, args.steps, profile=True)
     clocks = sampler.stop()
-    value = world * args.steps / (ms / 1e3)
+    value = replica_rate(world, args.steps, ms)
     # uniform (reference layout) for comparison
     ms_u, _, prof_u = timed(apply_u, args.steps, profile=True)
-    value_u = world * args.steps / (ms_u / 1e3)
+    value_u = replica_rate(world, args.steps, ms_u)
 
     # ── end to end through the public API (pinned host psi in, H·psi out) ──
     lib = ctx._lib
@@ -344,8 +352,8 @@ def run_ours(args, world, rank, local):
         e2e_u()
     ms_e2e, _, _ = timed(e2e_r, args.steps)
     ms_e2e_u, _, _ = timed(e2e_u, args.steps)
-    e2e_value = world * args.steps / (ms_e2e / 1e3)
-    e2e_value_u = world * args.steps / (ms_e2e_u / 1e3)
+    e2e_value = replica_rate(world, args.steps, ms_e2e)
+    e2e_value_u = replica_rate(world, args.steps, ms_e2e_u)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
