@@ -132,6 +132,13 @@ SB_API sb_status sb_tensor_info(const sb_tensor* t, int* kind, int* nd, int64_t*
  * ids = 1:n in that order, data packed accordingly.  Any pointer may be NULL. */
 SB_API sb_status sb_tensor_export_bs(sb_ctx* ctx, const sb_tensor* t, int64_t* keys, int64_t* ids,
                               double* data);
+/* sb_tensor_export_bs without the final synchronisation: keys and ids are
+ * written at once, the payload copy is enqueued on the context stream and is
+ * complete only after that stream reaches this point (sb_ctx_synchronize, or an
+ * event the caller records).  With pinned `data` the copy overlaps work on
+ * other streams, e.g. the next request of a serving loop.  No counterpart in
+ * the reference (its export is a plain array read).                          */
+SB_API sb_status sb_tensor_export_bs_async(sb_ctx* ctx, const sb_tensor* t, int64_t* keys, int64_t* ids, double* data);
 SB_API sb_status sb_tensor_export_coo(sb_ctx* ctx, const sb_tensor* t, int64_t* keys, double* vals);
 SB_API sb_status sb_tensor_export_aliased(sb_ctx* ctx, const sb_tensor* t, double* templates,
                                    int64_t* keys, int64_t* alias_ids, double* scalars);

@@ -45,6 +45,7 @@ SIGNATURES = {
     "sb_tensor_free": (C.c_int, [vp]),
     "sb_tensor_info": (C.c_int, [vp, P_int, P_int, P_i64, P_int, P_i64, P_i64, P_i64, P_int]),
     "sb_tensor_export_bs": (C.c_int, [vp, vp, P_i64, P_i64, P_f64]),
+    "sb_tensor_export_bs_async": (C.c_int, [vp, vp, P_i64, P_i64, P_f64]),
     "sb_tensor_export_coo": (C.c_int, [vp, vp, P_i64, P_f64]),
     "sb_tensor_export_aliased": (C.c_int, [vp, vp, P_f64, P_i64, P_i64, P_f64]),
     "sb_tensor_export_dense": (C.c_int, [vp, vp, P_f64]),

@@ -464,6 +464,22 @@ sb_status sb_tensor_export_bs(sb_ctx* ctx, const sb_tensor* t, int64_t* keys, in
   });
 }
 
+sb_status sb_tensor_export_bs_async(sb_ctx* ctx, const sb_tensor* t, int64_t* keys, int64_t* ids, double* data) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(t);
+    const Tensor& x = *t->impl;
+    require(x.kind == BS, SB_ERR_INVALID_ARG, "not a block-sparse tensor");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    if (keys) std::copy(x.keys.begin(), x.keys.end(), keys);
+    if (ids)
+      for (int64_t i = 0; i < x.nkeys; ++i) ids[i] = i + 1;
+    if (data && x.nkeys)
+      SB_CK(cudaMemcpyAsync(data, x.data.raw(), x.payload_len() * sizeof(double), cudaMemcpyDeviceToHost,
+                            ctx->impl.stream));
+  });
+}
+
 sb_status sb_tensor_export_coo(sb_ctx* ctx, const sb_tensor* t, int64_t* keys, double* vals) {
   return guard(ctx, [&] {
     check_ctx(ctx);
