@@ -121,6 +121,29 @@ class ClockSampler:
 
 # ── FP64 tensor-core peak (not in MEASURED_PEAKS.json): measured live ────
 
+def measured_hbm_gbs():
+    """HBM copy bandwidth measured on this pool (MEASURED_PEAKS.json), else the fallback."""
+    try:
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0
+
+
+# DRAM bytes (read + write) per launch from one ncu capture of this bench at the
+# given chi (--metrics dram__bytes_read.sum,dram__bytes_write.sum), averaged
+# over the captured launches of each kernel; see profiles/ for the commands.
+TRAFFIC = {
+    (2048, "k_gemm_f64"): (1067.9e6, "profiles/heff_chi2048_dram_traffic.md (mean of the psi*L and R*T3 launches)"),
+    (2048, "k_gemm_thin"): (1629.9e6, "profiles/heff_chi2048_dram_traffic.md (mean of the T1*W1 and T2*W2 launches)"),
+}
+
+
+def traffic_per_launch(chi: int, kernel: str):
+    t = TRAFFIC.get((chi, kernel))
+    return None if t is None else {"bytes": t[0], "source": t[1]}
+
+
 def fp64_peak_tflops():
     import torch
     n = 8192
@@ -293,7 +316,7 @@ def run_ours(args, world, rank, local):
             fn()
         e.record(stream)
         ctx.synchronize()
-        prof = {k: ctx.profile(k) for k in ("gemm", "permute", "outer", "axpy")} if profile else None
+        prof = {k: ctx.profile(k) for k in ("gemm", "gemm_thin", "permute", "outer", "axpy")} if profile else None
         if profile:
             ctx.set_profiling(False)
         barrier(world)
@@ -443,7 +466,10 @@ def run_ours(args, world, rank, local):
         return
     g = prof["gemm"]
     achieved = g["flops"] / (g["ms"] * 1e-3) / 1e12 if g["ms"] > 0 else 0.0
-    gu = prof_u["gemm"]
+    th = prof["gemm_thin"]
+    thin_gbs = th["bytes"] / (th["ms"] * 1e-3) / 1e9 if th["ms"] > 0 else 0.0
+    hbm_peak = measured_hbm_gbs()
+    gu, gtu = prof_u["gemm"], prof_u["gemm_thin"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -455,14 +481,24 @@ def run_ours(args, world, rank, local):
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (operators ~0.6 GB, intermediates ~2.3 GB each)"},
         "gflops_algorithmic": flops_alg * value / 1e9,
-        "roofline": {"bound": "tensor", "kernel": "k_gemm_f64 (DMMA m8n8k4)", "achieved": achieved,
-                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+        "roofline": {"bound": "tensor", "kernel": "k_gemm_f64 (DMMA m8n8k4; steps psi*L and R*T3)",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                      "peak_source": "measured live: torch.matmul float64 8192^3, best of 10 (cuBLAS DGEMM)",
-                     "traffic": None, "launches": g["launches"], "kernel_ms_per_step": g["ms"] / args.steps},
+                     "flops_per_launch": g["flops"] / max(g["launches"], 1),
+                     "traffic": traffic_per_launch(args.chi, "k_gemm_f64"), "launches": g["launches"],
+                     "kernel_ms_per_step": g["ms"] / args.steps},
+        "roofline_mpo_steps": {"bound": "hbm", "kernel": "k_gemm_thin (steps T1*W1 and T2*W2, K <= 16)",
+                               "achieved": thin_gbs, "peak": hbm_peak, "unit": "GB/s",
+                               "frac": thin_gbs / hbm_peak if hbm_peak else None,
+                               "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                               "bytes_per_launch": th["bytes"] / max(th["launches"], 1),
+                               "traffic": traffic_per_launch(args.chi, "k_gemm_thin"), "launches": th["launches"],
+                               "kernel_ms_per_step": th["ms"] / args.steps},
         "kernel_time_share": {k: v["ms"] / max(1e-9, sum(x["ms"] for x in prof.values())) for k, v in prof.items()},
         "uniform_format": {"value": value_u, "ms_per_step": ms_u / args.steps,
                            "gflops_executed": flops_pad * value_u / 1e9,
-                           "gemm_tflops": gu["flops"] / (gu["ms"] * 1e-3) / 1e12 if gu["ms"] > 0 else 0.0,
+                           "gemm_tflops": (gu["flops"] + gtu["flops"]) / ((gu["ms"] + gtu["ms"]) * 1e-3) / 1e12
+                           if gu["ms"] + gtu["ms"] > 0 else 0.0,
                            "e2e": {"value": e2e_value_u, "unit": UNIT, "h2d_bytes_per_step": h2d_u,
                                    "d2h_bytes_per_step": d2h_u}},
         "ragged_vs_uniform_rel_diff": agree,

@@ -81,8 +81,10 @@ SB_API int64_t sb_ctx_launch_count(const sb_ctx* ctx);
  * (ta/contract_bs_dense.jl:46-202).  Enabling clears earlier records.       */
 SB_API sb_status sb_ctx_set_profiling(sb_ctx* ctx, int enable);
 /* Totals for one kernel class since profiling was enabled:
- * kind 0 = block GEMM, 1 = permute, 2 = outer-product accumulation,
- * 3 = segmented axpy, 4 = other.  Synchronises the context stream.          */
+ * kind 0 = tiled block GEMM (with its split-K reduction), 1 = permute,
+ * 2 = outer-product accumulation, 3 = segmented axpy, 4 = other (QR/SVD,
+ * gathers), 5 = vector-space operations, 6 = thin block GEMM (K <= 16).
+ * Synchronises the context stream.                                           */
 SB_API sb_status sb_ctx_profile_summary(sb_ctx* ctx, int kind, int64_t* launches, double* total_ms,
                                         double* flops, double* bytes);
 

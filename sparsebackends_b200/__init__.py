@@ -115,7 +115,7 @@ class Context:
     def launch_count(self) -> int:
         return int(self._lib.sb_ctx_launch_count(self._h))
 
-    PROFILE_KINDS = {"gemm": 0, "permute": 1, "outer": 2, "axpy": 3, "other": 4, "vector": 5}
+    PROFILE_KINDS = {"gemm": 0, "permute": 1, "outer": 2, "axpy": 3, "other": 4, "vector": 5, "gemm_thin": 6}
 
     def set_profiling(self, enable: bool) -> None:
         """Time every kernel launch with CUDA events on the context stream."""

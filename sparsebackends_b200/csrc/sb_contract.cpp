@@ -245,7 +245,7 @@ struct GemmPlan {
       }
       DevBuf dc = upload(ctx, cbs), dp = upload(ctx, pairs);
       {
-        ProfScope ps(ctx, PROF_GEMM, flops, bytes);
+        ProfScope ps(ctx, PROF_GEMM_THIN, flops, bytes);
         SB_CK(launch_gemm_f64_skinny(X, Y, C, dc.as<GemmCBlock>(), static_cast<int32_t>(cbs.size()), dp.as<GemmPair>(),
                                      nctas, xT, yT, small_rows, static_cast<int>(small_rows ? M : N),
                                      static_cast<int>(Kmax), ctx->stream));

@@ -282,9 +282,13 @@ struct ThinLayout {
   // long operand: X when !SR (rows), Y when SR (columns); small operand the other.
   static constexpr bool LONG_KCONTIG = SR ? !YT : XT;  // long tile stored [l][k] when k is contiguous
   static constexpr int LSZ = LONG_KCONTIG ? kThinBig * kThinKP : 16 * kThinBP;
-  static constexpr int SSZ = 16 * kThinKP;  // small tile [k][s]
+  // small operand: Y when !SR, X when SR; stored [s][k] when k is contiguous
+  // in global memory, else [k][s], so that consecutive threads load
+  // consecutive global addresses into consecutive shared addresses
+  static constexpr bool SMALL_KCONTIG = SR ? XT : !YT;
+  static constexpr int SSZ = 16 * kThinKP;
   __device__ static int lidx(int l, int k) { return LONG_KCONTIG ? l * kThinKP + k : k * kThinBP + l; }
-  __device__ static int sidx(int k, int s) { return k * kThinKP + s; }
+  __device__ static int sidx(int k, int s) { return SMALL_KCONTIG ? s * kThinKP + k : k * kThinKP + s; }
 };
 
 template <bool SR, bool XT, bool YT>
@@ -325,11 +329,12 @@ __global__ void __launch_bounds__(kThinThreads)
       else src = YT ? Y + pr.y_off + gl + (int64_t)k * pr.ldy : Y + pr.y_off + k + (int64_t)gl * pr.ldy;
       cp_async8(&Ls[stage][TL::lidx(l, k)], v ? src : (SR ? Y : X), v);
     }
-    // small tile: 16 x 16 as [k][s]
+    // small tile: 16 x 16, the global-contiguous index fastest across threads
 #pragma unroll
     for (int r = 0; r < 256 / kThinThreads; ++r) {
       const int e = tid + r * kThinThreads;
-      const int k = e % 16, sI = e / 16;
+      const int k = TL::SMALL_KCONTIG ? e % 16 : e / 16;
+      const int sI = TL::SMALL_KCONTIG ? e / 16 : e % 16;
       const bool v = sI < ns && k < K;
       const double* src;
       if (!SR) src = YT ? Y + pr.y_off + sI + (int64_t)k * pr.ldy : Y + pr.y_off + k + (int64_t)sI * pr.ldy;

@@ -54,7 +54,8 @@ class DevBuf {
 
 // Kernel classes reported by the in-library profiler.
 enum ProfKind : int {
-  PROF_GEMM = 0, PROF_PERMUTE = 1, PROF_OUTER = 2, PROF_AXPY = 3, PROF_OTHER = 4, PROF_VECTOR = 5, PROF_NKINDS = 6
+  PROF_GEMM = 0, PROF_PERMUTE = 1, PROF_OUTER = 2, PROF_AXPY = 3, PROF_OTHER = 4, PROF_VECTOR = 5,
+  PROF_GEMM_THIN = 6, PROF_NKINDS = 7
 };
 
 struct Ctx {
