@@ -98,40 +98,78 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
     lkt -= (pairs[lp].K + kBK - 1) / kBK;
     ++lp;
   }
-  // descriptor of the pair being loaded, kept in registers; the next one is
-  // fetched when the cursor moves on, a k-tile before it is needed
+  // Load geometry of this thread (fixed for the CTA): NT is a multiple of the
+  // tile's contiguous extent, so all elements a thread stages share one index
+  // (x_fix / y_fix) and step the other by a constant per unroll step r.
+  static_assert(NT % kBK == 0 && NT % BM == 0 && NT % BN == 0, "thread count must tile the operand rows");
+  constexpr int XR = XT ? NT / kBK : NT / BM;  // step of the varying index (XT: row i, else k)
+  constexpr int YR = YT ? NT / BN : NT / kBK;  // (YT: k, else column j)
+  const int x_fix = XT ? tid % kBK : tid % BM;
+  const int x_var = XT ? tid / kBK : tid / BM;
+  const int y_fix = YT ? tid % BN : tid % kBK;
+  const int y_var = YT ? tid / BN : tid / kBK;
+  const int sx0 = XT ? x_var * TL::KP + x_fix : x_var * (BM + 4) + x_fix;  // shared offsets at r = 0
+  const int sy0 = YT ? y_var * (BN + 4) + y_fix : y_var * TL::KP + y_fix;
+  constexpr int SXR = XT ? XR * TL::KP : XR * (BM + 4);
+  constexpr int SYR = YT ? YR * (BN + 4) : YR * TL::KP;
+  const int mleft = M - m0, nleft = N - n0;
+
+  // descriptor of the pair being loaded and this thread's global addresses in
+  // it, kept in registers; the next pair is fetched when the cursor moves on,
+  // a k-tile before it is needed
   GemmPair pr{};
-  if (lp < cb.pair_end) pr = pairs[lp];
+  const double *xg = X, *yg = Y;
+  int64_t xstep = 0, ystep = 0, xk = 1, yk = 1;
+  auto set_pair = [&]() {
+    if (XT) {
+      xg = X + pr.x_off + static_cast<int64_t>(m0 + x_var) * pr.ldx + x_fix;
+      xk = 1;
+    } else {
+      xg = X + pr.x_off + (m0 + x_fix) + static_cast<int64_t>(x_var) * pr.ldx;
+      xk = pr.ldx;
+    }
+    xstep = static_cast<int64_t>(XR) * pr.ldx;
+    if (YT) {
+      yg = Y + pr.y_off + (n0 + y_fix) + static_cast<int64_t>(y_var) * pr.ldy;
+      yk = pr.ldy;
+    } else {
+      yg = Y + pr.y_off + y_fix + static_cast<int64_t>(n0 + y_var) * pr.ldy;
+      yk = 1;
+    }
+    ystep = static_cast<int64_t>(YR) * pr.ldy;
+  };
+  if (lp < cb.pair_end) {
+    pr = pairs[lp];
+    set_pair();
+  }
 
   auto issue_load = [&](int stage) {
     const int k0 = lkt * kBK;
-    const double* xb = X + pr.x_off;
+    const int kleft = pr.K - k0;  // valid k entries of this k-tile
+    const double* xp = xg + static_cast<int64_t>(k0) * xk;
+    const double* yp = yg + static_cast<int64_t>(k0) * yk;
+    const double* xb = X + pr.x_off;  // a valid address for zero-filled entries
     const double* yb = Y + pr.y_off;
-    double* xs = Xs + stage * TL::XSZ;
-    double* ys = Ys + stage * TL::YSZ;
+    double* xs = Xs + stage * TL::XSZ + sx0;
+    double* ys = Ys + stage * TL::YSZ + sy0;
 #pragma unroll
     for (int r = 0; r < XLOADS; ++r) {
-      const int e = tid + r * NT;
-      int i, k;
-      if (!XT) { i = e % BM; k = e / BM; } else { k = e % kBK; i = e / kBK; }
-      const int gi = m0 + i, gk = k0 + k;
-      const bool v = (gi < M) && (gk < pr.K);
-      const double* src = v ? (XT ? xb + gk + (int64_t)gi * pr.ldx : xb + gi + (int64_t)gk * pr.ldx) : xb;
-      cp_async8(xs + TL::xidx(i, k), src, v);
+      const int var = x_var + r * XR;
+      const bool v = XT ? (var < mleft && x_fix < kleft) : (x_fix < mleft && var < kleft);
+      cp_async8(xs + r * SXR, v ? xp + r * xstep : xb, v);
     }
 #pragma unroll
     for (int r = 0; r < YLOADS; ++r) {
-      const int e = tid + r * NT;
-      int k, j;
-      if (!YT) { k = e % kBK; j = e / kBK; } else { j = e % BN; k = e / BN; }
-      const int gk = k0 + k, gj = n0 + j;
-      const bool v = (gj < N) && (gk < pr.K);
-      const double* src = v ? (YT ? yb + gj + (int64_t)gk * pr.ldy : yb + gk + (int64_t)gj * pr.ldy) : yb;
-      cp_async8(ys + TL::yidx(k, j), src, v);
+      const int var = y_var + r * YR;
+      const bool v = YT ? (y_fix < nleft && var < kleft) : (var < nleft && y_fix < kleft);
+      cp_async8(ys + r * SYR, v ? yp + r * ystep : yb, v);
     }
     if (++lkt * kBK >= pr.K) {
       lkt = 0;
-      if (++lp < cb.pair_end) pr = pairs[lp];
+      if (++lp < cb.pair_end) {
+        pr = pairs[lp];
+        set_pair();
+      }
     }
   };
 

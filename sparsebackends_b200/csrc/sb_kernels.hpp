@@ -165,7 +165,7 @@ cudaError_t launch_blocks_to_strided(const double* data, const int64_t* d_lin, i
 // chunks of sum_t (s*X[x_off+t]) * (s*Y[y_off+t]) with s = S[s_idx] (s = 1
 // when s_idx < 0); d_partial holds nchunks doubles.  Fixed reduction order:
 // identical bits on every call.
-constexpr int kDotChunk = 4096;
+constexpr int kDotChunk = 1024;  // 4 elements per thread of a 256-thread CTA
 struct DotChunk {
   int64_t x_off, y_off;
   int64_t s_idx;

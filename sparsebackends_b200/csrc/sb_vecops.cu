@@ -22,14 +22,21 @@ __global__ void __launch_bounds__(kDotThreads)
   const DotChunk c = chunks[blockIdx.x];
   const double* x = X + c.x_off;
   const double* y = Y + c.y_off;
-  double acc = 0.0;
-  if (c.s_idx < 0) {
-    for (int t = threadIdx.x; t < c.len; t += kDotThreads) acc = __fma_rn(x[t], y[t], acc);
-  } else {
-    const double sc = S[c.s_idx];
-    for (int t = threadIdx.x; t < c.len; t += kDotThreads)
-      acc = __fma_rn(__dmul_rn(sc, x[t]), __dmul_rn(sc, y[t]), acc);
+  // a chunk is at most kDotChunk = 4 * kDotThreads elements: every thread
+  // issues its (up to) four loads of each operand before the first FMA
+  constexpr int kPer = kDotChunk / kDotThreads;
+  double xv[kPer], yv[kPer];
+#pragma unroll
+  for (int r = 0; r < kPer; ++r) {
+    const int t = threadIdx.x + r * kDotThreads;
+    xv[r] = t < c.len ? x[t] : 0.0;
+    yv[r] = t < c.len ? y[t] : 0.0;
   }
+  const double sc = c.s_idx < 0 ? 1.0 : S[c.s_idx];
+  double acc = 0.0;
+#pragma unroll
+  for (int r = 0; r < kPer; ++r)
+    acc = c.s_idx < 0 ? __fma_rn(xv[r], yv[r], acc) : __fma_rn(__dmul_rn(sc, xv[r]), __dmul_rn(sc, yv[r]), acc);
   red[threadIdx.x] = acc;
   __syncthreads();
 #pragma unroll
