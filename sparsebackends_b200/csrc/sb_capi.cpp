@@ -103,6 +103,7 @@ sb_status sb_ctx_create(int device, unsigned flags, sb_ctx** out) {
       else if (v == "32x128") c->impl.gemm_tile = 2;
       else if (v == "128x64") c->impl.gemm_tile = 3;
       else if (v == "64x128") c->impl.gemm_tile = 4;
+      else if (v == "64x32") c->impl.gemm_tile = 5;
     }
     if (const char* th = std::getenv("SPARSEB_GEMM_THIN")) c->impl.gemm_thin = std::atoi(th);
     if (const char* sk = std::getenv("SPARSEB_GEMM_SPLITK")) c->impl.gemm_splitk = std::max(0, std::atoi(sk));

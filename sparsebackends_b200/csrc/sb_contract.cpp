@@ -269,6 +269,17 @@ struct GemmPlan {
     if (an <= 32 && am >= 128) shape = GemmShape::T128x32;
     else if (am <= 32 && an >= 128) shape = GemmShape::T32x128;
     else if (am >= 1024 && an >= 512) shape = am >= an ? GemmShape::T128x64 : GemmShape::T64x128;
+    if (shape == GemmShape::T64x64) {
+      // few 64x64 tiles with long K (the split-K regime): smaller tiles with a
+      // deeper pipeline keep more CTAs busy
+      int64_t t64 = 0, kt = 0;
+      for (auto& c : cbs) {
+        const int64_t nt = ((c.M + 63) / 64) * ((c.N + 63) / 64);
+        t64 += nt;
+        for (int p = c.pair_begin; p < c.pair_end; ++p) kt += nt * ((pairs[p].K + 15) / 16);
+      }
+      if (t64 < 3 * 148 * 4 && t64 > 0 && kt / t64 >= 64) shape = GemmShape::T64x32;
+    }
     if (ctx->gemm_tile >= 0) shape = static_cast<GemmShape>(ctx->gemm_tile);
     int bm, bn;
     gemm_tile_dims(shape, &bm, &bn);

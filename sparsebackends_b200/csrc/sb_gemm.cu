@@ -483,6 +483,7 @@ void gemm_tile_dims(GemmShape shape, int* bm, int* bn) {
     case GemmShape::T32x128: *bm = 32; *bn = 128; break;
     case GemmShape::T128x64: *bm = 128; *bn = 64; break;
     case GemmShape::T64x128: *bm = 64; *bn = 128; break;
+    case GemmShape::T64x32: *bm = 64; *bn = 32; break;
     default: *bm = 64; *bn = 64; break;
   }
 }
@@ -509,6 +510,8 @@ cudaError_t launch_gemm_f64(const double* X, const double* Y, double* C,
       return dispatch_t<128, 64, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, splitk, partial, s);
     case GemmShape::T64x128:
       return dispatch_t<64, 128, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, splitk, partial, s);
+    case GemmShape::T64x32:
+      return dispatch_t<64, 32, 32, 16, 16, 4>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, splitk, partial, s);
     default:
       return dispatch_t<64, 64, 32, 32>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, ntiles, splitk, partial, s);
   }

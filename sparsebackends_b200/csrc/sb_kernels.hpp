@@ -31,11 +31,13 @@ struct GemmPair {
   int32_t K, ldx, ldy, pad;
 };
 
-// CTA tile shapes, all with 32x32 warp tiles, k-tile 16, 3 stages.  Measured
-// on the H_eff steps (64x64 tiles, chi = 2048): 32x64 / 64x32 warp tiles need
+// CTA tile shapes with 32x32 warp tiles, k-tile 16, 3 stages, plus T64x32.
+// Measured on the H_eff steps (chi = 2048): 32x64 / 64x32 warp tiles need
 // 190-250 registers, halve the resident CTAs and run 4-16% slower; 4 stages,
-// k-tile 32 (2 or 3 stages) and eight 32x16 warps run 0-18% slower.
-enum class GemmShape : int { T64x64 = 0, T128x32 = 1, T32x128 = 2, T128x64 = 3, T64x128 = 4 };
+// k-tile 32 and eight 32x16 warps run 0-18% slower on the psi*L step.
+// T64x32: four 32x16 warps, 4 stages, used for the few-tile, long-K launches
+// that otherwise go to split-K (H_eff R*T3: 2.17 against 2.26 ms).
+enum class GemmShape : int { T64x64 = 0, T128x32 = 1, T32x128 = 2, T128x64 = 3, T64x128 = 4, T64x32 = 5 };
 
 // splitk > 1: the concatenated K range of every C tile is cut into splitk
 // segments computed by separate CTAs into partial (splitk * ntiles * BM*BN
