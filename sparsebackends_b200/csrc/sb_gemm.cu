@@ -49,7 +49,7 @@ struct TileLayout {
 };
 
 template <int BM, int BN, int WM, int WN, bool XT, bool YT, int BK = kBK, int ST = kStages>
-__global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
+__global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32, 512 / ((BM / WM) * (BN / WN) * 32))
     k_gemm_f64(const double* __restrict__ X, const double* __restrict__ Y, double* __restrict__ C,
                const GemmCBlock* __restrict__ cblocks, int32_t ncb, const GemmPair* __restrict__ pairs,
                int32_t splitk, int32_t ntiles, double* __restrict__ partial) {
@@ -143,27 +143,40 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
     set_pair();
   }
 
-  auto issue_load = [&](int stage) {
+  // Staging of one k-tile, in kParts slices so that the copies of the next
+  // stage interleave with the DMMAs of the current one.
+  constexpr int kParts = kBK / 4;
+  static_assert(XLOADS % kParts == 0 && YLOADS % kParts == 0, "loads must split evenly over the k4 steps");
+  int kleft = 0;
+  const double *xp = X, *yp = Y, *xb = X, *yb = Y;
+  double *xs_st = Xs, *ys_st = Ys;
+  auto begin_load = [&](int stage) {
     const int k0 = lkt * kBK;
-    const int kleft = pr.K - k0;  // valid k entries of this k-tile
-    const double* xp = xg + static_cast<int64_t>(k0) * xk;
-    const double* yp = yg + static_cast<int64_t>(k0) * yk;
-    const double* xb = X + pr.x_off;  // a valid address for zero-filled entries
-    const double* yb = Y + pr.y_off;
-    double* xs = Xs + stage * TL::XSZ + sx0;
-    double* ys = Ys + stage * TL::YSZ + sy0;
+    kleft = pr.K - k0;  // valid k entries of this k-tile
+    xp = xg + static_cast<int64_t>(k0) * xk;
+    yp = yg + static_cast<int64_t>(k0) * yk;
+    xb = X + pr.x_off;  // a valid address for zero-filled entries
+    yb = Y + pr.y_off;
+    xs_st = Xs + stage * TL::XSZ + sx0;
+    ys_st = Ys + stage * TL::YSZ + sy0;
+  };
+  auto load_part = [&](int part) {
 #pragma unroll
-    for (int r = 0; r < XLOADS; ++r) {
+    for (int q = 0; q < XLOADS / kParts; ++q) {
+      const int r = part * (XLOADS / kParts) + q;
       const int var = x_var + r * XR;
       const bool v = XT ? (var < mleft && x_fix < kleft) : (x_fix < mleft && var < kleft);
-      cp_async8(xs + r * SXR, v ? xp + r * xstep : xb, v);
+      cp_async8(xs_st + r * SXR, v ? xp + r * xstep : xb, v);
     }
 #pragma unroll
-    for (int r = 0; r < YLOADS; ++r) {
+    for (int q = 0; q < YLOADS / kParts; ++q) {
+      const int r = part * (YLOADS / kParts) + q;
       const int var = y_var + r * YR;
       const bool v = YT ? (y_fix < nleft && var < kleft) : (var < nleft && y_fix < kleft);
-      cp_async8(ys + r * SYR, v ? yp + r * ystep : yb, v);
+      cp_async8(ys_st + r * SYR, v ? yp + r * ystep : yb, v);
     }
+  };
+  auto end_load = [&]() {
     if (++lkt * kBK >= pr.K) {
       lkt = 0;
       if (++lp < cb.pair_end) {
@@ -171,6 +184,12 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
         set_pair();
       }
     }
+  };
+  auto issue_load = [&](int stage) {
+    begin_load(stage);
+#pragma unroll
+    for (int part = 0; part < kParts; ++part) load_part(part);
+    end_load();
   };
 
   const int warp = tid >> 5, lane = tid & 31;
@@ -192,12 +211,13 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
   for (int it = 0; it < total; ++it) {
     cp_async_wait<kStages - 2>();
     __syncthreads();
-    if (it + kStages - 1 < total) issue_load((it + kStages - 1) % kStages);
-    cp_async_commit();
+    const bool more = it + kStages - 1 < total;
+    if (more) begin_load((it + kStages - 1) % kStages);
     const double* xs = Xs + (it % kStages) * TL::XSZ;
     const double* ys = Ys + (it % kStages) * TL::YSZ;
 #pragma unroll
     for (int k4 = 0; k4 < kBK; k4 += 4) {
+      if (more) load_part(k4 / 4);
       double af[MT], bf[NTL];
 #pragma unroll
       for (int a = 0; a < MT; ++a) af[a] = xs[TL::xidx(wm * WM + a * 8 + g, k4 + t)];
@@ -208,6 +228,8 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
 #pragma unroll
         for (int b = 0; b < NTL; ++b) dmma_8x8x4(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
     }
+    if (more) end_load();
+    cp_async_commit();
   }
   cp_async_wait<0>();
 
