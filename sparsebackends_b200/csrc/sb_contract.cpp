@@ -236,6 +236,8 @@ struct GemmPlan {
     const bool skinny_m = Kmax <= 16 && M <= 16;
     if ((skinny_n || skinny_m) && ctx->gemm_tile < 0 && ctx->gemm_thin != 0) {
       const bool small_rows = skinny_m;
+      bool every_block_has_pairs = true;
+      for (auto& c : cbs) every_block_has_pairs = every_block_has_pairs && c.pair_end > c.pair_begin;
       int64_t nctas = 0;
       for (auto& c : cbs) {
         const int64_t bigx = small_rows ? c.N : c.M;
@@ -248,7 +250,7 @@ struct GemmPlan {
         ProfScope ps(ctx, PROF_GEMM_THIN, flops, bytes);
         SB_CK(launch_gemm_f64_skinny(X, Y, C, dc.as<GemmCBlock>(), static_cast<int32_t>(cbs.size()), dp.as<GemmPair>(),
                                      nctas, xT, yT, small_rows, static_cast<int>(small_rows ? M : N),
-                                     static_cast<int>(Kmax), ctx->stream));
+                                     static_cast<int>(Kmax), ctx->stream, ctx->gemm_thin != 1 && every_block_has_pairs));
       }
       ctx->note_launch();
       return;

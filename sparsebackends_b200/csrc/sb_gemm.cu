@@ -352,7 +352,7 @@ struct ThinLayout {
 };
 
 template <bool SR, bool XT, bool YT>
-__global__ void __launch_bounds__(kThinThreads)
+__global__ void __launch_bounds__(kThinThreads, 5)
     k_gemm_thin(const double* __restrict__ X, const double* __restrict__ Y, double* __restrict__ C,
                 const GemmCBlock* __restrict__ cblocks, int32_t ncb, const GemmPair* __restrict__ pairs) {
   using TL = ThinLayout<SR, XT, YT>;
@@ -373,33 +373,47 @@ __global__ void __launch_bounds__(kThinThreads)
   const int l0 = (bid - cb.tile_begin) * kThinBig;
   const int tid = threadIdx.x;
 
-  auto load = [&](int stage, int p) {
-    const GemmPair pr = pairs[p];
+  // Load geometry: the long tile's elements of this thread share their k
+  // (k-contiguous layout) or their l (l-contiguous layout) and step the other
+  // index by a constant; the small tile's by 8 rows.
+  const int lleft = L - l0;
+  const int tq = tid & 15, tr = tid >> 4;
+  auto load = [&](int stage, const GemmPair& pr) {
     const int K = pr.K;
+    const double* lbase = SR ? Y + pr.y_off : X + pr.x_off;
+    const double* sbase = SR ? X + pr.x_off : Y + pr.y_off;
+    const int64_t lld = SR ? pr.ldy : pr.ldx;
+    const int64_t sld = SR ? pr.ldx : pr.ldy;
     // long tile: kThinBig x 16
+    constexpr int LR = kThinBig * 16 / kThinThreads;
+    if (TL::LONG_KCONTIG) {
+      // element (l = tr + 8 r, k = tq) at lbase + k + (l0 + l) * lld
+      const double* lp = lbase + tq + static_cast<int64_t>(l0 + tr) * lld;
+      double* dst = &Ls[stage][tr * kThinKP + tq];
 #pragma unroll
-    for (int r = 0; r < kThinBig * 16 / kThinThreads; ++r) {
-      const int e = tid + r * kThinThreads;
-      int l, k;
-      if (TL::LONG_KCONTIG) { k = e % 16; l = e / 16; } else { l = e % kThinBig; k = e / kThinBig; }
-      const int gl = l0 + l;
-      const bool v = gl < L && k < K;
-      const double* src;
-      if (!SR) src = XT ? X + pr.x_off + k + (int64_t)gl * pr.ldx : X + pr.x_off + gl + (int64_t)k * pr.ldx;
-      else src = YT ? Y + pr.y_off + gl + (int64_t)k * pr.ldy : Y + pr.y_off + k + (int64_t)gl * pr.ldy;
-      cp_async8(&Ls[stage][TL::lidx(l, k)], v ? src : (SR ? Y : X), v);
+      for (int r = 0; r < LR; ++r) {
+        const bool v = tr + 8 * r < lleft && tq < K;
+        cp_async8(dst + r * 8 * kThinKP, v ? lp + static_cast<int64_t>(8 * r) * lld : lbase, v);
+      }
+    } else {
+      // element (l = tid, k = r) at lbase + (l0 + l) + k * lld
+      const double* lp = lbase + l0 + tid;
+      double* dst = &Ls[stage][tid];
+#pragma unroll
+      for (int r = 0; r < LR; ++r) {
+        const bool v = tid < lleft && r < K;
+        cp_async8(dst + r * kThinBP, v ? lp + static_cast<int64_t>(r) * lld : lbase, v);
+      }
     }
-    // small tile: 16 x 16, the global-contiguous index fastest across threads
+    // small tile: 16 x 16; the global-contiguous index (k or s) is tq, the
+    // other one tr + 8 r
+    const double* sp = sbase + tq + static_cast<int64_t>(tr) * sld;
+    double* sdst = &Ss[stage][tr * kThinKP + tq];
 #pragma unroll
     for (int r = 0; r < 256 / kThinThreads; ++r) {
-      const int e = tid + r * kThinThreads;
-      const int k = TL::SMALL_KCONTIG ? e % 16 : e / 16;
-      const int sI = TL::SMALL_KCONTIG ? e / 16 : e % 16;
-      const bool v = sI < ns && k < K;
-      const double* src;
-      if (!SR) src = YT ? Y + pr.y_off + sI + (int64_t)k * pr.ldy : Y + pr.y_off + k + (int64_t)sI * pr.ldy;
-      else src = XT ? X + pr.x_off + k + (int64_t)sI * pr.ldx : X + pr.x_off + sI + (int64_t)k * pr.ldx;
-      cp_async8(&Ss[stage][TL::sidx(k, sI)], v ? src : (SR ? X : Y), v);
+      const int o = tr + 8 * r;
+      const bool v = TL::SMALL_KCONTIG ? (o < ns && tq < K) : (tq < ns && o < K);
+      cp_async8(sdst + r * 8 * kThinKP, v ? sp + static_cast<int64_t>(8 * r) * sld : sbase, v);
     }
   };
 
@@ -412,11 +426,17 @@ __global__ void __launch_bounds__(kThinThreads)
   for (int a = 0; a < 8; ++a) acc[a][0] = acc[a][1] = 0.0;
 
   const int p0 = cb.pair_begin, p1 = cb.pair_end;
-  if (p0 < p1) load(0, p0);
+  // pair descriptors are read one pair ahead of their copies
+  GemmPair pnext{};
+  if (p0 < p1) load(0, pairs[p0]);
+  if (p0 + 1 < p1) pnext = pairs[p0 + 1];
   cp_async_commit();
   for (int p = p0; p < p1; ++p) {
     const int st = (p - p0) & 1;
-    if (p + 1 < p1) load(st ^ 1, p + 1);
+    if (p + 1 < p1) {
+      load(st ^ 1, pnext);
+      if (p + 2 < p1) pnext = pairs[p + 2];
+    }
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
@@ -486,9 +506,184 @@ __global__ void __launch_bounds__(kThinThreads)
   }
 }
 
+// Persistent variant of k_gemm_thin: a fixed grid of CTAs walks the 128-long
+// strips (tiles) with stride gridDim.x, and the double-buffered copy pipeline
+// runs across tile boundaries, so the first pair of the next strip is in
+// flight while the current one finishes; C is stored straight from the DMMA
+// fragments (runs of 8 consecutive doubles per column).
+template <bool SR, bool XT, bool YT>
+__global__ void __launch_bounds__(kThinThreads, 5)
+    k_gemm_thin_p(const double* __restrict__ X, const double* __restrict__ Y, double* __restrict__ C,
+                  const GemmCBlock* __restrict__ cblocks, int32_t ncb, const GemmPair* __restrict__ pairs,
+                  int32_t ntiles) {
+  using TL = ThinLayout<SR, XT, YT>;
+  __shared__ double Ls[2][TL::LSZ];
+  __shared__ double Ss[2][TL::SSZ];
+  const int tid = threadIdx.x;
+  const int tq = tid & 15, tr = tid >> 4;
+
+  auto find = [&](int tile, GemmCBlock& cb, int& l0) {
+    int lo = 0, hi = ncb - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (cblocks[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
+    }
+    cb = cblocks[lo];
+    l0 = (tile - cb.tile_begin) * kThinBig;
+  };
+  auto load = [&](int stage, const GemmPair& pr, const GemmCBlock& cb, int l0) {
+    const int K = pr.K;
+    const int L = SR ? cb.N : cb.M, ns = SR ? cb.M : cb.N;
+    const int lleft = L - l0;
+    const double* lbase = SR ? Y + pr.y_off : X + pr.x_off;
+    const double* sbase = SR ? X + pr.x_off : Y + pr.y_off;
+    const int64_t lld = SR ? pr.ldy : pr.ldx;
+    const int64_t sld = SR ? pr.ldx : pr.ldy;
+    constexpr int LR = kThinBig * 16 / kThinThreads;
+    if (TL::LONG_KCONTIG) {
+      const double* lp = lbase + tq + static_cast<int64_t>(l0 + tr) * lld;
+      double* dst = &Ls[stage][tr * kThinKP + tq];
+#pragma unroll
+      for (int r = 0; r < LR; ++r) {
+        const bool v = tr + 8 * r < lleft && tq < K;
+        cp_async8(dst + r * 8 * kThinKP, v ? lp + static_cast<int64_t>(8 * r) * lld : lbase, v);
+      }
+    } else {
+      const double* lp = lbase + l0 + tid;
+      double* dst = &Ls[stage][tid];
+#pragma unroll
+      for (int r = 0; r < LR; ++r) {
+        const bool v = tid < lleft && r < K;
+        cp_async8(dst + r * kThinBP, v ? lp + static_cast<int64_t>(r) * lld : lbase, v);
+      }
+    }
+    const double* sp = sbase + tq + static_cast<int64_t>(tr) * sld;
+    double* sdst = &Ss[stage][tr * kThinKP + tq];
+#pragma unroll
+    for (int r = 0; r < 256 / kThinThreads; ++r) {
+      const int o = tr + 8 * r;
+      const bool v = TL::SMALL_KCONTIG ? (o < ns && tq < K) : (tq < ns && o < K);
+      cp_async8(sdst + r * 8 * kThinKP, v ? sp + static_cast<int64_t>(8 * r) * sld : sbase, v);
+    }
+  };
+
+  int ltile = blockIdx.x;
+  if (ltile >= ntiles) return;
+  GemmCBlock lcb, ccb;
+  int ll0, cl0;
+  find(ltile, lcb, ll0);
+  int lp = lcb.pair_begin;
+  load(0, pairs[lp], lcb, ll0);
+  cp_async_commit();
+  ccb = lcb;
+  cl0 = ll0;
+  int cpair = lp;
+  auto advance = [&]() {
+    if (++lp >= lcb.pair_end) {
+      ltile += gridDim.x;
+      if (ltile < ntiles) {
+        find(ltile, lcb, ll0);
+        lp = lcb.pair_begin;
+      }
+    }
+  };
+  advance();
+
+  const int warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;
+  double acc[8][2];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) acc[a][0] = acc[a][1] = 0.0;
+  int st = 0;
+  while (true) {
+    const bool more = ltile < ntiles;
+    if (more) load(st ^ 1, pairs[lp], lcb, ll0);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const double* ls = Ls[st];
+    const double* ss = Ss[st];
+#pragma unroll
+    for (int k4 = 0; k4 < 16; k4 += 4) {
+      if (!SR) {
+        double af[4], bf[2];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) af[a] = ls[TL::lidx(warp * 32 + a * 8 + g, k4 + t)];
+#pragma unroll
+        for (int b = 0; b < 2; ++b) bf[b] = ss[TL::sidx(k4 + t, b * 8 + g)];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 2; ++b) dmma_8x8x4(acc[a * 2 + b][0], acc[a * 2 + b][1], af[a], bf[b]);
+      } else {
+        double af[2], bf[4];
+#pragma unroll
+        for (int a = 0; a < 2; ++a) af[a] = ss[TL::sidx(k4 + t, a * 8 + g)];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) bf[b] = ls[TL::lidx(warp * 32 + b * 8 + g, k4 + t)];
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) dmma_8x8x4(acc[a * 4 + b][0], acc[a * 4 + b][1], af[a], bf[b]);
+      }
+    }
+    __syncthreads();  // stage st is free for the next copy
+    if (cpair + 1 == ccb.pair_end) {
+      // last pair of this strip: store it from the fragments and start over
+      const int M = ccb.M;
+      double* cbase = C + ccb.c_off;
+      if (!SR) {
+        const int L = M, ns = ccb.N;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          const int l = cl0 + warp * 32 + a * 8 + g;
+#pragma unroll
+          for (int b = 0; b < 2; ++b) {
+            const int s0 = b * 8 + 2 * t;
+            if (l < L && s0 < ns) cbase[l + static_cast<int64_t>(s0) * M] = acc[a * 2 + b][0];
+            if (l < L && s0 + 1 < ns) cbase[l + static_cast<int64_t>(s0 + 1) * M] = acc[a * 2 + b][1];
+          }
+        }
+      } else {
+        const int L = ccb.N, ns = M;
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+          const int sI = a * 8 + g;
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const int l = cl0 + warp * 32 + b * 8 + 2 * t;
+            if (sI < ns && l < L) cbase[sI + static_cast<int64_t>(l) * M] = acc[a * 4 + b][0];
+            if (sI < ns && l + 1 < L) cbase[sI + static_cast<int64_t>(l + 1) * M] = acc[a * 4 + b][1];
+          }
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < 8; ++a) acc[a][0] = acc[a][1] = 0.0;
+    }
+    if (!more) break;
+    ccb = lcb;
+    cl0 = ll0;
+    cpair = lp;
+    advance();
+    st ^= 1;
+  }
+  cp_async_wait<0>();
+}
+
 template <bool SR>
 cudaError_t thin_t(bool xT, bool yT, const double* X, const double* Y, double* C, const GemmCBlock* cb, int32_t ncb,
-                   const GemmPair* pr, int64_t nctas, cudaStream_t s) {
+                   const GemmPair* pr, int64_t nctas, bool persistent, cudaStream_t s) {
+  if (persistent) {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned g = static_cast<unsigned>(std::min<int64_t>(nctas, static_cast<int64_t>(sms) * 5));
+    const int32_t nt = static_cast<int32_t>(nctas);
+    if (!xT && !yT) k_gemm_thin_p<SR, false, false><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr, nt);
+    else if (!xT && yT) k_gemm_thin_p<SR, false, true><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr, nt);
+    else if (xT && !yT) k_gemm_thin_p<SR, true, false><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr, nt);
+    else k_gemm_thin_p<SR, true, true><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr, nt);
+    return cudaGetLastError();
+  }
   const unsigned g = static_cast<unsigned>(nctas);
   if (!xT && !yT) k_gemm_thin<SR, false, false><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr);
   else if (!xT && yT) k_gemm_thin<SR, false, true><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr);
@@ -512,11 +707,11 @@ void gemm_tile_dims(GemmShape shape, int* bm, int* bn) {
 
 cudaError_t launch_gemm_f64_skinny(const double* X, const double* Y, double* C, const GemmCBlock* d_cblocks,
                                    int32_t ncb, const GemmPair* d_pairs, int64_t nctas, bool xT, bool yT,
-                                   bool small_rows, int small_max, int k_max, cudaStream_t s) {
+                                   bool small_rows, int small_max, int k_max, cudaStream_t s, bool persistent) {
   if (nctas <= 0) return cudaSuccess;
   if (nctas > 0x7fffffffLL || small_max > 16 || k_max > 16) return cudaErrorInvalidValue;
-  return small_rows ? thin_t<true>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, s)
-                    : thin_t<false>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, s);
+  return small_rows ? thin_t<true>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, persistent, s)
+                    : thin_t<false>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, persistent, s);
 }
 
 cudaError_t launch_gemm_f64(const double* X, const double* Y, double* C,

@@ -81,8 +81,9 @@ struct Ctx {
   int gemm_tile = -1;
   // SPARSEB_GEMM_SPLITK=<n> forces the split-K factor (tuning); 0 = auto.
   int gemm_splitk = 0;
-  // SPARSEB_GEMM_THIN=0 keeps K<=16 launches on the tiled kernel (tuning);
-  // -1 = auto (the thin kernel for every launch it can serve).
+  // SPARSEB_GEMM_THIN=0 keeps K<=16 launches on the tiled kernel, =1 uses the
+  // one-CTA-per-strip thin kernel (tuning); -1 = auto: the persistent thin
+  // kernel for every launch it can serve.
   int gemm_thin = -1;
   // Pinned staging ring for host-to-device plan uploads: a copy from pinned
   // memory does not synchronise the stream, so host planning of the next

@@ -48,13 +48,16 @@ cudaError_t launch_gemm_f64(const double* X, const double* Y, double* C,
                             int splitk = 1, double* partial = nullptr);
 
 // Thin variant for launches whose every pair has K <= 16 and whose C blocks
-// have min(M, N) <= 16 (HBM-bound): DMMA on 128 x 16 tiles of the long side,
-// cp.async double buffering across pairs, shared-memory staged stores.
-// CTAs of C block c: [tile_begin, tile_begin + ceil(long/128)) (mtiles unused).
+// have min(M, N) <= 16 (HBM-bound): DMMA on 128 x 16 strips of the long side,
+// cp.async double buffering across pairs.  Strips of C block c:
+// [tile_begin, tile_begin + ceil(long/128)) (mtiles unused).  persistent: a
+// grid of 5 CTAs per SM walks the strips with the copy pipeline running
+// across strip boundaries and stores C from the fragments (needs >= 1 pair
+// per C block); otherwise one CTA per strip with shared-memory staged stores.
 cudaError_t launch_gemm_f64_skinny(const double* X, const double* Y, double* C,
                                    const GemmCBlock* d_cblocks, int32_t ncblocks, const GemmPair* d_pairs,
                                    int64_t nctas, bool xT, bool yT, bool small_rows, int small_max,
-                                   int k_max, cudaStream_t s);
+                                   int k_max, cudaStream_t s, bool persistent = false);
 
 // Number of tiles of a (M, N) C block for the given tile shape.
 void gemm_tile_dims(GemmShape shape, int* bm, int* bn);

@@ -91,10 +91,11 @@ def test_unit_extents(sb):
     assert abs(sb.norm(r) - np.sqrt(4 + 1 + 0.25)) < 1e-15
 
 
-@pytest.mark.parametrize("thin", ["auto", "0"])
+@pytest.mark.parametrize("thin", ["auto", "0", "1"])
 def test_more_than_65535_blocks(sb, thin):
-    """90000 output blocks (300 x 300 prefix pairs), 2 x 2 tails: the thin
-    kernel in the automatic choice, the tiled kernel with SPARSEB_GEMM_THIN=0."""
+    """90000 output blocks (300 x 300 prefix pairs), 2 x 2 tails: the
+    persistent thin kernel in the automatic choice, the tiled kernel with
+    SPARSEB_GEMM_THIN=0, the one-CTA-per-strip thin kernel with =1."""
     rng = np.random.Generator(np.random.PCG64(4))
     n = 300
     A = so.blocksparse_from_dense(rng.standard_normal((n, 1, 2, 2)), 2)
