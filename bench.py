@@ -134,8 +134,8 @@ def measured_hbm_gbs():
 # given chi (--metrics dram__bytes_read.sum,dram__bytes_write.sum), averaged
 # over the captured launches of each kernel; see profiles/ for the commands.
 TRAFFIC = {
-    (2048, "k_gemm_f64"): (1067.9e6, "profiles/heff_chi2048_dram_traffic.md (mean of the psi*L and R*T3 launches)"),
-    (2048, "k_gemm_thin"): (1629.9e6, "profiles/heff_chi2048_dram_traffic.md (mean of the T1*W1 and T2*W2 launches)"),
+    (2048, "k_gemm_f64"): (1024.2e6, "profiles/heff_chi2048_dram_traffic.md (mean of the psi*L and R*T3 launches)"),
+    (2048, "k_gemm_thin"): (1640.7e6, "profiles/heff_chi2048_dram_traffic.md (mean of the T1*W1 and T2*W2 launches)"),
 }
 
 
@@ -487,7 +487,7 @@ def run_ours(args, world, rank, local):
                      "flops_per_launch": g["flops"] / max(g["launches"], 1),
                      "traffic": traffic_per_launch(args.chi, "k_gemm_f64"), "launches": g["launches"],
                      "kernel_ms_per_step": g["ms"] / args.steps},
-        "roofline_mpo_steps": {"bound": "hbm", "kernel": "k_gemm_thin (steps T1*W1 and T2*W2, K <= 16)",
+        "roofline_mpo_steps": {"bound": "hbm", "kernel": "k_gemm_thin_p (steps T1*W1 and T2*W2, K <= 16)",
                                "achieved": thin_gbs, "peak": hbm_peak, "unit": "GB/s",
                                "frac": thin_gbs / hbm_peak if hbm_peak else None,
                                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
