@@ -438,6 +438,38 @@ def run_ours(args, world, rank, local):
     for sl in slots:  # every request returned H·psi (deterministic kernels: bit-exact)
         assert np.array_equal(sl.pin_out.numpy()[:out_len], chain_r.out["T4"].data)
 
+    # ── the same matvec replayed as one CUDA graph (host planning paid once),
+    # at chi=2048 and at a small bond dimension where host work would dominate
+    chain_g = qn.HeffChain(layout, ctx)
+    graph = chain_g.capture(dev_r["psi"], dev_r["L"], dev_r["W1"], dev_r["W2"], dev_r["R"])
+    for _ in range(3):
+        graph.launch()
+    ms_g, _, _ = timed(graph.launch, args.steps)
+    assert np.array_equal(chain_g.out["T4"].data, chain_r.out["T4"].data)
+
+    def small_chi_rates(chi_s, steps):
+        lay_s = workload(chi_s)
+        _, hr = host_tensors(lay_s, args.seed, with_ragged=True)
+        ds = {n: sb.NewBlockSparseSorted(lay_s.dims[n], lay_s.n2[n], k, None, d, ctx=ctx, block_dims=e)
+              for n, (k, d, e) in hr.items()}
+        ch = qn.HeffChain(lay_s, ctx)
+        args_s = (ds["psi"], ds["L"], ds["W1"], ds["W2"], ds["R"])
+        for _ in range(3):
+            ch.apply(*args_s)
+        ms_e, _, _ = timed(lambda: ch.apply(*args_s), steps)
+        chg = qn.HeffChain(lay_s, ctx)
+        gs = chg.capture(*args_s)
+        for _ in range(3):
+            gs.launch()
+        ms_s, _, _ = timed(gs.launch, steps)
+        assert np.array_equal(chg.out["T4"].data, ch.out["T4"].data)
+        return {"chi": chi_s, "eager_matvec_per_s": replica_rate(world, steps, ms_e),
+                "graph_matvec_per_s": replica_rate(world, steps, ms_s)}
+
+    graph_leg = {"value": replica_rate(world, args.steps, ms_g), "unit": UNIT,
+                 "note": "the H_eff chain captured once (sb_ctx_capture_begin/end) and replayed with sb_graph_launch",
+                 "small_chi": small_chi_rates(256, 200)}
+
     # ── one Lanczos eigensolve as DMRG calls it (krylovdim 3, maxiter 1) ──
     from sparsebackends_b200 import krylov
     op = qn.HeffOperator(layout, dev_r["L"], dev_r["W1"], dev_r["W2"], dev_r["R"], ctx)
@@ -509,6 +541,7 @@ def run_ours(args, world, rank, local):
                 "serial": {"value": e2e_serial, "unit": UNIT,
                            "mode": "one request at a time: upload, apply, blocking read-back"}},
         "lanczos": lanczos,
+        "graph_replay": graph_leg,
         "gpu_launches": launches,
         "clocks": clocks,
     }

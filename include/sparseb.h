@@ -195,6 +195,29 @@ SB_API sb_status sb_to_dense(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out);
 /* to_blocksparse(::AliasedBlockSparse) (aliased/conversions.jl:18-32).       */
 SB_API sb_status sb_aliased_to_blocksparse(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out);
 
+/* ── CUDA graph capture of a sequence of calls ───────────────────────────────
+ * No counterpart in the reference (its calls are Julia function calls).  For
+ * repeated contractions with fixed block structure, e.g. the H_eff matvec of
+ * every Lanczos step, the host planning and the launches of a sequence of
+ * calls are captured once and replayed as one CUDA graph on the context
+ * stream.  Rules:
+ *  - run the sequence once before capturing, so every output tensor already
+ *    has its storage (a capture that would leave new device buffers alive
+ *    fails with SB_ERR_INVALID_ARG);
+ *  - calls whose output structure depends on values read back from the GPU
+ *    (dense_bb, dense_bd, dense_index, COO x COO, *_from_dense) and host
+ *    readbacks (exports, norm, dot) cannot be captured: they fail and the
+ *    capture is abandoned;
+ *  - a replay recomputes the values of the captured outputs from the current
+ *    contents of the captured inputs' device storage (same tensors, same
+ *    structure); the host-side structure of the outputs is the one at capture.
+ * Plan arrays the graph reads are device buffers owned by the graph.         */
+typedef struct sb_graph sb_graph;
+SB_API sb_status sb_ctx_capture_begin(sb_ctx* ctx);
+SB_API sb_status sb_ctx_capture_end(sb_ctx* ctx, sb_graph** out);
+SB_API sb_status sb_graph_launch(sb_ctx* ctx, const sb_graph* g);
+SB_API sb_status sb_graph_free(sb_graph* g);
+
 /* ── vector-space operations (Krylov solvers) ────────────────────────────────
  * The hooks KrylovKit's Lanczos needs from stored tensors
  * (SparseBackends/src/tensor_wrappers.jl:793-923; aliased variants

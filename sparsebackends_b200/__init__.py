@@ -30,14 +30,14 @@ from __future__ import annotations
 
 import ctypes as C
 import hashlib
-from typing import Any, Iterable, List, Optional, Sequence, Tuple
+from typing import Any, Iterable, List, Optional, Sequence, Tuple, Callable
 
 import numpy as np
 
 from . import _lib
 
 __all__ = [
-    "SparseBackendsError", "Context", "default_context", "DenseTensor", "NewBlockSparseSorted", "COOTensor",
+    "SparseBackendsError", "Context", "Graph", "default_context", "DenseTensor", "NewBlockSparseSorted", "COOTensor",
     "AliasedBlockSparse", "contract_", "contract_bs_bs_to_dense", "blocksparse_from_dense", "coo_from_dense",
     "to_dense", "to_blocksparse", "permutedims", "sort_", "compression_ratio", "output_inds", "label_key",
     "to_uniform", "to_ragged", "norm", "dot", "inner", "copy", "similar", "scale_", "fill_", "map_", "axpy_",
@@ -128,11 +128,46 @@ class Context:
                                                       C.byref(fl), C.byref(by)))
         return dict(launches=n.value, ms=ms.value, flops=fl.value, bytes=by.value)
 
+    def capture(self, fn: Callable[[], Any], keep: Sequence[Any] = ()) -> "Graph":
+        """Capture the library calls that ``fn()`` makes on this context into a
+        CUDA graph (sb_ctx_capture_begin/end).  Run ``fn`` once eagerly before,
+        so that its outputs already have their storage.  ``keep``: tensors the
+        graph reads or writes; the Graph holds them so they outlive it."""
+        _check(self, self._lib.sb_ctx_capture_begin(self._h))
+        try:
+            fn()
+        finally:
+            g = C.c_void_p()
+            st = self._lib.sb_ctx_capture_end(self._h, C.byref(g))
+        _check(self, st)
+        return Graph(self, g, keep)
+
     def __del__(self):
         h = getattr(self, "_h", None)
         lib = getattr(self, "_lib", None)
         if h is not None and h.value and lib is not None:
             lib.sb_ctx_destroy(h)  # deferred by the library while tensors are alive
+            self._h = None
+
+
+class Graph:
+    """A captured sequence of library calls, replayed on its context's stream.
+    Each replay recomputes the captured outputs from the current device values
+    of the captured inputs (same tensors, same block structure)."""
+
+    def __init__(self, ctx: Context, handle: C.c_void_p, keep: Sequence[Any] = ()):
+        self.ctx = ctx
+        self._h = handle
+        self._keep = list(keep)
+
+    def launch(self) -> None:
+        _check(self.ctx, self.ctx._lib.sb_graph_launch(self.ctx._h, self._h))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        ctx = getattr(self, "ctx", None)
+        if h is not None and h.value and ctx is not None and getattr(ctx, "_lib", None) is not None:
+            ctx._lib.sb_graph_free(h)
             self._h = None
 
 

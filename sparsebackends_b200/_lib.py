@@ -57,6 +57,10 @@ SIGNATURES = {
     "sb_coo_from_dense": (C.c_int, [vp, vp, C.c_double, C.c_double, C.POINTER(vp)]),
     "sb_to_dense": (C.c_int, [vp, vp, C.POINTER(vp)]),
     "sb_aliased_to_blocksparse": (C.c_int, [vp, vp, C.POINTER(vp)]),
+    "sb_ctx_capture_begin": (C.c_int, [vp]),
+    "sb_ctx_capture_end": (C.c_int, [vp, C.POINTER(vp)]),
+    "sb_graph_launch": (C.c_int, [vp, vp]),
+    "sb_graph_free": (C.c_int, [vp]),
     "sb_tensor_norm": (C.c_int, [vp, vp, P_f64]),
     "sb_tensor_dot": (C.c_int, [vp, vp, vp, P_f64]),
     "sb_tensor_copy": (C.c_int, [vp, vp, C.POINTER(vp)]),

@@ -762,4 +762,95 @@ sb_status sb_fuse_axes(sb_ctx* ctx, const sb_tensor* A, int ax1, int ax2, sb_ten
   });
 }
 
+// ── CUDA graph capture ─────────────────────────────────────────────────────
+
+sb_status sb_ctx_capture_begin(sb_ctx* ctx) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    Ctx& c = ctx->impl;
+    require(!c.capturing, SB_ERR_INVALID_ARG, "a capture is already open on this context");
+    require(!c.profiling, SB_ERR_INVALID_ARG, "switch profiling off before capturing");
+    SB_CK(cudaSetDevice(c.device));
+    c.sync();  // staged plan uploads of earlier calls are complete
+    SB_CK(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeRelaxed));
+    c.capturing = true;
+    c.capture_keep.clear();
+    c.capture_keep_async.clear();
+  });
+}
+
+sb_status sb_ctx_capture_end(sb_ctx* ctx, sb_graph** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    Ctx& c = ctx->impl;
+    require(c.capturing, SB_ERR_INVALID_ARG, "no capture is open on this context");
+    SB_CK(cudaSetDevice(c.device));
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c.stream, &graph);
+    c.capturing = false;
+    (void)cudaGetLastError();  // an abandoned capture leaves its error as the last error: clear it
+    std::vector<void*> keep, keep_async;
+    keep.swap(c.capture_keep);
+    keep_async.swap(c.capture_keep_async);
+    // buffers released during the capture are freed only now that no graph
+    // will read them (the stream is idle: nothing captured ever ran)
+    auto drop = [&] {
+      if (graph) cudaGraphDestroy(graph);
+      for (void* p : keep) cudaFree(p);
+      for (void* p : keep_async) cudaFreeAsync(p, c.stream);
+    };
+    if (e != cudaSuccess || !graph) {
+      drop();
+      check_cuda(e != cudaSuccess ? e : cudaErrorStreamCaptureInvalidated, "cudaStreamEndCapture");
+    }
+    if (out == nullptr) {
+      drop();
+      fail(SB_ERR_INVALID_ARG, "out is NULL");
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    if (ei != cudaSuccess) {
+      drop();
+      check_cuda(ei, "cudaGraphInstantiate");
+    }
+    auto* g = new sb_graph;
+    g->owner = ctx;
+    g->graph = graph;
+    g->exec = exec;
+    g->keep = std::move(keep);
+    g->keep_async = std::move(keep_async);
+    ++c.live_tensors;
+    *out = g;
+  });
+}
+
+sb_status sb_graph_launch(sb_ctx* ctx, const sb_graph* g) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    require(g != nullptr && g->exec, SB_ERR_INVALID_ARG, "graph is NULL");
+    require(g->owner == ctx, SB_ERR_INVALID_ARG, "graph belongs to another context");
+    require(!ctx->impl.capturing, SB_ERR_INVALID_ARG, "cannot launch a graph while capturing");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    SB_CK(cudaGraphLaunch(g->exec, ctx->impl.stream));
+    ctx->impl.note_launch();
+  });
+}
+
+sb_status sb_graph_free(sb_graph* g) {
+  if (!g) return SB_OK;
+  sb_ctx* ctx = g->owner;
+  if (ctx) {
+    cudaSetDevice(ctx->impl.device);
+    cudaStreamSynchronize(ctx->impl.stream);
+  }
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  for (void* p : g->keep) cudaFree(p);
+  if (ctx)
+    for (void* p : g->keep_async) cudaFreeAsync(p, ctx->impl.stream);
+  delete g;
+  if (ctx && --ctx->impl.live_tensors == 0 && ctx->impl.destroy_pending) destroy_ctx_now(ctx);
+  return SB_OK;
+}
+
 }  // extern "C"

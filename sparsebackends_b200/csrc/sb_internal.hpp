@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <memory>
 #include <stdexcept>
@@ -50,6 +51,7 @@ class DevBuf {
   Ctx* ctx_ = nullptr;
   void* p_ = nullptr;
   size_t n_ = 0;
+  bool plain_ = false;  // cudaMalloc'd (allocated while a capture was open) instead of stream-ordered
 };
 
 // Kernel classes reported by the in-library profiler.
@@ -101,8 +103,17 @@ struct Ctx {
   void release_staging();
   // Tensors keep their context alive: sb_ctx_destroy with live tensors only
   // marks the context, and the last sb_tensor_free destroys it.
-  int64_t live_tensors = 0;
+  int64_t live_tensors = 0;  // tensors and graphs that still reference this context
   bool destroy_pending = false;
+  // Stream capture into a CUDA graph (sb_ctx_capture_begin/end).  While a
+  // capture is open, new device buffers are plain cudaMalloc allocations
+  // (plan arrays are filled by synchronous copies outside the captured
+  // stream), and every buffer released is handed to the graph instead of
+  // being freed: the captured kernels may read it on every replay, so it lives
+  // until sb_graph_free.
+  bool capturing = false;
+  std::vector<void*> capture_keep;        // plain buffers, cudaFree at graph free
+  std::vector<void*> capture_keep_async;  // stream-ordered buffers, cudaFreeAsync at graph free
   void note_launch(int64_t n = 1) { launches += n; }
   void sync();
   void clear_profile();
@@ -125,6 +136,12 @@ class ProfScope {
 template <class T>
 DevBuf upload(Ctx* ctx, const std::vector<T>& v) {
   DevBuf b(ctx, v.size() * sizeof(T));
+  if (ctx->capturing) {
+    // outside the captured stream: the plan is on the device before any replay
+    if (!v.empty()) check_cuda(cudaMemcpy(b.raw(), v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice),
+                               "capture plan copy");
+    return b;
+  }
   if (!v.empty()) ctx->stage_copy(b.raw(), v.data(), v.size() * sizeof(T));
   return b;
 }
@@ -266,6 +283,12 @@ void contract(Ctx* ctx, Tensor& C, const Labels& lC, const Tensor& A, const Labe
 
 struct sb_ctx {
   sb::Ctx impl;
+};
+struct sb_graph {
+  sb_ctx* owner = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<void*> keep, keep_async;  // buffers the captured kernels may read
 };
 struct sb_tensor {
   sb::TensorPtr impl;

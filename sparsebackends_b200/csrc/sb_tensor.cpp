@@ -67,7 +67,7 @@ void Ctx::clear_profile() {
 }
 
 ProfScope::ProfScope(Ctx* c, int kind, double flops, double bytes) : c_(c), kind_(kind), flops_(flops), bytes_(bytes) {
-  if (!c_->profiling) return;
+  if (!c_->profiling || c_->capturing) return;
   SB_CK(cudaEventCreate(&a_));
   SB_CK(cudaEventRecord(a_, c_->stream));
 }
@@ -83,13 +83,28 @@ ProfScope::~ProfScope() {
 }
 
 DevBuf::DevBuf(Ctx* ctx, size_t bytes) : ctx_(ctx), n_(bytes) {
-  if (bytes) SB_CK(cudaMallocAsync(&p_, bytes, ctx->stream));
+  if (!bytes) return;
+  if (ctx->capturing) {
+    SB_CK(cudaMalloc(&p_, bytes));
+    plain_ = true;
+  } else {
+    SB_CK(cudaMallocAsync(&p_, bytes, ctx->stream));
+  }
 }
 DevBuf::~DevBuf() { reset(); }
 void DevBuf::reset() {
-  if (p_) cudaFreeAsync(p_, ctx_->stream);
+  if (p_) {
+    if (ctx_->capturing) {
+      (plain_ ? ctx_->capture_keep : ctx_->capture_keep_async).push_back(p_);
+    } else if (plain_) {
+      cudaFree(p_);
+    } else {
+      cudaFreeAsync(p_, ctx_->stream);
+    }
+  }
   p_ = nullptr;
   n_ = 0;
+  plain_ = false;
 }
 DevBuf& DevBuf::operator=(DevBuf&& o) noexcept {
   if (this != &o) {
@@ -97,8 +112,10 @@ DevBuf& DevBuf::operator=(DevBuf&& o) noexcept {
     ctx_ = o.ctx_;
     p_ = o.p_;
     n_ = o.n_;
+    plain_ = o.plain_;
     o.p_ = nullptr;
     o.n_ = 0;
+    o.plain_ = false;
   }
   return *this;
 }

@@ -276,15 +276,26 @@ class HeffOperator:
     each call runs the four-contraction chain and copies the result out of the
     chain's reused output buffer."""
 
-    def __init__(self, layout: HeffLayout, L, W1, W2, R, ctx=None):
+    def __init__(self, layout: HeffLayout, L, W1, W2, R, ctx=None, graph_like=None):
+        """With ``graph_like`` (a vector with the layout of the inputs to come)
+        the chain is captured once as a CUDA graph on a private input buffer;
+        each call copies its input there and replays the graph."""
         import sparsebackends_b200 as sb
         self.sb = sb
         self.chain = HeffChain(layout, ctx)
         self.ops = (L, W1, W2, R)
         self.calls = 0
+        self.graph = None
+        if graph_like is not None:
+            self.x = sb.copy(graph_like)
+            self.graph = self.chain.capture(self.x, *self.ops)
 
     def __call__(self, psi):
         self.calls += 1
+        if self.graph is not None:
+            self.sb.map_(self.x, psi, self.sb.MAP_COPY)
+            self.graph.launch()
+            return self.sb.copy(self.chain.out["T4"])
         return self.sb.copy(self.chain.apply(psi, *self.ops))
 
 
@@ -350,6 +361,15 @@ class HeffChain:
         for c, a, b in self.STEPS:
             self.sb.contract_(t[c], lab[c], t[a], lab[a], t[b], lab[b])
         return self.out["T4"]
+
+    def capture(self, psi, L, W1, W2, R):
+        """Run the chain once, then capture it as one CUDA graph bound to these
+        tensors.  ``graph.launch()`` recomputes ``self.out["T4"]`` from the
+        current values of ``psi`` (and of the operators): the per-call host
+        planning and plan uploads are paid once, at capture."""
+        self.apply(psi, L, W1, W2, R)
+        return psi.ctx.capture(lambda: self.apply(psi, L, W1, W2, R),
+                               keep=[psi, L, W1, W2, R, *self.out.values()])
 
 
 GRADE = {"ml": "ql", "mlp": "qlp", "mr": "qr", "mrp": "qrp", "mwl": "qwl", "mwm": "qwm", "mwr": "qwr"}
