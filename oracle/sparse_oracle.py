@@ -520,8 +520,15 @@ def _advance_run(keys: List[Key], i0: int, n: int, pos: List[int]) -> int:
 
 
 def _cmp_join(akey, bkey, posA, posB) -> int:
-    """``_cmp_join_tuple`` (contract_bs_bs.jl:430-442)."""
-    for pa, pb in zip(posA, posB):
+    """``_cmp_join_tuple`` (contract_bs_bs.jl:430-442), with one correction.
+
+    The join axes are the last prefix axes of the permuted operands and keys
+    are sorted column-major, so the last join axis is the most significant; the
+    reference compares the first one first, and with two or more join axes
+    whose value sets differ between the operands its merge skips matched pairs.
+    Comparing from the last join axis down keeps the merge consistent with the
+    sort; wherever the reference's merge finds every match the two agree."""
+    for pa, pb in reversed(list(zip(posA, posB))):
         av, bv = akey[pa - 1], bkey[pb - 1]
         if av < bv:
             return -1

@@ -590,8 +590,15 @@ SharedPlan plan_shared(const Labels& lC, int PC, const Op& A, const Op& B, const
   return sp;
 }
 
+// Order of two keys on their join tuples.  The operands are permuted so that
+// the join axes are the last prefix axes, and keys are sorted column-major,
+// so the LAST join axis is the most significant: compare from it down.  (The
+// reference's _cmp_join_tuple, contract_bs_bs.jl:430-442, compares the first
+// join axis first; with two or more join axes whose value sets differ between
+// A and B its merge loses matched pairs.  Where it loses none, both orders
+// visit the same runs in the same order.)
 int cmp_join(const int64_t* a, const int64_t* b, const std::vector<int>& pa, const std::vector<int>& pb) {
-  for (size_t t = 0; t < pa.size(); ++t) {
+  for (size_t t = pa.size(); t-- > 0;) {
     const int64_t x = a[pa[t] - 1], y = b[pb[t] - 1];
     if (x < y) return -1;
     if (x > y) return 1;

@@ -133,3 +133,17 @@ def test_vector_ops_on_empty(sb):
     sb.scale_(e, 2.0)
     sb.fill_(e, 1.0)
     assert e.keys == []
+
+
+def test_two_label_join_with_unequal_tuple_sets(sb):
+    """Two shared prefix labels whose (w, s) value sets differ between A and B:
+    every matched pair contributes (the merge compares in key-sort order)."""
+    rng = np.random.Generator(np.random.PCG64(3))
+    Ad = np.zeros((2, 3, 2, 4))
+    Ad[:, 1] = rng.standard_normal((2, 2, 4))
+    Bd = rng.standard_normal((3, 2, 3, 5))
+    A, B = so.blocksparse_from_dense(Ad, 1), so.blocksparse_from_dense(Bd, 1)
+    Cg, Cref = _run(sb, so.BS.empty((2, 3, 4, 5), 2), ["p", "t", "m", "n"], A, ["p", "w", "s", "m"], B,
+                    ["w", "s", "t", "n"])
+    assert_bs_equal(Cg, Cref)
+    assert rel_err(sb.to_dense(Cg), np.einsum("pwsm,wstn->ptmn", Ad, Bd)) <= 1e-13
