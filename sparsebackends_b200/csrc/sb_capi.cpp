@@ -106,6 +106,7 @@ sb_status sb_ctx_create(int device, unsigned flags, sb_ctx** out) {
       else if (v == "64x32") c->impl.gemm_tile = 5;
     }
     if (const char* th = std::getenv("SPARSEB_GEMM_THIN")) c->impl.gemm_thin = std::atoi(th);
+    if (const char* ge = std::getenv("SPARSEB_GEMM_EDGES")) c->impl.gemm_edges = std::atoi(ge);
     if (const char* sk = std::getenv("SPARSEB_GEMM_SPLITK")) c->impl.gemm_splitk = std::max(0, std::atoi(sk));
     // Keep freed device memory cached in the stream-ordered pool.
     cudaMemPool_t pool;
@@ -545,13 +546,16 @@ sb_status sb_contract(sb_ctx* ctx, sb_tensor* C, const uint64_t* labelsC, int nC
     check_t(B);
     SB_CK(cudaSetDevice(ctx->impl.device));
     const auto t0 = std::chrono::steady_clock::now();
+    ctx->impl.gemm_desc[0] = '\0';
     contract(&ctx->impl, *C->impl, read_labels(labelsC, nC), *A->impl, read_labels(labelsA, nA), *B->impl,
              read_labels(labelsB, nB));
     if (ctx->impl.trace) {
       const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-      std::fprintf(stderr, "[sparseb] %s  A(kind=%d, keys=%lld) x B(kind=%d, keys=%lld) -> C(keys=%lld)  host %.3f ms\n",
+      std::fprintf(stderr,
+                   "[sparseb] %s  A(kind=%d, keys=%lld) x B(kind=%d, keys=%lld) -> C(keys=%lld)  host %.3f ms%s%s\n",
                    ctx->impl.kernel_name, A->impl->kind, static_cast<long long>(A->impl->nkeys), B->impl->kind,
-                   static_cast<long long>(B->impl->nkeys), static_cast<long long>(C->impl->nkeys), ms);
+                   static_cast<long long>(B->impl->nkeys), static_cast<long long>(C->impl->nkeys), ms,
+                   ctx->impl.gemm_desc[0] ? "  gemm: " : "", ctx->impl.gemm_desc);
     }
   });
 }

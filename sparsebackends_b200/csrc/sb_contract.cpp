@@ -22,6 +22,7 @@
 //   bs_bs_to_dense()           contract_bs_bs.jl:736-754
 #include <algorithm>
 #include <climits>
+#include <cstdio>
 #include <map>
 #include <numeric>
 #include <unordered_map>
@@ -205,7 +206,8 @@ struct GemmPlan {
   void add_cblock(int64_t c_off, int64_t M, int64_t N) {
     require(M < (1LL << 31) && N < (1LL << 31), SB_ERR_INVALID_ARG, "block matrix extent exceeds 2^31");
     cbs.push_back(GemmCBlock{c_off, static_cast<int32_t>(M), static_cast<int32_t>(N),
-                             static_cast<int32_t>(pairs.size()), static_cast<int32_t>(pairs.size()), 0, 1});
+                             static_cast<int32_t>(pairs.size()), static_cast<int32_t>(pairs.size()), 0, 1,
+                             static_cast<int32_t>(M), 0});
   }
   void add_pair(int64_t x_off, int64_t y_off, int64_t K, int64_t ldx, int64_t ldy) {
     require(K < (1LL << 31) && ldx < (1LL << 31) && ldy < (1LL << 31), SB_ERR_INVALID_ARG,
@@ -236,6 +238,7 @@ struct GemmPlan {
     const bool skinny_m = Kmax <= 16 && M <= 16;
     if ((skinny_n || skinny_m) && ctx->gemm_tile < 0 && ctx->gemm_thin != 0) {
       const bool small_rows = skinny_m;
+      const bool interleaved = interleave_shared_long(small_rows, xT, yT);
       bool every_block_has_pairs = true;
       for (auto& c : cbs) every_block_has_pairs = every_block_has_pairs && c.pair_end > c.pair_begin;
       int64_t nctas = 0;
@@ -245,12 +248,15 @@ struct GemmPlan {
         c.mtiles = 1;
         nctas += (bigx + 127) / 128;
       }
+      const bool persistent = ctx->gemm_thin != 1 && every_block_has_pairs;
+      std::snprintf(ctx->gemm_desc, sizeof(ctx->gemm_desc), "thin%s %s%s", persistent ? " persistent" : "",
+                    small_rows ? "rows<=16" : "cols<=16", interleaved ? " interleaved" : "");
       DevBuf dc = upload(ctx, cbs), dp = upload(ctx, pairs);
       {
         ProfScope ps(ctx, PROF_GEMM_THIN, flops, bytes);
         SB_CK(launch_gemm_f64_skinny(X, Y, C, dc.as<GemmCBlock>(), static_cast<int32_t>(cbs.size()), dp.as<GemmPair>(),
                                      nctas, xT, yT, small_rows, static_cast<int>(small_rows ? M : N),
-                                     static_cast<int>(Kmax), ctx->stream, ctx->gemm_thin != 1 && every_block_has_pairs));
+                                     static_cast<int>(Kmax), ctx->stream, persistent));
       }
       ctx->note_launch();
       return;
@@ -271,6 +277,8 @@ struct GemmPlan {
     if (an <= 32 && am >= 128) shape = GemmShape::T128x32;
     else if (am <= 32 && an >= 128) shape = GemmShape::T32x128;
     else if (am >= 1024 && an >= 512) shape = am >= an ? GemmShape::T128x64 : GemmShape::T64x128;
+    if (shape == GemmShape::T64x64 && ctx->gemm_tile < 0 && ctx->gemm_edges != 0 && launch_edges(ctx, X, Y, C, xT, yT, flops, bytes))
+      return;
     if (shape == GemmShape::T64x64) {
       // few 64x64 tiles with long K (the split-K regime): smaller tiles with a
       // deeper pipeline keep more CTAs busy
@@ -302,10 +310,8 @@ struct GemmPlan {
       kt_avg += kt * ((c.M + bm - 1) / bm) * ((c.N + bn - 1) / bn);
     }
     kt_avg = ntiles ? kt_avg / ntiles : 0;
-    int splitk = 1;
-    const int64_t wave = 148 * 4;
-    while (splitk < 16 && ntiles * splitk < 3 * wave && kt_avg / (2 * splitk) >= 32) splitk *= 2;
-    if (ctx->gemm_splitk > 0) splitk = ctx->gemm_splitk;
+    const int splitk = choose_splitk(ctx, ntiles, kt_avg);
+    std::snprintf(ctx->gemm_desc, sizeof(ctx->gemm_desc), "tiled %dx%d sk%d", bm, bn, splitk);
     DevBuf dc = upload(ctx, cbs), dp = upload(ctx, pairs);
     DevBuf part;
     if (splitk > 1) part = DevBuf(ctx, static_cast<size_t>(splitk) * ntiles * bm * bn * sizeof(double));
@@ -315,6 +321,189 @@ struct GemmPlan {
                             xT, yT, shape, ctx->stream, splitk, part.d()));
     }
     ctx->note_launch(splitk > 1 ? 2 : 1);
+  }
+
+  // Thin launches (K <= 16): output blocks whose pairs read the same block of
+  // the long operand (the MPO steps of H_eff, where one T1 block feeds up to
+  // two output blocks) are cut into chunks of kThinChunk long-side elements
+  // and emitted chunk by chunk in turn, so that the second read of a long
+  // chunk follows the first within a few MB of traffic and hits L2 (126 MB)
+  // instead of DRAM.  Row chunks keep the parent's ldc.  Returns whether
+  // anything was reordered.
+  static constexpr int64_t kThinChunk = 256 * 128;
+  bool interleave_shared_long(bool small_rows, bool xT, bool yT) {
+    const int n = static_cast<int>(cbs.size());
+    std::vector<int> parent(n);
+    std::iota(parent.begin(), parent.end(), 0);
+    auto root = [&](int c) {
+      while (parent[c] != c) c = parent[c] = parent[parent[c]];
+      return c;
+    };
+    std::unordered_map<int64_t, int> user;  // long-operand block offset -> first C block reading it
+    bool shared = false;
+    for (int c = 0; c < n; ++c)
+      for (int p = cbs[c].pair_begin; p < cbs[c].pair_end; ++p) {
+        const int64_t off = small_rows ? pairs[p].y_off : pairs[p].x_off;
+        auto it = user.emplace(off, c);
+        if (it.second) continue;
+        const int a = root(c), b = root(it.first->second);
+        if (a != b) {
+          parent[std::max(a, b)] = std::min(a, b);
+          shared = true;
+        }
+      }
+    if (!shared) return false;
+    std::vector<std::vector<int>> comps;
+    std::vector<int> comp_of(n, -1);
+    for (int c = 0; c < n; ++c) {
+      const int r = root(c);
+      if (comp_of[r] < 0) {
+        comp_of[r] = static_cast<int>(comps.size());
+        comps.emplace_back();
+      }
+      comps[comp_of[r]].push_back(c);
+    }
+    std::vector<GemmCBlock> nc;
+    std::vector<GemmPair> np;
+    nc.reserve(cbs.size());
+    np.reserve(pairs.size());
+    for (auto& comp : comps) {
+      int64_t lmax = 0;
+      for (int c : comp) lmax = std::max<int64_t>(lmax, small_rows ? cbs[c].N : cbs[c].M);
+      const int64_t step = comp.size() > 1 ? kThinChunk : std::max<int64_t>(lmax, 1);
+      for (int64_t l0 = 0; l0 < std::max<int64_t>(lmax, 1); l0 += step)
+        for (int c : comp) {
+          const GemmCBlock& b = cbs[c];
+          const int64_t L = small_rows ? b.N : b.M;
+          if (l0 > 0 && l0 >= L) continue;
+          const int32_t len = static_cast<int32_t>(std::min<int64_t>(step, L - l0));
+          GemmCBlock s = b;
+          if (small_rows) {
+            s.c_off = b.c_off + l0 * b.ldc;
+            s.N = len;
+          } else {
+            s.c_off = b.c_off + l0;
+            s.M = len;
+          }
+          s.pair_begin = static_cast<int32_t>(np.size());
+          for (int p = b.pair_begin; p < b.pair_end; ++p) {
+            GemmPair q = pairs[p];
+            if (small_rows) q.y_off += yT ? l0 : l0 * q.ldy;
+            else q.x_off += xT ? l0 * q.ldx : l0;
+            np.push_back(q);
+          }
+          s.pair_end = static_cast<int32_t>(np.size());
+          nc.push_back(s);
+        }
+    }
+    require(np.size() < (1ULL << 31), SB_ERR_INVALID_ARG, "too many GEMM block pairs in one launch");
+    cbs.swap(nc);
+    pairs.swap(np);
+    return true;
+  }
+
+  // Split-K factor for ntiles tiles averaging kt_avg k-tiles: split while the
+  // tiles fill less than ~3 waves of 148 SMs x 4 CTAs and every segment keeps
+  // >= 32 k-tiles.
+  static int choose_splitk(Ctx* ctx, int64_t ntiles, int64_t kt_avg) {
+    int splitk = 1;
+    const int64_t wave = 148 * 4;
+    while (splitk < 16 && ntiles * splitk < 3 * wave && kt_avg / (2 * splitk) >= 32) splitk *= 2;
+    if (ctx->gemm_splitk > 0) splitk = ctx->gemm_splitk;
+    return splitk;
+  }
+  // 64x64 tiles with the edges cut off: a column edge of width N % 64 <= 32
+  // (the whole block when N <= 32) goes to 64x32 tiles, a row edge of height
+  // M % 64 <= 32 to 32x64 tiles, one launch for all three (ragged sector
+  // extents: 1.165 -> 1.092 executed/algorithmic FLOPs on the chi=2048 R*T3
+  // step).  Returns false, launching nothing, when that saves < 3% of the
+  // padded 64x64 work.
+  bool launch_edges(Ctx* ctx, const double* X, const double* Y, double* C, bool xT, bool yT, double flops,
+                    double bytes) {
+    auto up = [](int64_t v, int64_t t) { return (v + t - 1) / t * t; };
+    auto rows64 = [](int64_t M) { const int64_t e = M % 64; return e > 0 && e <= 32 ? M - e : M; };
+    double w64 = 0.0, wseg = 0.0;
+    for (auto& c : cbs) {
+      int64_t kt = 0;
+      for (int p = c.pair_begin; p < c.pair_end; ++p) kt += (pairs[p].K + 15) / 16;
+      kt = std::max<int64_t>(kt, 1);
+      const int64_t mm = rows64(c.M), nm = rows64(c.N);
+      w64 += static_cast<double>(up(c.M, 64) * up(c.N, 64)) * kt;
+      wseg += static_cast<double>(up(mm, 64) * up(nm, 64) + up(c.M, 64) * up(c.N - nm, 32) +
+                                  (nm > 0 ? up(c.M - mm, 32) * up(nm, 64) : 0)) * kt;
+    }
+    if (!(wseg < 0.97 * w64)) return false;
+    // Sub-blocks of one C block stay adjacent (its tiles run together and
+    // share the operand panels in L2: ragged chi=2048 L*psi reads 405 MB
+    // instead of 657 MB): body, column edge, row edge.
+    std::vector<GemmCBlock> sc;
+    std::vector<GemmPair> ep(pairs);
+    sc.reserve(cbs.size() * 3);
+    int64_t ntiles = 0, kts = 0;
+    for (auto& c : cbs) {
+      int64_t kt = 0;
+      for (int p = c.pair_begin; p < c.pair_end; ++p) kt += (pairs[p].K + 15) / 16;
+      const int32_t mm = static_cast<int32_t>(rows64(c.M)), nm = static_cast<int32_t>(rows64(c.N));
+      auto sub = [&](int32_t shape, int32_t r0, int32_t c0, int32_t rows, int32_t cols) {
+        const int bm = shape == 2 ? 32 : 64, bn = shape == 1 ? 32 : 64;
+        GemmCBlock s{c.c_off + r0 + static_cast<int64_t>(c0) * c.ldc, rows, cols, c.pair_begin, c.pair_end, 0, 0,
+                     c.ldc, shape};
+        if (r0 != 0 || c0 != 0) {
+          s.pair_begin = static_cast<int32_t>(ep.size());
+          for (int p = c.pair_begin; p < c.pair_end; ++p) {
+            GemmPair q = pairs[p];
+            q.x_off += xT ? static_cast<int64_t>(r0) * q.ldx : r0;
+            q.y_off += yT ? c0 : static_cast<int64_t>(c0) * q.ldy;
+            ep.push_back(q);
+          }
+          s.pair_end = static_cast<int32_t>(ep.size());
+        }
+        const int64_t mt = (rows + bm - 1) / bm, ntl = (cols + bn - 1) / bn;
+        require(ntiles + mt * ntl < (1LL << 31), SB_ERR_INVALID_ARG, "too many GEMM tiles in one launch");
+        s.tile_begin = static_cast<int32_t>(ntiles);
+        s.mtiles = static_cast<int32_t>(mt);
+        ntiles += mt * ntl;
+        kts += mt * ntl * kt;
+        sc.push_back(s);
+      };
+      if (mm > 0 && nm > 0) sub(0, 0, 0, mm, nm);
+      if (nm < c.N) sub(1, 0, nm, c.M, c.N - nm);
+      if (mm < c.M && nm > 0) sub(2, mm, 0, c.M - mm, nm);
+    }
+    require(ep.size() < (1ULL << 31), SB_ERR_INVALID_ARG, "too many GEMM block pairs in one launch");
+    const int64_t kt_avg = ntiles ? kts / ntiles : 0;
+    if (kt_avg >= 64) {
+      // Long K loops: the tiles that share an operand panel stream it in
+      // step only when they advance at one speed, so tiles of one shape run
+      // together: all bodies, then all column edges, then all row edges
+      // (zero-padded chi=2048 R*T3: 8.5 against 14.7 GB read, 7.98 against
+      // 8.48 ms).
+      std::stable_sort(sc.begin(), sc.end(),
+                       [](const GemmCBlock& a, const GemmCBlock& b) { return a.tshape < b.tshape; });
+      ntiles = 0;
+      for (auto& b : sc) {
+        const int64_t bn = b.tshape == 1 ? 32 : 64;
+        b.tile_begin = static_cast<int32_t>(ntiles);
+        ntiles += static_cast<int64_t>(b.mtiles) * ((b.N + bn - 1) / bn);
+      }
+    }
+    const int splitk = choose_splitk(ctx, ntiles, kt_avg);
+    int64_t nshape[3] = {0, 0, 0};
+    for (auto& b : sc) nshape[b.tshape] += static_cast<int64_t>(b.mtiles) *
+                                           ((b.N + (b.tshape == 1 ? 31 : 63)) / (b.tshape == 1 ? 32 : 64));
+    std::snprintf(ctx->gemm_desc, sizeof(ctx->gemm_desc), "edges 64x64:%lld 64x32:%lld 32x64:%lld sk%d",
+                  static_cast<long long>(nshape[0]), static_cast<long long>(nshape[1]),
+                  static_cast<long long>(nshape[2]), splitk);
+    DevBuf dc = upload(ctx, sc), dp = upload(ctx, ep);
+    DevBuf part;
+    if (splitk > 1) part = DevBuf(ctx, static_cast<size_t>(splitk) * ntiles * 64 * 64 * sizeof(double));
+    {
+      ProfScope ps(ctx, PROF_GEMM, flops, bytes);
+      SB_CK(launch_gemm_f64_edges(X, Y, C, dc.as<GemmCBlock>(), static_cast<int32_t>(sc.size()), dp.as<GemmPair>(),
+                                  ntiles, xT, yT, ctx->stream, splitk, part.d()));
+    }
+    ctx->note_launch(splitk > 1 ? 2 : 1);
+    return true;
   }
 };
 

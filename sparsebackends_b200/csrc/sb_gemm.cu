@@ -5,6 +5,7 @@
 // Y are staged into shared memory by a 3-stage cp.async pipeline that runs
 // straight across the pairs of one C block (the K loops of all pairs feeding a
 // C tile are concatenated), so one CTA owns one C tile and writes it once.
+#include <algorithm>
 #include <cstdio>
 
 #include "../../include/sparseb.h"
@@ -48,11 +49,23 @@ struct TileLayout {
   __device__ static int yidx(int k, int j) { return YT ? k * (BN + 4) + j : j * KP + k; }
 };
 
-template <int BM, int BN, int WM, int WN, bool XT, bool YT, int BK = kBK, int ST = kStages>
-__global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32, 512 / ((BM / WM) * (BN / WN) * 32))
-    k_gemm_f64(const double* __restrict__ X, const double* __restrict__ Y, double* __restrict__ C,
-               const GemmCBlock* __restrict__ cblocks, int32_t ncb, const GemmPair* __restrict__ pairs,
-               int32_t splitk, int32_t ntiles, double* __restrict__ partial) {
+// C block of tile `bid`: the last c with tile_begin <= bid.
+__device__ __forceinline__ int tile_cblock(const GemmCBlock* __restrict__ cblocks, int32_t ncb, int bid) {
+  int lo = 0, hi = ncb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (cblocks[mid].tile_begin <= bid) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// One CTA of the tiled GEMM: tile lt of C block cb, k-segment seg of splitk;
+// with splitk > 1 the BM x BN tile goes to pt (column-major) instead of C.
+template <int BM, int BN, int WM, int WN, bool XT, bool YT, int BK, int ST>
+__device__ __forceinline__ void gemm_cta(const double* __restrict__ X, const double* __restrict__ Y,
+                                         double* __restrict__ C, const GemmCBlock& cb,
+                                         const GemmPair* __restrict__ pairs, int lt, int seg, int32_t splitk,
+                                         double* __restrict__ pt, double* smem) {
   constexpr int kBK = BK;
   constexpr int kStages = ST;
   using TL = TileLayout<BM, BN, XT, YT, BK, ST>;
@@ -65,23 +78,10 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32, 512 / ((BM / WM) *
   constexpr int YLOADS = BN * kBK / NT;
   static_assert(BM * kBK % NT == 0 && BN * kBK % NT == 0, "tile/threads mismatch");
 
-  extern __shared__ double smem[];
   double* Xs = smem;                    // kStages tiles of TL::XSZ
   double* Ys = smem + kStages * TL::XSZ;  // kStages tiles of TL::YSZ
 
-  // Split-K: CTA = (segment, tile), segments outermost so that concurrently
-  // running CTAs work on the same K range of neighbouring tiles.
-  const int seg = static_cast<int>(blockIdx.x) / ntiles;
-  const int bid = static_cast<int>(blockIdx.x) % ntiles;
-  // C block of this CTA: last c with tile_begin <= bid
-  int lo = 0, hi = ncb - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (cblocks[mid].tile_begin <= bid) lo = mid; else hi = mid - 1;
-  }
-  const GemmCBlock cb = cblocks[lo];
   const int M = cb.M, N = cb.N;
-  const int lt = bid - cb.tile_begin;
   const int m0 = (lt % cb.mtiles) * BM, n0 = (lt / cb.mtiles) * BN;
   const int tid = threadIdx.x;
 
@@ -235,7 +235,6 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32, 512 / ((BM / WM) *
 
   if (splitk > 1) {
     // partial tile, column-major BM x BN, reduced by k_splitk_reduce
-    double* pt = partial + (static_cast<int64_t>(seg) * ntiles + bid) * (BM * BN);
 #pragma unroll
     for (int a = 0; a < MT; ++a) {
       const int rl = wm * WM + a * 8 + g;
@@ -256,34 +255,91 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32, 512 / ((BM / WM) *
 #pragma unroll
     for (int b = 0; b < NTL; ++b) {
       const int col = n0 + wn * WN + b * 8 + 2 * t;
-      if (col < N) cbase[row + (int64_t)col * M] = acc[a][b][0];
-      if (col + 1 < N) cbase[row + (int64_t)(col + 1) * M] = acc[a][b][1];
+      if (col < N) cbase[row + (int64_t)col * cb.ldc] = acc[a][b][0];
+      if (col + 1 < N) cbase[row + (int64_t)(col + 1) * cb.ldc] = acc[a][b][1];
     }
   }
 }
 
+// Split-K: CTA = (segment, tile), segments outermost so that concurrently
+// running CTAs work on the same K range of neighbouring tiles.
+template <int BM, int BN, int WM, int WN, bool XT, bool YT, int BK = kBK, int ST = kStages>
+__global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32, 512 / ((BM / WM) * (BN / WN) * 32))
+    k_gemm_f64(const double* __restrict__ X, const double* __restrict__ Y, double* __restrict__ C,
+               const GemmCBlock* __restrict__ cblocks, int32_t ncb, const GemmPair* __restrict__ pairs,
+               int32_t splitk, int32_t ntiles, double* __restrict__ partial) {
+  extern __shared__ double smem[];
+  const int seg = static_cast<int>(blockIdx.x) / ntiles;
+  const int bid = static_cast<int>(blockIdx.x) % ntiles;
+  const GemmCBlock cb = cblocks[tile_cblock(cblocks, ncb, bid)];
+  double* pt = splitk > 1 ? partial + (static_cast<int64_t>(seg) * ntiles + bid) * (BM * BN) : nullptr;
+  gemm_cta<BM, BN, WM, WN, XT, YT, BK, ST>(X, Y, C, cb, pairs, bid - cb.tile_begin, seg, splitk, pt, smem);
+}
+
+// Three tile shapes in one launch (launch_gemm_f64_edges): the tiles of every
+// C sub-block are numbered consecutively through tile_begin as usual, and the
+// sub-block's tshape picks the CTA's tile: 0 = 64x64 (32x32 warp tiles),
+// 1 = 64x32 (32x16), 2 = 32x64 (16x32), all four warps and 3 stages.
+// Partial tiles of split-K are kEdgePart doubles apart whatever their shape.
+constexpr int kEdgeThreads = 128;
+constexpr int kEdgePart = 64 * 64;
+template <bool XT, bool YT>
+__global__ void __launch_bounds__(kEdgeThreads, 4)
+    k_gemm_f64_edges(const double* __restrict__ X, const double* __restrict__ Y, double* __restrict__ C,
+                     const GemmCBlock* __restrict__ cblocks, int32_t ncb, const GemmPair* __restrict__ pairs,
+                     int32_t splitk, int32_t ntiles, double* __restrict__ partial) {
+  extern __shared__ double smem[];
+  const int seg = static_cast<int>(blockIdx.x) / ntiles;
+  const int bid = static_cast<int>(blockIdx.x) % ntiles;
+  const GemmCBlock cb = cblocks[tile_cblock(cblocks, ncb, bid)];
+  double* pt = splitk > 1 ? partial + (static_cast<int64_t>(seg) * ntiles + bid) * kEdgePart : nullptr;
+  const int lt = bid - cb.tile_begin;
+  if (cb.tshape == 0)
+    gemm_cta<64, 64, 32, 32, XT, YT, kBK, kStages>(X, Y, C, cb, pairs, lt, seg, splitk, pt, smem);
+  else if (cb.tshape == 1)
+    gemm_cta<64, 32, 32, 16, XT, YT, kBK, kStages>(X, Y, C, cb, pairs, lt, seg, splitk, pt, smem);
+  else
+    gemm_cta<32, 64, 16, 32, XT, YT, kBK, kStages>(X, Y, C, cb, pairs, lt, seg, splitk, pt, smem);
+}
+
 // Deterministic split-K reduction: C tile = sum over segments in order.
+// Element e: tile e / stride, offset e % stride in the column-major BM x BN
+// partial tile.
+__device__ __forceinline__ void splitk_reduce_elem(double* __restrict__ C, const GemmCBlock& cb, int bm, int bn,
+                                                   int lt, int w, int32_t splitk, int64_t seg_stride,
+                                                   const double* __restrict__ pt) {
+  if (w >= bm * bn) return;
+  const int rl = w % bm, cl = w / bm;
+  const int row = (lt % cb.mtiles) * bm + rl, col = (lt / cb.mtiles) * bn + cl;
+  if (row >= cb.M || col >= cb.N) return;
+  double acc = 0.0;
+  for (int sg = 0; sg < splitk; ++sg) acc += pt[sg * seg_stride + w];
+  C[cb.c_off + row + static_cast<int64_t>(col) * cb.ldc] = acc;
+}
+
 template <int BM, int BN>
 __global__ void k_splitk_reduce(double* __restrict__ C, const GemmCBlock* __restrict__ cblocks, int32_t ncb,
                                 int32_t splitk, int32_t ntiles, const double* __restrict__ partial) {
   const int64_t total = static_cast<int64_t>(ntiles) * BM * BN;
   for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
        e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int bid = static_cast<int>(e / (BM * BN));
-    const int w = static_cast<int>(e % (BM * BN));
-    const int rl = w % BM, cl = w / BM;
-    int lo = 0, hi = ncb - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (cblocks[mid].tile_begin <= bid) lo = mid; else hi = mid - 1;
-    }
-    const GemmCBlock cb = cblocks[lo];
-    const int lt = bid - cb.tile_begin;
-    const int row = (lt % cb.mtiles) * BM + rl, col = (lt / cb.mtiles) * BN + cl;
-    if (row >= cb.M || col >= cb.N) continue;
-    double acc = 0.0;
-    for (int sg = 0; sg < splitk; ++sg) acc += partial[(static_cast<int64_t>(sg) * ntiles + bid) * (BM * BN) + w];
-    C[cb.c_off + row + static_cast<int64_t>(col) * cb.M] = acc;
+    const int bid = static_cast<int>(e / (BM * BN)), w = static_cast<int>(e % (BM * BN));
+    const GemmCBlock cb = cblocks[tile_cblock(cblocks, ncb, bid)];
+    splitk_reduce_elem(C, cb, BM, BN, bid - cb.tile_begin, w, splitk, static_cast<int64_t>(ntiles) * BM * BN,
+                       partial + static_cast<int64_t>(bid) * BM * BN);
+  }
+}
+
+__global__ void k_splitk_reduce_edges(double* __restrict__ C, const GemmCBlock* __restrict__ cblocks, int32_t ncb,
+                                      int32_t splitk, int32_t ntiles, const double* __restrict__ partial) {
+  const int64_t total = static_cast<int64_t>(ntiles) * kEdgePart;
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int bid = static_cast<int>(e / kEdgePart), w = static_cast<int>(e % kEdgePart);
+    const GemmCBlock cb = cblocks[tile_cblock(cblocks, ncb, bid)];
+    const int bm = cb.tshape == 2 ? 32 : 64, bn = cb.tshape == 1 ? 32 : 64;
+    splitk_reduce_elem(C, cb, bm, bn, bid - cb.tile_begin, w, splitk, static_cast<int64_t>(ntiles) * kEdgePart,
+                       partial + static_cast<int64_t>(bid) * kEdgePart);
   }
 }
 
@@ -494,10 +550,10 @@ __global__ void __launch_bounds__(kThinThreads, 5)
   double* cbase = C + cb.c_off;
   const int nl = min(kThinBig, L - l0);
   if (!SR) {
-    // C(i = l0 + l, j = s) at i + j*M: coalesced along l for each s
+    // C(i = l0 + l, j = s) at i + j*ldc: coalesced along l for each s
     for (int e = tid; e < nl * ns; e += kThinThreads) {
       const int l = e % nl, s = e / nl;
-      cbase[(l0 + l) + (int64_t)s * M] = Cs[l * 17 + s];
+      cbase[(l0 + l) + (int64_t)s * cb.ldc] = Cs[l * 17 + s];
     }
   } else {
     // C(i = s, j = l0 + l) at s + (l0 + l)*M with M = ns: one contiguous run
@@ -522,12 +578,24 @@ __global__ void __launch_bounds__(kThinThreads, 5)
   const int tid = threadIdx.x;
   const int tq = tid & 15, tr = tid >> 4;
 
+  // C block of a strip: the last c with tile_begin <= tile.  A CTA visits its
+  // strips in increasing order, so the search gallops forward from the block
+  // of the previous strip and then bisects; with blocks of many strips it is
+  // one probe, where a bisection over all blocks is a chain of ~log2(ncb)
+  // dependent global loads on the loop's critical path.
+  int cur = 0;
   auto find = [&](int tile, GemmCBlock& cb, int& l0) {
-    int lo = 0, hi = ncb - 1;
+    int lo = cur, step = 1;
+    while (lo + step < ncb && cblocks[lo + step].tile_begin <= tile) {
+      lo += step;
+      step <<= 1;
+    }
+    int hi = min(lo + step, ncb) - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
       if (cblocks[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
     }
+    cur = lo;
     cb = cblocks[lo];
     l0 = (tile - cb.tile_begin) * kThinBig;
   };
@@ -599,6 +667,11 @@ __global__ void __launch_bounds__(kThinThreads, 5)
     const bool more = ltile < ntiles;
     if (more) load(st ^ 1, pairs[lp], lcb, ll0);
     cp_async_commit();
+    // the pair just issued becomes current next iteration; look up the one
+    // after it now, while this stage's copies are still in flight
+    const GemmCBlock icb = lcb;
+    const int il0 = ll0, ipair = lp;
+    if (more) advance();
     cp_async_wait<1>();
     __syncthreads();
     const double* ls = Ls[st];
@@ -631,6 +704,7 @@ __global__ void __launch_bounds__(kThinThreads, 5)
     if (cpair + 1 == ccb.pair_end) {
       // last pair of this strip: store it from the fragments and start over
       const int M = ccb.M;
+      const int64_t ldc = ccb.ldc;
       double* cbase = C + ccb.c_off;
       if (!SR) {
         const int L = M, ns = ccb.N;
@@ -640,8 +714,8 @@ __global__ void __launch_bounds__(kThinThreads, 5)
 #pragma unroll
           for (int b = 0; b < 2; ++b) {
             const int s0 = b * 8 + 2 * t;
-            if (l < L && s0 < ns) cbase[l + static_cast<int64_t>(s0) * M] = acc[a * 2 + b][0];
-            if (l < L && s0 + 1 < ns) cbase[l + static_cast<int64_t>(s0 + 1) * M] = acc[a * 2 + b][1];
+            if (l < L && s0 < ns) cbase[l + s0 * ldc] = acc[a * 2 + b][0];
+            if (l < L && s0 + 1 < ns) cbase[l + (s0 + 1) * ldc] = acc[a * 2 + b][1];
           }
         }
       } else {
@@ -652,8 +726,8 @@ __global__ void __launch_bounds__(kThinThreads, 5)
 #pragma unroll
           for (int b = 0; b < 4; ++b) {
             const int l = cl0 + warp * 32 + b * 8 + 2 * t;
-            if (sI < ns && l < L) cbase[sI + static_cast<int64_t>(l) * M] = acc[a * 4 + b][0];
-            if (sI < ns && l + 1 < L) cbase[sI + static_cast<int64_t>(l + 1) * M] = acc[a * 4 + b][1];
+            if (sI < ns && l < L) cbase[sI + l * ldc] = acc[a * 4 + b][0];
+            if (sI < ns && l + 1 < L) cbase[sI + (l + 1) * ldc] = acc[a * 4 + b][1];
           }
         }
       }
@@ -661,28 +735,46 @@ __global__ void __launch_bounds__(kThinThreads, 5)
       for (int a = 0; a < 8; ++a) acc[a][0] = acc[a][1] = 0.0;
     }
     if (!more) break;
-    ccb = lcb;
-    cl0 = ll0;
-    cpair = lp;
-    advance();
+    ccb = icb;
+    cl0 = il0;
+    cpair = ipair;
     st ^= 1;
   }
   cp_async_wait<0>();
+}
+
+// The persistent grid: every SM's resident CTAs of this instantiation (5 for
+// the 38 KB shared-memory layouts, 4 for the 45 KB ones), queried once per
+// device.
+template <bool SR, bool XT, bool YT>
+cudaError_t launch_thin_p(const double* X, const double* Y, double* C, const GemmCBlock* cb, int32_t ncb,
+                          const GemmPair* pr, int64_t nctas, cudaStream_t s) {
+  static int grid_of[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  int& grid = grid_of[dev & 63];
+  if (grid == 0) {
+    int sms = 0, per_sm = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gemm_thin_p<SR, XT, YT>, kThinThreads, 0);
+    if (e != cudaSuccess) return e;
+    grid = sms * std::max(per_sm, 1);
+  }
+  const unsigned g = static_cast<unsigned>(std::min<int64_t>(nctas, grid));
+  k_gemm_thin_p<SR, XT, YT><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr, static_cast<int32_t>(nctas));
+  return cudaGetLastError();
 }
 
 template <bool SR>
 cudaError_t thin_t(bool xT, bool yT, const double* X, const double* Y, double* C, const GemmCBlock* cb, int32_t ncb,
                    const GemmPair* pr, int64_t nctas, bool persistent, cudaStream_t s) {
   if (persistent) {
-    int dev = 0, sms = 148;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const unsigned g = static_cast<unsigned>(std::min<int64_t>(nctas, static_cast<int64_t>(sms) * 5));
-    const int32_t nt = static_cast<int32_t>(nctas);
-    if (!xT && !yT) k_gemm_thin_p<SR, false, false><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr, nt);
-    else if (!xT && yT) k_gemm_thin_p<SR, false, true><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr, nt);
-    else if (xT && !yT) k_gemm_thin_p<SR, true, false><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr, nt);
-    else k_gemm_thin_p<SR, true, true><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr, nt);
-    return cudaGetLastError();
+    if (!xT && !yT) return launch_thin_p<SR, false, false>(X, Y, C, cb, ncb, pr, nctas, s);
+    if (!xT && yT) return launch_thin_p<SR, false, true>(X, Y, C, cb, ncb, pr, nctas, s);
+    if (xT && !yT) return launch_thin_p<SR, true, false>(X, Y, C, cb, ncb, pr, nctas, s);
+    return launch_thin_p<SR, true, true>(X, Y, C, cb, ncb, pr, nctas, s);
   }
   const unsigned g = static_cast<unsigned>(nctas);
   if (!xT && !yT) k_gemm_thin<SR, false, false><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr);
@@ -712,6 +804,43 @@ cudaError_t launch_gemm_f64_skinny(const double* X, const double* Y, double* C, 
   if (nctas > 0x7fffffffLL || small_max > 16 || k_max > 16) return cudaErrorInvalidValue;
   return small_rows ? thin_t<true>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, persistent, s)
                     : thin_t<false>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, persistent, s);
+}
+
+template <bool XT, bool YT>
+cudaError_t launch_edges_t(const double* X, const double* Y, double* C, const GemmCBlock* cb, int32_t ncb,
+                           const GemmPair* pr, int64_t ntiles, int splitk, double* partial, cudaStream_t s) {
+  constexpr int smem = std::max(std::max(TileLayout<64, 64, XT, YT>::bytes(), TileLayout<64, 32, XT, YT>::bytes()),
+                                TileLayout<32, 64, XT, YT>::bytes());
+  auto kern = k_gemm_f64_edges<XT, YT>;
+  static unsigned long long configured = 0;  // one bit per device ordinal
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (!(configured & bit)) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    configured |= bit;
+  }
+  kern<<<static_cast<unsigned>(ntiles * splitk), kEdgeThreads, smem, s>>>(X, Y, C, cb, ncb, pr, splitk,
+                                                                          static_cast<int32_t>(ntiles), partial);
+  e = cudaGetLastError();
+  if (e != cudaSuccess || splitk == 1) return e;
+  const int64_t elems = ntiles * kEdgePart;
+  const unsigned g = static_cast<unsigned>(std::min<int64_t>((elems + 255) / 256, 148LL * 64));
+  k_splitk_reduce_edges<<<g, 256, 0, s>>>(C, cb, ncb, splitk, static_cast<int32_t>(ntiles), partial);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_f64_edges(const double* X, const double* Y, double* C, const GemmCBlock* d_cblocks,
+                                  int32_t ncb, const GemmPair* d_pairs, int64_t ntiles, bool xT, bool yT,
+                                  cudaStream_t s, int splitk, double* partial) {
+  if (ntiles <= 0) return cudaSuccess;
+  if (splitk < 1 || ntiles * splitk > 0x7fffffffLL || (splitk > 1 && !partial)) return cudaErrorInvalidValue;
+  if (!xT && !yT) return launch_edges_t<false, false>(X, Y, C, d_cblocks, ncb, d_pairs, ntiles, splitk, partial, s);
+  if (!xT && yT) return launch_edges_t<false, true>(X, Y, C, d_cblocks, ncb, d_pairs, ntiles, splitk, partial, s);
+  if (xT && !yT) return launch_edges_t<true, false>(X, Y, C, d_cblocks, ncb, d_pairs, ntiles, splitk, partial, s);
+  return launch_edges_t<true, true>(X, Y, C, d_cblocks, ncb, d_pairs, ntiles, splitk, partial, s);
 }
 
 cudaError_t launch_gemm_f64(const double* X, const double* Y, double* C,
@@ -836,7 +965,7 @@ extern "C" SB_API sb_status sb_block_gemm_f64_noalloc(void* stream, const double
     const int64_t mt = (c_rows[c] + bm - 1) / bm, nt = (c_cols[c] + bn - 1) / bn;
     if (ntiles + mt * nt >= (1LL << 31)) return noalloc_fail(SB_ERR_INVALID_ARG, "too many GEMM tiles");
     t_cblocks[c] = sb::GemmCBlock{c_off[c], c_rows[c], c_cols[c], c_pair_begin[c], c_pair_begin[c + 1],
-                                  static_cast<int32_t>(ntiles), static_cast<int32_t>(mt)};
+                                  static_cast<int32_t>(ntiles), static_cast<int32_t>(mt), c_rows[c], 0};
     ntiles += mt * nt;
   }
   for (int32_t p = 0; p < n_pairs; ++p) {

@@ -79,6 +79,8 @@ struct Ctx {
   // call on stderr with the kernel chosen, block counts and host time.
   bool trace = false;
   const char* kernel_name = "";
+  // The last GEMM variant a contraction launched (e.g. "tiled 64x64 sk1"), for the trace line.
+  char gemm_desc[64] = "";
   // SPARSEB_GEMM_TILE=<BM>x<BN> forces one GEMM tile shape (tuning); -1 = auto.
   int gemm_tile = -1;
   // SPARSEB_GEMM_SPLITK=<n> forces the split-K factor (tuning); 0 = auto.
@@ -87,6 +89,9 @@ struct Ctx {
   // one-CTA-per-strip thin kernel (tuning); -1 = auto: the persistent thin
   // kernel for every launch it can serve.
   int gemm_thin = -1;
+  // SPARSEB_GEMM_EDGES=0 keeps 64x64-tile launches in one tile shape (tuning);
+  // -1 = auto: column / row edges of <= 32 go to 64x32 / 32x64 tiles.
+  int gemm_edges = -1;
   // Pinned staging ring for host-to-device plan uploads: a copy from pinned
   // memory does not synchronise the stream, so host planning of the next
   // contraction overlaps the device work of the current one.  A slot is

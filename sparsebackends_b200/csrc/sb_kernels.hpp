@@ -20,11 +20,17 @@ namespace sb {
 // Tiles of C block c are CTAs [tile_begin, tile_begin + mtiles*ntiles); the
 // kernel finds its C block by binary search over tile_begin, so no per-tile
 // descriptor list is built or uploaded.
+// ldc: column stride of the C block in C.  It equals M except for sub-blocks
+// that are a row range of a larger block (the edges of launch_gemm_f64_edges,
+// the long-row chunks of launch_gemm_f64_skinny); the thin kernels with small
+// rows (small_rows) require ldc == M.  tshape: tile shape of the block in
+// launch_gemm_f64_edges (0 = 64x64, 1 = 64x32, 2 = 32x64), else 0.
 struct GemmCBlock {
   int64_t c_off;
   int32_t M, N;
   int32_t pair_begin, pair_end;
   int32_t tile_begin, mtiles;
+  int32_t ldc, tshape;
 };
 struct GemmPair {
   int64_t x_off, y_off;
@@ -46,6 +52,16 @@ cudaError_t launch_gemm_f64(const double* X, const double* Y, double* C,
                             const GemmCBlock* d_cblocks, int32_t ncblocks, const GemmPair* d_pairs,
                             int64_t ntiles, bool xT, bool yT, GemmShape shape, cudaStream_t s,
                             int splitk = 1, double* partial = nullptr);
+
+// Tiled GEMM over C sub-blocks of three tile shapes in one launch: each
+// GemmCBlock's tshape gives its tile (0 = 64x64, 1 = 64x32 for column edges
+// of width <= 32, 2 = 32x64 for row edges of height <= 32); tiles are
+// numbered through tile_begin / mtiles of that shape.  Sub-blocks carry their
+// own ldc and pairs whose offsets start at the sub-block's first row and
+// column.  splitk > 1: partial holds splitk * ntiles * 4096 doubles.
+cudaError_t launch_gemm_f64_edges(const double* X, const double* Y, double* C, const GemmCBlock* d_cblocks,
+                                  int32_t ncblocks, const GemmPair* d_pairs, int64_t ntiles, bool xT, bool yT,
+                                  cudaStream_t s, int splitk = 1, double* partial = nullptr);
 
 // Thin variant for launches whose every pair has K <= 16 and whose C blocks
 // have min(M, N) <= 16 (HBM-bound): DMMA on 128 x 16 strips of the long side,
