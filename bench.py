@@ -134,8 +134,8 @@ def measured_hbm_gbs():
 # given chi (--metrics dram__bytes_read.sum,dram__bytes_write.sum), averaged
 # over the captured launches of each kernel; see profiles/ for the commands.
 TRAFFIC = {
-    (2048, "k_gemm_f64"): (1024.2e6, "profiles/heff_chi2048_dram_traffic.md (mean of the psi*L and R*T3 launches)"),
-    (2048, "k_gemm_thin"): (1640.7e6, "profiles/heff_chi2048_dram_traffic.md (mean of the T1*W1 and T2*W2 launches)"),
+    (2048, "k_gemm_f64"): (1211.8e6, "profiles/heff_chi2048_dram_traffic.md (mean of the psi*L and R*T3 launches)"),
+    (2048, "k_gemm_thin"): (1544.0e6, "profiles/heff_chi2048_dram_traffic.md (mean of the T1*W1 and T2*W2 launches)"),
 }
 
 
@@ -513,7 +513,8 @@ def run_ours(args, world, rank, local):
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (operators ~0.6 GB, intermediates ~2.3 GB each)"},
         "gflops_algorithmic": flops_alg * value / 1e9,
-        "roofline": {"bound": "tensor", "kernel": "k_gemm_f64 (DMMA m8n8k4; steps psi*L and R*T3)",
+        "roofline": {"bound": "tensor", "kernel": "k_gemm_f64_edges (DMMA m8n8k4, 64x64 tiles with 64x32 / 32x64 "
+                                                       "edge tiles; steps psi*L and R*T3)",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                      "peak_source": "measured live: torch.matmul float64 8192^3, best of 10 (cuBLAS DGEMM)",
                      "flops_per_launch": g["flops"] / max(g["launches"], 1),
