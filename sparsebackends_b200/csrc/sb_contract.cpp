@@ -301,8 +301,8 @@ struct GemmPlan {
       c.mtiles = static_cast<int32_t>(mt);
       ntiles += mt * nt;
     }
-    // Split-K when the tiles fill less than ~3 waves of the 148 SMs and each
-    // tile has a long K loop (segments of >= 32 k-tiles).
+    // Split-K when the tiles fill few waves of the 148 SMs and each tile has a
+    // long K loop (choose_splitk).
     int64_t kt_avg = 0;
     for (auto& c : cbs) {
       int64_t kt = 0;
@@ -403,12 +403,13 @@ struct GemmPlan {
   }
 
   // Split-K factor for ntiles tiles averaging kt_avg k-tiles: split while the
-  // tiles fill less than ~3 waves of 148 SMs x 4 CTAs and every segment keeps
-  // >= 32 k-tiles.
+  // tiles fill less than ~6 waves of 148 SMs x 4 CTAs and every segment keeps
+  // >= 32 k-tiles (6 waves against 3: R*T3 at chi=2048 2.02 -> 1.98 ms ragged,
+  // 8.04 -> 7.89 ms zero-padded; the shorter CTAs balance the uneven K loops).
   static int choose_splitk(Ctx* ctx, int64_t ntiles, int64_t kt_avg) {
     int splitk = 1;
     const int64_t wave = 148 * 4;
-    while (splitk < 16 && ntiles * splitk < 3 * wave && kt_avg / (2 * splitk) >= 32) splitk *= 2;
+    while (splitk < 16 && ntiles * splitk < 6 * wave && kt_avg / (2 * splitk) >= 32) splitk *= 2;
     if (ctx->gemm_splitk > 0) splitk = ctx->gemm_splitk;
     return splitk;
   }

@@ -59,6 +59,26 @@ __device__ __forceinline__ int tile_cblock(const GemmCBlock* __restrict__ cblock
   return lo;
 }
 
+// The same lookup by a full warp (every lane gets the result): each round
+// tests 32 evenly spaced candidates at once, so 120 blocks take two dependent
+// loads and 30000 take three, against 7 and 15 for a bisection.  The answer
+// stays in [lo, hi] with tile_begin[lo] <= bid; the lanes whose candidate
+// still starts at or before bid form a prefix, so their count narrows the
+// range to one step.
+__device__ __forceinline__ int tile_cblock_warp(const GemmCBlock* __restrict__ cblocks, int32_t ncb, int bid) {
+  const int lane = static_cast<int>(threadIdx.x & 31);
+  int lo = 0, hi = ncb - 1;
+  while (lo < hi) {
+    const int step = (hi - lo + 32) / 32;
+    const int idx = lo + (lane + 1) * step;
+    const bool le = idx <= hi && cblocks[idx].tile_begin <= bid;
+    const int k = __popc(__ballot_sync(0xffffffffu, le));
+    lo += k * step;
+    hi = min(hi, lo + step - 1);
+  }
+  return lo;
+}
+
 // One CTA of the tiled GEMM: tile lt of C block cb, k-segment seg of splitk;
 // with splitk > 1 the BM x BN tile goes to pt (column-major) instead of C.
 template <int BM, int BN, int WM, int WN, bool XT, bool YT, int BK, int ST>
@@ -85,8 +105,12 @@ __device__ __forceinline__ void gemm_cta(const double* __restrict__ X, const dou
   const int m0 = (lt % cb.mtiles) * BM, n0 = (lt / cb.mtiles) * BN;
   const int tid = threadIdx.x;
 
+  // k-tiles of all pairs: the lanes of each warp sum a stride of the pairs
   int ktot = 0;
-  for (int p = cb.pair_begin; p < cb.pair_end; ++p) ktot += (pairs[p].K + kBK - 1) / kBK;
+  for (int p = cb.pair_begin + static_cast<int>(threadIdx.x & 31); p < cb.pair_end; p += 32)
+    ktot += (pairs[p].K + kBK - 1) / kBK;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) ktot += __shfl_xor_sync(0xffffffffu, ktot, o);
   // this segment's range of the concatenated k-tiles
   const int kb = static_cast<int>(static_cast<int64_t>(ktot) * seg / splitk);
   const int ke = static_cast<int>(static_cast<int64_t>(ktot) * (seg + 1) / splitk);
@@ -271,7 +295,7 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32, 512 / ((BM / WM) *
   extern __shared__ double smem[];
   const int seg = static_cast<int>(blockIdx.x) / ntiles;
   const int bid = static_cast<int>(blockIdx.x) % ntiles;
-  const GemmCBlock cb = cblocks[tile_cblock(cblocks, ncb, bid)];
+  const GemmCBlock cb = cblocks[tile_cblock_warp(cblocks, ncb, bid)];
   double* pt = splitk > 1 ? partial + (static_cast<int64_t>(seg) * ntiles + bid) * (BM * BN) : nullptr;
   gemm_cta<BM, BN, WM, WN, XT, YT, BK, ST>(X, Y, C, cb, pairs, bid - cb.tile_begin, seg, splitk, pt, smem);
 }
@@ -291,7 +315,7 @@ __global__ void __launch_bounds__(kEdgeThreads, 4)
   extern __shared__ double smem[];
   const int seg = static_cast<int>(blockIdx.x) / ntiles;
   const int bid = static_cast<int>(blockIdx.x) % ntiles;
-  const GemmCBlock cb = cblocks[tile_cblock(cblocks, ncb, bid)];
+  const GemmCBlock cb = cblocks[tile_cblock_warp(cblocks, ncb, bid)];
   double* pt = splitk > 1 ? partial + (static_cast<int64_t>(seg) * ntiles + bid) * kEdgePart : nullptr;
   const int lt = bid - cb.tile_begin;
   if (cb.tshape == 0)
