@@ -413,25 +413,29 @@ struct GemmPlan {
     if (ctx->gemm_splitk > 0) splitk = ctx->gemm_splitk;
     return splitk;
   }
-  // 64x64 tiles with the edges cut off: a column edge of width N % 64 <= 32
-  // (the whole block when N <= 32) goes to 64x32 tiles, a row edge of height
-  // M % 64 <= 32 to 32x64 tiles, one launch for all three (ragged sector
-  // extents: 1.165 -> 1.092 executed/algorithmic FLOPs on the chi=2048 R*T3
-  // step).  Returns false, launching nothing, when that saves < 3% of the
-  // padded 64x64 work.
+  // 64x64 tiles with the edges cut off: a column remainder N mod 64 of <= 32
+  // or <= 48 (the whole block when N is that small) goes to 64x32 or 64x48
+  // tiles, a row remainder likewise to 32x64 or 48x64 tiles, one launch for
+  // all five shapes (ragged sector extents at chi=2048: executed/algorithmic
+  // FLOPs 1.109 -> 1.047 on L*psi, 1.165 -> 1.050 on R*T3).  Returns false,
+  // launching nothing, when that saves < 3% of the padded 64x64 work.
+  static int edge_rows(int shape) { return shape == 2 ? 32 : shape == 4 ? 48 : 64; }
+  static int edge_cols(int shape) { return shape == 1 ? 32 : shape == 3 ? 48 : 64; }
   bool launch_edges(Ctx* ctx, const double* X, const double* Y, double* C, bool xT, bool yT, double flops,
                     double bytes) {
     auto up = [](int64_t v, int64_t t) { return (v + t - 1) / t * t; };
-    auto rows64 = [](int64_t M) { const int64_t e = M % 64; return e > 0 && e <= 32 ? M - e : M; };
+    auto body64 = [](int64_t v) { const int64_t e = v % 64; return e > 0 && e <= 48 ? v - e : v; };
+    auto edge = [](int64_t e) -> int64_t { return e <= 32 ? 32 : 48; };
     double w64 = 0.0, wseg = 0.0;
     for (auto& c : cbs) {
       int64_t kt = 0;
       for (int p = c.pair_begin; p < c.pair_end; ++p) kt += (pairs[p].K + 15) / 16;
       kt = std::max<int64_t>(kt, 1);
-      const int64_t mm = rows64(c.M), nm = rows64(c.N);
+      const int64_t mm = body64(c.M), nm = body64(c.N);
       w64 += static_cast<double>(up(c.M, 64) * up(c.N, 64)) * kt;
-      wseg += static_cast<double>(up(mm, 64) * up(nm, 64) + up(c.M, 64) * up(c.N - nm, 32) +
-                                  (nm > 0 ? up(c.M - mm, 32) * up(nm, 64) : 0)) * kt;
+      wseg += static_cast<double>(up(mm, 64) * up(nm, 64) +
+                                  (nm < c.N ? up(c.M, 64) * up(c.N - nm, edge(c.N - nm)) : 0) +
+                                  (mm < c.M && nm > 0 ? up(c.M - mm, edge(c.M - mm)) * up(nm, 64) : 0)) * kt;
     }
     if (!(wseg < 0.97 * w64)) return false;
     // Sub-blocks of one C block stay adjacent (its tiles run together and
@@ -444,9 +448,9 @@ struct GemmPlan {
     for (auto& c : cbs) {
       int64_t kt = 0;
       for (int p = c.pair_begin; p < c.pair_end; ++p) kt += (pairs[p].K + 15) / 16;
-      const int32_t mm = static_cast<int32_t>(rows64(c.M)), nm = static_cast<int32_t>(rows64(c.N));
+      const int32_t mm = static_cast<int32_t>(body64(c.M)), nm = static_cast<int32_t>(body64(c.N));
       auto sub = [&](int32_t shape, int32_t r0, int32_t c0, int32_t rows, int32_t cols) {
-        const int bm = shape == 2 ? 32 : 64, bn = shape == 1 ? 32 : 64;
+        const int bm = edge_rows(shape), bn = edge_cols(shape);
         GemmCBlock s{c.c_off + r0 + static_cast<int64_t>(c0) * c.ldc, rows, cols, c.pair_begin, c.pair_end, 0, 0,
                      c.ldc, shape};
         if (r0 != 0 || c0 != 0) {
@@ -468,33 +472,32 @@ struct GemmPlan {
         sc.push_back(s);
       };
       if (mm > 0 && nm > 0) sub(0, 0, 0, mm, nm);
-      if (nm < c.N) sub(1, 0, nm, c.M, c.N - nm);
-      if (mm < c.M && nm > 0) sub(2, mm, 0, c.M - mm, nm);
+      if (nm < c.N) sub(c.N - nm <= 32 ? 1 : 3, 0, nm, c.M, c.N - nm);
+      if (mm < c.M && nm > 0) sub(c.M - mm <= 32 ? 2 : 4, mm, 0, c.M - mm, nm);
     }
     require(ep.size() < (1ULL << 31), SB_ERR_INVALID_ARG, "too many GEMM block pairs in one launch");
     const int64_t kt_avg = ntiles ? kts / ntiles : 0;
     if (kt_avg >= 64) {
       // Long K loops: the tiles that share an operand panel stream it in
       // step only when they advance at one speed, so tiles of one shape run
-      // together: all bodies, then all column edges, then all row edges
-      // (zero-padded chi=2048 R*T3: 8.5 against 14.7 GB read, 7.98 against
-      // 8.48 ms).
+      // together: all bodies, then the edges shape by shape (zero-padded
+      // chi=2048 R*T3: 8.5 against 14.7 GB read, 7.98 against 8.48 ms).
       std::stable_sort(sc.begin(), sc.end(),
                        [](const GemmCBlock& a, const GemmCBlock& b) { return a.tshape < b.tshape; });
       ntiles = 0;
       for (auto& b : sc) {
-        const int64_t bn = b.tshape == 1 ? 32 : 64;
+        const int64_t bn = edge_cols(b.tshape);
         b.tile_begin = static_cast<int32_t>(ntiles);
         ntiles += static_cast<int64_t>(b.mtiles) * ((b.N + bn - 1) / bn);
       }
     }
     const int splitk = choose_splitk(ctx, ntiles, kt_avg);
-    int64_t nshape[3] = {0, 0, 0};
-    for (auto& b : sc) nshape[b.tshape] += static_cast<int64_t>(b.mtiles) *
-                                           ((b.N + (b.tshape == 1 ? 31 : 63)) / (b.tshape == 1 ? 32 : 64));
-    std::snprintf(ctx->gemm_desc, sizeof(ctx->gemm_desc), "edges 64x64:%lld 64x32:%lld 32x64:%lld sk%d",
-                  static_cast<long long>(nshape[0]), static_cast<long long>(nshape[1]),
-                  static_cast<long long>(nshape[2]), splitk);
+    long long nshape[5] = {0, 0, 0, 0, 0};
+    for (auto& b : sc) nshape[b.tshape] += static_cast<long long>(b.mtiles) * ((b.N + edge_cols(b.tshape) - 1) /
+                                                                                edge_cols(b.tshape));
+    std::snprintf(ctx->gemm_desc, sizeof(ctx->gemm_desc),
+                  "edges 64x64:%lld 64x32:%lld 32x64:%lld 64x48:%lld 48x64:%lld sk%d", nshape[0], nshape[1],
+                  nshape[2], nshape[3], nshape[4], splitk);
     DevBuf dc = upload(ctx, sc), dp = upload(ctx, ep);
     DevBuf part;
     if (splitk > 1) part = DevBuf(ctx, static_cast<size_t>(splitk) * ntiles * 64 * 64 * sizeof(double));

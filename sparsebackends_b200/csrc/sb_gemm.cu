@@ -80,8 +80,11 @@ __device__ __forceinline__ int tile_cblock_warp(const GemmCBlock* __restrict__ c
 }
 
 // One CTA of the tiled GEMM: tile lt of C block cb, k-segment seg of splitk;
-// with splitk > 1 the BM x BN tile goes to pt (column-major) instead of C.
-template <int BM, int BN, int WM, int WN, bool XT, bool YT, int BK, int ST>
+// with splitk > 1 the BMC x BNC tile goes to pt (column-major) instead of C.
+// BM x BN is the staged (shared-memory) tile; the C tile BMC x BNC may be
+// narrower (48 of 64 rows or columns: the operand copies past BMC / BNC are
+// zero-filled without reading memory, and no warp multiplies them).
+template <int BM, int BN, int WM, int WN, bool XT, bool YT, int BK, int ST, int BMC = BM, int BNC = BN>
 __device__ __forceinline__ void gemm_cta(const double* __restrict__ X, const double* __restrict__ Y,
                                          double* __restrict__ C, const GemmCBlock& cb,
                                          const GemmPair* __restrict__ pairs, int lt, int seg, int32_t splitk,
@@ -89,8 +92,9 @@ __device__ __forceinline__ void gemm_cta(const double* __restrict__ X, const dou
   constexpr int kBK = BK;
   constexpr int kStages = ST;
   using TL = TileLayout<BM, BN, XT, YT, BK, ST>;
-  constexpr int NWM = BM / WM;
-  constexpr int NWN = BN / WN;
+  static_assert(BMC <= BM && BNC <= BN && BMC % WM == 0 && BNC % WN == 0, "compute tile must tile the warps");
+  constexpr int NWM = BMC / WM;
+  constexpr int NWN = BNC / WN;
   constexpr int NT = NWM * NWN * 32;
   constexpr int MT = WM / 8;
   constexpr int NTL = WN / 8;
@@ -102,7 +106,7 @@ __device__ __forceinline__ void gemm_cta(const double* __restrict__ X, const dou
   double* Ys = smem + kStages * TL::XSZ;  // kStages tiles of TL::YSZ
 
   const int M = cb.M, N = cb.N;
-  const int m0 = (lt % cb.mtiles) * BM, n0 = (lt / cb.mtiles) * BN;
+  const int m0 = (lt % cb.mtiles) * BMC, n0 = (lt / cb.mtiles) * BNC;
   const int tid = threadIdx.x;
 
   // k-tiles of all pairs: the lanes of each warp sum a stride of the pairs
@@ -136,7 +140,7 @@ __device__ __forceinline__ void gemm_cta(const double* __restrict__ X, const dou
   const int sy0 = YT ? y_var * (BN + 4) + y_fix : y_var * TL::KP + y_fix;
   constexpr int SXR = XT ? XR * TL::KP : XR * (BM + 4);
   constexpr int SYR = YT ? YR * (BN + 4) : YR * TL::KP;
-  const int mleft = M - m0, nleft = N - n0;
+  const int mleft = min(M - m0, BMC), nleft = min(N - n0, BNC);
 
   // descriptor of the pair being loaded and this thread's global addresses in
   // it, kept in registers; the next pair is fetched when the cursor moves on,
@@ -258,15 +262,15 @@ __device__ __forceinline__ void gemm_cta(const double* __restrict__ X, const dou
   cp_async_wait<0>();
 
   if (splitk > 1) {
-    // partial tile, column-major BM x BN, reduced by k_splitk_reduce
+    // partial tile, column-major BMC x BNC, reduced by k_splitk_reduce
 #pragma unroll
     for (int a = 0; a < MT; ++a) {
       const int rl = wm * WM + a * 8 + g;
 #pragma unroll
       for (int b = 0; b < NTL; ++b) {
         const int cl = wn * WN + b * 8 + 2 * t;
-        pt[rl + cl * BM] = acc[a][b][0];
-        pt[rl + (cl + 1) * BM] = acc[a][b][1];
+        pt[rl + cl * BMC] = acc[a][b][0];
+        pt[rl + (cl + 1) * BMC] = acc[a][b][1];
       }
     }
     return;
@@ -300,10 +304,11 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32, 512 / ((BM / WM) *
   gemm_cta<BM, BN, WM, WN, XT, YT, BK, ST>(X, Y, C, cb, pairs, bid - cb.tile_begin, seg, splitk, pt, smem);
 }
 
-// Three tile shapes in one launch (launch_gemm_f64_edges): the tiles of every
+// Five tile shapes in one launch (launch_gemm_f64_edges): the tiles of every
 // C sub-block are numbered consecutively through tile_begin as usual, and the
 // sub-block's tshape picks the CTA's tile: 0 = 64x64 (32x32 warp tiles),
-// 1 = 64x32 (32x16), 2 = 32x64 (16x32), all four warps and 3 stages.
+// 1 = 64x32 (32x16), 2 = 32x64 (16x32), 3 = 64x48 (32x24), 4 = 48x64 (24x32),
+// all four warps and 3 stages (the 48-wide ones stage 64x64 operand tiles).
 // Partial tiles of split-K are kEdgePart doubles apart whatever their shape.
 constexpr int kEdgeThreads = 128;
 constexpr int kEdgePart = 64 * 64;
@@ -322,8 +327,12 @@ __global__ void __launch_bounds__(kEdgeThreads, 4)
     gemm_cta<64, 64, 32, 32, XT, YT, kBK, kStages>(X, Y, C, cb, pairs, lt, seg, splitk, pt, smem);
   else if (cb.tshape == 1)
     gemm_cta<64, 32, 32, 16, XT, YT, kBK, kStages>(X, Y, C, cb, pairs, lt, seg, splitk, pt, smem);
-  else
+  else if (cb.tshape == 2)
     gemm_cta<32, 64, 16, 32, XT, YT, kBK, kStages>(X, Y, C, cb, pairs, lt, seg, splitk, pt, smem);
+  else if (cb.tshape == 3)
+    gemm_cta<64, 64, 32, 24, XT, YT, kBK, kStages, 64, 48>(X, Y, C, cb, pairs, lt, seg, splitk, pt, smem);
+  else
+    gemm_cta<64, 64, 24, 32, XT, YT, kBK, kStages, 48, 64>(X, Y, C, cb, pairs, lt, seg, splitk, pt, smem);
 }
 
 // Deterministic split-K reduction: C tile = sum over segments in order.
@@ -361,7 +370,8 @@ __global__ void k_splitk_reduce_edges(double* __restrict__ C, const GemmCBlock* 
        e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int bid = static_cast<int>(e / kEdgePart), w = static_cast<int>(e % kEdgePart);
     const GemmCBlock cb = cblocks[tile_cblock(cblocks, ncb, bid)];
-    const int bm = cb.tshape == 2 ? 32 : 64, bn = cb.tshape == 1 ? 32 : 64;
+    const int bm = cb.tshape == 2 ? 32 : cb.tshape == 4 ? 48 : 64;
+    const int bn = cb.tshape == 1 ? 32 : cb.tshape == 3 ? 48 : 64;
     splitk_reduce_elem(C, cb, bm, bn, bid - cb.tile_begin, w, splitk, static_cast<int64_t>(ntiles) * kEdgePart,
                        partial + static_cast<int64_t>(bid) * kEdgePart);
   }

@@ -80,7 +80,7 @@ struct Ctx {
   bool trace = false;
   const char* kernel_name = "";
   // The last GEMM variant a contraction launched (e.g. "tiled 64x64 sk1"), for the trace line.
-  char gemm_desc[64] = "";
+  char gemm_desc[96] = "";
   // SPARSEB_GEMM_TILE=<BM>x<BN> forces one GEMM tile shape (tuning); -1 = auto.
   int gemm_tile = -1;
   // SPARSEB_GEMM_SPLITK=<n> forces the split-K factor (tuning); 0 = auto.

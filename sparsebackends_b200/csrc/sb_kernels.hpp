@@ -24,7 +24,8 @@ namespace sb {
 // that are a row range of a larger block (the edges of launch_gemm_f64_edges,
 // the long-row chunks of launch_gemm_f64_skinny); the thin kernels with small
 // rows (small_rows) require ldc == M.  tshape: tile shape of the block in
-// launch_gemm_f64_edges (0 = 64x64, 1 = 64x32, 2 = 32x64), else 0.
+// launch_gemm_f64_edges (0 = 64x64, 1 = 64x32, 2 = 32x64, 3 = 64x48,
+// 4 = 48x64), else 0.
 struct GemmCBlock {
   int64_t c_off;
   int32_t M, N;
@@ -53,9 +54,10 @@ cudaError_t launch_gemm_f64(const double* X, const double* Y, double* C,
                             int64_t ntiles, bool xT, bool yT, GemmShape shape, cudaStream_t s,
                             int splitk = 1, double* partial = nullptr);
 
-// Tiled GEMM over C sub-blocks of three tile shapes in one launch: each
-// GemmCBlock's tshape gives its tile (0 = 64x64, 1 = 64x32 for column edges
-// of width <= 32, 2 = 32x64 for row edges of height <= 32); tiles are
+// Tiled GEMM over C sub-blocks of five tile shapes in one launch: each
+// GemmCBlock's tshape gives its tile (0 = 64x64; 1 = 64x32 and 3 = 64x48 for
+// column edges of width <= 32 and <= 48; 2 = 32x64 and 4 = 48x64 for row
+// edges of height <= 32 and <= 48); tiles are
 // numbered through tile_begin / mtiles of that shape.  Sub-blocks carry their
 // own ldc and pairs whose offsets start at the sub-block's first row and
 // column.  splitk > 1: partial holds splitk * ntiles * 4096 doubles.

@@ -1,6 +1,7 @@
 """The tiled block GEMM with its edges cut off (64x64 tiles for the body,
-64x32 tiles for column edges of width <= 32, 32x64 tiles for row edges of
-height <= 32, one launch) against numpy and against the single-shape launch.
+64x32 / 64x48 tiles for column edges of width <= 32 / <= 48, 32x64 / 48x64
+tiles for row edges, one launch) against numpy and against the single-shape
+launch.
 
 Every C element is summed over the same k-tiles in the same order whatever
 tile covers it, so at equal split-K the two launches agree bit for bit.  The
@@ -16,9 +17,10 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-# (M, K, N) per block; K >= 1024 (133 x 1100 x 150) takes the long-K tile order
+# (M, K, N) per block; K >= 1024 (133 x 1100 x 150, 45 x 1100 x 300) takes
+# the long-K tile order; 100, 107, 40, 45 and 300 have 48-wide edges
 SHAPES = [(133, 70, 411), (20, 40, 150), (96, 33, 18), (200, 300, 100), (64, 64, 64), (18, 2000, 411),
-          (133, 1100, 150)]
+          (133, 1100, 150), (100, 70, 107), (96, 33, 40), (45, 1100, 300)]
 
 
 @pytest.fixture(scope="module")
@@ -76,10 +78,15 @@ def _expect_edges(Mc, Nc):
     if (Nc <= 32 and Mc >= 128) or (Mc <= 32 and Nc >= 128) or (Mc >= 1024 and Nc >= 512):
         return False
     up = lambda v, t: -(-v // t) * t
-    rows64 = lambda v: v - v % 64 if 0 < v % 64 <= 32 else v
-    mm, nm = rows64(Mc), rows64(Nc)
+    body64 = lambda v: v - v % 64 if 0 < v % 64 <= 48 else v
+    edge = lambda e: 32 if e <= 32 else 48
+    mm, nm = body64(Mc), body64(Nc)
     w64 = up(Mc, 64) * up(Nc, 64)
-    wseg = up(mm, 64) * up(nm, 64) + up(Mc, 64) * up(Nc - nm, 32) + (up(Mc - mm, 32) * up(nm, 64) if nm else 0)
+    wseg = up(mm, 64) * up(nm, 64)
+    if nm < Nc:
+        wseg += up(Mc, 64) * up(Nc - nm, edge(Nc - nm))
+    if mm < Mc and nm:
+        wseg += up(Mc - mm, edge(Mc - mm)) * up(nm, 64)
     return wseg < 0.97 * w64
 
 
@@ -114,11 +121,11 @@ def test_edge_tiles_ragged_blocks(sb, capfd):
     """Ragged operands: every C block has its own extents, so one launch mixes
     blocks with and without edges (and blocks that are all edge)."""
     rng = np.random.Generator(np.random.PCG64(12))
-    ms, ks, ns = [18, 133, 64, 96], [40, 250], [411, 20, 70]
+    ms, ks, ns = [18, 133, 64, 96, 100], [40, 250], [411, 20, 70, 107]
     # A[(i, q) | m, k], B[(j, q) | k, n]: block (i, q) of A is ms[i] x ks[q],
     # block (j, q) of B is ks[q] x ns[j]; C[(i, j) | m, n] sums over q.
-    Akeys = [(i + 1, q + 1) for q in range(2) for i in range(4)]
-    Bkeys = [(j + 1, q + 1) for q in range(2) for j in range(3)]
+    Akeys = [(i + 1, q + 1) for q in range(2) for i in range(len(ms))]
+    Bkeys = [(j + 1, q + 1) for q in range(2) for j in range(len(ns))]
     Ab = {k: rng.standard_normal((ms[k[0] - 1], ks[k[1] - 1])) for k in Akeys}
     Bb = {k: rng.standard_normal((ks[k[1] - 1], ns[k[0] - 1])) for k in Bkeys}
 
@@ -129,16 +136,16 @@ def test_edge_tiles_ragged_blocks(sb, capfd):
     outs = []
     for kv in ({}, {"SPARSEB_GEMM_EDGES": 0, "SPARSEB_GEMM_TILE": "64x64"}):
         ctx = _ctx(sb, SPARSEB_GEMM_SPLITK=1, **kv)
-        A = tensor(ctx, Akeys, Ab, (4, 2, max(ms), max(ks)))
-        B = tensor(ctx, Bkeys, Bb, (3, 2, max(ks), max(ns)))
-        C = sb.NewBlockSparseSorted.empty((4, 3, max(ms), max(ns)), 2, ctx=ctx)
+        A = tensor(ctx, Akeys, Ab, (len(ms), 2, max(ms), max(ks)))
+        B = tensor(ctx, Bkeys, Bb, (len(ns), 2, max(ks), max(ns)))
+        C = sb.NewBlockSparseSorted.empty((len(ms), len(ns), max(ms), max(ns)), 2, ctx=ctx)
         sb.contract_(C, ["i", "j", "m", "n"], A, ["i", "q", "m", "k"], B, ["j", "q", "k", "n"])
         outs.append((sb.to_dense(sb.to_uniform(C)), capfd.readouterr().err))
     (got, tr), (ref, _) = outs
     assert "gemm: edges" in tr
     assert np.array_equal(got, ref)
-    for i in range(4):
-        for j in range(3):
+    for i in range(len(ms)):
+        for j in range(len(ns)):
             want = sum(Ab[(i + 1, q + 1)] @ Bb[(j + 1, q + 1)] for q in range(2))
             blk = got[i, j, :ms[i], :ns[j]]
             assert np.linalg.norm(blk - want) <= 1e-13 * np.linalg.norm(want)
