@@ -134,8 +134,8 @@ def measured_hbm_gbs():
 # given chi (--metrics dram__bytes_read.sum,dram__bytes_write.sum), averaged
 # over the captured launches of each kernel; see profiles/ for the commands.
 TRAFFIC = {
-    (2048, "k_gemm_f64"): (1211.8e6, "profiles/heff_chi2048_dram_traffic.md (mean of the psi*L and R*T3 launches)"),
-    (2048, "k_gemm_thin"): (1544.0e6, "profiles/heff_chi2048_dram_traffic.md (mean of the T1*W1 and T2*W2 launches)"),
+    (2048, "k_gemm_f64"): (1121.8e6, "profiles/heff_chi2048_dram_traffic.md (mean of the psi*L and R*T3 launches)"),
+    (2048, "k_gemm_thin"): (1549.8e6, "profiles/heff_chi2048_dram_traffic.md (mean of the T1*W1 and T2*W2 launches)"),
 }
 
 
