@@ -147,22 +147,18 @@ __device__ __forceinline__ void gemm_cta(const double* __restrict__ X, const dou
   // a k-tile before it is needed
   GemmPair pr{};
   const double *xg = X, *yg = Y;
-  int64_t xstep = 0, ystep = 0, xk = 1, yk = 1;
+  int64_t xstep = 0, ystep = 0;
   auto set_pair = [&]() {
     if (XT) {
       xg = X + pr.x_off + static_cast<int64_t>(m0 + x_var) * pr.ldx + x_fix;
-      xk = 1;
     } else {
       xg = X + pr.x_off + (m0 + x_fix) + static_cast<int64_t>(x_var) * pr.ldx;
-      xk = pr.ldx;
     }
     xstep = static_cast<int64_t>(XR) * pr.ldx;
     if (YT) {
       yg = Y + pr.y_off + (n0 + y_fix) + static_cast<int64_t>(y_var) * pr.ldy;
-      yk = pr.ldy;
     } else {
       yg = Y + pr.y_off + y_fix + static_cast<int64_t>(n0 + y_var) * pr.ldy;
-      yk = 1;
     }
     ystep = static_cast<int64_t>(YR) * pr.ldy;
   };
@@ -176,15 +172,13 @@ __device__ __forceinline__ void gemm_cta(const double* __restrict__ X, const dou
   constexpr int kParts = kBK / 4;
   static_assert(XLOADS % kParts == 0 && YLOADS % kParts == 0, "loads must split evenly over the k4 steps");
   int kleft = 0;
-  const double *xp = X, *yp = Y, *xb = X, *yb = Y;
+  const double *xp = X, *yp = Y;
   double *xs_st = Xs, *ys_st = Ys;
   auto begin_load = [&](int stage) {
     const int k0 = lkt * kBK;
     kleft = pr.K - k0;  // valid k entries of this k-tile
-    xp = xg + static_cast<int64_t>(k0) * xk;
-    yp = yg + static_cast<int64_t>(k0) * yk;
-    xb = X + pr.x_off;  // a valid address for zero-filled entries
-    yb = Y + pr.y_off;
+    xp = xg + (XT ? static_cast<int64_t>(k0) : static_cast<int64_t>(k0) * pr.ldx);
+    yp = yg + (YT ? static_cast<int64_t>(k0) * pr.ldy : static_cast<int64_t>(k0));
     xs_st = Xs + stage * TL::XSZ + sx0;
     ys_st = Ys + stage * TL::YSZ + sy0;
   };
@@ -194,14 +188,14 @@ __device__ __forceinline__ void gemm_cta(const double* __restrict__ X, const dou
       const int r = part * (XLOADS / kParts) + q;
       const int var = x_var + r * XR;
       const bool v = XT ? (var < mleft && x_fix < kleft) : (x_fix < mleft && var < kleft);
-      cp_async8(xs_st + r * SXR, v ? xp + r * xstep : xb, v);
+      cp_async8(xs_st + r * SXR, v ? xp + r * xstep : X, v);
     }
 #pragma unroll
     for (int q = 0; q < YLOADS / kParts; ++q) {
       const int r = part * (YLOADS / kParts) + q;
       const int var = y_var + r * YR;
       const bool v = YT ? (y_fix < nleft && var < kleft) : (var < nleft && y_fix < kleft);
-      cp_async8(ys_st + r * SYR, v ? yp + r * ystep : yb, v);
+      cp_async8(ys_st + r * SYR, v ? yp + r * ystep : Y, v);
     }
   };
   auto end_load = [&]() {
