@@ -135,7 +135,7 @@ def measured_hbm_gbs():
 # over the captured launches of each kernel; see profiles/ for the commands.
 TRAFFIC = {
     (2048, "k_gemm_f64"): (1121.8e6, "profiles/heff_chi2048_dram_traffic.md (mean of the psi*L and R*T3 launches)"),
-    (2048, "k_gemm_thin"): (1549.8e6, "profiles/heff_chi2048_dram_traffic.md (mean of the T1*W1 and T2*W2 launches)"),
+    (2048, "k_gemm_thin"): (1315.3e6, "profiles/heff_chi2048_dram_traffic.md (mean of the T1*W1 and T2*W2 launches)"),
 }
 
 

@@ -238,15 +238,24 @@ struct GemmPlan {
     const bool skinny_m = Kmax <= 16 && M <= 16;
     if ((skinny_n || skinny_m) && ctx->gemm_tile < 0 && ctx->gemm_thin != 0) {
       const bool small_rows = skinny_m;
-      const bool interleaved = interleave_shared_long(small_rows, xT, yT);
+      std::vector<int> group;
+      const bool interleaved = group_shared_long(small_rows, group);
       bool every_block_has_pairs = true;
       for (auto& c : cbs) every_block_has_pairs = every_block_has_pairs && c.pair_end > c.pair_begin;
+      // strips of a group of S blocks: strip s of member j is the group's
+      // strip s*S + j; every member carries the group's tile_begin and S in
+      // mtiles (the thin kernels find the group's last block and step back)
       int64_t nctas = 0;
-      for (auto& c : cbs) {
-        const int64_t bigx = small_rows ? c.N : c.M;
-        c.tile_begin = static_cast<int32_t>(nctas);
-        c.mtiles = 1;
-        nctas += (bigx + 127) / 128;
+      for (size_t i = 0; i < cbs.size();) {
+        const int S = group[i];
+        const int64_t bigx = small_rows ? cbs[i].N : cbs[i].M;
+        for (int j = 0; j < S; ++j) {
+          cbs[i + j].tile_begin = static_cast<int32_t>(nctas);
+          cbs[i + j].mtiles = S;
+        }
+        nctas += S * ((bigx + 127) / 128);
+        require(nctas < (1LL << 31), SB_ERR_INVALID_ARG, "too many GEMM strips in one launch");
+        i += S;
       }
       const bool persistent = ctx->gemm_thin != 1 && every_block_has_pairs;
       std::snprintf(ctx->gemm_desc, sizeof(ctx->gemm_desc), "thin%s %s%s", persistent ? " persistent" : "",
@@ -325,13 +334,13 @@ struct GemmPlan {
 
   // Thin launches (K <= 16): output blocks whose pairs read the same block of
   // the long operand (the MPO steps of H_eff, where one T1 block feeds up to
-  // two output blocks) are cut into chunks of kThinChunk long-side elements
-  // and emitted chunk by chunk in turn, so that the second read of a long
-  // chunk follows the first within a few MB of traffic and hits L2 (126 MB)
-  // instead of DRAM.  Row chunks keep the parent's ldc.  Returns whether
-  // anything was reordered.
-  static constexpr int64_t kThinChunk = 256 * 128;
-  bool interleave_shared_long(bool small_rows, bool xT, bool yT) {
+  // two output blocks) are made adjacent in cbs as one group per shared
+  // operand set and long extent, and their strips are numbered in turn (strip
+  // s of every member, then strip s + 1), so that the reads of one long-operand
+  // strip by the group's members follow each other and all but the first hit
+  // L2 instead of DRAM.  group[i] = size of the group of cbs[i] (1 when
+  // alone).  Returns whether any group has two or more members.
+  bool group_shared_long(bool small_rows, std::vector<int>& group) {
     const int n = static_cast<int>(cbs.size());
     std::vector<int> parent(n);
     std::iota(parent.begin(), parent.end(), 0);
@@ -352,7 +361,11 @@ struct GemmPlan {
           shared = true;
         }
       }
+    group.assign(n, 1);
     if (!shared) return false;
+    // components in order of their first block; inside one, members of equal
+    // long extent form a group (blocks that share operand rows have the same
+    // extent, so this splits nothing in practice)
     std::vector<std::vector<int>> comps;
     std::vector<int> comp_of(n, -1);
     for (int c = 0; c < n; ++c) {
@@ -364,42 +377,24 @@ struct GemmPlan {
       comps[comp_of[r]].push_back(c);
     }
     std::vector<GemmCBlock> nc;
-    std::vector<GemmPair> np;
     nc.reserve(cbs.size());
-    np.reserve(pairs.size());
+    bool any = false;
     for (auto& comp : comps) {
-      int64_t lmax = 0;
-      for (int c : comp) lmax = std::max<int64_t>(lmax, small_rows ? cbs[c].N : cbs[c].M);
-      const int64_t step = comp.size() > 1 ? kThinChunk : std::max<int64_t>(lmax, 1);
-      for (int64_t l0 = 0; l0 < std::max<int64_t>(lmax, 1); l0 += step)
-        for (int c : comp) {
-          const GemmCBlock& b = cbs[c];
-          const int64_t L = small_rows ? b.N : b.M;
-          if (l0 > 0 && l0 >= L) continue;
-          const int32_t len = static_cast<int32_t>(std::min<int64_t>(step, L - l0));
-          GemmCBlock s = b;
-          if (small_rows) {
-            s.c_off = b.c_off + l0 * b.ldc;
-            s.N = len;
-          } else {
-            s.c_off = b.c_off + l0;
-            s.M = len;
-          }
-          s.pair_begin = static_cast<int32_t>(np.size());
-          for (int p = b.pair_begin; p < b.pair_end; ++p) {
-            GemmPair q = pairs[p];
-            if (small_rows) q.y_off += yT ? l0 : l0 * q.ldy;
-            else q.x_off += xT ? l0 * q.ldx : l0;
-            np.push_back(q);
-          }
-          s.pair_end = static_cast<int32_t>(np.size());
-          nc.push_back(s);
+      auto len = [&](int c) { return small_rows ? cbs[c].N : cbs[c].M; };
+      std::stable_sort(comp.begin(), comp.end(), [&](int a, int b) { return len(a) < len(b); });
+      for (size_t a = 0; a < comp.size();) {
+        size_t b = a;
+        while (b < comp.size() && len(comp[b]) == len(comp[a])) ++b;
+        for (size_t k = a; k < b; ++k) {
+          nc.push_back(cbs[comp[k]]);
+          group[nc.size() - 1] = static_cast<int>(b - a);
         }
+        any = any || b - a > 1;
+        a = b;
+      }
     }
-    require(np.size() < (1ULL << 31), SB_ERR_INVALID_ARG, "too many GEMM block pairs in one launch");
     cbs.swap(nc);
-    pairs.swap(np);
-    return true;
+    return any;
   }
 
   // Split-K factor for ntiles tiles averaging kt_avg k-tiles: split while the

@@ -450,11 +450,13 @@ __global__ void __launch_bounds__(kThinThreads, 5)
     const int mid = (lo + hi + 1) >> 1;
     if (cblocks[mid].tile_begin <= bid) lo = mid; else hi = mid - 1;
   }
-  const GemmCBlock cb = cblocks[lo];
+  // a group of S = mtiles blocks ending at lo numbers its strips in turn
+  const int grp = cblocks[lo].mtiles, rel = bid - cblocks[lo].tile_begin;
+  const GemmCBlock cb = cblocks[lo - (grp - 1) + rel % grp];
   const int M = cb.M, N = cb.N;
   const int L = SR ? N : M;   // long extent
   const int ns = SR ? M : N;  // short extent (<= 16)
-  const int l0 = (bid - cb.tile_begin) * kThinBig;
+  const int l0 = (rel / grp) * kThinBig;
   const int tid = threadIdx.x;
 
   // Load geometry: the long tile's elements of this thread share their k
@@ -624,8 +626,10 @@ __global__ void __launch_bounds__(kThinThreads, 5)
       if (cblocks[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
     }
     cur = lo;
-    cb = cblocks[lo];
-    l0 = (tile - cb.tile_begin) * kThinBig;
+    // a group of S = mtiles blocks ending at lo numbers its strips in turn
+    const int grp = cblocks[lo].mtiles, rel = tile - cblocks[lo].tile_begin;
+    cb = cblocks[lo - (grp - 1) + rel % grp];
+    l0 = (rel / grp) * kThinBig;
   };
   auto load = [&](int stage, const GemmPair& pr, const GemmCBlock& cb, int l0) {
     const int K = pr.K;

@@ -20,10 +20,9 @@ namespace sb {
 // Tiles of C block c are CTAs [tile_begin, tile_begin + mtiles*ntiles); the
 // kernel finds its C block by binary search over tile_begin, so no per-tile
 // descriptor list is built or uploaded.
-// ldc: column stride of the C block in C.  It equals M except for sub-blocks
-// that are a row range of a larger block (the edges of launch_gemm_f64_edges,
-// the long-row chunks of launch_gemm_f64_skinny); the thin kernels with small
-// rows (small_rows) require ldc == M.  tshape: tile shape of the block in
+// ldc: column stride of the C block in C.  It equals M except for the edge
+// sub-blocks of launch_gemm_f64_edges (a row range of a larger block); the
+// thin kernels with small rows (small_rows) require ldc == M.  tshape: tile shape of the block in
 // launch_gemm_f64_edges (0 = 64x64, 1 = 64x32, 2 = 32x64, 3 = 64x48,
 // 4 = 48x64), else 0.
 struct GemmCBlock {
@@ -68,7 +67,10 @@ cudaError_t launch_gemm_f64_edges(const double* X, const double* Y, double* C, c
 // Thin variant for launches whose every pair has K <= 16 and whose C blocks
 // have min(M, N) <= 16 (HBM-bound): DMMA on 128 x 16 strips of the long side,
 // cp.async double buffering across pairs.  Strips of C block c:
-// [tile_begin, tile_begin + ceil(long/128)) (mtiles unused).  persistent: a
+// [tile_begin, tile_begin + ceil(long/128)) when mtiles == 1; a group of S
+// consecutive blocks with equal long extent, each carrying the group's
+// tile_begin and mtiles = S, takes strips in turn (strip s of member j is
+// tile_begin + s*S + j).  persistent: a
 // grid of 5 CTAs per SM walks the strips with the copy pipeline running
 // across strip boundaries and stores C from the fragments (needs >= 1 pair
 // per C block); otherwise one CTA per strip with shared-memory staged stores.

@@ -1,9 +1,9 @@
 """Thin block GEMMs (K <= 16, one side <= 16) whose output blocks share blocks
-of the long operand: the planner cuts those output blocks into chunks of
-32768 long-side elements and interleaves the chunks of blocks that read the
-same operand block.  Results must equal numpy and, bit for bit, the tiled
-kernel (same pair order, same DMMA k-steps), for both thin orientations and
-for the persistent and the one-CTA-per-strip thin kernels.
+of the long operand: the planner groups the output blocks that read the same
+operand block and the kernels take the group's strips in turn (strip s of
+every member, then strip s + 1).  Results must equal numpy and, bit for bit,
+the tiled kernel (same pair order, same DMMA k-steps), for both thin
+orientations and for the persistent and the one-CTA-per-strip thin kernels.
 """
 import contextlib
 import os
@@ -43,7 +43,7 @@ def _bs(sb, ctx, dense, n2):
 @pytest.mark.parametrize("long_rows", [True, False])
 def test_shared_long_operand_chunks(sb, capfd, long_rows):
     rng = np.random.Generator(np.random.PCG64(21))
-    M, K, N = 70000, 6, 5  # three 32768-long chunks per output block
+    M, K, N = 70000, 6, 5  # 547 strips per output block, three blocks per group
     Ad = rng.standard_normal((2, M, K))
     Bd = rng.standard_normal((3, N, K))
     lC = ["i", "j", "m", "n"] if long_rows else ["i", "j", "n", "m"]
