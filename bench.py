@@ -144,6 +144,76 @@ def traffic_per_launch(chi: int, kernel: str):
     return None if t is None else {"bytes": t[0], "source": t[1]}
 
 
+def cublas_block_lists(layout, steps: int = 10):
+    """cuBLAS DGEMM (torch.matmul / addmm) on the block lists of the two
+    tensor-bound H_eff steps, psi*L and R*T3: per output block one GEMM per
+    matched pair, accumulated in pair order, on random operands of the same
+    shapes (unpadded sector extents).  Returns ms per step for both steps
+    together, eager and replayed from a CUDA graph."""
+    import torch
+    from sparsebackends_b200 import qn
+    lab = layout.labels
+
+    def ext(kv, x):
+        q = qn.GRADE[x]
+        return qn._link_of(layout, q).dims[kv[q] - 1]
+
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    work, flops = [], 0
+    for st in qn.chain_structure(layout):
+        if st["C"] not in ("T1", "T4"):
+            continue
+        lc = lab[st["C"]]
+        pc = len(lc) - layout.n2[st["C"]]
+        cbs = {}
+        for kv in st["pairs"]:
+            m = int(np.prod([ext(kv, x) for x in st["keepA"]] or [1]))
+            n = int(np.prod([ext(kv, x) for x in st["keepB"]] or [1]))
+            k = int(np.prod([ext(kv, x) for x in st["red"]] or [1]))
+            cbs.setdefault(tuple(kv[x] for x in lc[:pc]), []).append((m, n, k))
+        for prs in cbs.values():
+            m, n = prs[0][0], prs[0][1]
+            ops = [(torch.randn((m, k), dtype=torch.float64, device="cuda", generator=gen),
+                    torch.randn((k, n), dtype=torch.float64, device="cuda", generator=gen)) for _, _, k in prs]
+            work.append((torch.empty((m, n), dtype=torch.float64, device="cuda"), ops))
+            flops += sum(2 * m * n * k for _, _, k in prs)
+
+    def run():
+        for c, ops in work:
+            torch.matmul(ops[0][0], ops[0][1], out=c)
+            for x, y in ops[1:]:
+                c.addmm_(x, y)
+
+    def timed_ms(fn):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(steps):
+            fn()
+        e.record()
+        e.synchronize()
+        return s.elapsed_time(e) / steps
+
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    eager = timed_ms(run)
+    graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        run()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(graph):
+            run()
+    torch.cuda.synchronize()
+    replay = timed_ms(graph.replay)
+    del graph, work
+    torch.cuda.empty_cache()
+    return {"what": "cuBLAS DGEMM (torch.matmul / addmm) per output block and matched pair, on the psi*L and R*T3 "
+                    "block lists of this workload (unpadded extents, random operands of the same shapes)",
+            "gflop_per_step": flops / 1e9, "ms_per_step": eager, "tflops": flops / eager / 1e9,
+            "graph_ms_per_step": replay, "graph_tflops": flops / replay / 1e9}
+
+
 def fp64_peak_tflops():
     import torch
     n = 8192
@@ -302,6 +372,7 @@ def run_ours(args, world, rank, local):
     agree = float(np.linalg.norm(d_r - d_u) / max(np.linalg.norm(d_u), 1e-300))
     assert agree < 1e-12, agree
     peak = fp64_peak_tflops() if rank == 0 else 0.0
+    library = cublas_block_lists(layout) if rank == 0 else None
     torch.cuda.synchronize()
 
     def timed(fn, steps, profile=False):
@@ -542,6 +613,7 @@ def run_ours(args, world, rank, local):
                                "traffic": traffic_per_launch(args.chi, "k_gemm_thin"), "launches": th["launches"],
                                "kernel_ms_per_step": th["ms"] / args.steps},
         "kernel_time_share": {k: v["ms"] / max(1e-9, sum(x["ms"] for x in prof.values())) for k, v in prof.items()},
+        "library_baseline": library,
         "uniform_format": {"value": value_u, "ms_per_step": ms_u / args.steps,
                            "gflops_executed": flops_pad * value_u / 1e9,
                            "gemm_tflops": (gu["flops"] + gtu["flops"]) / ((gu["ms"] + gtu["ms"]) * 1e-3) / 1e12
