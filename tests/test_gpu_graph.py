@@ -7,7 +7,10 @@
   value and vector as on the eager operator;
 * a call that reads values back to the host (value-dependent block creation)
   cannot be captured: the capture fails with an error status and the context
-  keeps working for eager calls.
+  keeps working for eager calls;
+* a capture that holds the first kernel launches of a process (kernel
+  attributes and persistent grid sizes are set up then) replays to the eager
+  result.
 """
 import numpy as np
 import pytest
@@ -86,3 +89,37 @@ def test_capture_of_a_readback_call_fails_cleanly():
     C2 = sb.NewBlockSparseSorted.empty((3, 2, 4, 6), 2, ctx=ctx)
     sb.contract_(C2, lab[0], A, lab[1], B, lab[2])
     assert np.array_equal(C2.data, want)
+
+
+_FIRST_CALL_CAPTURED = r"""
+import sys
+sys.path.insert(0, {root!r})
+import numpy as np
+from tests.test_gpu_graph import _setup
+sb, qn, lay, ctx, T, psi, rng = _setup({ragged}, chi=64)
+chain = qn.HeffChain(lay, ctx)
+# no eager call before: the GEMM kernels' first launches of this process are captured
+g = ctx.capture(lambda: chain.apply(psi, T["L"], T["W1"], T["W2"], T["R"]),
+                keep=[psi, T["L"], T["W1"], T["W2"], T["R"], *chain.out.values()])
+g.launch()
+got = chain.out["T4"].data
+eager = qn.HeffChain(lay, ctx)
+want = eager.apply(psi, T["L"], T["W1"], T["W2"], T["R"]).data
+assert np.array_equal(got, want)
+del g
+print("ok")
+"""
+
+
+@pytest.mark.parametrize("ragged", [True, False])
+def test_capture_as_the_first_launches_of_a_process(ragged):
+    """Kernel attributes and persistent-grid sizes are set up on a kernel's
+    first launch; a capture that holds those first launches (a fresh process,
+    nothing run eagerly before) must replay to the eager result."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", _FIRST_CALL_CAPTURED.format(root=root, ragged=ragged)],
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0 and out.stdout.strip().endswith("ok"), out.stderr[-2000:]
