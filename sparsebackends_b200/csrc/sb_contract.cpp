@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstdio>
+#include <cstring>
 #include <map>
 #include <numeric>
 #include <unordered_map>
@@ -199,6 +200,47 @@ void reset_output(Ctx* ctx, Tensor& C, int64_t nkeys, int64_t payload) {
 }
 
 // ── launch helpers ────────────────────────────────────────────────────────
+// A prepared block GEMM: the plan arrays on the device and the launch
+// parameters, so that a contraction with an unchanged block structure can be
+// launched again without planning or uploads (the plan cache of shared_bb).
+struct GemmLaunch {
+  enum Kind { NONE, THIN, TILED, EDGES } kind = NONE;
+  DevBuf dc, dp;
+  int32_t ncb = 0;
+  int64_t n = 0;  // strips (thin) or tiles
+  bool xT = false, yT = false, small_rows = false, persistent = false;
+  int small_max = 0, k_max = 0, splitk = 1, bm = 64, bn = 64;
+  GemmShape shape = GemmShape::T64x64;
+  double flops = 0.0, bytes = 0.0;
+  char desc[sizeof(Ctx::gemm_desc)] = "";
+  void run(Ctx* ctx, const double* X, const double* Y, double* C) const {
+    if (kind == NONE) return;
+    std::memcpy(ctx->gemm_desc, desc, sizeof(desc));
+    if (kind == THIN) {
+      {
+        ProfScope ps(ctx, PROF_GEMM_THIN, flops, bytes);
+        SB_CK(launch_gemm_f64_skinny(X, Y, C, dc.as<GemmCBlock>(), ncb, dp.as<GemmPair>(), n, xT, yT, small_rows,
+                                     small_max, k_max, ctx->stream, persistent));
+      }
+      ctx->note_launch();
+      return;
+    }
+    DevBuf part;
+    const int64_t tile = kind == EDGES ? 64 * 64 : static_cast<int64_t>(bm) * bn;
+    if (splitk > 1) part = DevBuf(ctx, static_cast<size_t>(splitk) * n * tile * sizeof(double));
+    {
+      ProfScope ps(ctx, PROF_GEMM, flops, bytes);
+      if (kind == EDGES)
+        SB_CK(launch_gemm_f64_edges(X, Y, C, dc.as<GemmCBlock>(), ncb, dp.as<GemmPair>(), n, xT, yT, ctx->stream,
+                                    splitk, part.d()));
+      else
+        SB_CK(launch_gemm_f64(X, Y, C, dc.as<GemmCBlock>(), ncb, dp.as<GemmPair>(), n, xT, yT, shape, ctx->stream,
+                              splitk, part.d()));
+    }
+    ctx->note_launch(splitk > 1 ? 2 : 1);
+  }
+};
+
 struct GemmPlan {
   std::vector<GemmCBlock> cbs;
   std::vector<GemmPair> pairs;
@@ -217,7 +259,13 @@ struct GemmPlan {
     cbs.back().pair_end = static_cast<int32_t>(pairs.size());
   }
   void launch(Ctx* ctx, const double* X, const double* Y, double* C, bool xT, bool yT) {
-    if (cbs.empty()) return;
+    prepare(ctx, xT, yT).run(ctx, X, Y, C);
+  }
+  GemmLaunch prepare(Ctx* ctx, bool xT, bool yT) {
+    GemmLaunch g;
+    g.xT = xT;
+    g.yT = yT;
+    if (cbs.empty()) return g;
     int64_t M = 0, N = 0, Kmax = 0;
     double flops = 0.0, bytes = 0.0;
     for (auto& c : cbs) {
@@ -257,18 +305,20 @@ struct GemmPlan {
         require(nctas < (1LL << 31), SB_ERR_INVALID_ARG, "too many GEMM strips in one launch");
         i += S;
       }
-      const bool persistent = ctx->gemm_thin != 1 && every_block_has_pairs;
-      std::snprintf(ctx->gemm_desc, sizeof(ctx->gemm_desc), "thin%s %s%s", persistent ? " persistent" : "",
+      g.persistent = ctx->gemm_thin != 1 && every_block_has_pairs;
+      std::snprintf(g.desc, sizeof(g.desc), "thin%s %s%s", g.persistent ? " persistent" : "",
                     small_rows ? "rows<=16" : "cols<=16", interleaved ? " interleaved" : "");
-      DevBuf dc = upload(ctx, cbs), dp = upload(ctx, pairs);
-      {
-        ProfScope ps(ctx, PROF_GEMM_THIN, flops, bytes);
-        SB_CK(launch_gemm_f64_skinny(X, Y, C, dc.as<GemmCBlock>(), static_cast<int32_t>(cbs.size()), dp.as<GemmPair>(),
-                                     nctas, xT, yT, small_rows, static_cast<int>(small_rows ? M : N),
-                                     static_cast<int>(Kmax), ctx->stream, persistent));
-      }
-      ctx->note_launch();
-      return;
+      g.kind = GemmLaunch::THIN;
+      g.dc = upload(ctx, cbs);
+      g.dp = upload(ctx, pairs);
+      g.ncb = static_cast<int32_t>(cbs.size());
+      g.n = nctas;
+      g.small_rows = small_rows;
+      g.small_max = static_cast<int>(small_rows ? M : N);
+      g.k_max = static_cast<int>(Kmax);
+      g.flops = flops;
+      g.bytes = bytes;
+      return g;
     }
     // Tile shape from the FLOP-weighted block shape (ragged launches mix
     // large and small blocks; the heavy ones decide).
@@ -286,8 +336,8 @@ struct GemmPlan {
     if (an <= 32 && am >= 128) shape = GemmShape::T128x32;
     else if (am <= 32 && an >= 128) shape = GemmShape::T32x128;
     else if (am >= 1024 && an >= 512) shape = am >= an ? GemmShape::T128x64 : GemmShape::T64x128;
-    if (shape == GemmShape::T64x64 && ctx->gemm_tile < 0 && ctx->gemm_edges != 0 && launch_edges(ctx, X, Y, C, xT, yT, flops, bytes))
-      return;
+    if (shape == GemmShape::T64x64 && ctx->gemm_tile < 0 && ctx->gemm_edges != 0 && prepare_edges(ctx, g, flops, bytes))
+      return g;
     if (shape == GemmShape::T64x64) {
       // few 64x64 tiles with long K (the split-K regime): smaller tiles with a
       // deeper pipeline keep more CTAs busy
@@ -320,16 +370,19 @@ struct GemmPlan {
     }
     kt_avg = ntiles ? kt_avg / ntiles : 0;
     const int splitk = choose_splitk(ctx, ntiles, kt_avg);
-    std::snprintf(ctx->gemm_desc, sizeof(ctx->gemm_desc), "tiled %dx%d sk%d", bm, bn, splitk);
-    DevBuf dc = upload(ctx, cbs), dp = upload(ctx, pairs);
-    DevBuf part;
-    if (splitk > 1) part = DevBuf(ctx, static_cast<size_t>(splitk) * ntiles * bm * bn * sizeof(double));
-    {
-      ProfScope ps(ctx, PROF_GEMM, flops, bytes);
-      SB_CK(launch_gemm_f64(X, Y, C, dc.as<GemmCBlock>(), static_cast<int32_t>(cbs.size()), dp.as<GemmPair>(), ntiles,
-                            xT, yT, shape, ctx->stream, splitk, part.d()));
-    }
-    ctx->note_launch(splitk > 1 ? 2 : 1);
+    std::snprintf(g.desc, sizeof(g.desc), "tiled %dx%d sk%d", bm, bn, splitk);
+    g.kind = GemmLaunch::TILED;
+    g.dc = upload(ctx, cbs);
+    g.dp = upload(ctx, pairs);
+    g.ncb = static_cast<int32_t>(cbs.size());
+    g.n = ntiles;
+    g.shape = shape;
+    g.bm = bm;
+    g.bn = bn;
+    g.splitk = splitk;
+    g.flops = flops;
+    g.bytes = bytes;
+    return g;
   }
 
   // Thin launches (K <= 16): output blocks whose pairs read the same block of
@@ -416,8 +469,8 @@ struct GemmPlan {
   // launching nothing, when that saves < 3% of the padded 64x64 work.
   static int edge_rows(int shape) { return shape == 2 ? 32 : shape == 4 ? 48 : 64; }
   static int edge_cols(int shape) { return shape == 1 ? 32 : shape == 3 ? 48 : 64; }
-  bool launch_edges(Ctx* ctx, const double* X, const double* Y, double* C, bool xT, bool yT, double flops,
-                    double bytes) {
+  bool prepare_edges(Ctx* ctx, GemmLaunch& g, double flops, double bytes) {
+    const bool xT = g.xT, yT = g.yT;
     auto up = [](int64_t v, int64_t t) { return (v + t - 1) / t * t; };
     auto body64 = [](int64_t v) { const int64_t e = v % 64; return e > 0 && e <= 48 ? v - e : v; };
     auto edge = [](int64_t e) -> int64_t { return e <= 32 ? 32 : 48; };
@@ -490,18 +543,16 @@ struct GemmPlan {
     long long nshape[5] = {0, 0, 0, 0, 0};
     for (auto& b : sc) nshape[b.tshape] += static_cast<long long>(b.mtiles) * ((b.N + edge_cols(b.tshape) - 1) /
                                                                                 edge_cols(b.tshape));
-    std::snprintf(ctx->gemm_desc, sizeof(ctx->gemm_desc),
-                  "edges 64x64:%lld 64x32:%lld 32x64:%lld 64x48:%lld 48x64:%lld sk%d", nshape[0], nshape[1],
-                  nshape[2], nshape[3], nshape[4], splitk);
-    DevBuf dc = upload(ctx, sc), dp = upload(ctx, ep);
-    DevBuf part;
-    if (splitk > 1) part = DevBuf(ctx, static_cast<size_t>(splitk) * ntiles * 64 * 64 * sizeof(double));
-    {
-      ProfScope ps(ctx, PROF_GEMM, flops, bytes);
-      SB_CK(launch_gemm_f64_edges(X, Y, C, dc.as<GemmCBlock>(), static_cast<int32_t>(sc.size()), dp.as<GemmPair>(),
-                                  ntiles, xT, yT, ctx->stream, splitk, part.d()));
-    }
-    ctx->note_launch(splitk > 1 ? 2 : 1);
+    std::snprintf(g.desc, sizeof(g.desc), "edges 64x64:%lld 64x32:%lld 32x64:%lld 64x48:%lld 48x64:%lld sk%d",
+                  nshape[0], nshape[1], nshape[2], nshape[3], nshape[4], splitk);
+    g.kind = GemmLaunch::EDGES;
+    g.dc = upload(ctx, sc);
+    g.dp = upload(ctx, ep);
+    g.ncb = static_cast<int32_t>(sc.size());
+    g.n = ntiles;
+    g.splitk = splitk;
+    g.flops = flops;
+    g.bytes = bytes;
     return true;
   }
 };
@@ -835,10 +886,86 @@ std::vector<int> csrc_AB(const Labels& lC, int PC, const Op& A, const Op& B, boo
   return src;
 }
 
+// Plan cache of contract_shared! (BS x BS).  An entry holds what a call
+// derives from block structure alone: the output keys and layout, and the
+// prepared GEMM (plan arrays already on the device).  It is used when the
+// labels and both operands' structure (dims, tail count, keys, block extents)
+// equal the entry's exactly, as in the H_eff contractions of every Lanczos
+// step; nothing in it depends on values.  Not used while a capture is open
+// (a graph keeps the buffers allocated during its capture, the cache keeps
+// its own).  The 32 most recent structures are kept.
+struct SharedPlanEntry {
+  std::vector<uint64_t> sig;  // labels of C, A, B; dims and tail counts; flags
+  std::vector<int64_t> akeys, abd, bkeys, bbd;
+  int64_t c_nkeys = 0, c_payload = 0;
+  std::vector<int64_t> c_keys, c_bdims, c_boff;
+  bool c_ragged = false;
+  GemmLaunch gemm;
+};
+struct SharedPlanCache {
+  std::vector<std::unique_ptr<SharedPlanEntry>> entries;  // most recent last
+  static constexpr size_t kMax = 32;
+};
+
+std::vector<uint64_t> shared_signature(const Tensor& C, const Labels& lC, const Op& A0, const Op& B0) {
+  std::vector<uint64_t> sig;
+  auto labels = [&](const Labels& l) {
+    sig.push_back(l.size());
+    for (auto& x : l) {
+      sig.push_back(x.id);
+      sig.push_back(x.plev);
+    }
+  };
+  // C contributes only its shape (it is overwritten); the operands also their
+  // layout flag and block count (their keys and extents are compared apart)
+  auto shape = [&](const Tensor& t, bool operand) {
+    sig.push_back(static_cast<uint64_t>(t.kind));
+    sig.push_back(t.dims.size());
+    for (auto d : t.dims) sig.push_back(static_cast<uint64_t>(d));
+    sig.push_back(static_cast<uint64_t>(t.n2));
+    if (!operand) return;
+    sig.push_back(t.ragged ? 1 : 0);
+    sig.push_back(static_cast<uint64_t>(t.nkeys));
+  };
+  labels(lC);
+  labels(A0.labels);
+  labels(B0.labels);
+  shape(C, false);
+  shape(*A0, true);
+  shape(*B0, true);
+  return sig;
+}
+
 void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Labels& shared) {
   ctx->kernel_name = "contract_shared! (BS x BS)";
   const int PC = C.P();
   SharedPlan sp = plan_shared(lC, PC, A0, B0, shared, false);
+  const bool cacheable = ctx->plan_cache_on && !ctx->capturing;
+  std::vector<uint64_t> sig;
+  SharedPlanCache* cache = nullptr;
+  if (cacheable) {
+    if (!ctx->plan_cache) ctx->plan_cache = std::make_shared<SharedPlanCache>();
+    cache = static_cast<SharedPlanCache*>(ctx->plan_cache.get());
+    sig = shared_signature(C, lC, A0, B0);
+    for (auto it = cache->entries.rbegin(); it != cache->entries.rend(); ++it) {
+      const SharedPlanEntry& e = **it;
+      if (e.sig != sig || e.akeys != A0->keys || e.bkeys != B0->keys || e.abd != A0->bdims || e.bbd != B0->bdims)
+        continue;
+      Op A = permuted(ctx, A0, sp.permA);
+      Op B = permuted(ctx, B0, sp.permB);
+      reset_output(ctx, C, e.c_nkeys, e.c_payload);
+      C.keys = e.c_keys;
+      if (e.c_ragged) {
+        C.ragged = true;
+        C.bdims = e.c_bdims;
+        C.boff = e.c_boff;
+      }
+      if (sp.mode == Mode::AthenB) e.gemm.run(ctx, A->data.d(), B->data.d(), C.data.d());
+      else e.gemm.run(ctx, B->data.d(), A->data.d(), C.data.d());
+      ctx->plan_cache_hit = true;
+      return;
+    }
+  }
   Op A = permuted(ctx, A0, sp.permA);
   Op B = permuted(ctx, B0, sp.permB);
   const int PA = A->P(), PB = B->P();
@@ -928,8 +1055,26 @@ void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0
       else gp.add_pair(yb, xa, d.k, d.k, d.m);
     }
   }
-  if (athenb) gp.launch(ctx, A->data.d(), B->data.d(), C.data.d(), false, false);
-  else gp.launch(ctx, B->data.d(), A->data.d(), C.data.d(), true, true);
+  GemmLaunch g = athenb ? gp.prepare(ctx, false, false) : gp.prepare(ctx, true, true);
+  if (athenb) g.run(ctx, A->data.d(), B->data.d(), C.data.d());
+  else g.run(ctx, B->data.d(), A->data.d(), C.data.d());
+  if (cache) {
+    auto e = std::make_unique<SharedPlanEntry>();
+    e->sig = std::move(sig);
+    e->akeys = A0->keys;
+    e->abd = A0->bdims;
+    e->bkeys = B0->keys;
+    e->bbd = B0->bdims;
+    e->c_nkeys = C.nkeys;
+    e->c_payload = C.payload_len();
+    e->c_keys = C.keys;
+    e->c_ragged = C.ragged;
+    e->c_bdims = C.bdims;
+    e->c_boff = C.boff;
+    e->gemm = std::move(g);
+    if (cache->entries.size() >= SharedPlanCache::kMax) cache->entries.erase(cache->entries.begin());
+    cache->entries.push_back(std::move(e));
+  }
 }
 
 // ══════════════════════════ BS × Dense ═══════════════════════════════════

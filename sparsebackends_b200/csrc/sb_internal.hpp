@@ -92,6 +92,13 @@ struct Ctx {
   // SPARSEB_GEMM_EDGES=0 keeps 64x64-tile launches in one tile shape (tuning);
   // -1 = auto: column / row edges of <= 32 go to 64x32 / 32x64 tiles.
   int gemm_edges = -1;
+  // Plan cache of the BS x BS contract_shared! path (sb_contract.cpp): the
+  // output block structure and the prepared block GEMM of recent
+  // contractions, reused when the same labels meet operands of the same block
+  // structure.  SPARSEB_PLAN_CACHE=0 turns it off.  Opaque here.
+  bool plan_cache_on = true;
+  bool plan_cache_hit = false;  // the last contraction reused a cached plan (trace line)
+  std::shared_ptr<void> plan_cache;
   // Pinned staging ring for host-to-device plan uploads: a copy from pinned
   // memory does not synchronise the stream, so host planning of the next
   // contraction overlaps the device work of the current one.  A slot is
