@@ -82,6 +82,53 @@ Op permuted(Ctx* ctx, const Op& in, const std::vector<int>& perm) {
   return o;
 }
 
+// A block-sparse operand whose permutation moves prefix axes only keeps
+// every block's payload as it is: the permuted tensor re-sorts the keys and
+// points each block at its payload in the original tensor (no copy, no
+// launch).  Other permutations copy as `permuted` does.
+Op permuted_keys_only(Ctx* ctx, const Op& in, const std::vector<int>& perm) {
+  const Tensor& A = *in.t;
+  if (is_identity(perm) || A.kind != BS) return permuted(ctx, in, perm);
+  const int N = A.N(), P = A.P();
+  for (int r = 0; r < A.n2; ++r)
+    if (perm[P + r] != P + r + 1) return permuted(ctx, in, perm);
+  check_no_cross_perm(perm, N, P);
+  std::vector<int64_t> dims(N);
+  for (int j = 0; j < N; ++j) dims[j] = A.dims[perm[j] - 1];
+  auto v = make_tensor(ctx, BS, dims, A.n2);
+  const int64_t n = A.nkeys;
+  std::vector<int64_t> nk(n * P), lin(n), ord(n);
+  for (int64_t i = 0; i < n; ++i) {
+    for (int j = 0; j < P; ++j) nk[i * P + j] = A.key(i)[perm[j] - 1];
+    lin[i] = lin0(&nk[i * P], dims.data(), P);
+  }
+  std::iota(ord.begin(), ord.end(), 0);
+  std::stable_sort(ord.begin(), ord.end(), [&](int64_t a, int64_t b) { return lin[a] < lin[b]; });
+  v->keys.resize(n * P);
+  v->voff.resize(n);
+  v->nkeys = n;
+  v->ragged = A.ragged;
+  if (A.ragged) {
+    v->bdims.resize(n * A.n2);
+    v->boff.assign(n + 1, 0);
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t o = ord[i];
+    std::copy(&nk[o * P], &nk[o * P] + P, &v->keys[i * P]);
+    v->voff[i] = A.block_off(o);
+    if (A.ragged) {
+      for (int r = 0; r < A.n2; ++r) v->bdims[i * A.n2 + r] = A.block_dim(o, r);
+      v->boff[i + 1] = v->boff[i] + A.block_len(o);
+    }
+  }
+  v->vdata = A.payload();
+  Op out;
+  out.owned = std::move(v);
+  out.t = out.owned.get();
+  for (int p : perm) out.labels.push_back(in.labels[p - 1]);
+  return out;
+}
+
 // _find_permutation_for_tensor (contract_bs_bs.jl:33-45); axisr is 1-based.
 std::vector<int> perm_r_last(int P, int N, int axisr) {
   std::vector<int> perm;
@@ -951,8 +998,8 @@ void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0
       const SharedPlanEntry& e = **it;
       if (e.sig != sig || e.akeys != A0->keys || e.bkeys != B0->keys || e.abd != A0->bdims || e.bbd != B0->bdims)
         continue;
-      Op A = permuted(ctx, A0, sp.permA);
-      Op B = permuted(ctx, B0, sp.permB);
+      Op A = permuted_keys_only(ctx, A0, sp.permA);
+      Op B = permuted_keys_only(ctx, B0, sp.permB);
       reset_output(ctx, C, e.c_nkeys, e.c_payload);
       C.keys = e.c_keys;
       if (e.c_ragged) {
@@ -960,14 +1007,14 @@ void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0
         C.bdims = e.c_bdims;
         C.boff = e.c_boff;
       }
-      if (sp.mode == Mode::AthenB) e.gemm.run(ctx, A->data.d(), B->data.d(), C.data.d());
-      else e.gemm.run(ctx, B->data.d(), A->data.d(), C.data.d());
+      if (sp.mode == Mode::AthenB) e.gemm.run(ctx, A->payload(), B->payload(), C.data.d());
+      else e.gemm.run(ctx, B->payload(), A->payload(), C.data.d());
       ctx->plan_cache_hit = true;
       return;
     }
   }
-  Op A = permuted(ctx, A0, sp.permA);
-  Op B = permuted(ctx, B0, sp.permB);
+  Op A = permuted_keys_only(ctx, A0, sp.permA);
+  Op B = permuted_keys_only(ctx, B0, sp.permB);
   const int PA = A->P(), PB = B->P();
   const int nkA = static_cast<int>(sp.dkA.size()), nkB = static_cast<int>(sp.dkB.size()),
             nred = static_cast<int>(sp.red_dense.size());
@@ -1056,8 +1103,8 @@ void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0
     }
   }
   GemmLaunch g = athenb ? gp.prepare(ctx, false, false) : gp.prepare(ctx, true, true);
-  if (athenb) g.run(ctx, A->data.d(), B->data.d(), C.data.d());
-  else g.run(ctx, B->data.d(), A->data.d(), C.data.d());
+  if (athenb) g.run(ctx, A->payload(), B->payload(), C.data.d());
+  else g.run(ctx, B->payload(), A->payload(), C.data.d());
   if (cache) {
     auto e = std::make_unique<SharedPlanEntry>();
     e->sig = std::move(sig);

@@ -190,6 +190,12 @@ struct Tensor {
   bool ragged = false;
   std::vector<int64_t> bdims;
   std::vector<int64_t> boff;
+  // Key-reordering view of another tensor's payload (the operands of
+  // contract_shared! whose permutation moves prefix axes only): vdata is the
+  // other tensor's payload and voff[i] the offset of block i in it; data
+  // stays empty.  Only the contraction that made the view reads it.
+  const double* vdata = nullptr;
+  std::vector<int64_t> voff;
 
   int N() const { return static_cast<int>(dims.size()); }
   int P() const { return N() - n2; }
@@ -206,7 +212,8 @@ struct Tensor {
   const int64_t* key(int64_t i) const { return keys.data() + i * (kind == COO ? N() : P()); }
   int64_t key_len() const { return kind == COO ? N() : P(); }
   // Per-block layout, valid for uniform and ragged tensors.
-  int64_t block_off(int64_t i) const { return ragged ? boff[i] : i * blksize(); }
+  int64_t block_off(int64_t i) const { return !voff.empty() ? voff[i] : ragged ? boff[i] : i * blksize(); }
+  const double* payload() const { return vdata ? vdata : data.d(); }
   int64_t block_len(int64_t i) const { return ragged ? boff[i + 1] - boff[i] : blksize(); }
   int64_t block_dim(int64_t i, int t) const { return ragged ? bdims[i * n2 + t] : dims[P() + t]; }
   int64_t payload_len() const {
