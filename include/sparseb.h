@@ -155,6 +155,15 @@ SB_API sb_status sb_tensor_block_dims(const sb_tensor* t, int* ragged, int64_t* 
 SB_API sb_status sb_tensor_to_uniform(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out);
 SB_API sb_status sb_tensor_to_ragged(sb_ctx* ctx, const sb_tensor* A, const int64_t* block_dims,
                                      int check_zero, sb_tensor** out);
+/* Zero padding removed from the values: the ragged tensor whose blocks are
+ * A's blocks cropped, axis by axis, to the smallest extents that keep every
+ * nonzero entry (an all-zero block keeps extent 1).  For operands in the
+ * reference's layout (src/blocksparse/storage.jl:3-9), where every U(1)
+ * sector is zero-padded to the largest one, this recovers the sector extents
+ * without the caller knowing them; contractions on the result equal those
+ * of A up to rounding (sb_tensor_to_uniform pads a result back).  No
+ * counterpart in the reference.  One device scan and one read-back.          */
+SB_API sb_status sb_tensor_crop_padding(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out);
 /* Device pointer and length (doubles) of the payload (dense data, block data,
  * COO values or aliased templates), for zero-copy interop.                   */
 SB_API sb_status sb_tensor_device_data(const sb_tensor* t, double** d_ptr, int64_t* len);

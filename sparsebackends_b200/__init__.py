@@ -40,7 +40,7 @@ __all__ = [
     "SparseBackendsError", "Context", "Graph", "default_context", "DenseTensor", "NewBlockSparseSorted", "COOTensor",
     "AliasedBlockSparse", "contract_", "contract_bs_bs_to_dense", "blocksparse_from_dense", "coo_from_dense",
     "to_dense", "to_blocksparse", "permutedims", "sort_", "compression_ratio", "output_inds", "label_key",
-    "to_uniform", "to_ragged", "norm", "dot", "inner", "copy", "similar", "scale_", "fill_", "map_", "axpy_",
+    "to_uniform", "to_ragged", "crop_padding", "norm", "dot", "inner", "copy", "similar", "scale_", "fill_", "map_", "axpy_",
     "axpby_", "add", "MAP_AXPY", "MAP_AXPBY", "MAP_COPY", "MAP_MUL", "blocksparse_left_qr", "blocksparse_svd",
     "fuse_axes",
 ]
@@ -502,6 +502,15 @@ def to_ragged(A: NewBlockSparseSorted, block_dims: Sequence[Sequence[int]], chec
     bd = [int(x) for b in block_dims for x in b]
     h = C.c_void_p()
     _check(A.ctx, A.ctx._lib.sb_tensor_to_ragged(A.ctx._h, A._h, _i64(bd), int(check_zero), C.byref(h)))
+    return _from_handle(A.ctx, h)
+
+
+def crop_padding(A: NewBlockSparseSorted) -> NewBlockSparseSorted:
+    """The ragged tensor of A's blocks cropped to the smallest extents that keep
+    their nonzero entries: the zero padding of the reference layout (every
+    U(1) sector padded to the largest) removed without knowing the sectors."""
+    h = C.c_void_p()
+    _check(A.ctx, A.ctx._lib.sb_tensor_crop_padding(A.ctx._h, A._h, C.byref(h)))
     return _from_handle(A.ctx, h)
 
 

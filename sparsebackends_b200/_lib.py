@@ -39,6 +39,7 @@ SIGNATURES = {
     "sb_tensor_block_dims": (C.c_int, [vp, P_int, P_i64, P_i64]),
     "sb_tensor_to_uniform": (C.c_int, [vp, vp, C.POINTER(vp)]),
     "sb_tensor_to_ragged": (C.c_int, [vp, vp, P_i64, C.c_int, C.POINTER(vp)]),
+    "sb_tensor_crop_padding": (C.c_int, [vp, vp, C.POINTER(vp)]),
     "sb_tensor_create_coo": (C.c_int, [vp, C.c_int, P_i64, i64, P_i64, P_f64, C.c_int, C.POINTER(vp)]),
     "sb_tensor_create_aliased": (C.c_int, [vp, C.c_int, P_i64, C.c_int, i64, P_f64, i64, P_i64, P_i64, P_f64,
                                            C.POINTER(vp)]),

@@ -364,6 +364,16 @@ sb_status sb_tensor_to_ragged(sb_ctx* ctx, const sb_tensor* A, const int64_t* bl
   });
 }
 
+sb_status sb_tensor_crop_padding(sb_ctx* ctx, const sb_tensor* A, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    check_t(A);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    *out = wrap(ctx, bs_crop_padding(&ctx->impl, *A->impl));
+  });
+}
+
 sb_status sb_tensor_create_coo(sb_ctx* ctx, int nd, const int64_t* dims, int64_t nnz, const int64_t* keys,
                                const double* vals, int dirty, sb_tensor** out) {
   return guard(ctx, [&] {

@@ -254,6 +254,7 @@ TensorPtr aliased_to_bs(Ctx* ctx, const Tensor& A);
 // Ragged <-> uniform adapters (zero padding / cropping).
 TensorPtr bs_to_uniform(Ctx* ctx, const Tensor& A);
 TensorPtr bs_to_ragged(Ctx* ctx, const Tensor& A, const std::vector<int64_t>& bdims, bool check_zero);
+TensorPtr bs_crop_padding(Ctx* ctx, const Tensor& A);
 // Copies variable-size blocks: dst[dst_off[i] + e] = src[src_off[i] + e], e < len[i].
 void copy_blocks(Ctx* ctx, const double* src, double* dst, const std::vector<int64_t>& src_off,
                  const std::vector<int64_t>& dst_off, const std::vector<int64_t>& len);

@@ -374,6 +374,50 @@ cudaError_t launch_perm_blocks(const double* src, double* dst, const BlockPerm* 
   return cudaGetLastError();
 }
 
+// Smallest tail extents of every block that keep all its nonzero entries:
+// block b (payload at off[b], tail extents dims[b*n2 ..]) gives ext[b*n2 + r]
+// = 1 + the largest axis-r coordinate of a nonzero element (1 for an
+// all-zero block).  One CTA per block (grid-stride); each thread keeps its
+// maxima in registers and merges them through shared-memory atomics.
+__global__ void k_block_extents(const double* __restrict__ src, const int64_t* __restrict__ off,
+                                const int64_t* __restrict__ dims, int64_t nblocks, int n2, int64_t* __restrict__ ext) {
+  __shared__ int smax[kMaxRank];
+  for (int64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
+    if (threadIdx.x < kMaxRank) smax[threadIdx.x] = 1;
+    __syncthreads();
+    int mx[kMaxRank];
+    int64_t len = 1;
+    for (int r = 0; r < n2; ++r) {
+      mx[r] = 1;
+      len *= dims[b * n2 + r];
+    }
+    const double* blk = src + off[b];
+    for (int64_t e = threadIdx.x; e < len; e += blockDim.x) {
+      if (blk[e] == 0.0) continue;
+      int64_t q = e;
+      for (int r = 0; r < n2; ++r) {
+        const int64_t d = dims[b * n2 + r];
+        const int c = static_cast<int>(q % d) + 1;
+        q /= d;
+        mx[r] = max(mx[r], c);
+      }
+    }
+    for (int r = 0; r < n2; ++r) atomicMax(&smax[r], mx[r]);
+    __syncthreads();
+    if (threadIdx.x < n2) ext[b * n2 + threadIdx.x] = smax[threadIdx.x];
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_block_extents(const double* src, const int64_t* d_off, const int64_t* d_dims, int64_t nblocks,
+                                 int n2, int64_t* d_ext, cudaStream_t s) {
+  if (nblocks <= 0) return cudaSuccess;
+  if (n2 < 1 || n2 > kMaxRank) return cudaErrorInvalidValue;
+  const unsigned g = static_cast<unsigned>(std::min<int64_t>(nblocks, 148LL * 8));
+  k_block_extents<<<g, 256, 0, s>>>(src, d_off, d_dims, nblocks, n2, d_ext);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_outside_nonzero(const double* src, const BlockPerm* d_items, int64_t n, int64_t max_len,
                                    uint8_t* flags, cudaStream_t s) {
   (void)max_len;

@@ -270,6 +270,29 @@ TensorPtr bs_to_uniform(Ctx* ctx, const Tensor& A) {
   return out;
 }
 
+// The ragged tensor whose blocks are A's blocks cropped to the smallest tail
+// extents that keep their nonzero entries: the reference layout's zero
+// padding (every U(1) sector padded to the largest) found from the values.
+TensorPtr bs_crop_padding(Ctx* ctx, const Tensor& A) {
+  require(A.kind == BS, SB_ERR_INVALID_ARG, "crop_padding needs a block-sparse tensor");
+  const int64_t n = A.nkeys;
+  std::vector<int64_t> bd(n * A.n2);
+  if (n > 0 && A.n2 > 0) {
+    std::vector<int64_t> off(n), dims(n * A.n2);
+    for (int64_t i = 0; i < n; ++i) {
+      off[i] = A.block_off(i);
+      for (int t = 0; t < A.n2; ++t) dims[i * A.n2 + t] = A.block_dim(i, t);
+    }
+    DevBuf doff = upload(ctx, off), ddims = upload(ctx, dims);
+    DevBuf dext(ctx, bd.size() * sizeof(int64_t));
+    SB_CK(launch_block_extents(A.payload(), doff.as<int64_t>(), ddims.as<int64_t>(), n, A.n2, dext.as<int64_t>(),
+                               ctx->stream));
+    ctx->note_launch();
+    bd = download<int64_t>(ctx, dext.raw(), bd.size());
+  }
+  return bs_to_ragged(ctx, A, bd, false);
+}
+
 TensorPtr bs_to_ragged(Ctx* ctx, const Tensor& A, const std::vector<int64_t>& bd, bool check_zero) {
   require(A.kind == BS, SB_ERR_INVALID_ARG, "to_ragged needs a block-sparse tensor");
   require(static_cast<int64_t>(bd.size()) == A.nkeys * A.n2, SB_ERR_INVALID_ARG, "block_dims must be nkeys x n_tail");
@@ -308,14 +331,14 @@ TensorPtr bs_to_ragged(Ctx* ctx, const Tensor& A, const std::vector<int64_t>& bd
     for (auto& c : checks) mx = std::max(mx, c.len);
     DevBuf dc = upload(ctx, checks);
     DevBuf fl(ctx, checks.size());
-    SB_CK(launch_outside_nonzero(A.data.d(), dc.as<BlockPerm>(), static_cast<int64_t>(checks.size()), mx,
+    SB_CK(launch_outside_nonzero(A.payload(), dc.as<BlockPerm>(), static_cast<int64_t>(checks.size()), mx,
                                  fl.as<uint8_t>(), ctx->stream));
     ctx->note_launch();
     auto f = download<uint8_t>(ctx, fl.raw(), checks.size());
     for (size_t i = 0; i < f.size(); ++i)
       require(!f[i], SB_ERR_ASSERTION, "cropping would drop nonzero entries of block " + std::to_string(i + 1));
   }
-  perm_blocks(ctx, A.data.d(), out->data.d(), items);
+  perm_blocks(ctx, A.payload(), out->data.d(), items);
   return out;
 }
 
