@@ -1,7 +1,8 @@
 """Benchmark: plain-FP64 two-site H_eff matvec at chi = 2048 (U(1), J1-J2-sized MPO).
 
 One step = one application of the two-site effective Hamiltonian
-(psi·L, ·W1, ·W2, ·R: four contract! calls) on synthetic, seeded inputs with
+(psi·L, ·W1, ·W2, ·R: four contract! calls, ITensorMPS's order; the
+association psi·L·(W1·W2)·R is timed beside it) on synthetic, seeded inputs with
 the shapes of the chi = 2048 J1-J2 6x6-cylinder workload: 11 U(1) sectors with
 a Gaussian dimension profile summing to 2048 and an MPO link of 38 channels
 graded by charge {-2: 12, 0: 14, +2: 12}.  The headline runs the ragged block
@@ -351,9 +352,12 @@ def run_ours(args, world, rank, local):
              for n, (k, d, e) in host_r.items()}
     dev_u = {n: sb.NewBlockSparseSorted(layout.dims[n], layout.n2[n], k, None, d, ctx=ctx) for n, (k, d) in host.items()}
     chain_r, chain_u = qn.HeffChain(layout, ctx), qn.HeffChain(layout, ctx)
+    # the same matvec associated as psi·L·(W1·W2)·R (W12 recomputed every step)
+    chain_w = qn.HeffChain(layout, ctx, w12=True)
     stream = torch.cuda.ExternalStream(ctx.stream)
     flops_alg = qn.chain_flops(layout, padded=False)
     flops_pad = qn.chain_flops(layout, padded=True)
+    flops_w = qn.chain_flops(layout, padded=False, steps=qn.HeffChain.STEPS_W12)
 
     def apply_r():
         return chain_r.apply(dev_r["psi"], dev_r["L"], dev_r["W1"], dev_r["W2"], dev_r["R"])
@@ -361,10 +365,17 @@ def run_ours(args, world, rank, local):
     def apply_u():
         return chain_u.apply(dev_u["psi"], dev_u["L"], dev_u["W1"], dev_u["W2"], dev_u["R"])
 
+    def apply_w():
+        return chain_w.apply(dev_r["psi"], dev_r["L"], dev_r["W1"], dev_r["W2"], dev_r["R"])
+
     for _ in range(max(args.warmup, 3)):
         apply_r()
         apply_u()
+        apply_w()
     ctx.synchronize()
+    d_w, d_r4 = chain_w.out["T4"].data, chain_r.out["T4"].data
+    agree_w = float(np.linalg.norm(d_w - d_r4) / max(np.linalg.norm(d_r4), 1e-300))
+    assert chain_w.out["T4"].keys == chain_r.out["T4"].keys and agree_w < 1e-12, agree_w
     # the two forms agree (same keys; unpadded blocks equal the padded result)
     ur, uu = sb.to_uniform(chain_r.out["T4"]), chain_u.out["T4"]
     assert ur.keys == uu.keys
@@ -406,6 +417,10 @@ def run_ours(args, world, rank, local):
     ms_u, _, _ = timed(apply_u, args.steps)
     _, _, prof_u = timed(apply_u, args.steps, profile=True)
     value_u = replica_rate(world, args.steps, ms_u)
+    # the W12 association
+    ms_w, _, _ = timed(apply_w, args.steps)
+    _, _, prof_w = timed(apply_w, args.steps, profile=True)
+    value_w = replica_rate(world, args.steps, ms_w)
 
     # ── end to end through the public API (pinned host psi in, H·psi out) ──
     lib = ctx._lib
@@ -623,6 +638,13 @@ def run_ours(args, world, rank, local):
                            "e2e": {"value": e2e_value_u, "unit": UNIT, "h2d_bytes_per_step": h2d_u,
                                    "d2h_bytes_per_step": d2h_u}},
         "ragged_vs_uniform_rel_diff": agree,
+        "w12_association": {"value": value_w, "unit": UNIT, "ms_per_step": ms_w / args.steps,
+                            "steps": "W12 = W1*W2, T1 = psi*L, T3 = T1*W12, T4 = R*T3 (four contract! calls, "
+                                     "W12 recomputed every step; the headline runs ITensorMPS's order psi*L, *W1, "
+                                     "*W2, *R)",
+                            "gflops_algorithmic": flops_w * value_w / 1e9,
+                            "mpo_step_ms": prof_w["gemm_thin"]["ms"] / args.steps,
+                            "rel_diff_vs_reference_order": agree_w},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_r, "d2h_bytes_per_step": d2h_r,
                 "mode": "two requests in flight (two contexts/streams; copies overlap the other request's "

@@ -109,10 +109,12 @@ class HeffLayout:
             "T2": ["qlp", "qr", "s1p", "qwm", "s2", "mr", "mlp", "mwm"],
             "T3": ["qlp", "s1p", "s2p", "qwr", "qr", "mwr", "mr", "mlp"],
             "T4": ["qlp", "s1p", "s2p", "qrp", "mlp", "mrp"],
+            # two-site MPO W1·W2 (the alternative association of the chain)
+            "W12": ["qwl", "s1p", "s1", "s2p", "s2", "qwr", "mwl", "mwr"],
             # one-site MPS tensor (environment updates)
             "A": ["ql", "s1", "qr", "ml", "mr"],
         }
-        n2 = {"psi": 2, "L": 3, "W1": 2, "W2": 2, "R": 3, "T1": 3, "T2": 3, "T3": 3, "T4": 2, "A": 2}
+        n2 = {"psi": 2, "L": 3, "W1": 2, "W2": 2, "R": 3, "T1": 3, "T2": 3, "T3": 3, "T4": 2, "A": 2, "W12": 2}
         self.labels = lab
         self.n2 = n2
         self.dims = {k: tuple(ext[x] for x in v) for k, v in lab.items()}
@@ -273,16 +275,17 @@ def hermitian_operators(layout: HeffLayout, rng: np.random.Generator, scales=Non
 class HeffOperator:
     """x -> H_eff x as a new device tensor (the operator KrylovKit's eigsolve
     applies: ITensorMPS ``product(::ProjMPO, v)``).  Operands stay resident;
-    each call runs the four-contraction chain and copies the result out of the
+    each call runs the contraction chain and copies the result out of the
     chain's reused output buffer."""
 
-    def __init__(self, layout: HeffLayout, L, W1, W2, R, ctx=None, graph_like=None):
+    def __init__(self, layout: HeffLayout, L, W1, W2, R, ctx=None, graph_like=None, w12: bool = False):
         """With ``graph_like`` (a vector with the layout of the inputs to come)
         the chain is captured once as a CUDA graph on a private input buffer;
-        each call copies its input there and replays the graph."""
+        each call copies its input there and replays the graph.  ``w12`` picks
+        the chain ψ·L·(W1·W2)·R (``HeffChain``)."""
         import sparsebackends_b200 as sb
         self.sb = sb
-        self.chain = HeffChain(layout, ctx)
+        self.chain = HeffChain(layout, ctx, w12=w12)
         self.ops = (L, W1, W2, R)
         self.calls = 0
         self.graph = None
@@ -341,24 +344,32 @@ def make_R(R, B, W):
 
 
 class HeffChain:
-    """Two-site H_eff · ψ through four ``contract!`` calls on the device.
+    """Two-site H_eff · ψ through ``contract!`` calls on the device.
+
+    The default order is ITensorMPS ``product(::ProjMPO, v)``'s: ψ·L, ·W1, ·W2,
+    ·R (four contractions).  With ``w12=True`` the two MPO tensors are
+    contracted with each other first, W12 = W1·W2 (a contraction of MPO blocks
+    only, recomputed by every apply), and ψ·L·W12·R takes three: the same
+    FLOPs in the MPO steps, with the T2 intermediate never written or read.
 
     The intermediate and output tensors are allocated once and overwritten by
     every apply (``contract!`` semantics)."""
 
     STEPS = (("T1", "L", "psi"), ("T2", "T1", "W1"), ("T3", "T2", "W2"), ("T4", "R", "T3"))
+    STEPS_W12 = (("W12", "W1", "W2"), ("T1", "L", "psi"), ("T3", "T1", "W12"), ("T4", "R", "T3"))
 
-    def __init__(self, layout: HeffLayout, ctx=None):
+    def __init__(self, layout: HeffLayout, ctx=None, w12: bool = False):
         import sparsebackends_b200 as sb
         self.sb = sb
         self.layout = layout
+        self.steps = self.STEPS_W12 if w12 else self.STEPS
         self.out = {n: sb.NewBlockSparseSorted.empty(layout.dims[n], layout.n2[n], ctx=ctx)
-                    for n in ("T1", "T2", "T3", "T4")}
+                    for n in {c for c, _, _ in self.steps}}
 
     def apply(self, psi, L, W1, W2, R):
         t = {"psi": psi, "L": L, "W1": W1, "W2": W2, "R": R, **self.out}
         lab = self.layout.labels
-        for c, a, b in self.STEPS:
+        for c, a, b in self.steps:
             self.sb.contract_(t[c], lab[c], t[a], lab[a], t[b], lab[b])
         return self.out["T4"]
 
@@ -383,15 +394,15 @@ def _link_of(layout: HeffLayout, qlabel: str) -> U1Link:
     return layout.mpo
 
 
-def chain_structure(layout: HeffLayout):
-    """Key-level simulation of the four steps: per step the matched block pairs
-    (as label->value dicts) and the output key set.  Pure integer work on the
-    host; used for FLOP accounting only."""
+def chain_structure(layout: HeffLayout, steps=HeffChain.STEPS):
+    """Key-level simulation of the chain's steps: per step the matched block
+    pairs (as label->value dicts) and the output key set.  Pure integer work on
+    the host; used for FLOP accounting only."""
     lab = layout.labels
     keys = {n: [dict(zip(lab[n][: len(lab[n]) - layout.n2[n]], k)) for k in layout.keys[n]]
             for n in ("psi", "L", "W1", "W2", "R")}
-    steps = []
-    for c, a, b in HeffChain.STEPS:
+    out = []
+    for c, a, b in steps:
         la, lb, lc = lab[a], lab[b], lab[c]
         Pa, Pb, Pc = (len(x) - layout.n2[n] for x, n in ((la, a), (lb, b), (lc, c)))
         shared_pref = [x for x in la[:Pa] if x in lb[:Pb]]
@@ -408,17 +419,17 @@ def chain_structure(layout: HeffLayout):
         red = [x for x in la[Pa:] if x in lb[Pb:]]
         keepA = [x for x in la[Pa:] if x not in red]
         keepB = [x for x in lb[Pb:] if x not in red]
-        steps.append(dict(C=c, A=a, B=b, pairs=pairs, nC=len(keys[c]), red=red, keepA=keepA, keepB=keepB))
-    return steps
+        out.append(dict(C=c, A=a, B=b, pairs=pairs, nC=len(keys[c]), red=red, keepA=keepA, keepB=keepB))
+    return out
 
 
-def chain_flops(layout: HeffLayout, padded: bool = True) -> float:
+def chain_flops(layout: HeffLayout, padded: bool = True, steps=HeffChain.STEPS) -> float:
     """FLOPs of one H_eff apply: the sum over matched block pairs of 2·m·n·k.
 
     ``padded=True`` counts the executed (zero-padded) GEMM shapes;
     ``padded=False`` counts the unpadded sector extents, the algorithmic work."""
     total = 0.0
-    for st in chain_structure(layout):
+    for st in chain_structure(layout, steps):
         for kv in st["pairs"]:
             def ext(x):
                 if padded:
