@@ -615,8 +615,8 @@ def run_ours(args, world, rank, local):
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (operators ~0.6 GB, intermediates ~2.3 GB each)"},
         "gflops_algorithmic": flops_alg * value / 1e9,
-        "roofline": {"bound": "tensor", "kernel": "k_gemm_f64_edges (DMMA m8n8k4, 64x64 tiles with 64x32 / 32x64 "
-                                                       "edge tiles; steps psi*L and R*T3)",
+        "roofline": {"bound": "tensor", "kernel": "k_gemm_f64_edges (DMMA m8n8k4, 64x64 tiles with 64x32 / 64x48 / "
+                                                       "32x64 / 48x64 edge tiles; steps psi*L and R*T3)",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                      "peak_source": "measured live: torch.matmul float64 8192^3, best of 10 (cuBLAS DGEMM)",
                      "flops_per_launch": g["flops"] / max(g["launches"], 1),
