@@ -215,6 +215,38 @@ def cublas_block_lists(layout, steps: int = 10):
             "graph_ms_per_step": replay, "graph_tflops": flops / replay / 1e9}
 
 
+def permute_stage(ctx, L, hbm_peak, reps: int = 5):
+    """The permute stage (permutedims, storage.jl:188-264) on the zero-padded
+    environment L of this workload (tail (mlp, mwl, ml), at chi = 2048 (411,
+    14, 411) in 31 blocks, 0.62 GB): one tail permutation per transpose
+    kernel.  Bytes are the algorithmic 16 per element (read once, written
+    once); at chi = 2048 every permute reads and writes far more than L2, so
+    no flush is needed."""
+    import sparsebackends_b200 as sb
+    cases = [("contiguous runs (k_permute_runs)", (1, 2, 3, 4, 6, 5)),
+             ("narrow transpose, 14-wide rows (k_permute_narrow)", (1, 2, 3, 5, 4, 6)),
+             ("tiled transpose, rows of one axis (k_permute_tiled)", (1, 2, 3, 6, 4, 5)),
+             ("tiled transpose, rows of two axes (k_permute_tiled)", (1, 2, 3, 6, 5, 4))]
+    out = []
+    for name, perm in cases:
+        sb.permutedims(L, perm)
+        ctx.synchronize()
+        ctx.set_profiling(True)
+        for _ in range(reps):
+            sb.permutedims(L, perm)
+        p = ctx.profile("permute")
+        ctx.set_profiling(False)
+        gbs = p["bytes"] / (p["ms"] * 1e-3) / 1e9 if p["ms"] > 0 else 0.0
+        out.append({"case": name, "perm": list(perm), "ms": p["ms"] / reps, "gb_per_s": gbs,
+                    "frac": gbs / hbm_peak if hbm_peak else None})
+    i = L._info()
+    gb = i["nkeys"] * i["blksize"] * 8 / 1e9
+    tail = i["dims"][len(i["dims"]) - i["n2"]:]
+    return {"tensor": f"uniform L, tail {tail}, {i['nkeys']} blocks, {gb:.2f} GB",
+            "peak_gb_per_s": hbm_peak,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)", "cases": out}
+
+
 def fp64_peak_tflops():
     import torch
     n = 8192
@@ -601,6 +633,7 @@ def run_ours(args, world, rank, local):
     thin_gbs = th["bytes"] / (th["ms"] * 1e-3) / 1e9 if th["ms"] > 0 else 0.0
     hbm_peak = measured_hbm_gbs()
     gu, gtu = prof_u["gemm"], prof_u["gemm_thin"]
+    permute = permute_stage(ctx, dev_u["L"], hbm_peak)
     # the vendor library on the same block lists, after every timed leg (its
     # many small launches stay out of the launch lists profiled from this run)
     library = cublas_block_lists(layout)
@@ -631,6 +664,7 @@ def run_ours(args, world, rank, local):
                                "kernel_ms_per_step": th["ms"] / args.steps},
         "kernel_time_share": {k: v["ms"] / max(1e-9, sum(x["ms"] for x in prof.values())) for k, v in prof.items()},
         "library_baseline": library,
+        "permute_stage": permute,
         "uniform_format": {"value": value_u, "ms_per_step": ms_u / args.steps,
                            "gflops_executed": flops_pad * value_u / 1e9,
                            "gemm_tflops": (gu["flops"] + gtu["flops"]) / ((gu["ms"] + gtu["ms"]) * 1e-3) / 1e12

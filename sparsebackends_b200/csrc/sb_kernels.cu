@@ -85,13 +85,42 @@ __global__ void k_permute_general(const double* __restrict__ src, double* __rest
   }
 }
 
-// Tiled transpose: output axis 0 (unit output stride) is read with source
-// stride sv; output axis q has unit source stride.  A 32x32 tile is read
-// coalesced along q and written coalesced along axis 0; the remaining axes
-// are a batch.
+// Contiguous runs: output axis 0 has unit source stride too, so every run of
+// the leading output axes that are contiguous in both layouts (len doubles) is
+// a straight copy.  One warp per run: the source offset of a run is computed
+// once, then the lanes copy it with coalesced accesses, four loads in flight
+// per lane.
+__global__ void k_permute_runs(const double* __restrict__ src, double* __restrict__ dst,
+                               const int64_t* __restrict__ src_off, int64_t blk, int64_t len, int64_t runs_per_block,
+                               int64_t total_runs, PermDesc d, int first_outer) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t run = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; run < total_runs;
+       run += warps) {
+    const int64_t b = run / runs_per_block;
+    int64_t rr = run - b * runs_per_block;
+    const double* s = src + src_off[b];
+    double* o = dst + b * blk + rr * len;
+    for (int r = first_outer; r < d.rank; ++r) {
+      const int64_t c = rr % d.out_dims[r];
+      rr /= d.out_dims[r];
+      s += c * d.in_strides[r];
+    }
+#pragma unroll 4
+    for (int64_t e = lane; e < len; e += 32) o[e] = s[e];
+  }
+}
+
+// Transposes: output axis q is the first with unit source stride; the output
+// axes before it, flattened, are the row axis v (contiguous in the output,
+// extent dv, each row's source offset decomposed from its index), output
+// axis q is u (extent du, output stride dv), and the axes after it are a
+// batch.  A tile is read coalesced along u and written coalesced along v.
 struct TileDesc {
-  int64_t dv, du;        // extents of output axis 0 and output axis q
-  int64_t sv;            // source stride of output axis 0
+  int64_t dv, du;        // extents of the row axis (output axes before q) and of output axis q
+  int nv;                // number of output axes before q
+  int64_t vdims[kMaxRank];
+  int64_t vsrc[kMaxRank];  // their source strides
   int64_t ou;            // output stride of output axis q
   int nb;                // number of batch axes
   int64_t bdims[kMaxRank];
@@ -100,34 +129,140 @@ struct TileDesc {
   int64_t nbatch, tiles_u, tiles_v;
 };
 
-__global__ void k_permute_tiled(const double* __restrict__ src, double* __restrict__ dst,
-                                const int64_t* __restrict__ src_off, int64_t blk, TileDesc d,
-                                int64_t total_ctas) {
-  __shared__ double tile[32][33];
-  for (int64_t cta = blockIdx.x; cta < total_ctas; cta += gridDim.x) {
-    int64_t t = cta;
-    const int64_t tu = t % d.tiles_u; t /= d.tiles_u;
-    const int64_t tv = t % d.tiles_v; t /= d.tiles_v;
-    int64_t bt = t % d.nbatch;
-    const int64_t b = t / d.nbatch;
-    int64_t sb = src_off[b], db = b * blk;
-    for (int r = 0; r < d.nb; ++r) {
-      const int64_t c = bt % d.bdims[r];
-      bt /= d.bdims[r];
-      sb += c * d.bsrc[r];
-      db += c * d.bdst[r];
+// Source offset of row v (relative to the tile's batch base).
+__device__ __forceinline__ int64_t row_src(const TileDesc& d, int64_t v) {
+  int64_t off = 0;
+  for (int r = 0; r < d.nv - 1; ++r) {
+    const int64_t c = v % d.vdims[r];
+    v /= d.vdims[r];
+    off += c * d.vsrc[r];
+  }
+  return off + v * d.vsrc[d.nv - 1];
+}
+constexpr int kTileU = 64;   // tile extent along output axis q (unit source stride)
+constexpr int kTileV = 64;   // tile extent along output axis 0
+constexpr int kNarrowSmem = 64 * 1024;  // narrow transpose: shared memory of a tile (bytes)
+
+// Source and destination bases of tile `cta` (tiles_u x tiles_v x batch x block).
+__device__ __forceinline__ void tile_bases(const TileDesc& d, const int64_t* __restrict__ src_off, int64_t blk,
+                                           int64_t cta, int64_t& tu, int64_t& tv, int64_t& sb, int64_t& db) {
+  int64_t t = cta;
+  tu = t % d.tiles_u; t /= d.tiles_u;
+  tv = t % d.tiles_v; t /= d.tiles_v;
+  int64_t bt = t % d.nbatch;
+  const int64_t b = t / d.nbatch;
+  sb = src_off[b];
+  db = b * blk;
+  for (int r = 0; r < d.nb; ++r) {
+    const int64_t c = bt % d.bdims[r];
+    bt /= d.bdims[r];
+    sb += c * d.bsrc[r];
+    db += c * d.bdst[r];
+  }
+}
+
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+// Persistent: each CTA walks its tiles with stride gridDim.x through two
+// shared-memory buffers; the copies of the next tile (cp.async, no registers)
+// are in flight while the current one is stored.
+constexpr int kTilePitch = kTileV + 1;
+constexpr int kTileElems = kTileU * kTilePitch;
+__global__ void __launch_bounds__(256) k_permute_tiled(const double* __restrict__ src, double* __restrict__ dst,
+                                                      const int64_t* __restrict__ src_off, int64_t blk, TileDesc d,
+                                                      int64_t total_ctas) {
+  extern __shared__ double ttile[];
+  auto issue = [&](int64_t cta, double* buf) {
+    int64_t tu, tv, sb, db;
+    tile_bases(d, src_off, blk, cta, tu, tv, sb, db);
+    const int64_t u0 = tu * kTileU, v0 = tv * kTileV;
+#pragma unroll
+    for (int j = 0; j < kTileV / 8; ++j) {
+      const int yy = threadIdx.y + 8 * j;
+      const int64_t v = v0 + yy;
+      if (v >= d.dv) continue;
+      const double* row = src + sb + row_src(d, v);
+#pragma unroll
+      for (int h = 0; h < kTileU / 32; ++h) {
+        const int64_t u = u0 + h * 32 + threadIdx.x;
+        if (u < d.du) cp_async8(&buf[(h * 32 + threadIdx.x) * kTilePitch + yy], row + u);
+      }
     }
-    const int64_t u0 = tu * 32, v0 = tv * 32;
-    // load: threadIdx.x runs along u (unit source stride)
-    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
-      const int64_t v = v0 + yy, u = u0 + threadIdx.x;
-      if (v < d.dv && u < d.du) tile[yy][threadIdx.x] = src[sb + u + v * d.sv];
+  };
+  int64_t cta = blockIdx.x;
+  if (cta >= total_ctas) return;
+  issue(cta, ttile);
+  cp_async_commit();
+  int b = 0;
+  for (; cta < total_ctas; cta += gridDim.x) {
+    const int64_t next = cta + gridDim.x;
+    if (next < total_ctas) issue(next, ttile + (b ^ 1) * kTileElems);
+    cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();
+    const double* tile = ttile + b * kTileElems;
+    int64_t tu, tv, sb, db;
+    tile_bases(d, src_off, blk, cta, tu, tv, sb, db);
+    const int64_t u0 = tu * kTileU, v0 = tv * kTileV;
+    // store: threadIdx.x runs along v (unit output stride)
+#pragma unroll
+    for (int h = 0; h < kTileV / 32; ++h)
+#pragma unroll
+      for (int uu = threadIdx.y; uu < kTileU; uu += 8) {
+        const int64_t u = u0 + uu, v = v0 + h * 32 + threadIdx.x;
+        if (v < d.dv && u < d.du) dst[db + v + u * d.ou] = tile[uu * kTilePitch + h * 32 + threadIdx.x];
+      }
+    __syncthreads();  // buffer b is refilled by the next iteration's copies
+    b ^= 1;
+  }
+}
+
+// Narrow transpose: the row axis is short (dv <= 32), so the output of a tile
+// (all rows x tu of axis q) is one contiguous run.  A tile spans all of axis 1 when it fits in shared memory
+// (then its source rows are one contiguous slab too): rows are loaded by
+// warps, coalesced along axis 1 (unit source stride), and the run is stored
+// with consecutive threads on consecutive addresses.  The row pitch in shared
+// memory is odd, so both phases are free of bank conflicts.
+__global__ void k_permute_narrow(const double* __restrict__ src, double* __restrict__ dst,
+                                 const int64_t* __restrict__ src_off, int64_t blk, TileDesc d, int tu,
+                                 int64_t total_ctas) {
+  extern __shared__ double ntile[];
+  const int dv = static_cast<int>(d.dv);
+  const int pitch = dv | 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  // this thread's first output element of a run and the step per pass, as
+  // (u, v) = divmod(i, dv), advanced without dividing again
+  const int su = static_cast<int>(blockDim.x) / dv, sv = static_cast<int>(blockDim.x) % dv;
+  const int iu = static_cast<int>(threadIdx.x) / dv, iv = static_cast<int>(threadIdx.x) % dv;
+  for (int64_t cta = blockIdx.x; cta < total_ctas; cta += gridDim.x) {
+    int64_t tiu, tiv, sb, db;
+    tile_bases(d, src_off, blk, cta, tiu, tiv, sb, db);
+    const int64_t u0 = tiu * tu;
+    const int nu = static_cast<int>(d.du - u0 < tu ? d.du - u0 : tu);
+    const double* sp = src + sb + u0;
+    for (int v = warp; v < dv; v += nwarps) {
+      const double* row = sp + row_src(d, v);
+#pragma unroll 4
+      for (int u = lane; u < nu; u += 32) ntile[u * pitch + v] = row[u];
     }
     __syncthreads();
-    // store: threadIdx.x runs along v (unit output stride)
-    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
-      const int64_t u = u0 + yy, v = v0 + threadIdx.x;
-      if (v < d.dv && u < d.du) dst[db + v + u * d.ou] = tile[threadIdx.x][yy];
+    double* o = dst + db + u0 * dv;
+    const int n = nu * dv;
+    int u = iu, v = iv;
+#pragma unroll 4
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      o[i] = ntile[u * pitch + v];
+      u += su;
+      v += sv;
+      if (v >= dv) {
+        v -= dv;
+        ++u;
+      }
     }
     __syncthreads();
   }
@@ -325,34 +460,88 @@ cudaError_t launch_permute_blocks(const double* src, double* dst, const int64_t*
   for (int r = 0; r < desc.rank; ++r)
     if (desc.in_strides[r] == 1 && desc.out_dims[r] > 1) { q = r; break; }
   const bool first_unit = desc.rank == 0 || desc.in_strides[0] == 1 || desc.out_dims[0] == 1;
-  if (first_unit || q <= 0 || desc.out_dims[0] < 4 || desc.out_dims[q] < 4) {
+  if (desc.rank > 0 && desc.in_strides[0] == 1) {
+    // leading output axes contiguous in the source as well: one run
+    int j = 1;
+    int64_t len = desc.out_dims[0];
+    while (j < desc.rank && desc.in_strides[j] == len) len *= desc.out_dims[j++];
+    if (len >= 32) {
+      const int64_t runs = blk / len, total = nblocks * runs;
+      const int64_t ctas = std::min<int64_t>((total + 7) / 8, 148LL * 8);
+      k_permute_runs<<<static_cast<unsigned>(std::max<int64_t>(ctas, 1)), kThreads, 0, s>>>(
+          src, dst, d_src_off, blk, len, runs, total, desc, j);
+      return cudaGetLastError();
+    }
+  }
+  if (first_unit || q <= 0 || desc.out_dims[q] < 4) {
     k_permute_general<<<grid_for(nblocks * blk), kThreads, 0, s>>>(src, dst, d_src_off, nblocks, blk, desc);
     return cudaGetLastError();
   }
   TileDesc td{};
-  td.dv = desc.out_dims[0];
   td.du = desc.out_dims[q];
-  td.sv = desc.in_strides[0];
-  int64_t ostride = 1;
+  td.nv = q;
+  td.dv = 1;
+  for (int r = 0; r < q; ++r) {
+    td.vdims[r] = desc.out_dims[r];
+    td.vsrc[r] = desc.in_strides[r];
+    td.dv *= desc.out_dims[r];
+  }
+  td.ou = td.dv;
+  int64_t ostride = td.dv * td.du;
   int nb = 0;
-  for (int r = 0; r < desc.rank; ++r) {
-    if (r == q) td.ou = ostride;
-    if (r != 0 && r != q) {
-      td.bdims[nb] = desc.out_dims[r];
-      td.bsrc[nb] = desc.in_strides[r];
-      td.bdst[nb] = ostride;
-      ++nb;
-    }
+  for (int r = q + 1; r < desc.rank; ++r) {
+    td.bdims[nb] = desc.out_dims[r];
+    td.bsrc[nb] = desc.in_strides[r];
+    td.bdst[nb] = ostride;
+    ++nb;
     ostride *= desc.out_dims[r];
   }
   td.nb = nb;
   td.nbatch = 1;
   for (int r = 0; r < nb; ++r) td.nbatch *= td.bdims[r];
-  td.tiles_u = (td.du + 31) / 32;
-  td.tiles_v = (td.dv + 31) / 32;
+  if (td.dv <= 32) {
+    // the widest tile (a multiple of 32 along axis q, or all of it) that fits
+    const int pitch = static_cast<int>(td.dv) | 1;
+    int64_t tu = kNarrowSmem / 8 / pitch;
+    tu = td.du <= tu ? td.du : tu / 32 * 32;
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (!configured[dev & 63]) {
+      e = cudaFuncSetAttribute(k_permute_narrow, cudaFuncAttributeMaxDynamicSharedMemorySize, kNarrowSmem);
+      if (e != cudaSuccess) return e;
+      configured[dev & 63] = true;
+    }
+    td.tiles_u = (td.du + tu - 1) / tu;
+    td.tiles_v = 1;
+    const int64_t total = nblocks * td.nbatch * td.tiles_u;
+    const unsigned g = static_cast<unsigned>(total < 148LL * 8 ? total : 148LL * 8);
+    const size_t smem = static_cast<size_t>(tu) * pitch * sizeof(double);
+    k_permute_narrow<<<g, kThreads, smem, s>>>(src, dst, d_src_off, blk, td, static_cast<int>(tu), total);
+    return cudaGetLastError();
+  }
+  td.tiles_u = (td.du + kTileU - 1) / kTileU;
+  td.tiles_v = (td.dv + kTileV - 1) / kTileV;
   const int64_t total = nblocks * td.nbatch * td.tiles_u * td.tiles_v;
-  const unsigned g = static_cast<unsigned>(total < 148LL * 64 ? total : 148LL * 64);
-  k_permute_tiled<<<g, dim3(32, 8), 0, s>>>(src, dst, d_src_off, blk, td, total);
+  constexpr int smem = 2 * kTileElems * static_cast<int>(sizeof(double));
+  static int grid_of[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  int& grid = grid_of[dev & 63];
+  if (grid == 0) {
+    e = cudaFuncSetAttribute(k_permute_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    int sms = 0, per_sm = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_permute_tiled, 256, smem);
+    if (e != cudaSuccess) return e;
+    grid = sms * std::max(per_sm, 1);
+  }
+  const unsigned g = static_cast<unsigned>(total < grid ? total : grid);
+  k_permute_tiled<<<g, dim3(32, 8), smem, s>>>(src, dst, d_src_off, blk, td, total);
   return cudaGetLastError();
 }
 

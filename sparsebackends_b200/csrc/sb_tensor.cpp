@@ -382,7 +382,7 @@ TensorPtr bs_permute(Ctx* ctx, const Tensor& A, const std::vector<int>& perm) {
         dof[i] = out->boff[i];
         len[i] = A.block_len(p[i]);
       }
-      copy_blocks(ctx, A.data.d(), out->data.d(), so, dof, len);
+      copy_blocks(ctx, A.payload(), out->data.d(), so, dof, len);
     } else {
       std::vector<BlockPerm> items;
       for (int64_t i = 0; i < n; ++i) {
@@ -398,20 +398,20 @@ TensorPtr bs_permute(Ctx* ctx, const Tensor& A, const std::vector<int>& perm) {
         }
         items.push_back(make_block_perm(A.block_off(p[i]), out->boff[i], od, is, od));
       }
-      perm_blocks(ctx, A.data.d(), out->data.d(), items);
+      perm_blocks(ctx, A.payload(), out->data.d(), items);
     }
     return out;
   }
   out->data = DevBuf(ctx, n * blk * sizeof(double));
   std::vector<int64_t> soff(n);
-  for (int64_t i = 0; i < n; ++i) soff[i] = p[i] * blk;
+  for (int64_t i = 0; i < n; ++i) soff[i] = A.block_off(p[i]);
   auto so = cm_strides(A.dims, P, N);
   std::vector<int64_t> od(A.n2), is(A.n2);
   for (int r = 0; r < A.n2; ++r) {
     od[r] = dimsB[P + r];
     is[r] = so[perm[P + r] - 1 - P];
   }
-  permute_blocks(ctx, A.data.d(), out->data.d(), soff, blk, od, is);
+  permute_blocks(ctx, A.payload(), out->data.d(), soff, blk, od, is);
   return out;
 }
 
