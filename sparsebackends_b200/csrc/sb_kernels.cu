@@ -297,6 +297,38 @@ __global__ void k_perm_blocks(const double* __restrict__ src, double* __restrict
   }
 }
 
+// Rows of per-block permutes whose output axis 0 keeps unit source stride
+// (zero padding, cropping, permutes of the outer axes): one warp per row of
+// out_dims[0] elements, its source offset computed once; entries past the
+// source limits are written as zeros.
+__global__ void k_perm_block_rows(const double* __restrict__ src, double* __restrict__ dst,
+                                  const BlockPerm* __restrict__ items, int64_t n) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wpc = blockDim.x >> 5;
+  for (int64_t b = blockIdx.y; b < n; b += gridDim.y) {
+    const BlockPerm& it = items[b];
+    const int64_t d0 = it.out_dims[0];
+    const int64_t rows = it.len / d0;
+    const int64_t lim0 = it.in_lim[0] < d0 ? it.in_lim[0] : d0;
+    for (int64_t row = static_cast<int64_t>(blockIdx.x) * wpc + (threadIdx.x >> 5); row < rows;
+         row += static_cast<int64_t>(gridDim.x) * wpc) {
+      int64_t rr = row, so = 0;
+      bool in = true;
+      for (int r = 1; r < it.rank; ++r) {
+        const int64_t c = rr % it.out_dims[r];
+        rr /= it.out_dims[r];
+        in = in && c < it.in_lim[r];
+        so += c * it.in_strides[r];
+      }
+      const double* sp = src + it.src_off + so;
+      double* o = dst + it.dst_off + row * d0;
+      const int64_t lim = in ? lim0 : 0;
+#pragma unroll 4
+      for (int64_t e = lane; e < d0; e += 32) o[e] = e < lim ? sp[e] : 0.0;
+    }
+  }
+}
+
 __global__ void k_outside_nonzero(const double* __restrict__ src, const BlockPerm* __restrict__ items, int64_t n,
                                   uint8_t* __restrict__ flags) {
   for (int64_t b = blockIdx.x; b < n; b += gridDim.x) {
@@ -551,6 +583,17 @@ cudaError_t launch_copy_blocks(const double* src, double* dst, const BlockCopy* 
   dim3 grid(grid_for(max_len), static_cast<unsigned>(n < 65535 ? n : 65535));
   if ((int64_t)grid.x * grid.y > 148LL * 64) grid.x = static_cast<unsigned>(std::max<int64_t>(1, 148LL * 64 / grid.y));
   k_copy_blocks<<<grid, kThreads, 0, s>>>(src, dst, d_items, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_perm_block_rows(const double* src, double* dst, const BlockPerm* d_items, int64_t n,
+                                   int64_t max_rows, cudaStream_t s) {
+  if (n <= 0 || max_rows <= 0) return cudaSuccess;
+  const int64_t gy = n < 65535 ? n : 65535;
+  int64_t gx = (max_rows + 7) / 8;  // eight warps per CTA
+  gx = std::max<int64_t>(1, std::min<int64_t>(gx, 148LL * 16 / gy));
+  k_perm_block_rows<<<dim3(static_cast<unsigned>(gx), static_cast<unsigned>(gy)), kThreads, 0, s>>>(src, dst,
+                                                                                                    d_items, n);
   return cudaGetLastError();
 }
 

@@ -150,6 +150,10 @@ struct BlockPerm {
 };
 cudaError_t launch_perm_blocks(const double* src, double* dst, const BlockPerm* d_items, int64_t n,
                                int64_t max_len, cudaStream_t s);
+// The same for items whose out_dims[0] has in_strides[0] == 1 (one warp per
+// row of out_dims[0]); max_rows = the largest len / out_dims[0].
+cudaError_t launch_perm_block_rows(const double* src, double* dst, const BlockPerm* d_items, int64_t n,
+                                   int64_t max_rows, cudaStream_t s);
 // ext[b*n2 + r] = smallest axis-r extent of block b (payload at d_off[b],
 // extents d_dims[b*n2 ..]) that keeps all its nonzero entries (>= 1).
 cudaError_t launch_block_extents(const double* src, const int64_t* d_off, const int64_t* d_dims, int64_t nblocks,

@@ -211,15 +211,30 @@ void copy_blocks(Ctx* ctx, const double* src, double* dst, const std::vector<int
 // Per-block permute/pad/crop through BlockPerm descriptors.
 static void perm_blocks(Ctx* ctx, const double* src, double* dst, std::vector<BlockPerm>& items) {
   if (items.empty()) return;
-  int64_t mx = 0;
+  int64_t mx = 0, mx_rows = 0;
   double bytes = 0.0;
+  // rows of unit-stride runs (padding, cropping, outer-axis permutes) when
+  // every item has them and they are at least 16 long on average
+  bool rows = true;
+  int64_t elems = 0, nrows = 0;
   for (auto& it : items) {
     mx = std::max(mx, it.len);
     bytes += 16.0 * it.len;
+    rows = rows && it.rank >= 1 && it.in_strides[0] == 1 && it.out_dims[0] >= 1;
+    if (rows) {
+      mx_rows = std::max(mx_rows, it.len / it.out_dims[0]);
+      elems += it.len;
+      nrows += it.len / it.out_dims[0];
+    }
   }
+  rows = rows && elems >= 16 * nrows;
   DevBuf d = upload(ctx, items);
   ProfScope ps(ctx, PROF_PERMUTE, 0.0, bytes);
-  SB_CK(launch_perm_blocks(src, dst, d.as<BlockPerm>(), static_cast<int64_t>(items.size()), mx, ctx->stream));
+  if (rows)
+    SB_CK(launch_perm_block_rows(src, dst, d.as<BlockPerm>(), static_cast<int64_t>(items.size()), mx_rows,
+                                 ctx->stream));
+  else
+    SB_CK(launch_perm_blocks(src, dst, d.as<BlockPerm>(), static_cast<int64_t>(items.size()), mx, ctx->stream));
   ctx->note_launch();
 }
 
