@@ -110,6 +110,7 @@ sb_status sb_ctx_create(int device, unsigned flags, sb_ctx** out) {
     if (const char* th = std::getenv("SPARSEB_GEMM_THIN")) c->impl.gemm_thin = std::atoi(th);
     if (const char* ge = std::getenv("SPARSEB_GEMM_EDGES")) c->impl.gemm_edges = std::atoi(ge);
     if (const char* pc = std::getenv("SPARSEB_PLAN_CACHE")) c->impl.plan_cache_on = std::atoi(pc) != 0;
+    if (const char* ac = std::getenv("SPARSEB_AUTO_CROP")) c->impl.auto_crop = std::atoi(ac);
     if (const char* sk = std::getenv("SPARSEB_GEMM_SPLITK")) c->impl.gemm_splitk = std::max(0, std::atoi(sk));
     // Keep freed device memory cached in the stream-ordered pool.
     cudaMemPool_t pool;
@@ -561,16 +562,18 @@ sb_status sb_contract(sb_ctx* ctx, sb_tensor* C, const uint64_t* labelsC, int nC
     const auto t0 = std::chrono::steady_clock::now();
     ctx->impl.gemm_desc[0] = '\0';
     ctx->impl.plan_cache_hit = false;
+    ctx->impl.auto_cropped = false;
     contract(&ctx->impl, *C->impl, read_labels(labelsC, nC), *A->impl, read_labels(labelsA, nA), *B->impl,
              read_labels(labelsB, nB));
     if (ctx->impl.trace) {
       const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
       std::fprintf(stderr,
-                   "[sparseb] %s  A(kind=%d, keys=%lld) x B(kind=%d, keys=%lld) -> C(keys=%lld)  host %.3f ms%s%s%s\n",
+                   "[sparseb] %s  A(kind=%d, keys=%lld) x B(kind=%d, keys=%lld) -> C(keys=%lld)  host %.3f ms%s%s%s%s\n",
                    ctx->impl.kernel_name, A->impl->kind, static_cast<long long>(A->impl->nkeys), B->impl->kind,
                    static_cast<long long>(B->impl->nkeys), static_cast<long long>(C->impl->nkeys), ms,
                    ctx->impl.gemm_desc[0] ? "  gemm: " : "", ctx->impl.gemm_desc,
-                   ctx->impl.plan_cache_hit ? "  (cached plan)" : "");
+                   ctx->impl.plan_cache_hit ? "  (cached plan)" : "",
+                   ctx->impl.auto_cropped ? "  (zero padding cropped)" : "");
     }
   });
 }

@@ -983,7 +983,115 @@ std::vector<uint64_t> shared_signature(const Tensor& C, const Labels& lC, const 
   return sig;
 }
 
+void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Labels& shared);
+
+// Zero padding cropped from uniform operands (the reference layout pads
+// every U(1) sector block to the largest sector).  The operands' nonzero
+// extents are scanned on the device and made consistent over the block
+// pairs: the reduced axes of a matched pair, and each kept axis over all the
+// pairs that feed one output block, take one extent, the largest scanned in
+// their class (a union-find over (block, axis)).  The operands are cropped to
+// these extents, the contraction runs on the ragged blocks and its result is
+// padded back into C.  No nonzero entry is cropped, so C equals the uniform
+// contraction up to the order in which zero products are (not) added.  Runs
+// for compute-heavy contractions only (every GEMM extent >= 32, >= 1e8 padded
+// FLOPs) when the cropped work is at most 0.8 of the padded work; never while
+// a capture is open (the scan reads extents back to the host).
+bool shared_bb_cropped(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Labels& shared) {
+  if (ctx->auto_crop <= 0 || ctx->capturing) return false;
+  const Tensor& TA = *A0;
+  const Tensor& TB = *B0;
+  if (TA.ragged || TB.ragged || C.kind != BS || TA.nkeys == 0 || TB.nkeys == 0 || !TA.voff.empty() ||
+      !TB.voff.empty())
+    return false;
+  const int PC = C.P();
+  SharedPlan sp = plan_shared(lC, PC, A0, B0, shared, false);
+  auto tail_kept = [](const std::vector<int>& perm, const Tensor& T) {
+    for (int r = 0; r < T.n2; ++r)
+      if (perm[T.P() + r] != T.P() + r + 1) return false;
+    return true;
+  };
+  if (!tail_kept(sp.permA, TA) || !tail_kept(sp.permB, TB)) return false;
+  const int nkA = static_cast<int>(sp.dkA.size()), nkB = static_cast<int>(sp.dkB.size()),
+            nred = static_cast<int>(sp.red_dense.size());
+  const int PA = TA.P(), PB = TB.P();
+  const int64_t M = prod(TA.dims, PA, PA + nkA), K = prod(TA.dims, PA + nkA, TA.N()), N = prod(TB.dims, PB + nred, TB.N());
+  if (ctx->auto_crop < 2 && (M < 32 || N < 32 || K < 32)) return false;
+  // the join (key-sorted views of the operands, as shared_bb makes them)
+  Op A = permuted_keys_only(ctx, A0, sp.permA);
+  Op B = permuted_keys_only(ctx, B0, sp.permB);
+  auto orig = [](const Op& V, const Tensor& T0, int64_t i) { return V.t == &T0 ? i : V->voff[i] / T0.blksize(); };
+  auto src = csrc_AB(lC, PC, A, B, true);
+  std::vector<int> jA, jB;
+  for (auto& l : sp.shared_prefix) { jA.push_back(find(A.labels, l) + 1); jB.push_back(find(B.labels, l) + 1); }
+  CKeys ck(C);
+  std::vector<std::pair<int64_t, int64_t>> pr;
+  std::vector<int64_t> k(PC);
+  merge_join(*A, jA, *B, jB, [&](int64_t a, int64_t b) {
+    for (int q = 0; q < PC; ++q) k[q] = src[q] > 0 ? A->key(a)[src[q] - 1] : B->key(b)[-src[q] - 1];
+    ck.touch(k);
+    pr.emplace_back(orig(A, TA, a), orig(B, TB, b));
+  });
+  const double padded = 2.0 * static_cast<double>(M) * static_cast<double>(K) * static_cast<double>(N) *
+                        static_cast<double>(pr.size());
+  if (pr.empty() || (ctx->auto_crop < 2 && padded < 1e8)) return false;
+  // scanned extents, harmonised
+  const auto scans = bs_nonzero_extents(ctx, {&TA, &TB});
+  const std::vector<int64_t>& sA = scans[0];
+  const std::vector<int64_t>& sB = scans[1];
+  const int64_t nvA = TA.nkeys * TA.n2, nv = nvA + TB.nkeys * TB.n2;
+  std::vector<int64_t> parent(nv);
+  std::iota(parent.begin(), parent.end(), 0);
+  auto root = [&](int64_t v) {
+    while (parent[v] != v) v = parent[v] = parent[parent[v]];
+    return v;
+  };
+  auto unite = [&](int64_t a, int64_t b) {
+    a = root(a);
+    b = root(b);
+    if (a != b) parent[std::max(a, b)] = std::min(a, b);
+  };
+  auto vA = [&](int64_t o, int t) { return o * TA.n2 + t; };
+  auto vB = [&](int64_t o, int t) { return nvA + o * TB.n2 + t; };
+  for (auto& p : pr)
+    for (int t = 0; t < nred; ++t) unite(vA(p.first, nkA + t), vB(p.second, t));
+  for (auto& cs : ck.contribs)
+    for (size_t i = 1; i < cs.size(); ++i) {
+      const auto& p0 = pr[cs[0]];
+      const auto& p = pr[cs[i]];
+      for (int t = 0; t < nkA; ++t) unite(vA(p.first, t), vA(p0.first, t));
+      for (int t = 0; t < nkB; ++t) unite(vB(p.second, nred + t), vB(p0.second, nred + t));
+    }
+  std::vector<int64_t> mx(nv, 1);
+  for (int64_t v = 0; v < nv; ++v) {
+    const int64_t r = root(v);
+    mx[r] = std::max(mx[r], v < nvA ? sA[v] : sB[v - nvA]);
+  }
+  std::vector<int64_t> eA(nvA), eB(nv - nvA);
+  for (int64_t v = 0; v < nv; ++v) (v < nvA ? eA[v] : eB[v - nvA]) = mx[root(v)];
+  double cropped = 0.0;
+  for (auto& p : pr) {
+    double m = 1, kk = 1, n = 1;
+    for (int t = 0; t < nkA; ++t) m *= static_cast<double>(eA[vA(p.first, t)]);
+    for (int t = 0; t < nred; ++t) kk *= static_cast<double>(eA[vA(p.first, nkA + t)]);
+    for (int t = 0; t < nkB; ++t) n *= static_cast<double>(eB[vB(p.second, nred + t) - nvA]);
+    cropped += 2.0 * m * kk * n;
+  }
+  if (!(cropped <= (ctx->auto_crop < 2 ? 0.8 : 1.0) * padded) || (ctx->auto_crop >= 2 && cropped >= padded))
+    return false;
+  TensorPtr Ar = bs_to_ragged(ctx, TA, eA, false);
+  TensorPtr Br = bs_to_ragged(ctx, TB, eB, false);
+  auto Cr = make_tensor(ctx, BS, C.dims, C.n2);
+  shared_bb(ctx, *Cr, lC, view(*Ar, A0.labels), view(*Br, B0.labels), shared);
+  reset_output(ctx, C, Cr->nkeys, Cr->nkeys * C.blksize());
+  C.keys = Cr->keys;
+  bs_pad_into(ctx, *Cr, C.data.d());
+  ctx->auto_cropped = true;
+  return true;
+}
+
 void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Labels& shared) {
+  if (shared_bb_cropped(ctx, C, lC, A0, B0, shared)) return;
   ctx->kernel_name = "contract_shared! (BS x BS)";
   const int PC = C.P();
   SharedPlan sp = plan_shared(lC, PC, A0, B0, shared, false);

@@ -98,6 +98,12 @@ struct Ctx {
   // structure.  SPARSEB_PLAN_CACHE=0 turns it off.  Opaque here.
   bool plan_cache_on = true;
   bool plan_cache_hit = false;  // the last contraction reused a cached plan (trace line)
+  // Zero padding cropped inside contract_shared! (BS x BS) on uniform
+  // operands: SPARSEB_AUTO_CROP=0 off, 1 (default) for compute-heavy
+  // contractions that the scan shows to be padded, 2 whenever the cropped
+  // work is smaller (tests).
+  int auto_crop = 1;
+  bool auto_cropped = false;  // the last contraction ran cropped (trace line)
   std::shared_ptr<void> plan_cache;
   // Pinned staging ring for host-to-device plan uploads: a copy from pinned
   // memory does not synchronise the stream, so host planning of the next
@@ -255,6 +261,8 @@ TensorPtr aliased_to_bs(Ctx* ctx, const Tensor& A);
 TensorPtr bs_to_uniform(Ctx* ctx, const Tensor& A);
 TensorPtr bs_to_ragged(Ctx* ctx, const Tensor& A, const std::vector<int64_t>& bdims, bool check_zero);
 TensorPtr bs_crop_padding(Ctx* ctx, const Tensor& A);
+std::vector<std::vector<int64_t>> bs_nonzero_extents(Ctx* ctx, const std::vector<const Tensor*>& ts);
+void bs_pad_into(Ctx* ctx, const Tensor& A, double* dst);
 // Copies variable-size blocks: dst[dst_off[i] + e] = src[src_off[i] + e], e < len[i].
 void copy_blocks(Ctx* ctx, const double* src, double* dst, const std::vector<int64_t>& src_off,
                  const std::vector<int64_t>& dst_off, const std::vector<int64_t>& len);

@@ -607,46 +607,112 @@ cudaError_t launch_perm_blocks(const double* src, double* dst, const BlockPerm* 
 }
 
 // Smallest tail extents of every block that keep all its nonzero entries:
-// block b (payload at off[b], tail extents dims[b*n2 ..]) gives ext[b*n2 + r]
-// = 1 + the largest axis-r coordinate of a nonzero element (1 for an
-// all-zero block).  One CTA per block (grid-stride); each thread keeps its
-// maxima in registers and merges them through shared-memory atomics.
+// ext[b*n2 + r] = 1 + the largest axis-r coordinate of a nonzero element
+// (ext holds 1s on entry).  A block is a column-major matrix of d0 rows
+// (axis 0) and cols columns (the other axes, flattened).  Work comes in warp
+// tasks, task_begin[b] .. task_begin[b+1] for block b, in one of three forms
+// fixed by (d0, cols) alone (ext_task_shape): rows of one column split into
+// 8192-long segments (cols == 1); a run of columns, one at a time by the whole
+// warp (d0 >= 32); 2048 columns, one lane per column (d0 < 32).  A column with
+// a nonzero entry has its other coordinates decomposed once; the maxima go to
+// ext with one atomicMax per axis and task.
+__host__ __device__ inline int64_t ext_task_cols(int64_t d0, int64_t cols) {
+  if (cols == 1) return 1;
+  if (d0 < 32) return 2048;
+  const int64_t per = 8192 / d0;
+  return per < 1 ? 1 : per > 32 ? 32 : per;
+}
+__host__ __device__ inline int64_t ext_tasks(int64_t d0, int64_t cols) {
+  if (d0 == 0 || cols == 0) return 0;
+  if (cols == 1) return (d0 + 8191) / 8192;
+  const int64_t per = ext_task_cols(d0, cols);
+  return (cols + per - 1) / per;
+}
+
 __global__ void k_block_extents(const double* __restrict__ src, const int64_t* __restrict__ off,
-                                const int64_t* __restrict__ dims, int64_t nblocks, int n2, int64_t* __restrict__ ext) {
-  __shared__ int smax[kMaxRank];
-  for (int64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
-    if (threadIdx.x < kMaxRank) smax[threadIdx.x] = 1;
-    __syncthreads();
-    int mx[kMaxRank];
-    int64_t len = 1;
-    for (int r = 0; r < n2; ++r) {
-      mx[r] = 1;
-      len *= dims[b * n2 + r];
+                                const int64_t* __restrict__ dims, const int64_t* __restrict__ task_begin,
+                                int64_t nblocks, int n2, int* __restrict__ ext) {
+  const int lane = threadIdx.x & 31;
+  const int64_t ntasks = task_begin[nblocks];
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t w = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; w < ntasks; w += warps) {
+    int64_t lo = 0, hi = nblocks - 1;  // the last block with task_begin <= w
+    while (lo < hi) {
+      const int64_t mid = (lo + hi + 1) >> 1;
+      if (task_begin[mid] <= w) lo = mid; else hi = mid - 1;
     }
-    const double* blk = src + off[b];
-    for (int64_t e = threadIdx.x; e < len; e += blockDim.x) {
-      if (blk[e] == 0.0) continue;
-      int64_t q = e;
-      for (int r = 0; r < n2; ++r) {
-        const int64_t d = dims[b * n2 + r];
-        const int c = static_cast<int>(q % d) + 1;
-        q /= d;
-        mx[r] = max(mx[r], c);
+    const int64_t b = lo, t = w - task_begin[b];
+    const int64_t* bd = dims + b * n2;
+    const int64_t d0 = bd[0];
+    int64_t cols = 1;
+    for (int r = 1; r < n2; ++r) cols *= bd[r];
+    const double* base = src + off[b];
+    int64_t mrow = 0;
+    int64_t mc[kMaxRank];
+    for (int r = 1; r < n2; ++r) mc[r] = 0;
+    auto note_col = [&](int64_t c) {
+      int64_t q = c;
+      for (int r = 1; r < n2; ++r) {
+        const int64_t x = q % bd[r] + 1;
+        q /= bd[r];
+        mc[r] = x > mc[r] ? x : mc[r];
+      }
+    };
+    if (cols == 1 || d0 >= 32) {
+      const int64_t per = ext_task_cols(d0, cols);
+      const int64_t c0 = cols == 1 ? 0 : t * per, c1 = cols == 1 ? 1 : (c0 + per < cols ? c0 + per : cols);
+      const int64_t r0 = cols == 1 ? t * 8192 : 0, r1 = cols == 1 ? (r0 + 8192 < d0 ? r0 + 8192 : d0) : d0;
+      for (int64_t c = c0; c < c1; ++c) {
+        const double* col = base + c * d0;
+        int64_t m = 0;
+#pragma unroll 4
+        for (int64_t r = r0 + lane; r < r1; r += 32)
+          if (col[r] != 0.0) m = r + 1;
+        if (__any_sync(0xffffffffu, m > 0)) {
+          mrow = m > mrow ? m : mrow;
+          note_col(c);
+        }
+      }
+    } else {
+      // one lane per column; the warp's 32 columns are one contiguous run
+      const int64_t c0 = t * 2048, c1 = c0 + 2048 < cols ? c0 + 2048 : cols;
+      for (int64_t c = c0 + lane; c < c1; c += 32) {
+        const double* col = base + c * d0;
+        int64_t m = 0;
+        for (int64_t r = 0; r < d0; ++r)
+          if (col[r] != 0.0) m = r + 1;
+        if (m > 0) {
+          mrow = m > mrow ? m : mrow;
+          note_col(c);
+        }
       }
     }
-    for (int r = 0; r < n2; ++r) atomicMax(&smax[r], mx[r]);
-    __syncthreads();
-    if (threadIdx.x < n2) ext[b * n2 + threadIdx.x] = smax[threadIdx.x];
-    __syncthreads();
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const int64_t y = __shfl_xor_sync(0xffffffffu, mrow, o);
+      mrow = y > mrow ? y : mrow;
+      for (int r = 1; r < n2; ++r) {
+        const int64_t z = __shfl_xor_sync(0xffffffffu, mc[r], o);
+        mc[r] = z > mc[r] ? z : mc[r];
+      }
+    }
+    if (lane == 0 && mrow > 0) {
+      atomicMax(&ext[b * n2], static_cast<int>(mrow));
+      for (int r = 1; r < n2; ++r) atomicMax(&ext[b * n2 + r], static_cast<int>(mc[r]));
+    }
   }
 }
 
-cudaError_t launch_block_extents(const double* src, const int64_t* d_off, const int64_t* d_dims, int64_t nblocks,
-                                 int n2, int64_t* d_ext, cudaStream_t s) {
-  if (nblocks <= 0) return cudaSuccess;
+int64_t block_extent_tasks(int64_t d0, int64_t cols) { return ext_tasks(d0, cols); }
+
+cudaError_t launch_block_extents(const double* src, const int64_t* d_off, const int64_t* d_dims,
+                                 const int64_t* d_task_begin, int64_t nblocks, int64_t ntasks, int n2, int* d_ext,
+                                 cudaStream_t s) {
+  if (ntasks <= 0 || nblocks <= 0) return cudaSuccess;
   if (n2 < 1 || n2 > kMaxRank) return cudaErrorInvalidValue;
-  const unsigned g = static_cast<unsigned>(std::min<int64_t>(nblocks, 148LL * 8));
-  k_block_extents<<<g, 256, 0, s>>>(src, d_off, d_dims, nblocks, n2, d_ext);
+  const int64_t ctas = std::min<int64_t>((ntasks + 7) / 8, 148LL * 8);
+  k_block_extents<<<static_cast<unsigned>(ctas), kThreads, 0, s>>>(src, d_off, d_dims, d_task_begin, nblocks, n2,
+                                                                    d_ext);
   return cudaGetLastError();
 }
 

@@ -155,9 +155,15 @@ cudaError_t launch_perm_blocks(const double* src, double* dst, const BlockPerm* 
 cudaError_t launch_perm_block_rows(const double* src, double* dst, const BlockPerm* d_items, int64_t n,
                                    int64_t max_rows, cudaStream_t s);
 // ext[b*n2 + r] = smallest axis-r extent of block b (payload at d_off[b],
-// extents d_dims[b*n2 ..]) that keeps all its nonzero entries (>= 1).
-cudaError_t launch_block_extents(const double* src, const int64_t* d_off, const int64_t* d_dims, int64_t nblocks,
-                                 int n2, int64_t* d_ext, cudaStream_t s);
+// extents d_dims[b*n2 ..]) that keeps all its nonzero entries (>= 1; d_ext
+// holds 1s on entry).  The scan runs in warp tasks: block b has
+// block_extent_tasks(d0, cols) of them (d0 = its first extent, cols = the
+// product of the others), starting at d_task_begin[b]; d_task_begin has
+// nblocks + 1 entries, the last = ntasks.
+int64_t block_extent_tasks(int64_t d0, int64_t cols);
+cudaError_t launch_block_extents(const double* src, const int64_t* d_off, const int64_t* d_dims,
+                                 const int64_t* d_task_begin, int64_t nblocks, int64_t ntasks, int n2, int* d_ext,
+                                 cudaStream_t s);
 // flags[i] = 1 if block i of src holds a nonzero outside its box in_lim
 // (used to check that cropping a padded block loses nothing).
 cudaError_t launch_outside_nonzero(const double* src, const BlockPerm* d_items, int64_t n, int64_t max_len,

@@ -255,18 +255,14 @@ static BlockPerm make_block_perm(int64_t src_off, int64_t dst_off, const std::ve
   return b;
 }
 
-TensorPtr bs_to_uniform(Ctx* ctx, const Tensor& A) {
-  require(A.kind == BS, SB_ERR_INVALID_ARG, "to_uniform needs a block-sparse tensor");
-  auto out = make_tensor(ctx, BS, A.dims, A.n2);
-  out->keys = A.keys;
-  out->nkeys = A.nkeys;
+// The uniform (zero-padded) blocks of A, in key order, written to dst
+// (nkeys x blksize doubles).
+void bs_pad_into(Ctx* ctx, const Tensor& A, double* dst) {
   const int64_t blk = A.blksize();
-  out->data = DevBuf(ctx, A.nkeys * blk * sizeof(double));
   if (!A.ragged) {
     if (A.nkeys)
-      SB_CK(cudaMemcpyAsync(out->data.raw(), A.data.raw(), A.nkeys * blk * sizeof(double), cudaMemcpyDeviceToDevice,
-                            ctx->stream));
-    return out;
+      SB_CK(cudaMemcpyAsync(dst, A.payload(), A.nkeys * blk * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    return;
   }
   const int P = A.P();
   std::vector<int64_t> od(A.dims.begin() + P, A.dims.end());
@@ -281,7 +277,56 @@ TensorPtr bs_to_uniform(Ctx* ctx, const Tensor& A) {
     }
     items.push_back(make_block_perm(A.block_off(i), i * blk, od, st, lim));
   }
-  perm_blocks(ctx, A.data.d(), out->data.d(), items);
+  perm_blocks(ctx, A.payload(), dst, items);
+}
+
+TensorPtr bs_to_uniform(Ctx* ctx, const Tensor& A) {
+  require(A.kind == BS, SB_ERR_INVALID_ARG, "to_uniform needs a block-sparse tensor");
+  auto out = make_tensor(ctx, BS, A.dims, A.n2);
+  out->keys = A.keys;
+  out->nkeys = A.nkeys;
+  out->data = DevBuf(ctx, A.nkeys * A.blksize() * sizeof(double));
+  bs_pad_into(ctx, A, out->data.d());
+  return out;
+}
+
+// Per block (key order) and tail axis: 1 + the largest coordinate of a
+// nonzero entry (1 for an all-zero block), for each of the tensors: one device
+// scan each, one read-back for all of them.
+std::vector<std::vector<int64_t>> bs_nonzero_extents(Ctx* ctx, const std::vector<const Tensor*>& ts) {
+  std::vector<std::vector<int64_t>> out(ts.size());
+  std::vector<int64_t> base(ts.size() + 1, 0);
+  for (size_t k = 0; k < ts.size(); ++k) base[k + 1] = base[k] + ts[k]->nkeys * ts[k]->n2;
+  if (base.back() == 0) {
+    for (size_t k = 0; k < ts.size(); ++k) out[k].assign(ts[k]->nkeys * ts[k]->n2, 1);
+    return out;
+  }
+  DevBuf dext = upload(ctx, std::vector<int>(base.back(), 1));
+  std::vector<DevBuf> keep;
+  for (size_t k = 0; k < ts.size(); ++k) {
+    const Tensor& A = *ts[k];
+    const int64_t n = A.nkeys;
+    if (n == 0 || A.n2 == 0) continue;
+    std::vector<int64_t> off(n), dims(n * A.n2), tb(n + 1, 0);
+    for (int64_t i = 0; i < n; ++i) {
+      off[i] = A.block_off(i);
+      int64_t cols = 1;
+      for (int t = 0; t < A.n2; ++t) {
+        dims[i * A.n2 + t] = A.block_dim(i, t);
+        if (t > 0) cols *= dims[i * A.n2 + t];
+      }
+      tb[i + 1] = tb[i] + block_extent_tasks(dims[i * A.n2], cols);
+    }
+    keep.push_back(upload(ctx, off));
+    keep.push_back(upload(ctx, dims));
+    keep.push_back(upload(ctx, tb));
+    const size_t m = keep.size();
+    SB_CK(launch_block_extents(A.payload(), keep[m - 3].as<int64_t>(), keep[m - 2].as<int64_t>(),
+                               keep[m - 1].as<int64_t>(), n, tb[n], A.n2, dext.as<int>() + base[k], ctx->stream));
+    ctx->note_launch();
+  }
+  const auto e = download<int>(ctx, dext.raw(), base.back());
+  for (size_t k = 0; k < ts.size(); ++k) out[k].assign(e.begin() + base[k], e.begin() + base[k + 1]);
   return out;
 }
 
@@ -290,22 +335,7 @@ TensorPtr bs_to_uniform(Ctx* ctx, const Tensor& A) {
 // padding (every U(1) sector padded to the largest) found from the values.
 TensorPtr bs_crop_padding(Ctx* ctx, const Tensor& A) {
   require(A.kind == BS, SB_ERR_INVALID_ARG, "crop_padding needs a block-sparse tensor");
-  const int64_t n = A.nkeys;
-  std::vector<int64_t> bd(n * A.n2);
-  if (n > 0 && A.n2 > 0) {
-    std::vector<int64_t> off(n), dims(n * A.n2);
-    for (int64_t i = 0; i < n; ++i) {
-      off[i] = A.block_off(i);
-      for (int t = 0; t < A.n2; ++t) dims[i * A.n2 + t] = A.block_dim(i, t);
-    }
-    DevBuf doff = upload(ctx, off), ddims = upload(ctx, dims);
-    DevBuf dext(ctx, bd.size() * sizeof(int64_t));
-    SB_CK(launch_block_extents(A.payload(), doff.as<int64_t>(), ddims.as<int64_t>(), n, A.n2, dext.as<int64_t>(),
-                               ctx->stream));
-    ctx->note_launch();
-    bd = download<int64_t>(ctx, dext.raw(), bd.size());
-  }
-  return bs_to_ragged(ctx, A, bd, false);
+  return bs_to_ragged(ctx, A, bs_nonzero_extents(ctx, {&A})[0], false);
 }
 
 TensorPtr bs_to_ragged(Ctx* ctx, const Tensor& A, const std::vector<int64_t>& bd, bool check_zero) {
