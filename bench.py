@@ -449,6 +449,42 @@ def run_ours(args, world, rank, local):
     ms_u, _, _ = timed(apply_u, args.steps)
     _, _, prof_u = timed(apply_u, args.steps, profile=True)
     value_u = replica_rate(world, args.steps, ms_u)
+    # the reference layout without cropping its zero padding (a context with
+    # SPARSEB_AUTO_CROP=0: every block GEMM runs on the padded extents)
+    saved = os.environ.get("SPARSEB_AUTO_CROP")
+    os.environ["SPARSEB_AUTO_CROP"] = "0"
+    try:
+        ctx_nc = sb.Context(local)
+    finally:
+        if saved is None:
+            os.environ.pop("SPARSEB_AUTO_CROP", None)
+        else:
+            os.environ["SPARSEB_AUTO_CROP"] = saved
+    dev_nc = {n: sb.NewBlockSparseSorted(layout.dims[n], layout.n2[n], k, None, d, ctx=ctx_nc)
+              for n, (k, d) in host.items()}
+    chain_nc = qn.HeffChain(layout, ctx_nc)
+    stream_nc = torch.cuda.ExternalStream(ctx_nc.stream)
+
+    def apply_nc():
+        return chain_nc.apply(dev_nc["psi"], dev_nc["L"], dev_nc["W1"], dev_nc["W2"], dev_nc["R"])
+
+    for _ in range(2):
+        apply_nc()
+    barrier(world)
+    ctx_nc.synchronize()
+    s_nc, e_nc = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s_nc.record(stream_nc)
+    for _ in range(args.steps):
+        apply_nc()
+    e_nc.record(stream_nc)
+    ctx_nc.synchronize()
+    barrier(world)
+    ms_nc = reduce_max(s_nc.elapsed_time(e_nc), world)
+    nc_diff = float(np.linalg.norm(chain_nc.out["T4"].data - chain_u.out["T4"].data) /
+                    max(np.linalg.norm(chain_nc.out["T4"].data), 1e-300))
+    assert nc_diff < 1e-12, nc_diff
+    del chain_nc, dev_nc
+    value_nc = replica_rate(world, args.steps, ms_nc)
     # the W12 association
     ms_w, _, _ = timed(apply_w, args.steps)
     _, _, prof_w = timed(apply_w, args.steps, profile=True)
@@ -666,11 +702,17 @@ def run_ours(args, world, rank, local):
         "library_baseline": library,
         "permute_stage": permute,
         "uniform_format": {"value": value_u, "ms_per_step": ms_u / args.steps,
-                           "gflops_executed": flops_pad * value_u / 1e9,
+                           "note": "contract! on the reference's zero-padded blocks; psi*L and R*T3 crop the padding "
+                                   "inside contract_shared! (scan, harmonised extents, ragged GEMM, padded result)",
+                           "gflops_executed": (gu["flops"] + gtu["flops"]) / args.steps * value_u / 1e9,
                            "gemm_tflops": (gu["flops"] + gtu["flops"]) / ((gu["ms"] + gtu["ms"]) * 1e-3) / 1e12
                            if gu["ms"] + gtu["ms"] > 0 else 0.0,
                            "e2e": {"value": e2e_value_u, "unit": UNIT, "h2d_bytes_per_step": h2d_u,
-                                   "d2h_bytes_per_step": d2h_u}},
+                                   "d2h_bytes_per_step": d2h_u},
+                           "no_crop": {"value": value_nc, "ms_per_step": ms_nc / args.steps,
+                                       "gflops_executed": flops_pad * value_nc / 1e9,
+                                       "rel_diff_vs_cropped": nc_diff,
+                                       "note": "SPARSEB_AUTO_CROP=0: every block GEMM on the padded extents"}},
         "ragged_vs_uniform_rel_diff": agree,
         "w12_association": {"value": value_w, "unit": UNIT, "ms_per_step": ms_w / args.steps,
                             "steps": "W12 = W1*W2, T1 = psi*L, T3 = T1*W12, T4 = R*T3 (four contract! calls, "

@@ -62,6 +62,7 @@ void destroy_ctx_now(sb_ctx* ctx) {
   cudaStreamSynchronize(ctx->impl.stream);
   ctx->impl.clear_profile();
   ctx->impl.plan_cache.reset();  // its device buffers are released on the stream
+  ctx->impl.crop_scratch.reset();
   cudaStreamSynchronize(ctx->impl.stream);
   ctx->impl.release_staging();
   if (ctx->impl.own_stream) cudaStreamDestroy(ctx->impl.stream);

@@ -985,6 +985,14 @@ std::vector<uint64_t> shared_signature(const Tensor& C, const Labels& lC, const 
 
 void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Labels& shared);
 
+struct CropScratch {
+  DevBuf a, b, c;
+};
+struct CropScratchMap {
+  static constexpr size_t kMax = 16;
+  std::unordered_map<const Tensor*, CropScratch> m;
+};
+
 // Zero padding cropped from uniform operands (the reference layout pads
 // every U(1) sector block to the largest sector).  The operands' nonzero
 // extents are scanned on the device and made consistent over the block
@@ -1079,13 +1087,24 @@ bool shared_bb_cropped(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, cons
   }
   if (!(cropped <= (ctx->auto_crop < 2 ? 0.8 : 1.0) * padded) || (ctx->auto_crop >= 2 && cropped >= padded))
     return false;
-  TensorPtr Ar = bs_to_ragged(ctx, TA, eA, false);
-  TensorPtr Br = bs_to_ragged(ctx, TB, eB, false);
+  // the cropped operands and the ragged result live in buffers kept for this
+  // output tensor: a contraction repeated on one structure (every Lanczos
+  // step) allocates nothing
+  if (!ctx->crop_scratch) ctx->crop_scratch = std::make_shared<CropScratchMap>();
+  auto& scm = static_cast<CropScratchMap*>(ctx->crop_scratch.get())->m;
+  if (scm.size() >= CropScratchMap::kMax && !scm.count(&C)) scm.clear();
+  CropScratch& sc = scm[&C];
+  TensorPtr Ar = bs_to_ragged(ctx, TA, eA, false, &sc.a);
+  TensorPtr Br = bs_to_ragged(ctx, TB, eB, false, &sc.b);
   auto Cr = make_tensor(ctx, BS, C.dims, C.n2);
+  Cr->data = std::move(sc.c);
   shared_bb(ctx, *Cr, lC, view(*Ar, A0.labels), view(*Br, B0.labels), shared);
   reset_output(ctx, C, Cr->nkeys, Cr->nkeys * C.blksize());
   C.keys = Cr->keys;
   bs_pad_into(ctx, *Cr, C.data.d());
+  sc.a = std::move(Ar->data);
+  sc.b = std::move(Br->data);
+  sc.c = std::move(Cr->data);
   ctx->auto_cropped = true;
   return true;
 }

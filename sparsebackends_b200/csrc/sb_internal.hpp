@@ -104,6 +104,10 @@ struct Ctx {
   // work is smaller (tests).
   int auto_crop = 1;
   bool auto_cropped = false;  // the last contraction ran cropped (trace line)
+  // Device buffers of the cropped operands and result, kept per output tensor
+  // between calls (sb_contract.cpp), so that repeated contractions of one
+  // structure allocate nothing.  Opaque here.
+  std::shared_ptr<void> crop_scratch;
   std::shared_ptr<void> plan_cache;
   // Pinned staging ring for host-to-device plan uploads: a copy from pinned
   // memory does not synchronise the stream, so host planning of the next
@@ -259,7 +263,10 @@ TensorPtr to_dense(Ctx* ctx, const Tensor& A);
 TensorPtr aliased_to_bs(Ctx* ctx, const Tensor& A);
 // Ragged <-> uniform adapters (zero padding / cropping).
 TensorPtr bs_to_uniform(Ctx* ctx, const Tensor& A);
-TensorPtr bs_to_ragged(Ctx* ctx, const Tensor& A, const std::vector<int64_t>& bdims, bool check_zero);
+// reuse: a buffer to hold the payload when its size is exactly the one needed
+// (moved into the result; a new one is allocated otherwise).
+TensorPtr bs_to_ragged(Ctx* ctx, const Tensor& A, const std::vector<int64_t>& bdims, bool check_zero,
+                       DevBuf* reuse = nullptr);
 TensorPtr bs_crop_padding(Ctx* ctx, const Tensor& A);
 std::vector<std::vector<int64_t>> bs_nonzero_extents(Ctx* ctx, const std::vector<const Tensor*>& ts);
 void bs_pad_into(Ctx* ctx, const Tensor& A, double* dst);

@@ -338,7 +338,7 @@ TensorPtr bs_crop_padding(Ctx* ctx, const Tensor& A) {
   return bs_to_ragged(ctx, A, bs_nonzero_extents(ctx, {&A})[0], false);
 }
 
-TensorPtr bs_to_ragged(Ctx* ctx, const Tensor& A, const std::vector<int64_t>& bd, bool check_zero) {
+TensorPtr bs_to_ragged(Ctx* ctx, const Tensor& A, const std::vector<int64_t>& bd, bool check_zero, DevBuf* reuse) {
   require(A.kind == BS, SB_ERR_INVALID_ARG, "to_ragged needs a block-sparse tensor");
   require(static_cast<int64_t>(bd.size()) == A.nkeys * A.n2, SB_ERR_INVALID_ARG, "block_dims must be nkeys x n_tail");
   const int P = A.P();
@@ -357,7 +357,9 @@ TensorPtr bs_to_ragged(Ctx* ctx, const Tensor& A, const std::vector<int64_t>& bd
     }
     out->boff[i + 1] = out->boff[i] + len;
   }
-  out->data = DevBuf(ctx, out->boff[A.nkeys] * sizeof(double));
+  const size_t need = out->boff[A.nkeys] * sizeof(double);
+  if (reuse && reuse->bytes() == need) out->data = std::move(*reuse);
+  else out->data = DevBuf(ctx, need);
   std::vector<BlockPerm> items, checks;
   for (int64_t i = 0; i < A.nkeys; ++i) {
     std::vector<int64_t> od(A.n2), st(A.n2), full(A.n2);
