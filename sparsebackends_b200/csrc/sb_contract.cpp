@@ -989,7 +989,7 @@ struct CropScratch {
   DevBuf a, b, c;
 };
 struct CropScratchMap {
-  static constexpr size_t kMax = 16;
+  static constexpr size_t kMax = 8;  // output tensors whose buffers are kept
   std::unordered_map<const Tensor*, CropScratch> m;
 };
 
