@@ -282,6 +282,25 @@ __global__ void k_perm_blocks(const double* __restrict__ src, double* __restrict
                               const BlockPerm* __restrict__ items, int64_t n) {
   for (int64_t b = blockIdx.y; b < n; b += gridDim.y) {
     const BlockPerm& it = items[b];
+    if (it.len < (int64_t{1} << 31)) {
+      // a block below 2^31 elements: 32-bit index arithmetic (every extent and
+      // coordinate of it fits), several times cheaper than 64-bit division
+      for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < it.len;
+           e0 += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t e = static_cast<uint32_t>(e0);
+        int64_t so = 0;
+        bool in = true;
+        for (int r = 0; r < it.rank; ++r) {
+          const uint32_t d = static_cast<uint32_t>(it.out_dims[r]);
+          const uint32_t c = e % d;
+          e /= d;
+          in = in && c < it.in_lim[r];
+          so += static_cast<int64_t>(c) * it.in_strides[r];
+        }
+        dst[it.dst_off + e0] = in ? src[it.src_off + so] : 0.0;
+      }
+      continue;
+    }
     for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < it.len;
          e0 += (int64_t)gridDim.x * blockDim.x) {
       int64_t e = e0, so = 0;
