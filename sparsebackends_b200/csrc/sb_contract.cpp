@@ -1009,8 +1009,8 @@ bool shared_bb_cropped(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, cons
   if (ctx->auto_crop <= 0 || ctx->capturing) return false;
   const Tensor& TA = *A0;
   const Tensor& TB = *B0;
-  if (TA.ragged || TB.ragged || C.kind != BS || TA.nkeys == 0 || TB.nkeys == 0 || !TA.voff.empty() ||
-      !TB.voff.empty())
+  if (TA.ragged || TB.ragged || C.kind != BS || TA.nkeys == 0 || TB.nkeys == 0 || TA.n2 == 0 || TB.n2 == 0 ||
+      C.n2 == 0 || !TA.voff.empty() || !TB.voff.empty())
     return false;
   const int PC = C.P();
   SharedPlan sp = plan_shared(lC, PC, A0, B0, shared, false);
