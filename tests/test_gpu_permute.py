@@ -65,3 +65,27 @@ def test_dense_permutes_each_kernel():
         D = rng.standard_normal(shape)
         got = sb.to_dense(sb.permutedims(sb.DenseTensor(D), list(perm)))
         assert np.array_equal(got, np.transpose(D, [p - 1 for p in perm])), (shape, perm)
+
+
+@pytest.mark.parametrize("tperm", [(1, 3, 2), (1, 2, 3), (2, 1, 3), (3, 2, 1)])
+def test_ragged_tail_permutes(tperm):
+    """Ragged blocks (each at its own extents): permuting then padding equals
+    padding then permuting, bit for bit.  Tail orders that keep axis 0 run the
+    per-block row copy; the others the per-block gather."""
+    import sparsebackends_b200 as sb
+    rng = np.random.Generator(np.random.PCG64(sum(tperm) * 7 + tperm[0]))
+    dims = (3, 4, 37, 6, 5)
+    keys = sorted({(int(rng.integers(1, 4)), int(rng.integers(1, 5))) for _ in range(7)}, key=lambda k: k[::-1])
+    exts = [(int(rng.integers(1, 38)), int(rng.integers(1, 7)), int(rng.integers(1, 6))) for _ in keys]
+    data = np.concatenate([rng.standard_normal(int(np.prod(e))) for e in exts])
+    A = sb.NewBlockSparseSorted(dims, 3, keys, None, data, block_dims=exts)
+    perm = [2, 1] + [2 + t for t in tperm]
+    P = sb.permutedims(A, perm)
+    assert P.is_ragged
+    # block extents travel with their blocks (keys re-sorted by the prefix swap)
+    ext_of = {(k[1], k[0]): tuple(e[t - 1] for t in tperm) for k, e in zip(keys, exts)}
+    assert P.block_dims == [ext_of[k] for k in P.keys]
+    got = sb.to_uniform(P)
+    want = sb.permutedims(sb.to_uniform(A), perm)
+    assert got.keys == want.keys
+    assert np.array_equal(got.data, want.data)
