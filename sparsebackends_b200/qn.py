@@ -230,6 +230,93 @@ def pad_ragged(layout: HeffLayout, name: str, keys, data, exts):
     return out
 
 
+def split_two_site(layout: HeffLayout, keys, data, exts, maxdim: int = 2 ** 62, cutoff: float = 0.0,
+                   absorb: str = "right"):
+    """Two-site tensor ψ[(ql, s1, s2, qr) | (ml, mr)] (ragged host triple) →
+    A[(ql, s1, qc) | (ml, mc)] · B[(qc, s2, qr) | (mc, mr)], the U(1) split of a
+    two-site DMRG step.
+
+    Rows (ql, s1, ml) and columns (s2, qr, mr) are grouped by the charge c of
+    the bond between the sites, Q(ql) + σ(s1) = Q(qr) − σ(s2); one SVD per
+    charge; the singular values of all charges are truncated together: keep at
+    most ``maxdim`` of them and drop the smallest as long as the dropped weight
+    Σ s² / Σ s² stays ≤ ``cutoff`` (at least one is kept).  ``absorb="right"``
+    gives a left-orthonormal A and B = S·V†; ``"left"`` gives A = U·S and a
+    right-orthonormal B.  Returns (A, B, link, svals, truncerr) with A and B as
+    (keys, data, exts) in the "A" layout of ``HeffLayout(left, link)`` and
+    ``HeffLayout(link, right)`` (keys column-major sorted), ``link`` the new
+    bond's sectors, ``svals`` the kept singular values (descending) and
+    ``truncerr`` the dropped weight."""
+    if absorb not in ("left", "right"):
+        raise ValueError("absorb must be 'left' or 'right'")
+    left, right = layout.left, layout.right
+    blocks, off = {}, 0
+    for k, e in zip(keys, exts):
+        n = int(np.prod(e))
+        blocks[tuple(k)] = np.asarray(data[off: off + n]).reshape(e, order="F")
+        off += n
+    rows, cols = {}, {}
+    for (ql, s1, s2, qr) in blocks:
+        c = left.charges[ql - 1] + PHYS[s1 - 1]
+        rows.setdefault(c, set()).add((ql, s1))
+        cols.setdefault(c, set()).add((s2, qr))
+    svd = {}
+    for c in sorted(rows):
+        rseg = sorted(rows[c], key=lambda x: (x[1], x[0]))
+        cseg = sorted(cols[c], key=lambda x: (x[1], x[0]))
+        roff, coff, r0, c0 = {}, {}, 0, 0
+        for ql, s1 in rseg:
+            roff[(ql, s1)] = r0
+            r0 += left.dims[ql - 1]
+        for s2, qr in cseg:
+            coff[(s2, qr)] = c0
+            c0 += right.dims[qr - 1]
+        M = np.zeros((r0, c0))
+        for (ql, s1, s2, qr), b in blocks.items():
+            if left.charges[ql - 1] + PHYS[s1 - 1] != c:
+                continue
+            r, cc = roff[(ql, s1)], coff[(s2, qr)]
+            M[r: r + b.shape[0], cc: cc + b.shape[1]] = b
+        U, S, Vt = np.linalg.svd(M, full_matrices=False)
+        svd[c] = (U, S, Vt, rseg, roff, cseg, coff)
+    allsv = sorted(((float(sv), c, i) for c, (U, S, Vt, *_r) in svd.items() for i, sv in enumerate(S)),
+                   key=lambda t: (-t[0], t[1], t[2]))
+    w = np.array([t[0] ** 2 for t in allsv])
+    total = float(w.sum())
+    m = len(allsv)
+    if total > 0.0 and cutoff > 0.0:
+        tail = np.cumsum(w[::-1])[::-1]  # tail[i] = weight of values i..end
+        m = next((i for i in range(1, len(allsv) + 1) if i == len(allsv) or tail[i] <= cutoff * total), m)
+    m = max(1, min(m, maxdim, len(allsv)))
+    kept = {}
+    for sv, c, i in allsv[:m]:
+        kept[c] = kept.get(c, 0) + 1
+    charges = sorted(kept)
+    link = U1Link(charges, [kept[c] for c in charges])
+    A_blocks, B_blocks = {}, {}
+    for qc, c in enumerate(charges, start=1):
+        U, S, Vt, rseg, roff, cseg, coff = svd[c]
+        k = kept[c]
+        Uk, Sk, Vk = U[:, :k], S[:k], Vt[:k, :]
+        if absorb == "right":
+            Vk = Sk[:, None] * Vk
+        else:
+            Uk = Uk * Sk[None, :]
+        for ql, s1 in rseg:
+            r = roff[(ql, s1)]
+            A_blocks[(ql, s1, qc)] = Uk[r: r + left.dims[ql - 1], :]
+        for s2, qr in cseg:
+            cc = coff[(s2, qr)]
+            B_blocks[(qc, s2, qr)] = Vk[:, cc: cc + right.dims[qr - 1]]
+
+    def pack(bl):
+        ks = sorted(bl, key=lambda k: k[::-1])
+        return (ks, np.concatenate([bl[k].reshape(-1, order="F") for k in ks]) if ks else np.zeros(0),
+                [bl[k].shape for k in ks])
+
+    return pack(A_blocks), pack(B_blocks), link, np.array([t[0] for t in allsv[:m]]), float(w[m:].sum())
+
+
 def _channel_conj(layout: HeffLayout, qw: int) -> int:
     """1-based sector index of the conjugate MPO channel sector (charge -c)."""
     w = layout.mpo
