@@ -1,0 +1,175 @@
+"""Two-site DMRG on the U(1) block format, the sweep of ITensorMPS ``dmrg``
+(called by the reference's tests with krylovdim 3, maxiter 1 per bond:
+``test_product_dmrg_state.jl:221-226``), run through the library's kernels.
+
+Per bond (i, i+1) of a sweep: ψ = A_i·A_{i+1} (``contract!``), the lowest
+eigenpair of the two-site H_eff by the device Lanczos (``krylov.eigsolve`` on
+``qn.HeffOperator``), the U(1) split of the eigenvector
+(``qn.split_two_site``, host SVD per centre charge) into the new site tensors,
+and the environment update (``qn.make_L`` / ``qn.make_R``).  Site tensors are
+ragged block tensors A[(ql, s, qr) | (ml, mr)] in the "A" layout of
+``qn.HeffLayout``; links are ``qn.U1Link`` with charge = 2Sz of the sites to
+their left.  The MPO is the XXZ chain's (bond dimension 5: I, S+, S-, Sz, I)
+with its link graded by the charge a channel carries.
+"""
+from __future__ import annotations
+
+from typing import List, Optional, Tuple
+
+import numpy as np
+
+from . import qn
+
+SP = np.array([[0.0, 1.0], [0.0, 0.0]])  # <s'|S+|s>, s = 1 up, 2 down
+SM = SP.T
+SZ = np.diag([0.5, -0.5])
+ID = np.eye(2)
+# channels: 1 = identity before, 2 = S+ placed (carries +2), 3 = S- placed
+# (-2), 4 = Sz placed, 5 = identity after; link sectors -2: [3], 0: [1, 4, 5],
+# +2: [2] -> (1-based sector, index in the sector)
+MPO_LINK = qn.mpo_link({-2: 1, 0: 3, 2: 1})
+CHANNEL = {1: (2, 1), 4: (2, 2), 5: (2, 3), 2: (3, 1), 3: (1, 1)}
+
+
+def xxz_terms(delta: float = 1.0):
+    """(left channel, right channel, one-site operator) of H = Σ Sx Sx + Sy Sy + Δ Sz Sz."""
+    return [(1, 1, ID), (5, 5, ID), (1, 2, SP), (2, 5, 0.5 * SM), (1, 3, SM), (3, 5, 0.5 * SP), (1, 4, SZ),
+            (4, 5, delta * SZ)]
+
+
+def mpo_tensor(ctx, delta: float = 1.0):
+    """W[(qwl, s', s, qwr) | (mwl, mwr)], ragged (every block at its channel-sector extents)."""
+    import sparsebackends_b200 as sb
+    w = MPO_LINK
+    blocks = {}
+    for wl, wr, op in xxz_terms(delta):
+        (ql, ml), (qr, mr) = CHANNEL[wl], CHANNEL[wr]
+        for sp in range(2):
+            for s in range(2):
+                if op[sp, s] == 0.0:
+                    continue
+                k = (ql, sp + 1, s + 1, qr)
+                blk = blocks.setdefault(k, np.zeros((w.dims[ql - 1], w.dims[qr - 1])))
+                blk[ml - 1, mr - 1] += op[sp, s]
+    keys = sorted(blocks, key=lambda k: k[::-1])
+    data = np.concatenate([blocks[k].reshape(-1, order="F") for k in keys])
+    return sb.NewBlockSparseSorted((w.S, 2, 2, w.S, w.D, w.D), 2, keys, None, data, ctx=ctx,
+                                   block_dims=[blocks[k].shape for k in keys])
+
+
+def boundary_envs(ctx):
+    """L0 holds the "identity before" channel, R0 the "identity after" one
+    (both on the charge-0 channel sector; bond sectors of dimension 1)."""
+    import sparsebackends_b200 as sb
+    w = MPO_LINK
+    q0 = w.index(0) + 1
+    d0 = w.dims[q0 - 1]
+    l0, r0 = np.zeros(d0), np.zeros(d0)
+    l0[CHANNEL[1][1] - 1] = 1.0
+    r0[CHANNEL[5][1] - 1] = 1.0
+    dims = (1, w.S, 1, 1, w.D, 1)
+    L = sb.NewBlockSparseSorted(dims, 3, [(1, q0, 1)], None, l0, ctx=ctx, block_dims=[(1, d0, 1)])
+    R = sb.NewBlockSparseSorted(dims, 3, [(1, q0, 1)], None, r0, ctx=ctx, block_dims=[(1, d0, 1)])
+    return L, R
+
+
+def _site(ctx, left: qn.U1Link, right: qn.U1Link, keys, data, exts):
+    import sparsebackends_b200 as sb
+    return sb.NewBlockSparseSorted((left.S, 2, right.S, left.D, right.D), 2, keys, None, data, ctx=ctx,
+                                   block_dims=exts)
+
+
+def neel_state(ctx, n: int):
+    """|up down up down ...> as site tensors with one 1x1 block each; bond b
+    carries the charge of the first b sites."""
+    bonds = [qn.U1Link([0], [1])]
+    sites = []
+    for i in range(n):
+        s = 1 if i % 2 == 0 else 2
+        bonds.append(qn.U1Link([bonds[-1].charges[0] + qn.PHYS[s - 1]], [1]))
+        sites.append(_site(ctx, bonds[i], bonds[i + 1], [(1, s, 1)], np.ones(1), [(1, 1)]))
+    return sites, bonds
+
+
+def _host(t):
+    return t.keys, np.array(t.data, copy=True), t.block_dims
+
+
+class DMRG:
+    """Two-site DMRG of the XXZ chain on ``n`` sites from the Néel state."""
+
+    def __init__(self, n: int, delta: float = 1.0, ctx=None):
+        import sparsebackends_b200 as sb
+        self.sb = sb
+        self.ctx = ctx or sb.default_context()
+        self.n = n
+        self.W = mpo_tensor(self.ctx, delta)
+        self.sites, self.bonds = neel_state(self.ctx, n)
+        L0, R0 = boundary_envs(self.ctx)
+        # Lenv[b]: sites 1..b, Renv[b]: sites b+1..n
+        self.Lenv: List = [None] * (n + 1)
+        self.Renv: List = [None] * (n + 1)
+        self.Lenv[0], self.Renv[n] = L0, R0
+        for b in range(n - 1, 0, -1):
+            self.Renv[b] = qn.make_R(self.Renv[b + 1], self.sites[b], self.W)
+        self.energy: Optional[float] = None
+        self.truncerr = 0.0
+
+    def _two_site(self, i: int):
+        """ψ of bond (i, i+1) (1-based sites) on every charge-allowed key."""
+        sb = self.sb
+        A, B = self.sites[i - 1], self.sites[i]
+        psi = qn.contract_new(["ql", "s1", "s2", "qr", "ml", "mr"], 2, A, ["ql", "s1", "qc", "ml", "mc"],
+                              B, ["qc", "s2", "qr", "mc", "mr"])
+        lay = qn.HeffLayout(self.bonds[i - 1], self.bonds[i + 1], MPO_LINK)
+        have = psi.blocks_by_key()
+        keys = sorted(lay.keys["psi"], key=lambda k: k[::-1])
+        exts = [lay.valid_extent("psi", k) for k in keys]
+        parts = [have[k] if k in have else np.zeros(int(np.prod(e))) for k, e in zip(keys, exts)]
+        data = np.concatenate(parts) if parts else np.zeros(0)
+        x = sb.NewBlockSparseSorted(lay.dims["psi"], 2, keys, None, data, ctx=self.ctx, block_dims=exts)
+        return lay, x
+
+    def _update(self, i: int, absorb: str, maxdim: int, cutoff: float, krylovdim: int, maxiter: int):
+        from . import krylov
+        lay, x = self._two_site(i)
+        op = qn.HeffOperator(lay, self.Lenv[i - 1], self.W, self.W, self.Renv[i + 1], self.ctx)
+        vals, vecs, _ = krylov.eigsolve(op, x, 1, "SR", krylovdim=krylovdim, maxiter=maxiter, tol=1e-14)
+        self.energy = float(vals[0])
+        (ak, ad, ae), (bk, bd, be), link, _, err = qn.split_two_site(lay, *_host(vecs[0]), maxdim=maxdim,
+                                                                   cutoff=cutoff, absorb=absorb)
+        self.truncerr = max(self.truncerr, err)
+        self.bonds[i] = link
+        self.sites[i - 1] = _site(self.ctx, self.bonds[i - 1], link, ak, ad, ae)
+        self.sites[i] = _site(self.ctx, link, self.bonds[i + 1], bk, bd, be)
+
+    def sweep(self, maxdim: int, cutoff: float = 0.0, krylovdim: int = 3, maxiter: int = 1) -> float:
+        """One left-to-right and one right-to-left pass; returns the last energy."""
+        n = self.n
+        for i in range(1, n):
+            self._update(i, "right", maxdim, cutoff, krylovdim, maxiter)
+            self.Lenv[i] = qn.make_L(self.Lenv[i - 1], self.sites[i - 1], self.W)
+        for i in range(n - 1, 0, -1):
+            self._update(i, "left", maxdim, cutoff, krylovdim, maxiter)
+            self.Renv[i] = qn.make_R(self.Renv[i + 1], self.sites[i], self.W)
+        return self.energy
+
+    def run(self, maxdims: List[int], cutoff: float = 0.0, krylovdim: int = 3, maxiter: int = 1) -> Tuple[float, list]:
+        energies = [self.sweep(m, cutoff, krylovdim, maxiter) for m in maxdims]
+        return energies[-1], energies
+
+
+def exact_ground_energy(n: int, delta: float = 1.0) -> float:
+    """Lowest eigenvalue of the XXZ chain in the total 2Sz = 0 sector (dense)."""
+    dim = 2 ** n
+    H = np.zeros((dim, dim))
+    for i in range(n - 1):
+        for a, b, c in ((SZ, SZ, delta), (SP, SM, 0.5), (SM, SP, 0.5)):
+            ops = [ID] * n
+            ops[i], ops[i + 1] = a, b
+            M = ops[0]
+            for o in ops[1:]:
+                M = np.kron(M, o)
+            H += c * M
+    idx = [s for s in range(dim) if bin(s).count("1") == n // 2]
+    return float(np.linalg.eigvalsh(H[np.ix_(idx, idx)])[0])
