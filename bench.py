@@ -247,6 +247,42 @@ def permute_stage(ctx, L, hbm_peak, reps: int = 5):
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)", "cases": out}
 
 
+def serving_leg(ctx, seed: int, nreq: int = 16):
+    """Ground-state solves served one at a time: a seeded stream of XXZ chains
+    (Delta ~ U[0.5, 1.5], N ~ U{8..12}, chi_max ~ log-uniform [8, 32], two-site
+    DMRG from the Neel state, 4 sweeps, cutoff 1e-10, krylovdim 3, maxiter 1)
+    through ``sparsebackends_b200.dmrg``.  The request shape of the serving
+    workload (N up to 128, chi_max up to 1024) is reduced so that the leg takes
+    seconds; requests run back to back, without batching.  Latency is the wall
+    time of one solve, synchronised at its end."""
+    from sparsebackends_b200 import dmrg
+    rng = np.random.Generator(np.random.PCG64(seed))
+    reqs = [(int(rng.integers(8, 13)), float(rng.uniform(0.5, 1.5)),
+             int(round(math.exp(rng.uniform(math.log(8), math.log(32)))))) for _ in range(nreq)]
+    dmrg.DMRG(8, 1.0, ctx).run([8], cutoff=1e-10)  # warm-up
+    ctx.synchronize()
+    lat, energies = [], []
+    t0 = time.perf_counter()
+    for n, delta, chi in reqs:
+        t = time.perf_counter()
+        e, _ = dmrg.DMRG(n, delta, ctx).run([chi] * 4, cutoff=1e-10, krylovdim=3, maxiter=1)
+        ctx.synchronize()
+        lat.append((time.perf_counter() - t) * 1e3)
+        energies.append(e)
+    total = time.perf_counter() - t0
+    srt = sorted(lat)
+
+    def pct(p):  # nearest rank
+        return srt[max(0, math.ceil(p / 100.0 * len(srt)) - 1)]
+
+    return {"solves_per_s": nreq / total, "p50_ms": pct(50), "p99_ms": pct(99), "requests": nreq,
+            "stream": "XXZ, Delta~U[0.5,1.5], N~U{8..12}, chi_max~logU[8,32], 4 sweeps, cutoff 1e-10, "
+                      "krylovdim 3, maxiter 1 (reduced from N<=128, chi_max<=1024)",
+            "mode": "plain FP64, one request at a time (no continuous batching)",
+            "energy_per_site_range": [min(e / n for e, (n, _, _) in zip(energies, reqs)),
+                                      max(e / n for e, (n, _, _) in zip(energies, reqs))]}
+
+
 def fp64_peak_tflops():
     import torch
     n = 8192
@@ -670,6 +706,7 @@ def run_ours(args, world, rank, local):
     hbm_peak = measured_hbm_gbs()
     gu, gtu = prof_u["gemm"], prof_u["gemm_thin"]
     permute = permute_stage(ctx, dev_u["L"], hbm_peak)
+    serving = serving_leg(ctx, args.seed)
     # the vendor library on the same block lists, after every timed leg (its
     # many small launches stay out of the launch lists profiled from this run)
     library = cublas_block_lists(layout)
@@ -701,6 +738,7 @@ def run_ours(args, world, rank, local):
         "kernel_time_share": {k: v["ms"] / max(1e-9, sum(x["ms"] for x in prof.values())) for k, v in prof.items()},
         "library_baseline": library,
         "permute_stage": permute,
+        "serving": serving,
         "uniform_format": {"value": value_u, "ms_per_step": ms_u / args.steps,
                            "note": "contract! on the reference's zero-padded blocks; psi*L and R*T3 crop the padding "
                                    "inside contract_shared! (scan, harmonised extents, ragged GEMM, padded result)",
