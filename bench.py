@@ -11,6 +11,11 @@ format (every block at its sector extents); the reference's uniform format
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+Beside the headline the line carries the reference's zero-padded layout
+(cropped inside contract! and not), the permute stage, CUDA-graph replay, one
+Lanczos solve, the cuBLAS block-list baseline and a small serving leg
+(two-site DMRG solves one at a time, solves/s with p50/p99).
+
 Prints one JSON line (rank 0).  `value` is whole-job matvecs/s with inputs
 resident in HBM; `e2e` is the same through the public API with psi uploaded
 from pinned host memory and H·psi read back every step.  Multi-GPU runs are
