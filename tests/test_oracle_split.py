@@ -7,7 +7,9 @@ of a two-site DMRG update on the block format:
 * ``maxdim`` keeps that many singular values in all, the largest ones, and
   the squared reconstruction error equals the reported dropped weight;
 * ``cutoff`` drops the smallest values while the dropped weight stays within
-  cutoff · Σ s², and no further one could be dropped.
+  cutoff · Σ s², and no further one could be dropped;
+* the dense ground-state energies that the DMRG tests compare with match
+  closed forms.
 """
 import numpy as np
 import pytest
@@ -93,3 +95,16 @@ def test_cutoff_rule():
     m = len(sv)
     assert err <= cut * total + 1e-15
     assert m == 1 or w[m - 1:].sum() > cut * total  # one more drop would exceed the cutoff
+
+
+def test_exact_diagonalisation_reference_energies():
+    """The dense reference of the DMRG tests against closed forms: the
+    two-site singlet (-3/4), four sites (-(3 + 2 sqrt 3)/4), and the XX chain
+    (Delta = 0), free fermions with single-particle energies cos(k pi/(N+1))
+    filled up to half filling."""
+    from sparsebackends_b200 import dmrg
+    assert dmrg.exact_ground_energy(2) == pytest.approx(-0.75, abs=1e-13)
+    assert dmrg.exact_ground_energy(4) == pytest.approx(-(3 + 2 * np.sqrt(3)) / 4, abs=1e-12)
+    n = 8
+    eps = np.sort(np.cos(np.arange(1, n + 1) * np.pi / (n + 1)))
+    assert dmrg.exact_ground_energy(n, 0.0) == pytest.approx(eps[: n // 2].sum(), abs=1e-12)
