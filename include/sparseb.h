@@ -4,9 +4,9 @@
  * Drop-in for SparseBackends' tensor-algebra entry point
  *     SparseBackends.contract!(C, labelsC, A, labelsA, B, labelsB)
  *     (SparseBackends/src/tensoralgebra/contract.jl:37-104)
- * and the storage/conversion functions it relies on.  A Julia `ccall` shim (see
- * INTEGRATION.md) replaces the Julia kernels with these calls; Python reaches
- * the same symbols through ctypes (package sparsebackends_b200).
+ * and the storage/conversion functions it relies on.  A Julia `ccall` shim
+ * replaces the Julia kernels with these calls; Python reaches the same
+ * symbols through ctypes (package sparsebackends_b200).
  *
  * Conventions (identical to the reference):
  *  - all tensors are FP64; dense payloads are column-major;
@@ -76,6 +76,32 @@ SB_API void* sb_ctx_get_stream(const sb_ctx* ctx);
 SB_API sb_status sb_ctx_synchronize(sb_ctx* ctx);
 /* Number of kernels this context has launched so far.                        */
 SB_API int64_t sb_ctx_launch_count(const sb_ctx* ctx);
+/* Arithmetic of the block GEMMs inside sb_contract (the per-pair mul! of
+ * ta/contract_bs_bs.jl:716-723 and ta/contract_bs_dense.jl:576-611, which the
+ * reference runs in FP64).  Tensors stay FP64 unless created with
+ * sb_tensor_create_bs_f32.
+ *   SB_PRECISION_F64    FP64 tensor-core (DMMA) GEMMs, the drop-in (default);
+ *   SB_PRECISION_TF32X3 tcgen05 tensor cores on FP32 copies of the operands,
+ *                       every value split into TF32 hi + lo and the three
+ *                       significant products summed in FP32 chunks that are
+ *                       added with Kahan compensation (a few 1e-7 to 1e-6
+ *                       relative per block);
+ *   SB_PRECISION_TF32   tcgen05, one TF32 product (about 3e-4 relative).
+ * Only the tiled GEMMs change; the K <= 16 (MPO) steps, outer products,
+ * Kahan sums and axpys compute in FP64.  Operands must lie in FP32's range.
+ * The FP32 copy of an FP64 operand is kept with its tensor and remade after
+ * the library writes the tensor or hands out its device pointer
+ * (sb_tensor_device_data); inside a captured graph it is remade on every
+ * replay.  Not while a capture is open.  A bounded wait of the tensor-core
+ * kernel that runs out is reported by the next sb_ctx_synchronize as
+ * SB_ERR_TIMEOUT.                                                           */
+typedef enum sb_precision {
+  SB_PRECISION_F64 = 0,
+  SB_PRECISION_TF32X3 = 1,
+  SB_PRECISION_TF32 = 2
+} sb_precision;
+SB_API sb_status sb_ctx_set_precision(sb_ctx* ctx, int precision);
+SB_API int sb_ctx_get_precision(const sb_ctx* ctx);
 /* Per-launch kernel timing (CUDA events on the context stream), the
  * replacement of the reference's SB_TRACE stage timers
  * (ta/contract_bs_dense.jl:46-202).  Enabling clears earlier records.       */
@@ -83,7 +109,8 @@ SB_API sb_status sb_ctx_set_profiling(sb_ctx* ctx, int enable);
 /* Totals for one kernel class since profiling was enabled:
  * kind 0 = tiled block GEMM (with its split-K reduction), 1 = permute,
  * 2 = outer-product accumulation, 3 = segmented axpy, 4 = other (QR/SVD,
- * gathers), 5 = vector-space operations, 6 = thin block GEMM (K <= 16).
+ * gathers), 5 = vector-space operations, 6 = thin block GEMM (K <= 16),
+ * 7 = tensor-core (tcgen05) block GEMM.
  * Synchronises the context stream.                                           */
 SB_API sb_status sb_ctx_profile_summary(sb_ctx* ctx, int kind, int64_t* launches, double* total_ms,
                                         double* flops, double* bytes);
@@ -115,6 +142,19 @@ SB_API sb_status sb_tensor_create_bs(sb_ctx* ctx, int nd, const int64_t* dims, i
 SB_API sb_status sb_tensor_create_bs_ragged(sb_ctx* ctx, int nd, const int64_t* dims, int n_tail,
                                             int64_t nblocks, const int64_t* keys, const int64_t* block_dims,
                                             const double* data, sb_tensor** out);
+/* Empty block-sparse tensor with FP32 storage, to receive the result of
+ * sb_contract in a tensor-core precision (SB_PRECISION_TF32X3 / _TF32): the
+ * intermediates of a two-site H_eff chain (psi*L, *W1, *W2) kept in FP32 halve
+ * the bytes of the memory-bound MPO steps.  Such tensors may be the output or
+ * an operand of a multi-label block-sparse contraction (contract_shared!,
+ * ta/contract_bs_bs.jl:572-730) only: as the long operand and result of a
+ * K <= 16 step, or as either operand or result of a tensor-core GEMM step;
+ * every other kernel rejects them with SB_ERR_UNSUPPORTED_TYPES.
+ * sb_tensor_export_bs widens their values to FP64.  No counterpart in the
+ * reference (FP64 throughout).                                              */
+SB_API sb_status sb_tensor_create_bs_f32(sb_ctx* ctx, int nd, const int64_t* dims, int n_tail, sb_tensor** out);
+/* *f32 = 1 for FP32 storage (sb_tensor_create_bs_f32), else 0.              */
+SB_API sb_status sb_tensor_storage_f32(const sb_tensor* t, int* f32);
 /* COOTensor{T,N}(dims, keys, vals, dirty) (src/coo/storage.jl:1-15).        */
 SB_API sb_status sb_tensor_create_coo(sb_ctx* ctx, int nd, const int64_t* dims, int64_t nnz,
                                const int64_t* keys, const double* vals, int dirty, sb_tensor** out);

@@ -115,7 +115,20 @@ class Context:
     def launch_count(self) -> int:
         return int(self._lib.sb_ctx_launch_count(self._h))
 
-    PROFILE_KINDS = {"gemm": 0, "permute": 1, "outer": 2, "axpy": 3, "other": 4, "vector": 5, "gemm_thin": 6}
+    PROFILE_KINDS = {"gemm": 0, "permute": 1, "outer": 2, "axpy": 3, "other": 4, "vector": 5, "gemm_thin": 6,
+                     "gemm_tc": 7}
+
+    PRECISIONS = {"f64": 0, "tf32x3": 1, "tf32": 2}
+
+    @property
+    def precision(self) -> str:
+        """Arithmetic of the tiled block GEMMs: "f64" (default, the drop-in),
+        "tf32x3" (tcgen05, operands split into TF32 hi + lo) or "tf32"."""
+        v = int(self._lib.sb_ctx_get_precision(self._h))
+        return {b: a for a, b in self.PRECISIONS.items()}[v]
+
+    def set_precision(self, precision: str) -> None:
+        _check(self, self._lib.sb_ctx_set_precision(self._h, self.PRECISIONS[precision]))
 
     def set_profiling(self, enable: bool) -> None:
         """Time every kernel launch with CUDA events on the context stream."""
@@ -384,9 +397,25 @@ class NewBlockSparseSorted(_Tensor):
         return out
 
     @staticmethod
-    def empty(dims: Sequence[int], n2: int, ctx: Optional[Context] = None) -> "NewBlockSparseSorted":
-        """``NewBlockSparseSorted{T,N,N2}(dims)`` (storage.jl:86-93)."""
-        return NewBlockSparseSorted(dims, n2, ctx=ctx)
+    def empty(dims: Sequence[int], n2: int, ctx: Optional[Context] = None,
+              f32: bool = False) -> "NewBlockSparseSorted":
+        """``NewBlockSparseSorted{T,N,N2}(dims)`` (storage.jl:86-93).  With
+        ``f32`` the tensor stores FP32 values (sb_tensor_create_bs_f32): an
+        output for tensor-core contractions, e.g. H_eff chain intermediates."""
+        if not f32:
+            return NewBlockSparseSorted(dims, n2, ctx=ctx)
+        ctx = ctx or default_context()
+        dims = tuple(int(d) for d in dims)
+        h = C.c_void_p()
+        _check(ctx, ctx._lib.sb_tensor_create_bs_f32(ctx._h, len(dims), _i64(dims), int(n2), C.byref(h)))
+        return NewBlockSparseSorted(dims, n2, ctx=ctx, _handle=h)
+
+    @property
+    def is_f32(self) -> bool:
+        """FP32 storage (values widened to FP64 on export)."""
+        v = C.c_int()
+        _check(self.ctx, self.ctx._lib.sb_tensor_storage_f32(self._h, C.byref(v)))
+        return bool(v.value)
 
 
 class COOTensor(_Tensor):

@@ -29,6 +29,8 @@ SIGNATURES = {
     "sb_ctx_get_stream": (vp, [vp]),
     "sb_ctx_synchronize": (C.c_int, [vp]),
     "sb_ctx_launch_count": (i64, [vp]),
+    "sb_ctx_set_precision": (C.c_int, [vp, C.c_int]),
+    "sb_ctx_get_precision": (C.c_int, [vp]),
     "sb_ctx_set_profiling": (C.c_int, [vp, C.c_int]),
     "sb_ctx_profile_summary": (C.c_int, [vp, C.c_int, P_i64, P_f64, P_f64, P_f64]),
     "sb_tensor_create_dense": (C.c_int, [vp, C.c_int, P_i64, P_f64, C.POINTER(vp)]),
@@ -37,6 +39,8 @@ SIGNATURES = {
     "sb_tensor_create_bs_ragged": (C.c_int, [vp, C.c_int, P_i64, C.c_int, i64, P_i64, P_i64, P_f64,
                                              C.POINTER(vp)]),
     "sb_tensor_block_dims": (C.c_int, [vp, P_int, P_i64, P_i64]),
+    "sb_tensor_create_bs_f32": (C.c_int, [vp, C.c_int, P_i64, C.c_int, C.POINTER(vp)]),
+    "sb_tensor_storage_f32": (C.c_int, [vp, P_int]),
     "sb_tensor_to_uniform": (C.c_int, [vp, vp, C.POINTER(vp)]),
     "sb_tensor_to_ragged": (C.c_int, [vp, vp, P_i64, C.c_int, C.POINTER(vp)]),
     "sb_tensor_crop_padding": (C.c_int, [vp, vp, C.POINTER(vp)]),

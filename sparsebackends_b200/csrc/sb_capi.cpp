@@ -63,6 +63,7 @@ void destroy_ctx_now(sb_ctx* ctx) {
   ctx->impl.clear_profile();
   ctx->impl.plan_cache.reset();  // its device buffers are released on the stream
   ctx->impl.crop_scratch.reset();
+  ctx->impl.tc_status.reset();
   cudaStreamSynchronize(ctx->impl.stream);
   ctx->impl.release_staging();
   if (ctx->impl.own_stream) cudaStreamDestroy(ctx->impl.stream);
@@ -78,6 +79,19 @@ void check_keys_in_range(const std::vector<int64_t>& keys, int64_t n, int klen, 
 }
 
 void check_ctx(sb_ctx* ctx) { require(ctx != nullptr, SB_ERR_INVALID_ARG, "context is NULL"); }
+
+// After a synchronisation: a tensor-core GEMM whose bounded wait ran out
+// left 1 in the context's status word (its results are invalid).
+void check_tc_status(sb_ctx* ctx) {
+  if (!ctx->impl.tc_launched || !ctx->impl.tc_status.raw()) return;
+  int st = 0;
+  SB_CK(cudaMemcpy(&st, ctx->impl.tc_status.raw(), sizeof(int), cudaMemcpyDeviceToHost));
+  ctx->impl.tc_launched = false;
+  if (st != 0) {
+    SB_CK(cudaMemset(ctx->impl.tc_status.raw(), 0, sizeof(int)));
+    sb::fail(SB_ERR_TIMEOUT, "tensor-core block GEMM: a bounded wait on the tensor core ran out; results are invalid");
+  }
+}
 void check_t(const sb_tensor* t) { require(t != nullptr && t->impl, SB_ERR_INVALID_ARG, "tensor is NULL"); }
 
 }  // namespace
@@ -113,6 +127,8 @@ sb_status sb_ctx_create(int device, unsigned flags, sb_ctx** out) {
     if (const char* pc = std::getenv("SPARSEB_PLAN_CACHE")) c->impl.plan_cache_on = std::atoi(pc) != 0;
     if (const char* ac = std::getenv("SPARSEB_AUTO_CROP")) c->impl.auto_crop = std::atoi(ac);
     if (const char* sk = std::getenv("SPARSEB_GEMM_SPLITK")) c->impl.gemm_splitk = std::max(0, std::atoi(sk));
+    if (const char* kc = std::getenv("SPARSEB_TC_KC")) c->impl.tc_kc = std::max(1, std::atoi(kc));
+    if (const char* po = std::getenv("SPARSEB_POISON_OUTPUT")) c->impl.poison_output = std::atoi(po) != 0;
     // Keep freed device memory cached in the stream-ordered pool.
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -153,8 +169,26 @@ sb_status sb_ctx_synchronize(sb_ctx* ctx) {
   return guard(ctx, [&] {
     check_ctx(ctx);
     ctx->impl.sync();
+    check_tc_status(ctx);
   });
 }
+
+sb_status sb_ctx_set_precision(sb_ctx* ctx, int precision) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    require(precision == SB_PRECISION_F64 || precision == SB_PRECISION_TF32X3 || precision == SB_PRECISION_TF32,
+            SB_ERR_INVALID_ARG, "unknown precision");
+    require(!ctx->impl.capturing, SB_ERR_INVALID_ARG, "precision cannot change while a capture is open");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    if (precision != SB_PRECISION_F64 && !ctx->impl.tc_status.raw()) {
+      ctx->impl.tc_status = sb::DevBuf(&ctx->impl, sizeof(int));
+      SB_CK(cudaMemsetAsync(ctx->impl.tc_status.raw(), 0, sizeof(int), ctx->impl.stream));
+    }
+    ctx->impl.precision = precision;
+  });
+}
+
+int sb_ctx_get_precision(const sb_ctx* ctx) { return ctx ? ctx->impl.precision : -1; }
 
 int64_t sb_ctx_launch_count(const sb_ctx* ctx) { return ctx ? ctx->impl.launches : 0; }
 
@@ -475,8 +509,17 @@ sb_status sb_tensor_export_bs(sb_ctx* ctx, const sb_tensor* t, int64_t* keys, in
     if (ids)
       for (int64_t i = 0; i < x.nkeys; ++i) ids[i] = i + 1;
     if (data && x.nkeys) {
-      SB_CK(cudaMemcpyAsync(data, x.data.raw(), x.payload_len() * sizeof(double), cudaMemcpyDeviceToHost, ctx->impl.stream));
-      ctx->impl.sync();
+      if (x.f32) {  // FP32 storage: widened on the host
+        std::vector<float> tmp(static_cast<size_t>(x.payload_len()));
+        SB_CK(cudaMemcpyAsync(tmp.data(), x.data.raw(), tmp.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                              ctx->impl.stream));
+        ctx->impl.sync();
+        std::copy(tmp.begin(), tmp.end(), data);
+      } else {
+        SB_CK(cudaMemcpyAsync(data, x.data.raw(), x.payload_len() * sizeof(double), cudaMemcpyDeviceToHost,
+                              ctx->impl.stream));
+        ctx->impl.sync();
+      }
     }
   });
 }
@@ -491,9 +534,30 @@ sb_status sb_tensor_export_bs_async(sb_ctx* ctx, const sb_tensor* t, int64_t* ke
     if (keys) std::copy(x.keys.begin(), x.keys.end(), keys);
     if (ids)
       for (int64_t i = 0; i < x.nkeys; ++i) ids[i] = i + 1;
+    require_f64(x, "sb_tensor_export_bs_async");
     if (data && x.nkeys)
       SB_CK(cudaMemcpyAsync(data, x.data.raw(), x.payload_len() * sizeof(double), cudaMemcpyDeviceToHost,
                             ctx->impl.stream));
+  });
+}
+
+sb_status sb_tensor_create_bs_f32(sb_ctx* ctx, int nd, const int64_t* dims, int n_tail, sb_tensor** out) {
+  return guard(ctx, [&] {
+    check_ctx(ctx);
+    require(out != nullptr, SB_ERR_INVALID_ARG, "out is NULL");
+    SB_CK(cudaSetDevice(ctx->impl.device));
+    auto d = read_dims(nd, dims);
+    require(n_tail > 0 && n_tail <= nd, SB_ERR_ASSERTION, "0 < N2 <= N required");
+    auto t = make_tensor(&ctx->impl, BS, d, n_tail);
+    t->f32 = true;
+    *out = wrap(ctx, std::move(t));
+  });
+}
+
+sb_status sb_tensor_storage_f32(const sb_tensor* t, int* f32) {
+  return guard(t ? t->owner : nullptr, [&] {
+    check_t(t);
+    if (f32) *f32 = t->impl->f32 ? 1 : 0;
   });
 }
 
@@ -547,6 +611,7 @@ sb_status sb_tensor_export_dense(sb_ctx* ctx, const sb_tensor* t, double* data) 
 sb_status sb_tensor_device_data(const sb_tensor* t, double** d_ptr, int64_t* len) {
   return guard(t ? t->owner : nullptr, [&] {
     check_t(t);
+    ++t->impl->version;  // the caller may write through the pointer
     if (d_ptr) *d_ptr = t->impl->data.d();
     if (len) *len = t->impl->payload_len();
   });
@@ -702,6 +767,7 @@ sb_status sb_tensor_scale(sb_ctx* ctx, sb_tensor* A, double alpha) {
     check_ctx(ctx);
     check_t(A);
     SB_CK(cudaSetDevice(ctx->impl.device));
+    ++A->impl->version;
     tensor_scale(&ctx->impl, *A->impl, alpha);
   });
 }
@@ -711,6 +777,7 @@ sb_status sb_tensor_fill(sb_ctx* ctx, sb_tensor* A, double x) {
     check_ctx(ctx);
     check_t(A);
     SB_CK(cudaSetDevice(ctx->impl.device));
+    ++A->impl->version;
     tensor_fill(&ctx->impl, *A->impl, x);
   });
 }
@@ -721,6 +788,7 @@ sb_status sb_tensor_map(sb_ctx* ctx, sb_tensor* R, const sb_tensor* A, int op, d
     check_t(R);
     check_t(A);
     SB_CK(cudaSetDevice(ctx->impl.device));
+    ++R->impl->version;
     tensor_map(&ctx->impl, *R->impl, *A->impl, op, alpha, beta);
   });
 }

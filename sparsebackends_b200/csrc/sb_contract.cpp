@@ -122,6 +122,8 @@ Op permuted_keys_only(Ctx* ctx, const Op& in, const std::vector<int>& perm) {
     }
   }
   v->vdata = A.payload();
+  v->vsrc = &A.owner();
+  v->f32 = A.f32;
   Op out;
   out.owned = std::move(v);
   out.t = out.owned.get();
@@ -235,11 +237,17 @@ struct CKeys {
 // payload buffer is kept when its size does not change: every element of it
 // is rewritten by the kernel that follows.
 void reset_output(Ctx* ctx, Tensor& C, int64_t nkeys, int64_t payload) {
+  ++C.version;
   C.keys.clear();
   C.alias_ids.clear();
   C.nkeys = nkeys;
   C.n_templates = 0;
-  if (C.data.bytes() != static_cast<size_t>(payload) * sizeof(double)) C.data = DevBuf(ctx, payload * sizeof(double));
+  const size_t esz = C.f32 ? sizeof(float) : sizeof(double);
+  if (C.data.bytes() != static_cast<size_t>(payload) * esz) C.data = DevBuf(ctx, payload * esz);
+  // SPARSEB_POISON_OUTPUT=1 (tests): every output payload starts as NaN, so
+  // an element that no kernel writes cannot pass for a computed value
+  if (ctx->poison_output && payload > 0)
+    SB_CK(cudaMemsetAsync(C.data.raw(), 0xFF, static_cast<size_t>(payload) * esz, ctx->stream));
   C.scalars.reset();
   C.ragged = false;
   C.bdims.clear();
@@ -251,23 +259,75 @@ void reset_output(Ctx* ctx, Tensor& C, int64_t nkeys, int64_t payload) {
 // parameters, so that a contraction with an unchanged block structure can be
 // launched again without planning or uploads (the plan cache of shared_bb).
 struct GemmLaunch {
-  enum Kind { NONE, THIN, TILED, EDGES } kind = NONE;
-  DevBuf dc, dp;
+  enum Kind { NONE, THIN, TILED, EDGES, TC } kind = NONE;
+  DevBuf dc, dp, dt, dsplit;
   int32_t ncb = 0;
   int64_t n = 0;  // strips (thin) or tiles
   bool xT = false, yT = false, small_rows = false, persistent = false;
   int small_max = 0, k_max = 0, splitk = 1, bm = 64, bn = 64;
   GemmShape shape = GemmShape::T64x64;
+  // tensor-core launches: explicit tile list, tiles [nz_begin, n) are the
+  // pair-less C blocks; swap puts Y on the 128-row side; passes 3 or 1
+  int32_t nz_begin = 0, nsplits = 0, nparts = 0;
+  bool swap = false;
+  int passes = 3, kc = 16;
+  int64_t x_len = 0, y_len = 0;  // elements of X and Y the pairs read (from offset 0)
   double flops = 0.0, bytes = 0.0;
   char desc[sizeof(Ctx::gemm_desc)] = "";
-  void run(Ctx* ctx, const double* X, const double* Y, double* C) const {
+  // Tensor-core launch on FP32 operands; C FP64 or FP32.
+  void run_tc(Ctx* ctx, const float* X, const float* Y, void* C, bool c_f64) const {
+    require(ctx->tc_status.raw() != nullptr, SB_ERR_INVALID_ARG, "tensor-core GEMM without a status word");
+    std::memcpy(ctx->gemm_desc, desc, sizeof(desc));
+    DevBuf part;  // k-segment partial tiles of split tiles (stream-ordered scratch)
+    if (nparts > 0) part = DevBuf(ctx, static_cast<size_t>(nparts) * 128 * 128 * sizeof(double));
+    {
+      ProfScope ps(ctx, PROF_GEMM_TC, flops, bytes);
+      SB_CK(launch_gemm_tc(X, Y, C, c_f64, dc.as<GemmCBlock>(), dp.as<GemmPair>(), dt.as<TcTile>(),
+                           static_cast<int32_t>(n), nz_begin, xT, yT, swap, passes, kc, part.d(),
+                           dsplit.as<TcSplit>(), nsplits, ctx->tc_status.as<int>(), ctx->stream));
+    }
+    ctx->tc_launched = true;
+    ctx->note_launch(nsplits > 0 ? 2 : 1);
+  }
+  // Operands and result as tensors: FP32-stored tensors (the intermediates of
+  // a tensor-core H_eff chain) go to the launches that read or write them,
+  // FP64 operands of a tensor-core launch through their FP32 copies.
+  void run_io(Ctx* ctx, const Tensor& Xt, const Tensor& Yt, Tensor& Ct) const {
     if (kind == NONE) return;
+    if (kind == TC) {
+      run_tc(ctx, f32_payload(ctx, Xt), f32_payload(ctx, Yt), Ct.data.raw(), !Ct.f32);
+      return;
+    }
+    if (kind == THIN) {
+      const Tensor& lt = small_rows ? Yt : Xt;
+      const Tensor& st = small_rows ? Xt : Yt;
+      require(lt.f32 == Ct.f32 && !st.f32, SB_ERR_UNSUPPORTED_TYPES,
+              "K <= 16 contraction with FP32 storage: the long operand and the result must both be FP32 and "
+              "the short operand FP64");
+      run(ctx, Xt.payload(), Yt.payload(), Ct.data.d(), lt.f32);
+      return;
+    }
+    require(!Xt.f32 && !Yt.f32 && !Ct.f32, SB_ERR_UNSUPPORTED_TYPES,
+            "FP32-stored tensors need a tensor-core precision (sb_ctx_set_precision)");
+    run(ctx, Xt.payload(), Yt.payload(), Ct.data.d());
+  }
+  void run(Ctx* ctx, const double* X, const double* Y, double* C, bool long_f32 = false) const {
+    if (kind == NONE) return;
+    if (kind == TC) {
+      // FP32 copies of the operand ranges the pairs read (no tensor to keep them with)
+      DevBuf x32(ctx, x_len * sizeof(float)), y32(ctx, y_len * sizeof(float));
+      SB_CK(launch_to_f32(X, x32.as<float>(), x_len, ctx->stream));
+      SB_CK(launch_to_f32(Y, y32.as<float>(), y_len, ctx->stream));
+      ctx->note_launch(2);
+      run_tc(ctx, x32.as<float>(), y32.as<float>(), C, true);
+      return;
+    }
     std::memcpy(ctx->gemm_desc, desc, sizeof(desc));
     if (kind == THIN) {
       {
         ProfScope ps(ctx, PROF_GEMM_THIN, flops, bytes);
         SB_CK(launch_gemm_f64_skinny(X, Y, C, dc.as<GemmCBlock>(), ncb, dp.as<GemmPair>(), n, xT, yT, small_rows,
-                                     small_max, k_max, ctx->stream, persistent));
+                                     small_max, k_max, ctx->stream, persistent, long_f32));
       }
       ctx->note_launch();
       return;
@@ -367,6 +427,10 @@ struct GemmPlan {
       g.bytes = bytes;
       return g;
     }
+    if (ctx->precision != SB_PRECISION_F64) {
+      prepare_tc(ctx, g, flops, bytes);
+      return g;
+    }
     // Tile shape from the FLOP-weighted block shape (ragged launches mix
     // large and small blocks; the heavy ones decide).
     double wm = 0.0, wn = 0.0, wsum = 0.0;
@@ -430,6 +494,107 @@ struct GemmPlan {
     g.flops = flops;
     g.bytes = bytes;
     return g;
+  }
+
+  // Tensor-core launch (launch_gemm_tc).  Orientation: the side of C that
+  // goes to the 128-row tiles pads to a multiple of 128, the other side to a
+  // multiple of 16, so the launch takes the orientation with less padded work
+  // (ragged H_eff psi*L: the long side N = chi_l' * w to the 128-row tiles).
+  // Each C block is cut into 128-row A-side tiles and as few B-side tiles of
+  // at most 128 rows as cover it, of equal width rounded up to 16.  When the
+  // tiles are too few to keep every SM busy for a balanced share (fewer than
+  // four per SM; H_eff R*T3 with its long concatenated K), tiles whose k-tile
+  // count exceeds the segment length are cut into k-segments that write FP64
+  // partial tiles, summed in order by a reduction launch.  The work items are
+  // sorted by work (k-tiles times width), largest first, so that the
+  // persistent grid's stride walk gives every SM a similar share.
+  void prepare_tc(Ctx* ctx, GemmLaunch& g, double flops, double bytes) {
+    auto up = [](int64_t v, int64_t m) { return (v + m - 1) / m * m; };
+    double w_keep = 0.0, w_swap = 0.0;
+    std::vector<int64_t> kt_of(cbs.size(), 0);  // k-tiles of each C block (its pairs' K ranges concatenated)
+    for (size_t c = 0; c < cbs.size(); ++c) {
+      for (int p = cbs[c].pair_begin; p < cbs[c].pair_end; ++p) kt_of[c] += (pairs[p].K + 31) / 32;
+      w_keep += static_cast<double>(up(cbs[c].M, 128)) * up(cbs[c].N, 16) * kt_of[c];
+      w_swap += static_cast<double>(up(cbs[c].N, 128)) * up(cbs[c].M, 16) * kt_of[c];
+    }
+    const bool swap = w_swap < w_keep;
+    struct Geo { int32_t c, a0, b0, nb; };
+    std::vector<Geo> geo, zero;
+    int64_t total_kt = 0;
+    for (size_t c = 0; c < cbs.size(); ++c) {
+      const int64_t ma = swap ? cbs[c].N : cbs[c].M, nbx = swap ? cbs[c].M : cbs[c].N;
+      const int64_t nbt = (nbx + kTcMaxN - 1) / kTcMaxN, nbs = up((nbx + nbt - 1) / nbt, 16);
+      for (int64_t a0 = 0; a0 < ma; a0 += 128)
+        for (int64_t j = 0; j < nbt; ++j) {
+          const int64_t b0 = j * nbs;
+          if (b0 >= nbx) break;
+          const Geo t{static_cast<int32_t>(c), static_cast<int32_t>(a0), static_cast<int32_t>(b0),
+                      static_cast<int32_t>(std::min(nbs, up(nbx - b0, 16)))};
+          (kt_of[c] > 0 ? geo : zero).push_back(t);
+          total_kt += kt_of[c];
+        }
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    const int64_t target = 4LL * sms;
+    // segment length in k-tiles; 0 = no splitting (enough tiles already)
+    int64_t seg = 0;
+    if (static_cast<int64_t>(geo.size()) < target && total_kt > 0)
+      seg = std::max<int64_t>(ctx->tc_kc, (total_kt + target - 1) / target);
+    struct W { TcTile t; int64_t work; };
+    std::vector<W> items;
+    std::vector<TcSplit> splits;
+    int32_t nparts = 0;
+    for (const Geo& t : geo) {
+      const int64_t kt = kt_of[t.c];
+      const int64_t nseg = (seg > 0 && 4 * kt > 5 * seg) ? (kt + seg - 1) / seg : 1;
+      int p = cbs[t.c].pair_begin, k0 = 0;  // walk the k-tiles of the C block's pairs
+      if (nseg > 1) splits.push_back(TcSplit{t.c, t.a0, t.b0, t.nb, nparts, static_cast<int32_t>(nseg), 0, 0});
+      for (int64_t q = 0; q < nseg; ++q) {
+        const int64_t kb = kt * q / nseg, ke = kt * (q + 1) / nseg;
+        items.push_back(W{TcTile{t.c, t.a0, t.b0, t.nb, p, k0, static_cast<int32_t>(ke - kb),
+                                 nseg > 1 ? nparts + static_cast<int32_t>(q) : -1},
+                          (ke - kb) * t.nb});
+        for (int64_t i = kb; i < ke; ++i) {  // advance to k-tile ke
+          k0 += 32;
+          if (k0 >= pairs[p].K) {
+            ++p;
+            k0 = 0;
+          }
+        }
+      }
+      if (nseg > 1) nparts += static_cast<int32_t>(nseg);
+    }
+    std::stable_sort(items.begin(), items.end(), [](const W& a, const W& b) { return a.work > b.work; });
+    std::vector<TcTile> tiles;
+    tiles.reserve(items.size() + zero.size());
+    for (auto& w : items) tiles.push_back(w.t);
+    for (auto& t : zero) tiles.push_back(TcTile{t.c, t.a0, t.b0, t.nb, 0, 0, 0, -1});
+    require(tiles.size() < (1ULL << 31), SB_ERR_INVALID_ARG, "too many GEMM tiles in one launch");
+    g.kind = GemmLaunch::TC;
+    g.dc = upload(ctx, cbs);
+    g.dp = upload(ctx, pairs);
+    g.dt = upload(ctx, tiles);
+    g.dsplit = upload(ctx, splits);
+    g.nsplits = static_cast<int32_t>(splits.size());
+    g.nparts = nparts;
+    g.ncb = static_cast<int32_t>(cbs.size());
+    g.n = static_cast<int64_t>(tiles.size());
+    g.nz_begin = static_cast<int32_t>(items.size());
+    g.swap = swap;
+    g.passes = ctx->precision == SB_PRECISION_TF32 ? 1 : 3;
+    g.kc = ctx->tc_kc;
+    for (size_t c = 0; c < cbs.size(); ++c)
+      for (int p = cbs[c].pair_begin; p < cbs[c].pair_end; ++p) {
+        const GemmPair& q = pairs[p];
+        const int64_t M = cbs[c].M, N = cbs[c].N, K = q.K;
+        g.x_len = std::max(g.x_len, q.x_off + (g.xT ? (M - 1) * q.ldx + K : (K - 1) * q.ldx + M));
+        g.y_len = std::max(g.y_len, q.y_off + (g.yT ? (K - 1) * q.ldy + N : (N - 1) * q.ldy + K));
+      }
+    g.flops = flops;
+    g.bytes = bytes;
+    std::snprintf(g.desc, sizeof(g.desc), "tcgen05 %s 128xN%s items:%lld split:%d", g.passes == 3 ? "3xtf32" : "tf32",
+                  swap ? " swapped" : "", static_cast<long long>(g.n), g.nsplits);
   }
 
   // Thin launches (K <= 16): output blocks whose pairs read the same block of
@@ -1006,7 +1171,7 @@ struct CropScratchMap {
 // FLOPs) when the cropped work is at most 0.8 of the padded work; never while
 // a capture is open (the scan reads extents back to the host).
 bool shared_bb_cropped(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Labels& shared) {
-  if (ctx->auto_crop <= 0 || ctx->capturing) return false;
+  if (ctx->auto_crop <= 0 || ctx->capturing || C.f32 || A0->f32 || B0->f32) return false;
   const Tensor& TA = *A0;
   const Tensor& TB = *B0;
   if (TA.ragged || TB.ragged || C.kind != BS || TA.nkeys == 0 || TB.nkeys == 0 || TA.n2 == 0 || TB.n2 == 0 ||
@@ -1121,6 +1286,8 @@ void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0
     if (!ctx->plan_cache) ctx->plan_cache = std::make_shared<SharedPlanCache>();
     cache = static_cast<SharedPlanCache*>(ctx->plan_cache.get());
     sig = shared_signature(C, lC, A0, B0);
+    sig.push_back(static_cast<uint64_t>(ctx->precision));
+    sig.push_back((C.f32 ? 1u : 0u) | (A0->f32 ? 2u : 0u) | (B0->f32 ? 4u : 0u));
     for (auto it = cache->entries.rbegin(); it != cache->entries.rend(); ++it) {
       const SharedPlanEntry& e = **it;
       if (e.sig != sig || e.akeys != A0->keys || e.bkeys != B0->keys || e.abd != A0->bdims || e.bbd != B0->bdims)
@@ -1134,8 +1301,8 @@ void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0
         C.bdims = e.c_bdims;
         C.boff = e.c_boff;
       }
-      if (sp.mode == Mode::AthenB) e.gemm.run(ctx, A->payload(), B->payload(), C.data.d());
-      else e.gemm.run(ctx, B->payload(), A->payload(), C.data.d());
+      if (sp.mode == Mode::AthenB) e.gemm.run_io(ctx, *A, *B, C);
+      else e.gemm.run_io(ctx, *B, *A, C);
       ctx->plan_cache_hit = true;
       return;
     }
@@ -1230,8 +1397,8 @@ void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0
     }
   }
   GemmLaunch g = athenb ? gp.prepare(ctx, false, false) : gp.prepare(ctx, true, true);
-  if (athenb) g.run(ctx, A->payload(), B->payload(), C.data.d());
-  else g.run(ctx, B->payload(), A->payload(), C.data.d());
+  if (athenb) g.run_io(ctx, *A, *B, C);
+  else g.run_io(ctx, *B, *A, C);
   if (cache) {
     auto e = std::make_unique<SharedPlanEntry>();
     e->sig = std::move(sig);
@@ -2221,6 +2388,8 @@ void contract(Ctx* ctx, Tensor& C, const Labels& lC, const Tensor& A, const Labe
   Op oA = view(A, lA), oB = view(B, lB);
   if (C.kind == DENSE) {
     // contract_bs_bs_to_dense! (contract_bs_bs.jl:736-754): P_C = 0 sink.
+    require_f64(A, "contract_bs_bs_to_dense!");
+    require_f64(B, "contract_bs_bs_to_dense!");
     require(A.kind == BS && B.kind == BS, SB_ERR_UNSUPPORTED_TYPES, "dense C needs block-sparse A and B");
     require_uniform(A.ragged ? A : B, "contract_bs_bs_to_dense!");
     auto sink = make_tensor(ctx, BS, C.dims, C.N());
@@ -2239,6 +2408,9 @@ void contract(Ctx* ctx, Tensor& C, const Labels& lC, const Tensor& A, const Labe
   for (auto& l : shared)
     if (!has(lC, l)) reduced.push_back(l);
   if (reduced.size() == 1) {
+    require_f64(C, "single-label contract!");
+    require_f64(A, "single-label contract!");
+    require_f64(B, "single-label contract!");
     require(shared.size() == 1, SB_ERR_ASSERTION, "Expected exactly 1 shared label");
     const Label r = reduced[0];
     require(A.dims[find(lA, r)] == B.dims[find(lB, r)], SB_ERR_DIM_MISMATCH, "Dim mismatch on shared label " + lab_str(r));
@@ -2272,6 +2444,9 @@ void contract(Ctx* ctx, Tensor& C, const Labels& lC, const Tensor& A, const Labe
   }
   const Kind c = C.kind, a = A.kind, b = B.kind;
   if (c == BS && a == BS && b == BS) return shared_bb(ctx, C, lC, oA, oB, shared);
+  require_f64(C, "contract_shared!");
+  require_f64(A, "contract_shared!");
+  require_f64(B, "contract_shared!");
   if (ragged_in) require_uniform(A.ragged ? A : B, "contract_shared!");
   if (c == BS && a == BS && b == DENSE) return shared_bd(ctx, C, lC, oA, oB, shared);
   if (c == ALIASED && a == ALIASED && (b == DENSE || b == ALIASED)) return shared_aliased(ctx, C, lC, oA, oB, shared);

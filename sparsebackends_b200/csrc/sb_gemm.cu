@@ -19,6 +19,11 @@ __device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool
   int bytes = valid ? 8 : 0;
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
 }
+__device__ __forceinline__ void cp_async4(float* smem, const float* gmem, bool valid) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  int bytes = valid ? 4 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -597,13 +602,15 @@ __global__ void __launch_bounds__(kThinThreads, 5)
 // runs across tile boundaries, so the first pair of the next strip is in
 // flight while the current one finishes; C is stored straight from the DMMA
 // fragments (runs of 8 consecutive doubles per column).
-template <bool SR, bool XT, bool YT>
+// LF: the long operand and C hold FP32 values (staged as FP32, widened to FP64
+// when read into the DMMA fragments; C rounded to FP32 when stored).
+template <bool SR, bool XT, bool YT, bool LF = false>
 __global__ void __launch_bounds__(kThinThreads, 5)
     k_gemm_thin_p(const double* __restrict__ X, const double* __restrict__ Y, double* __restrict__ C,
                   const GemmCBlock* __restrict__ cblocks, int32_t ncb, const GemmPair* __restrict__ pairs,
                   int32_t ntiles) {
   using TL = ThinLayout<SR, XT, YT>;
-  __shared__ double Ls[2][TL::LSZ];
+  __shared__ double Ls[2][TL::LSZ];  // FP32 long tiles use the first half of each stage
   __shared__ double Ss[2][TL::SSZ];
   const int tid = threadIdx.x;
   const int tq = tid & 15, tr = tid >> 4;
@@ -635,26 +642,48 @@ __global__ void __launch_bounds__(kThinThreads, 5)
     const int K = pr.K;
     const int L = SR ? cb.N : cb.M, ns = SR ? cb.M : cb.N;
     const int lleft = L - l0;
-    const double* lbase = SR ? Y + pr.y_off : X + pr.x_off;
     const double* sbase = SR ? X + pr.x_off : Y + pr.y_off;
     const int64_t lld = SR ? pr.ldy : pr.ldx;
     const int64_t sld = SR ? pr.ldx : pr.ldy;
     constexpr int LR = kThinBig * 16 / kThinThreads;
-    if (TL::LONG_KCONTIG) {
-      const double* lp = lbase + tq + static_cast<int64_t>(l0 + tr) * lld;
-      double* dst = &Ls[stage][tr * kThinKP + tq];
+    if (LF) {
+      const float* lbase = reinterpret_cast<const float*>(SR ? Y : X) + (SR ? pr.y_off : pr.x_off);
+      float* lsf = reinterpret_cast<float*>(&Ls[stage][0]);
+      if (TL::LONG_KCONTIG) {
+        const float* lp = lbase + tq + static_cast<int64_t>(l0 + tr) * lld;
+        float* dst = lsf + tr * kThinKP + tq;
 #pragma unroll
-      for (int r = 0; r < LR; ++r) {
-        const bool v = tr + 8 * r < lleft && tq < K;
-        cp_async8(dst + r * 8 * kThinKP, v ? lp + static_cast<int64_t>(8 * r) * lld : lbase, v);
+        for (int r = 0; r < LR; ++r) {
+          const bool v = tr + 8 * r < lleft && tq < K;
+          cp_async4(dst + r * 8 * kThinKP, v ? lp + static_cast<int64_t>(8 * r) * lld : lbase, v);
+        }
+      } else {
+        const float* lp = lbase + l0 + tid;
+        float* dst = lsf + tid;
+#pragma unroll
+        for (int r = 0; r < LR; ++r) {
+          const bool v = tid < lleft && r < K;
+          cp_async4(dst + r * kThinBP, v ? lp + static_cast<int64_t>(r) * lld : lbase, v);
+        }
       }
     } else {
-      const double* lp = lbase + l0 + tid;
-      double* dst = &Ls[stage][tid];
+      const double* lbase = SR ? Y + pr.y_off : X + pr.x_off;
+      if (TL::LONG_KCONTIG) {
+        const double* lp = lbase + tq + static_cast<int64_t>(l0 + tr) * lld;
+        double* dst = &Ls[stage][tr * kThinKP + tq];
 #pragma unroll
-      for (int r = 0; r < LR; ++r) {
-        const bool v = tid < lleft && r < K;
-        cp_async8(dst + r * kThinBP, v ? lp + static_cast<int64_t>(r) * lld : lbase, v);
+        for (int r = 0; r < LR; ++r) {
+          const bool v = tr + 8 * r < lleft && tq < K;
+          cp_async8(dst + r * 8 * kThinKP, v ? lp + static_cast<int64_t>(8 * r) * lld : lbase, v);
+        }
+      } else {
+        const double* lp = lbase + l0 + tid;
+        double* dst = &Ls[stage][tid];
+#pragma unroll
+        for (int r = 0; r < LR; ++r) {
+          const bool v = tid < lleft && r < K;
+          cp_async8(dst + r * kThinBP, v ? lp + static_cast<int64_t>(r) * lld : lbase, v);
+        }
       }
     }
     const double* sp = sbase + tq + static_cast<int64_t>(tr) * sld;
@@ -691,6 +720,10 @@ __global__ void __launch_bounds__(kThinThreads, 5)
 
   const int warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t = lane & 3;
+  auto lval = [&](const double* ls, int idx) -> double {
+    if (LF) return static_cast<double>(reinterpret_cast<const float*>(ls)[idx]);
+    return ls[idx];
+  };
   double acc[8][2];
 #pragma unroll
   for (int a = 0; a < 8; ++a) acc[a][0] = acc[a][1] = 0.0;
@@ -713,7 +746,7 @@ __global__ void __launch_bounds__(kThinThreads, 5)
       if (!SR) {
         double af[4], bf[2];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) af[a] = ls[TL::lidx(warp * 32 + a * 8 + g, k4 + t)];
+        for (int a = 0; a < 4; ++a) af[a] = lval(ls, TL::lidx(warp * 32 + a * 8 + g, k4 + t));
 #pragma unroll
         for (int b = 0; b < 2; ++b) bf[b] = ss[TL::sidx(k4 + t, b * 8 + g)];
 #pragma unroll
@@ -725,7 +758,7 @@ __global__ void __launch_bounds__(kThinThreads, 5)
 #pragma unroll
         for (int a = 0; a < 2; ++a) af[a] = ss[TL::sidx(k4 + t, a * 8 + g)];
 #pragma unroll
-        for (int b = 0; b < 4; ++b) bf[b] = ls[TL::lidx(warp * 32 + b * 8 + g, k4 + t)];
+        for (int b = 0; b < 4; ++b) bf[b] = lval(ls, TL::lidx(warp * 32 + b * 8 + g, k4 + t));
 #pragma unroll
         for (int a = 0; a < 2; ++a)
 #pragma unroll
@@ -737,7 +770,10 @@ __global__ void __launch_bounds__(kThinThreads, 5)
       // last pair of this strip: store it from the fragments and start over
       const int M = ccb.M;
       const int64_t ldc = ccb.ldc;
-      double* cbase = C + ccb.c_off;
+      auto cstore = [&](int64_t off, double v) {
+        if (LF) reinterpret_cast<float*>(C)[ccb.c_off + off] = static_cast<float>(v);
+        else C[ccb.c_off + off] = v;
+      };
       if (!SR) {
         const int L = M, ns = ccb.N;
 #pragma unroll
@@ -746,8 +782,8 @@ __global__ void __launch_bounds__(kThinThreads, 5)
 #pragma unroll
           for (int b = 0; b < 2; ++b) {
             const int s0 = b * 8 + 2 * t;
-            if (l < L && s0 < ns) cbase[l + s0 * ldc] = acc[a * 2 + b][0];
-            if (l < L && s0 + 1 < ns) cbase[l + (s0 + 1) * ldc] = acc[a * 2 + b][1];
+            if (l < L && s0 < ns) cstore(l + s0 * ldc, acc[a * 2 + b][0]);
+            if (l < L && s0 + 1 < ns) cstore(l + (s0 + 1) * ldc, acc[a * 2 + b][1]);
           }
         }
       } else {
@@ -758,8 +794,8 @@ __global__ void __launch_bounds__(kThinThreads, 5)
 #pragma unroll
           for (int b = 0; b < 4; ++b) {
             const int l = cl0 + warp * 32 + b * 8 + 2 * t;
-            if (sI < ns && l < L) cbase[sI + l * ldc] = acc[a * 4 + b][0];
-            if (sI < ns && l + 1 < L) cbase[sI + (l + 1) * ldc] = acc[a * 4 + b][1];
+            if (sI < ns && l < L) cstore(sI + l * ldc, acc[a * 4 + b][0]);
+            if (sI < ns && l + 1 < L) cstore(sI + (l + 1) * ldc, acc[a * 4 + b][1]);
           }
         }
       }
@@ -778,7 +814,7 @@ __global__ void __launch_bounds__(kThinThreads, 5)
 // The persistent grid: every SM's resident CTAs of this instantiation (5 for
 // the 38 KB shared-memory layouts, 4 for the 45 KB ones), queried once per
 // device.
-template <bool SR, bool XT, bool YT>
+template <bool SR, bool XT, bool YT, bool LF = false>
 cudaError_t launch_thin_p(const double* X, const double* Y, double* C, const GemmCBlock* cb, int32_t ncb,
                           const GemmPair* pr, int64_t nctas, cudaStream_t s) {
   static int grid_of[64] = {};
@@ -790,18 +826,25 @@ cudaError_t launch_thin_p(const double* X, const double* Y, double* C, const Gem
     int sms = 0, per_sm = 0;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gemm_thin_p<SR, XT, YT>, kThinThreads, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gemm_thin_p<SR, XT, YT, LF>, kThinThreads, 0);
     if (e != cudaSuccess) return e;
     grid = sms * std::max(per_sm, 1);
   }
   const unsigned g = static_cast<unsigned>(std::min<int64_t>(nctas, grid));
-  k_gemm_thin_p<SR, XT, YT><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr, static_cast<int32_t>(nctas));
+  k_gemm_thin_p<SR, XT, YT, LF><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr, static_cast<int32_t>(nctas));
   return cudaGetLastError();
 }
 
 template <bool SR>
 cudaError_t thin_t(bool xT, bool yT, const double* X, const double* Y, double* C, const GemmCBlock* cb, int32_t ncb,
-                   const GemmPair* pr, int64_t nctas, bool persistent, cudaStream_t s) {
+                   const GemmPair* pr, int64_t nctas, bool persistent, cudaStream_t s, bool lf) {
+  if (lf) {
+    if (!persistent) return cudaErrorInvalidValue;
+    if (!xT && !yT) return launch_thin_p<SR, false, false, true>(X, Y, C, cb, ncb, pr, nctas, s);
+    if (!xT && yT) return launch_thin_p<SR, false, true, true>(X, Y, C, cb, ncb, pr, nctas, s);
+    if (xT && !yT) return launch_thin_p<SR, true, false, true>(X, Y, C, cb, ncb, pr, nctas, s);
+    return launch_thin_p<SR, true, true, true>(X, Y, C, cb, ncb, pr, nctas, s);
+  }
   if (persistent) {
     if (!xT && !yT) return launch_thin_p<SR, false, false>(X, Y, C, cb, ncb, pr, nctas, s);
     if (!xT && yT) return launch_thin_p<SR, false, true>(X, Y, C, cb, ncb, pr, nctas, s);
@@ -831,11 +874,12 @@ void gemm_tile_dims(GemmShape shape, int* bm, int* bn) {
 
 cudaError_t launch_gemm_f64_skinny(const double* X, const double* Y, double* C, const GemmCBlock* d_cblocks,
                                    int32_t ncb, const GemmPair* d_pairs, int64_t nctas, bool xT, bool yT,
-                                   bool small_rows, int small_max, int k_max, cudaStream_t s, bool persistent) {
+                                   bool small_rows, int small_max, int k_max, cudaStream_t s, bool persistent,
+                                   bool long_f32) {
   if (nctas <= 0) return cudaSuccess;
   if (nctas > 0x7fffffffLL || small_max > 16 || k_max > 16) return cudaErrorInvalidValue;
-  return small_rows ? thin_t<true>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, persistent, s)
-                    : thin_t<false>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, persistent, s);
+  return small_rows ? thin_t<true>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, persistent, s, long_f32)
+                    : thin_t<false>(xT, yT, X, Y, C, d_cblocks, ncb, d_pairs, nctas, persistent, s, long_f32);
 }
 
 template <bool XT, bool YT>

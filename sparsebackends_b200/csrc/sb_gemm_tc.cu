@@ -1,0 +1,600 @@
+// Grouped block GEMM on the fifth-generation tensor cores (tcgen05): the
+// 3xTF32 split form and single-pass TF32, with FP32 operands and an FP32 or
+// FP64 result.
+//
+// Same plan as the FP64 DMMA kernels (GemmCBlock / GemmPair: for every C block
+// C_c = sum over its pairs of X_p * Y_p).  Every FP32 operand value is split
+// on its way into shared memory:  x = hi + lo  with  hi = tf32(x) and
+// lo = tf32(x - hi),  and each product is  a_hi*b_lo + a_lo*b_hi + a_hi*b_hi
+// (the lo*lo term is below FP32 rounding); single-pass TF32 keeps hi*hi.
+// FP64 operands are given to this kernel as FP32 copies (the host keeps them
+// per tensor), which keeps 24 of their bits, more than the 22 the split uses.
+//
+// Roles.  tcgen05.mma computes D[m, n] = sum_k A[m, k] * B[n, k] with M = 128
+// rows of A (TMEM lanes) and N <= 128 rows of B (TMEM columns).  A tile is
+// (C block, 128 rows on the A side, nb rows on the B side).  Without SWAP the
+// A side is X (rows i of C) and the B side is Y^T (columns j of C); with SWAP
+// the roles exchange.
+//
+// Pipeline of one k-tile (32 deep): all 256 threads hold the FP32 elements
+// of the k-tile two ahead in registers (loads in flight across two k-tiles of
+// tensor-core work), split the current one and store 16-byte chunks into
+// K-major 128-byte-swizzled images (the canonical SWIZZLE_128B K-major operand
+// layout: row r of an 8-row group at r*128 bytes, 16-byte chunk c at position
+// c ^ r), in one of three stages.  After a proxy fence and a CTA barrier one
+// thread issues the MMAs of the k-tile and commits them to the stage's
+// mbarrier, which the threads wait on before they overwrite that stage.
+//
+// Accumulation.  The tensor core accumulates in FP32 and its error grows with
+// the number of accumulation steps (measured: ~9e-5 relative over 17 000
+// terms).  The k-tiles of a tile are therefore cut into chunks of kc k-tiles;
+// each chunk accumulates from zero in one of two TMEM accumulators (the next
+// chunk runs in the other one), and the threads fold a finished chunk into a
+// Kahan pair (sum, compensation) also kept in TMEM: 4 x 128 columns in all.
+// A tile of one chunk is written straight from its accumulator.
+//
+// Every mbarrier wait is bounded (about two seconds of %globaltimer); a wait
+// that runs out sets *status = 1, and the CTA stops issuing MMAs and waiting,
+// so the kernel always returns and the host reports SB_ERR_TIMEOUT.
+#include <algorithm>
+#include <cstdio>
+
+#include "sb_kernels.hpp"
+
+namespace sb {
+namespace {
+
+constexpr int kTcThreads = 256;
+constexpr int kTcBK = 32;                 // k-tile: 32 TF32 values = one 128-byte swizzle row
+constexpr int kTcStages = 3;
+constexpr int kTcImg = 128 * 128;         // bytes of one plane image (128 rows x 128 B)
+constexpr int kTcStageBytes = 4 * kTcImg;  // hi and lo planes of A and B
+constexpr int kTcEpiBytes = 8 * 32 * 32 * 4;   // per-warp 32 x 32 FP32 transpose buffers of the epilogue
+constexpr int kTcSmemBytes = kTcStages * kTcStageBytes + kTcEpiBytes + 1024 /*alignment*/ + 256 /*barriers*/;
+constexpr int kTcTmemCols = 512;          // acc0, acc1, Kahan sum, Kahan compensation
+constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of every mbarrier wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for the completion of phase `parity` of the mbarrier.  Returns
+// false (and records the failure) when the bound runs out.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* status) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (true) {
+    if (mbar_try(bar, parity)) return true;
+    if (global_ns() - t0 > kWaitNs) {
+      atomicExch(status, 1);
+      return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory matrix descriptor of a K-major SWIZZLE_128B operand image:
+// start address >> 4, leading-byte offset 16 (unused by swizzled K-major
+// layouts), stride-byte offset 1024 (8 rows of 128 bytes), descriptor version
+// 1, layout type 2 (128-byte swizzle).  Advancing along K inside the 128-byte
+// row adds the byte offset to the start address.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  return static_cast<uint64_t>((addr & 0x3FFFFu) >> 4) | (1ull << 16) | (64ull << 32) | (1ull << 46) |
+         (2ull << 61);
+}
+
+// Instruction descriptor of kind::tf32, FP32 accumulator, both operands
+// K-major, M = 128, N = n (multiple of 16, 16..256).
+__device__ __forceinline__ uint32_t idesc_tf32(int n) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(n >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, bool accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate ? 1u : 0u));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+      "%14, %15, %16};" ::"r"(taddr),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+      "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+      "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+      "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+      "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+      "r"(__float_as_uint(v[15])));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// x = hi + lo with both parts exactly representable in TF32 (low 13 mantissa
+// bits zero).
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+  uint32_t h, l;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(x - __uint_as_float(h)));
+  hi = h;
+  lo = l;
+}
+
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
+}
+
+// Byte offset of the 16-byte chunk c (k = 4c..4c+3) of row r in a K-major
+// SWIZZLE_128B image.
+__device__ __forceinline__ uint32_t img_off(int r, int c) {
+  return static_cast<uint32_t>((r >> 3) * 1024 + (r & 7) * 128 + ((c ^ (r & 7)) << 4));
+}
+
+// Operand tile of 128 rows x 32 k: four chunks of four k values per thread.
+// K-contiguous sources (element (r, k) at r*ld + k): a warp covers 4 rows x 8
+// chunks; row-contiguous sources (at r + k*ld): a warp covers 32 consecutive
+// rows of one chunk, so each of its four loads reads 128 contiguous bytes.
+constexpr int kCH = 4;
+template <bool KC>
+__device__ __forceinline__ int map_row(int tid, int it) { return KC ? (tid >> 3) + 32 * it : tid & 127; }
+template <bool KC>
+__device__ __forceinline__ int map_chunk(int tid, int it) { return KC ? (tid & 7) : (tid >> 7) + 2 * it; }
+
+// Loads one k-tile of an operand: rows [0, rows) of the tile (the rest are
+// zero), k in [0, kv) from src (zero past kv).
+template <bool KC>
+__device__ __forceinline__ void load_tile(float (&r)[kCH][4], const float* __restrict__ src, int64_t ld, int rows,
+                                          int kv, int tid) {
+#pragma unroll
+  for (int it = 0; it < kCH; ++it) {
+    const int row = map_row<KC>(tid, it), c = map_chunk<KC>(tid, it);
+    const bool rv = row < rows;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = 4 * c + j;
+      const float* p = KC ? src + static_cast<int64_t>(row) * ld + k : src + row + static_cast<int64_t>(k) * ld;
+      r[it][j] = (rv && k < kv) ? __ldg(p) : 0.0f;
+    }
+  }
+}
+
+template <bool KC>
+__device__ __forceinline__ void store_tile(const float (&r)[kCH][4], uint32_t s_hi, uint32_t s_lo, bool split,
+                                           int tid) {
+#pragma unroll
+  for (int it = 0; it < kCH; ++it) {
+    const uint32_t off = img_off(map_row<KC>(tid, it), map_chunk<KC>(tid, it));
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) split_tf32(r[it][j], h[j], l[j]);
+    st_shared_v4(s_hi + off, h[0], h[1], h[2], h[3]);
+    if (split) st_shared_v4(s_lo + off, l[0], l[1], l[2], l[3]);
+  }
+}
+
+// Position of a k-tile: work item t (into the tile list), pair p of its C
+// block, k offset k0 inside the pair, k-tile index kt inside the item.
+struct Cursor {
+  int t, p, k0, kt;
+};
+
+// A finished chunk waiting to be folded or written.
+struct Chunk {
+  int t;          // tile
+  uint32_t cg;    // chunk counter of this CTA (accumulator cg & 1)
+  bool first;     // first chunk of its tile
+  bool last;      // last chunk of its tile
+};
+
+template <bool SWAP, bool A_KC, bool B_KC, bool OUT64>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_gemm_tc(const float* __restrict__ X, const float* __restrict__ Y, void* __restrict__ Cv,
+              const GemmCBlock* __restrict__ cblocks, const GemmPair* __restrict__ pairs,
+              const TcTile* __restrict__ tiles, int32_t ntiles, int32_t nz_begin, int32_t passes, int32_t kc,
+              double* __restrict__ partial, int* __restrict__ status) {
+  extern __shared__ unsigned char smem_raw[];
+  const int tid = static_cast<int>(threadIdx.x);
+  const int warp = tid >> 5, lane = tid & 31;
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;  // 1024-aligned swizzle atoms
+  float* const epi = reinterpret_cast<float*>(smem_raw + (base - raw) + kTcStages * kTcStageBytes) + warp * 1024;
+  const uint32_t bars = base + kTcStages * kTcStageBytes + kTcEpiBytes;
+  const uint32_t bar_empty0 = bars;                 // kTcStages barriers, 8 bytes apart
+  const uint32_t bar_acc0 = bars + 8 * kTcStages;   // two barriers (accumulators 0 and 1)
+  const uint32_t tmem_slot = bars + 64;
+  unsigned char* const tmem_slot_ptr = smem_raw + (tmem_slot - raw);
+  const bool split = passes == 3;
+
+  if (tid == 0) {
+    for (int s = 0; s < kTcStages; ++s) mbar_init(bar_empty0 + 8 * s, 1);
+    mbar_init(bar_acc0, 1);
+    mbar_init(bar_acc0 + 8, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tmem_slot),
+                 "r"(kTcTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(tmem_slot_ptr);
+  const uint32_t t_sum = tmem + 256, t_comp = tmem + 384;
+
+  bool failed = false;  // a bounded wait ran out: stop issuing and waiting
+
+  float ra0[kCH][4], rb0[kCH][4], ra1[kCH][4], rb1[kCH][4];
+
+  auto load = [&](const Cursor& c, float (&ra)[kCH][4], float (&rb)[kCH][4]) {
+    const TcTile tl = tiles[c.t];
+    const GemmCBlock cb = cblocks[tl.cb];
+    const GemmPair pr = pairs[c.p];
+    const int ma = SWAP ? cb.N : cb.M, nbv = SWAP ? cb.M : cb.N;
+    const int kv = min(kTcBK, pr.K - c.k0);
+    // A side: row a0 of the tile at k0; B side: row b0
+    const float* xa = X + pr.x_off;
+    const float* ya = Y + pr.y_off;
+    const int64_t lda = SWAP ? pr.ldy : pr.ldx, ldb = SWAP ? pr.ldx : pr.ldy;
+    const float* pa = SWAP ? ya : xa;
+    const float* pb = SWAP ? xa : ya;
+    pa += A_KC ? static_cast<int64_t>(tl.a0) * lda + c.k0 : tl.a0 + static_cast<int64_t>(c.k0) * lda;
+    pb += B_KC ? static_cast<int64_t>(tl.b0) * ldb + c.k0 : tl.b0 + static_cast<int64_t>(c.k0) * ldb;
+    load_tile<A_KC>(ra, pa, lda, min(128, ma - tl.a0), kv, tid);
+    load_tile<B_KC>(rb, pb, ldb, min(tl.nb, nbv - tl.b0), kv, tid);
+  };
+  // next k-tile after c (same pair, next pair of the tile, or the first pair
+  // of this CTA's next tile); t >= nz_begin marks the end
+  auto first_of = [&](int t) -> Cursor {
+    if (t >= nz_begin) return Cursor{t, 0, 0, 0};
+    const TcTile tl = tiles[t];
+    return Cursor{t, tl.p0, tl.k0, 0};
+  };
+  auto advance = [&](Cursor c) -> Cursor {
+    if (c.t >= nz_begin) return c;
+    if (c.kt + 1 >= tiles[c.t].nkt) return first_of(c.t + static_cast<int>(gridDim.x));
+    if (c.k0 + kTcBK < pairs[c.p].K) return Cursor{c.t, c.p, c.k0 + kTcBK, c.kt + 1};
+    return Cursor{c.t, c.p + 1, 0, c.kt + 1};
+  };
+
+  // Fold a finished chunk into the Kahan pair, or write the item: into C, or
+  // (a k-segment of a split tile) into its FP64 partial tile, column-major
+  // 128 x 128, for k_tc_reduce.
+  const int sub = warp & 3, half = warp >> 2;
+  auto finish_chunk = [&](const Chunk& ch) {
+    if (!failed) failed = !mbar_wait(bar_acc0 + 8 * (ch.cg & 1), (ch.cg >> 1) & 1, status);
+    tc_fence_after();
+    const TcTile tl = tiles[ch.t];
+    const GemmCBlock cb = cblocks[tl.cb];
+    const uint32_t lanes = static_cast<uint32_t>(32 * sub) << 16;
+    const uint32_t acc = tmem + 128 * (ch.cg & 1);
+    const int ma = SWAP ? cb.N : cb.M, nbv = SWAP ? cb.M : cb.N;
+    const int arow0 = tl.a0 + 32 * sub;        // first A-side row of this warp
+    const int arow = arow0 + lane;             // A-side row of this thread
+    const int rows_ok = min(32, ma - arow0);   // valid rows of this warp (may be <= 0)
+    for (int col0 = 64 * half; col0 < 64 * half + 64 && col0 < tl.nb; col0 += 32) {
+      const int nh = col0 + 16 < tl.nb ? 2 : 1;  // 16-column halves inside nb (warp-uniform)
+      for (int h = 0; h < nh; ++h) {
+        const int cc = col0 + 16 * h;
+        float v[16], sm[16], cm[16];
+        tmem_ld16(acc + lanes + cc, v);
+        if (!ch.first) {
+          tmem_ld16(t_sum + lanes + cc, sm);
+          tmem_ld16(t_comp + lanes + cc, cm);
+        }
+        tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          if (ch.first) {
+            sm[j] = v[j];
+            cm[j] = 0.0f;
+          } else {  // Kahan: s + v, lost low part kept (negated) in c
+            const float y = v[j] - cm[j];
+            const float t = sm[j] + y;
+            cm[j] = (t - sm[j]) - y;
+            sm[j] = t;
+          }
+        }
+        if (!ch.last) {
+          tmem_st16(t_sum + lanes + cc, sm);
+          tmem_st16(t_comp + lanes + cc, cm);
+          continue;
+        }
+        if (failed || rows_ok <= 0) continue;
+        if (tl.part >= 0) {
+          // partial tile (column-major 128 x 128): lanes write consecutive rows
+          double* pt = partial + static_cast<int64_t>(tl.part) * (128 * 128) + 32 * sub + lane;
+          if (lane < rows_ok)
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+              pt[(cc + j) * 128] = static_cast<double>(sm[j]) - static_cast<double>(cm[j]);
+          continue;
+        }
+        if (!SWAP) {
+          // C(i = arow, j = bcol) at arow + bcol * ldc: lanes write consecutive rows
+          if (lane < rows_ok)
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const int bcol = tl.b0 + cc + j;
+              if (bcol >= nbv) break;
+              const int64_t off = cb.c_off + arow + static_cast<int64_t>(bcol) * cb.ldc;
+              if (OUT64) static_cast<double*>(Cv)[off] = static_cast<double>(sm[j]) - static_cast<double>(cm[j]);
+              else static_cast<float*>(Cv)[off] = sm[j] - cm[j];
+            }
+          continue;
+        }
+        // SWAP: stage the warp's 32 rows x 16 columns in its shared buffer
+        // (XOR-swizzled: no bank conflicts either way) for the transposed store
+#pragma unroll
+        for (int j = 0; j < 16; ++j) epi[lane * 32 + ((16 * h + j) ^ lane)] = sm[j] - cm[j];
+      }
+      if (!SWAP || !ch.last || tl.part >= 0) continue;
+      // C(i = bcol, j = arow) at bcol + arow * ldc: lanes write consecutive
+      // columns of one row
+      __syncwarp();
+      if (!failed && rows_ok > 0) {
+        const int bcol = tl.b0 + col0 + lane;
+        const bool col_ok = bcol < nbv && lane < 16 * nh;
+        for (int r = 0; r < rows_ok; ++r) {
+          const float val = epi[r * 32 + (lane ^ r)];
+          if (!col_ok) continue;
+          const int64_t off = cb.c_off + bcol + static_cast<int64_t>(arow0 + r) * cb.ldc;
+          if (OUT64) static_cast<double*>(Cv)[off] = static_cast<double>(val);
+          else static_cast<float*>(Cv)[off] = val;
+        }
+      }
+      __syncwarp();
+    }
+    if (!ch.last) tmem_wait_st();
+    tc_fence_before();
+  };
+
+  Cursor cur = first_of(static_cast<int>(blockIdx.x));
+  Cursor nxt = advance(cur);   // k-tile held in the second register set
+  if (cur.t < nz_begin) load(cur, ra0, rb0);
+  if (nxt.t < nz_begin) load(nxt, ra1, rb1);
+
+  uint32_t g = 0;    // k-tiles staged by this CTA so far
+  uint32_t cg = 0;   // chunks started by this CTA so far
+  Chunk pending{0, 0, false, false};
+  bool has_pending = false;
+  int chunk_first_kt = 0;  // kt at which the current chunk started
+
+  // One k-tile: stage the registers of cursor c, prefetch two ahead into the
+  // same registers, issue the MMAs, fold a pending chunk.
+  auto step = [&](const Cursor& c, float (&ra)[kCH][4], float (&rb)[kCH][4], const Cursor& ahead2) {
+    const int s = static_cast<int>(g % kTcStages);
+    if (g >= kTcStages && !failed) failed = !mbar_wait(bar_empty0 + 8 * s, ((g / kTcStages) - 1) & 1, status);
+    const uint32_t sa_hi = base + s * kTcStageBytes, sa_lo = sa_hi + kTcImg;
+    const uint32_t sb_hi = sa_hi + 2 * kTcImg, sb_lo = sb_hi + kTcImg;
+    store_tile<A_KC>(ra, sa_hi, sa_lo, split, tid);
+    store_tile<B_KC>(rb, sb_hi, sb_lo, split, tid);
+    fence_proxy_async();
+    if (ahead2.t < nz_begin) load(ahead2, ra, rb);  // in flight during the next two k-tiles
+    __syncthreads();
+    const Cursor n1 = advance(c);
+    const bool tile_last = n1.t != c.t;
+    if (c.kt == 0) chunk_first_kt = 0;
+    const bool chunk_first = c.kt == chunk_first_kt;
+    const bool chunk_last = tile_last || (c.kt + 1 - chunk_first_kt) == kc;
+    const TcTile tl = tiles[c.t];
+    const uint32_t acc = tmem + 128 * (cg & 1);
+    if (tid == 0 && !failed) {
+      tc_fence_after();
+      const uint32_t idesc = idesc_tf32(tl.nb);
+#pragma unroll
+      for (int kk = 0; kk < kTcBK / 8; ++kk) {
+        const uint64_t ah = smem_desc(sa_hi + 32 * kk), bh = smem_desc(sb_hi + 32 * kk);
+        bool accum = !(chunk_first && kk == 0);
+        if (split) {
+          mma_tf32(acc, ah, smem_desc(sb_lo + 32 * kk), idesc, accum);
+          mma_tf32(acc, smem_desc(sa_lo + 32 * kk), bh, idesc, true);
+          accum = true;
+        }
+        mma_tf32(acc, ah, bh, idesc, accum);
+      }
+      mma_commit(bar_empty0 + 8 * s);
+      if (chunk_last) mma_commit(bar_acc0 + 8 * (cg & 1));
+    }
+    ++g;
+    if (has_pending) {  // the tensor core now works on the other accumulator
+      finish_chunk(pending);
+      has_pending = false;
+    }
+    if (chunk_last) {
+      pending = Chunk{c.t, cg, chunk_first_kt == 0, tile_last};
+      has_pending = true;
+      ++cg;
+      chunk_first_kt = c.kt + 1;
+    }
+  };
+
+  while (cur.t < nz_begin) {
+    const Cursor n2 = advance(nxt);
+    step(cur, ra0, rb0, n2);
+    cur = nxt;
+    nxt = n2;
+    if (cur.t >= nz_begin) break;
+    const Cursor n3 = advance(nxt);
+    step(cur, ra1, rb1, n3);
+    cur = nxt;
+    nxt = n3;
+  }
+  if (has_pending) finish_chunk(pending);
+
+  // C blocks without pairs (tiles [nz_begin, ntiles)): zeros
+  for (int t = nz_begin + static_cast<int>(blockIdx.x); t < ntiles; t += static_cast<int>(gridDim.x)) {
+    const TcTile tl = tiles[t];
+    const GemmCBlock cb = cblocks[tl.cb];
+    const int ma = SWAP ? cb.N : cb.M, nbv = SWAP ? cb.M : cb.N;
+    const int rows = min(128, ma - tl.a0), cols = min(tl.nb, nbv - tl.b0);
+    for (int e = tid; e < rows * cols; e += kTcThreads) {
+      const int r = tl.a0 + e % rows, c = tl.b0 + e / rows;
+      const int64_t off = cb.c_off + (SWAP ? c + static_cast<int64_t>(r) * cb.ldc : r + static_cast<int64_t>(c) * cb.ldc);
+      if (OUT64) static_cast<double*>(Cv)[off] = 0.0;
+      else static_cast<float*>(Cv)[off] = 0.0f;
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols));
+  }
+}
+
+template <bool SWAP, bool A_KC, bool B_KC, bool OUT64>
+cudaError_t launch_tc_t(const float* X, const float* Y, void* C, const GemmCBlock* cb, const GemmPair* pr,
+                        const TcTile* tiles, int32_t ntiles, int32_t nz_begin, int passes, int kc, double* partial,
+                        int* status, cudaStream_t s) {
+  auto kern = k_gemm_tc<SWAP, A_KC, B_KC, OUT64>;
+  static int grid_of[64] = {};  // one CTA per SM, per device ordinal
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  int& grid = grid_of[dev & 63];
+  if (grid == 0) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes);
+    if (e != cudaSuccess) return e;
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    grid = sms;
+  }
+  const unsigned g = static_cast<unsigned>(std::min<int64_t>(ntiles, grid));
+  kern<<<g, kTcThreads, kTcSmemBytes, s>>>(X, Y, C, cb, pr, tiles, ntiles, nz_begin, passes, kc, partial, status);
+  return cudaGetLastError();
+}
+
+// Sum of the k-segment partial tiles of split tiles, in segment order (FP64,
+// deterministic), into C.  One CTA per split tile; element e of the
+// column-major 128 x nb tile is (A-side row e % 128, B-side row e / 128).
+template <bool SWAP, bool OUT64>
+__global__ void k_tc_reduce(const double* __restrict__ partial, void* __restrict__ Cv,
+                            const GemmCBlock* __restrict__ cblocks, const TcSplit* __restrict__ splits) {
+  const TcSplit sp = splits[blockIdx.x];
+  const GemmCBlock cb = cblocks[sp.cb];
+  const int ma = SWAP ? cb.N : cb.M, nbv = SWAP ? cb.M : cb.N;
+  const int rows = min(128, ma - sp.a0), cols = min(sp.nb, nbv - sp.b0);
+  for (int e = static_cast<int>(threadIdx.x); e < 128 * cols; e += static_cast<int>(blockDim.x)) {
+    // SWAP: consecutive threads take consecutive B-side rows (contiguous in C)
+    const int r = SWAP ? e / cols : e % 128, c = SWAP ? e % cols : e / 128;
+    if (r >= rows) continue;
+    double acc = 0.0;
+    for (int q = 0; q < sp.nparts; ++q)
+      acc += partial[static_cast<int64_t>(sp.part0 + q) * (128 * 128) + r + c * 128];
+    const int arow = sp.a0 + r, bcol = sp.b0 + c;
+    const int64_t off = cb.c_off + (SWAP ? bcol + static_cast<int64_t>(arow) * cb.ldc
+                                         : arow + static_cast<int64_t>(bcol) * cb.ldc);
+    if (OUT64) static_cast<double*>(Cv)[off] = acc;
+    else static_cast<float*>(Cv)[off] = static_cast<float>(acc);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_gemm_tc_main(const float* X, const float* Y, void* C, bool c_f64, const GemmCBlock* d_cblocks,
+                                const GemmPair* d_pairs, const TcTile* d_tiles, int32_t ntiles, int32_t nz_begin,
+                                bool xT, bool yT, bool swap, int passes, int kc, double* d_partial, int* d_status,
+                                cudaStream_t s);
+
+cudaError_t launch_gemm_tc(const float* X, const float* Y, void* C, bool c_f64, const GemmCBlock* d_cblocks,
+                           const GemmPair* d_pairs, const TcTile* d_tiles, int32_t ntiles, int32_t nz_begin,
+                           bool xT, bool yT, bool swap, int passes, int kc, double* d_partial,
+                           const TcSplit* d_splits, int32_t nsplits, int* d_status, cudaStream_t s) {
+  if (ntiles <= 0) return cudaSuccess;
+  if ((passes != 1 && passes != 3) || kc < 1 || (nsplits > 0 && (!d_partial || !d_splits)))
+    return cudaErrorInvalidValue;
+  cudaError_t e = launch_gemm_tc_main(X, Y, C, c_f64, d_cblocks, d_pairs, d_tiles, ntiles, nz_begin, xT, yT, swap,
+                                      passes, kc, d_partial, d_status, s);
+  if (e != cudaSuccess || nsplits <= 0) return e;
+  if (swap) {
+    if (c_f64) k_tc_reduce<true, true><<<nsplits, 256, 0, s>>>(d_partial, C, d_cblocks, d_splits);
+    else k_tc_reduce<true, false><<<nsplits, 256, 0, s>>>(d_partial, C, d_cblocks, d_splits);
+  } else {
+    if (c_f64) k_tc_reduce<false, true><<<nsplits, 256, 0, s>>>(d_partial, C, d_cblocks, d_splits);
+    else k_tc_reduce<false, false><<<nsplits, 256, 0, s>>>(d_partial, C, d_cblocks, d_splits);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_tc_main(const float* X, const float* Y, void* C, bool c_f64, const GemmCBlock* d_cblocks,
+                                const GemmPair* d_pairs, const TcTile* d_tiles, int32_t ntiles, int32_t nz_begin,
+                                bool xT, bool yT, bool swap, int passes, int kc, double* d_partial, int* d_status,
+                                cudaStream_t s) {
+  // A side K-contiguous: X with xT (no swap) or Y without yT (swap); B side the other operand
+  const bool akc = swap ? !yT : xT;
+  const bool bkc = swap ? xT : !yT;
+#define SB_TC(SW, AK, BK)                                                                                       \
+  if (swap == SW && akc == AK && bkc == BK)                                                                     \
+    return c_f64 ? launch_tc_t<SW, AK, BK, true>(X, Y, C, d_cblocks, d_pairs, d_tiles, ntiles, nz_begin, passes, \
+                                                  kc, d_partial, d_status, s)                                   \
+                 : launch_tc_t<SW, AK, BK, false>(X, Y, C, d_cblocks, d_pairs, d_tiles, ntiles, nz_begin, passes, \
+                                                   kc, d_partial, d_status, s);
+  SB_TC(false, false, false) SB_TC(false, false, true) SB_TC(false, true, false) SB_TC(false, true, true)
+  SB_TC(true, false, false) SB_TC(true, false, true) SB_TC(true, true, false) SB_TC(true, true, true)
+#undef SB_TC
+  return cudaErrorInvalidValue;
+}
+
+// FP32 copy of FP64 values (operands of the tensor-core GEMM).
+__global__ void k_to_f32(const double* __restrict__ src, float* __restrict__ dst, int64_t n) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x * 2;
+  for (int64_t i = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 2; i < n; i += stride) {
+    dst[i] = __double2float_rn(src[i]);
+    if (i + 1 < n) dst[i + 1] = __double2float_rn(src[i + 1]);
+  }
+}
+
+cudaError_t launch_to_f32(const double* src, float* dst, int64_t n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const unsigned g = static_cast<unsigned>(std::min<int64_t>((n + 511) / 512, 148LL * 16));
+  k_to_f32<<<g, 256, 0, s>>>(src, dst, n);
+  return cudaGetLastError();
+}
+
+}  // namespace sb

@@ -57,7 +57,7 @@ class DevBuf {
 // Kernel classes reported by the in-library profiler.
 enum ProfKind : int {
   PROF_GEMM = 0, PROF_PERMUTE = 1, PROF_OUTER = 2, PROF_AXPY = 3, PROF_OTHER = 4, PROF_VECTOR = 5,
-  PROF_GEMM_THIN = 6, PROF_NKINDS = 7
+  PROF_GEMM_THIN = 6, PROF_GEMM_TC = 7, PROF_NKINDS = 8
 };
 
 struct Ctx {
@@ -92,6 +92,22 @@ struct Ctx {
   // SPARSEB_GEMM_EDGES=0 keeps 64x64-tile launches in one tile shape (tuning);
   // -1 = auto: column / row edges of <= 32 go to 64x32 / 32x64 tiles.
   int gemm_edges = -1;
+  // Arithmetic of the tiled block GEMMs (sb_ctx_set_precision): SB_PRECISION_F64
+  // (DMMA, the drop-in), SB_PRECISION_TF32X3 or SB_PRECISION_TF32 (tcgen05).
+  // The thin K <= 16 launches compute in FP64 in every mode (they are
+  // HBM-bound); they read and write FP32-stored intermediates as FP32.
+  int precision = SB_PRECISION_F64;
+  // k-tiles (32 deep) per FP32 accumulation chunk of the tensor-core GEMM
+  // (SPARSEB_TC_KC); chunks are summed with Kahan compensation.
+  int tc_kc = 16;
+  // SPARSEB_POISON_OUTPUT=1: contract! outputs are filled with NaN before the
+  // kernels write them (a test aid that exposes unwritten elements).
+  bool poison_output = false;
+  // Device status word of the tensor-core GEMM (set to 1 when one of its
+  // bounded waits ran out); allocated when a tensor-core precision is chosen
+  // and read by sb_ctx_synchronize.
+  DevBuf tc_status;
+  bool tc_launched = false;  // a tensor-core GEMM ran since the status was last read
   // Plan cache of the BS x BS contract_shared! path (sb_contract.cpp): the
   // output block structure and the prepared block GEMM of recent
   // contractions, reused when the same labels meet operands of the same block
@@ -206,6 +222,18 @@ struct Tensor {
   // stays empty.  Only the contraction that made the view reads it.
   const double* vdata = nullptr;
   std::vector<int64_t> voff;
+  const struct Tensor* vsrc = nullptr;  // the tensor whose payload a view points into
+  // FP32 storage (block-sparse only): the payload holds floats, one per
+  // element, at the same element offsets.  Only the tensor-core contraction
+  // path reads or writes such tensors (the intermediates of a TF32 H_eff
+  // chain); every other kernel rejects them.
+  bool f32 = false;
+  // Bumped by every library call that writes the payload (contract! output,
+  // vector-space updates, a device pointer handed out).  The FP32 copy of an
+  // FP64 payload used by the tensor-core GEMMs is kept while it matches.
+  uint64_t version = 0;
+  mutable DevBuf shadow;
+  mutable uint64_t shadow_version = ~0ull;
 
   int N() const { return static_cast<int>(dims.size()); }
   int P() const { return N() - n2; }
@@ -224,6 +252,8 @@ struct Tensor {
   // Per-block layout, valid for uniform and ragged tensors.
   int64_t block_off(int64_t i) const { return !voff.empty() ? voff[i] : ragged ? boff[i] : i * blksize(); }
   const double* payload() const { return vdata ? vdata : data.d(); }
+  // Tensor that owns the payload (itself unless a key-reordering view).
+  const Tensor& owner() const { return vsrc ? *vsrc : *this; }
   int64_t block_len(int64_t i) const { return ragged ? boff[i + 1] - boff[i] : blksize(); }
   int64_t block_dim(int64_t i, int t) const { return ragged ? bdims[i * n2 + t] : dims[P() + t]; }
   int64_t payload_len() const {
@@ -274,6 +304,13 @@ void bs_pad_into(Ctx* ctx, const Tensor& A, double* dst);
 void copy_blocks(Ctx* ctx, const double* src, double* dst, const std::vector<int64_t>& src_off,
                  const std::vector<int64_t>& dst_off, const std::vector<int64_t>& len);
 void require_uniform(const Tensor& t, const char* what);
+// Rejects FP32-stored tensors on paths that only handle FP64 payloads.
+void require_f64(const Tensor& t, const char* what);
+// FP32 values of a tensor's payload at its own element offsets: the payload
+// itself for FP32 storage, else the owner's FP32 copy (made on first use and
+// kept while the owner's version is unchanged; always remade while a capture
+// is open, so that a replay converts the current values).
+const float* f32_payload(Ctx* ctx, const Tensor& t);
 void check_no_cross_perm(const std::vector<int>& perm1, int N, int P);
 bool is_identity(const std::vector<int>& perm1);
 

@@ -74,13 +74,55 @@ cudaError_t launch_gemm_f64_edges(const double* X, const double* Y, double* C, c
 // grid of 5 CTAs per SM walks the strips with the copy pipeline running
 // across strip boundaries and stores C from the fragments (needs >= 1 pair
 // per C block); otherwise one CTA per strip with shared-memory staged stores.
+// long_f32: the long operand (Y when small_rows, else X) and C hold FP32
+// values (the intermediates of the tensor-core H_eff chain); the small
+// operand stays FP64 and the arithmetic FP64.  Persistent kernel only.
 cudaError_t launch_gemm_f64_skinny(const double* X, const double* Y, double* C,
                                    const GemmCBlock* d_cblocks, int32_t ncblocks, const GemmPair* d_pairs,
                                    int64_t nctas, bool xT, bool yT, bool small_rows, int small_max,
-                                   int k_max, cudaStream_t s, bool persistent = false);
+                                   int k_max, cudaStream_t s, bool persistent = false, bool long_f32 = false);
 
 // Number of tiles of a (M, N) C block for the given tile shape.
 void gemm_tile_dims(GemmShape shape, int* bm, int* bn);
+
+// ── the same grouped GEMM on the tcgen05 tensor cores (sb_gemm_tc.cu) ─────
+//
+// FP32 operands (X, Y: element offsets as in GemmPair), arithmetic in TF32
+// with FP32 accumulation, result FP64 (c_f64) or FP32.  passes = 3 splits
+// every operand into TF32 hi + lo parts and sums a_hi*b_lo + a_lo*b_hi +
+// a_hi*b_hi (about 22 significant bits per operand), passes = 1 multiplies
+// the TF32-rounded operands once.
+// Work items are listed explicitly: item i covers rows [a0, a0 + 128) of the
+// A side and [b0, b0 + nb) of the B side of C block cb (nb a multiple of 16
+// in 16..128), and nkt k-tiles (32 deep) of its C block's concatenated pair
+// K ranges starting at pair p0, offset k0 (a multiple of 32).  Without swap
+// the A side is X (rows of C) and the B side Y (columns of C); with swap the
+// other way round.  An item with part < 0 covers the whole K range and
+// writes C; part >= 0 marks a k-segment of a split tile, written in FP64 to
+// partial tile `part` (column-major 128 x 128 doubles) and summed in segment
+// order into C by the reduction that follows (one TcSplit per split tile:
+// its geometry and its parts [part0, part0 + nparts)).  Items [nz_begin,
+// ntiles) belong to C blocks without pairs and are written as zeros.  Within
+// an item the k-tiles accumulate in FP32 chunks of kc k-tiles that are summed
+// with Kahan compensation.  A persistent grid of one CTA per SM walks the list
+// with stride gridDim.x, so the list order (the host sorts by work) balances
+// the load.  *d_status is set to 1 if a bounded wait on the tensor core ran
+// out (the results are then invalid).
+struct TcTile {
+  int32_t cb, a0, b0, nb;
+  int32_t p0, k0, nkt, part;
+};
+struct TcSplit {
+  int32_t cb, a0, b0, nb;
+  int32_t part0, nparts, pad0, pad1;
+};
+constexpr int kTcMaxN = 128;
+cudaError_t launch_gemm_tc(const float* X, const float* Y, void* C, bool c_f64, const GemmCBlock* d_cblocks,
+                           const GemmPair* d_pairs, const TcTile* d_tiles, int32_t ntiles, int32_t nz_begin,
+                           bool xT, bool yT, bool swap, int passes, int kc, double* d_partial,
+                           const TcSplit* d_splits, int32_t nsplits, int* d_status, cudaStream_t s);
+// dst[i] = (float)src[i], i < n (FP32 operand copies for launch_gemm_tc).
+cudaError_t launch_to_f32(const double* src, float* dst, int64_t n, cudaStream_t s);
 
 // ── outer-product accumulation (K = 1 pairs) on CUDA cores ─────────────────
 //

@@ -191,6 +191,31 @@ void require_uniform(const Tensor& t, const char* what) {
                              "permutedims and the uniform/ragged adapters; convert with sb_tensor_to_uniform");
 }
 
+void require_f64(const Tensor& t, const char* what) {
+  if (t.f32)
+    fail(SB_ERR_UNSUPPORTED_TYPES,
+         std::string(what) + ": FP32-stored tensors (tensor-core chain intermediates) are supported by "
+                             "contract_shared! (BS x BS) and the exports only");
+}
+
+const float* f32_payload(Ctx* ctx, const Tensor& t) {
+  if (t.f32) return reinterpret_cast<const float*>(t.payload());
+  const Tensor& o = t.owner();
+  const int64_t n = o.payload_len();
+  if (n == 0) return nullptr;
+  if (!ctx->capturing && o.shadow.raw() && o.shadow_version == o.version &&
+      o.shadow.bytes() == static_cast<size_t>(n) * sizeof(float))
+    return o.shadow.as<const float>();
+  if (o.shadow.bytes() != static_cast<size_t>(n) * sizeof(float)) o.shadow = DevBuf(ctx, n * sizeof(float));
+  {
+    ProfScope ps(ctx, PROF_OTHER, 0.0, 12.0 * n);
+    SB_CK(launch_to_f32(o.payload(), o.shadow.as<float>(), n, ctx->stream));
+  }
+  ctx->note_launch();
+  o.shadow_version = ctx->capturing ? ~0ull : o.version;
+  return o.shadow.as<const float>();
+}
+
 void copy_blocks(Ctx* ctx, const double* src, double* dst, const std::vector<int64_t>& src_off,
                  const std::vector<int64_t>& dst_off, const std::vector<int64_t>& len) {
   if (src_off.empty()) return;

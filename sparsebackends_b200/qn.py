@@ -445,12 +445,16 @@ class HeffChain:
     STEPS = (("T1", "L", "psi"), ("T2", "T1", "W1"), ("T3", "T2", "W2"), ("T4", "R", "T3"))
     STEPS_W12 = (("W12", "W1", "W2"), ("T1", "L", "psi"), ("T3", "T1", "W12"), ("T4", "R", "T3"))
 
-    def __init__(self, layout: HeffLayout, ctx=None, w12: bool = False):
+    def __init__(self, layout: HeffLayout, ctx=None, w12: bool = False, f32_intermediates: bool = False):
+        """``f32_intermediates``: T1, T2, T3 (and W12) are stored in FP32
+        (sb_tensor_create_bs_f32), for a context in a tensor-core precision:
+        the MPO steps then move half the bytes; T4 stays FP64."""
         import sparsebackends_b200 as sb
         self.sb = sb
         self.layout = layout
         self.steps = self.STEPS_W12 if w12 else self.STEPS
-        self.out = {n: sb.NewBlockSparseSorted.empty(layout.dims[n], layout.n2[n], ctx=ctx)
+        self.out = {n: sb.NewBlockSparseSorted.empty(layout.dims[n], layout.n2[n], ctx=ctx,
+                                                     f32=f32_intermediates and n not in ("T4", "W12"))
                     for n in {c for c, _, _ in self.steps}}
 
     def apply(self, psi, L, W1, W2, R):
