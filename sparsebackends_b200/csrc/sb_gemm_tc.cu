@@ -44,12 +44,11 @@
 namespace sb {
 namespace {
 
-constexpr int kTcThreads = 256;
 constexpr int kTcBK = 32;                 // k-tile: 32 TF32 values = one 128-byte swizzle row
 constexpr int kTcStages = 3;
 constexpr int kTcImg = 128 * 128;         // bytes of one plane image (128 rows x 128 B)
 constexpr int kTcStageBytes = 4 * kTcImg;  // hi and lo planes of A and B
-constexpr int kTcEpiBytes = 8 * 32 * 32 * 4;   // per-warp 32 x 32 FP32 transpose buffers of the epilogue
+constexpr int kTcEpiBytes = 4 * 32 * 32 * 4;   // per-warp 32 x 32 FP32 transpose buffers of the drain warps
 constexpr int kTcSmemBytes = kTcStages * kTcStageBytes + kTcEpiBytes + 1024 /*alignment*/ + 256 /*barriers*/;
 constexpr int kTcTmemCols = 512;          // acc0, acc1, Kahan sum, Kahan compensation
 constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of every mbarrier wait
@@ -92,6 +91,10 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* st
       return false;
     }
   }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -221,16 +224,24 @@ struct Cursor {
   int t, p, k0, kt;
 };
 
-// A finished chunk waiting to be folded or written.
-struct Chunk {
-  int t;          // tile
-  uint32_t cg;    // chunk counter of this CTA (accumulator cg & 1)
-  bool first;     // first chunk of its tile
-  bool last;      // last chunk of its tile
-};
+// Roles (13 warps).  Warps 0-7 produce: they load the FP32 operand values of
+// a k-tile (two k-tiles ahead, in registers), split them and store the hi/lo
+// images into one of three shared-memory stages, then arrive on the stage's
+// "full" barrier.  Warp 8 issues the MMAs: it waits for a full stage, issues
+// the k-tile's MMAs into the accumulator of the current chunk and commits
+// them to the stage's "empty" barrier (and, at a chunk's end, to the
+// accumulator's "full" barrier).  Warps 9-12 drain: each owns one quarter of
+// the TMEM lanes (rows of the A side); for a finished chunk they fold it into
+// the Kahan pair, or write the item, then arrive on the accumulator's "empty"
+// barrier so that the MMA warp can start the chunk after next in it.  The
+// three roles walk the same sequence of items, k-tiles and chunks.
+constexpr int kTcProducers = 256;  // warps 0-7 (the operand loads map 256 threads)
+constexpr int kTcMmaWarp = 8;
+constexpr int kTcEpiWarp0 = 9;     // warps 9-12
+constexpr int kTcAllThreads = 13 * 32;
 
 template <bool SWAP, bool A_KC, bool B_KC, bool OUT64>
-__global__ void __launch_bounds__(kTcThreads, 1)
+__global__ void __launch_bounds__(kTcAllThreads, 1)
     k_gemm_tc(const float* __restrict__ X, const float* __restrict__ Y, void* __restrict__ Cv,
               const GemmCBlock* __restrict__ cblocks, const GemmPair* __restrict__ pairs,
               const TcTile* __restrict__ tiles, int32_t ntiles, int32_t nz_begin, int32_t passes, int32_t kc,
@@ -240,18 +251,26 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const int warp = tid >> 5, lane = tid & 31;
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;  // 1024-aligned swizzle atoms
-  float* const epi = reinterpret_cast<float*>(smem_raw + (base - raw) + kTcStages * kTcStageBytes) + warp * 1024;
-  const uint32_t bars = base + kTcStages * kTcStageBytes + kTcEpiBytes;
-  const uint32_t bar_empty0 = bars;                 // kTcStages barriers, 8 bytes apart
-  const uint32_t bar_acc0 = bars + 8 * kTcStages;   // two barriers (accumulators 0 and 1)
-  const uint32_t tmem_slot = bars + 64;
+  const uint32_t epi_addr = base + kTcStages * kTcStageBytes;
+  const uint32_t bars = epi_addr + kTcEpiBytes;
+  const uint32_t bar_full0 = bars;                // kTcStages barriers, 8 bytes apart
+  const uint32_t bar_empty0 = bars + 32;          // kTcStages
+  const uint32_t bar_accf0 = bars + 64;           // 2 (accumulators 0 and 1)
+  const uint32_t bar_acce0 = bars + 80;           // 2
+  const uint32_t tmem_slot = bars + 96;
   unsigned char* const tmem_slot_ptr = smem_raw + (tmem_slot - raw);
   const bool split = passes == 3;
+  const int grid = static_cast<int>(gridDim.x);
 
   if (tid == 0) {
-    for (int s = 0; s < kTcStages; ++s) mbar_init(bar_empty0 + 8 * s, 1);
-    mbar_init(bar_acc0, 1);
-    mbar_init(bar_acc0 + 8, 1);
+    for (int s = 0; s < kTcStages; ++s) {
+      mbar_init(bar_full0 + 8 * s, kTcProducers);
+      mbar_init(bar_empty0 + 8 * s, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(bar_accf0 + 8 * b, 1);
+      mbar_init(bar_acce0 + 8 * b, 4);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -263,219 +282,223 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(tmem_slot_ptr);
-  const uint32_t t_sum = tmem + 256, t_comp = tmem + 384;
 
-  bool failed = false;  // a bounded wait ran out: stop issuing and waiting
-
-  float ra0[kCH][4], rb0[kCH][4], ra1[kCH][4], rb1[kCH][4];
-
-  auto load = [&](const Cursor& c, float (&ra)[kCH][4], float (&rb)[kCH][4]) {
-    const TcTile tl = tiles[c.t];
-    const GemmCBlock cb = cblocks[tl.cb];
-    const GemmPair pr = pairs[c.p];
-    const int ma = SWAP ? cb.N : cb.M, nbv = SWAP ? cb.M : cb.N;
-    const int kv = min(kTcBK, pr.K - c.k0);
-    // A side: row a0 of the tile at k0; B side: row b0
-    const float* xa = X + pr.x_off;
-    const float* ya = Y + pr.y_off;
-    const int64_t lda = SWAP ? pr.ldy : pr.ldx, ldb = SWAP ? pr.ldx : pr.ldy;
-    const float* pa = SWAP ? ya : xa;
-    const float* pb = SWAP ? xa : ya;
-    pa += A_KC ? static_cast<int64_t>(tl.a0) * lda + c.k0 : tl.a0 + static_cast<int64_t>(c.k0) * lda;
-    pb += B_KC ? static_cast<int64_t>(tl.b0) * ldb + c.k0 : tl.b0 + static_cast<int64_t>(c.k0) * ldb;
-    load_tile<A_KC>(ra, pa, lda, min(128, ma - tl.a0), kv, tid);
-    load_tile<B_KC>(rb, pb, ldb, min(tl.nb, nbv - tl.b0), kv, tid);
-  };
-  // next k-tile after c (same pair, next pair of the tile, or the first pair
-  // of this CTA's next tile); t >= nz_begin marks the end
-  auto first_of = [&](int t) -> Cursor {
-    if (t >= nz_begin) return Cursor{t, 0, 0, 0};
-    const TcTile tl = tiles[t];
-    return Cursor{t, tl.p0, tl.k0, 0};
-  };
-  auto advance = [&](Cursor c) -> Cursor {
-    if (c.t >= nz_begin) return c;
-    if (c.kt + 1 >= tiles[c.t].nkt) return first_of(c.t + static_cast<int>(gridDim.x));
-    if (c.k0 + kTcBK < pairs[c.p].K) return Cursor{c.t, c.p, c.k0 + kTcBK, c.kt + 1};
-    return Cursor{c.t, c.p + 1, 0, c.kt + 1};
-  };
-
-  // Fold a finished chunk into the Kahan pair, or write the item: into C, or
-  // (a k-segment of a split tile) into its FP64 partial tile, column-major
-  // 128 x 128, for k_tc_reduce.
-  const int sub = warp & 3, half = warp >> 2;
-  auto finish_chunk = [&](const Chunk& ch) {
-    if (!failed) failed = !mbar_wait(bar_acc0 + 8 * (ch.cg & 1), (ch.cg >> 1) & 1, status);
-    tc_fence_after();
-    const TcTile tl = tiles[ch.t];
-    const GemmCBlock cb = cblocks[tl.cb];
-    const uint32_t lanes = static_cast<uint32_t>(32 * sub) << 16;
-    const uint32_t acc = tmem + 128 * (ch.cg & 1);
-    const int ma = SWAP ? cb.N : cb.M, nbv = SWAP ? cb.M : cb.N;
-    const int arow0 = tl.a0 + 32 * sub;        // first A-side row of this warp
-    const int arow = arow0 + lane;             // A-side row of this thread
-    const int rows_ok = min(32, ma - arow0);   // valid rows of this warp (may be <= 0)
-    for (int col0 = 64 * half; col0 < 64 * half + 64 && col0 < tl.nb; col0 += 32) {
-      const int nh = col0 + 16 < tl.nb ? 2 : 1;  // 16-column halves inside nb (warp-uniform)
-      for (int h = 0; h < nh; ++h) {
-        const int cc = col0 + 16 * h;
-        float v[16], sm[16], cm[16];
-        tmem_ld16(acc + lanes + cc, v);
-        if (!ch.first) {
-          tmem_ld16(t_sum + lanes + cc, sm);
-          tmem_ld16(t_comp + lanes + cc, cm);
-        }
-        tmem_wait_ld();
+  if (warp < kTcProducers / 32) {
+    // ── producers ─────────────────────────────────────────────────────────
+    bool failed = false;
+    auto first_of = [&](int t) -> Cursor {
+      if (t >= nz_begin) return Cursor{t, 0, 0, 0};
+      const TcTile tl = tiles[t];
+      return Cursor{t, tl.p0, tl.k0, 0};
+    };
+    auto advance = [&](Cursor c) -> Cursor {
+      if (c.t >= nz_begin) return c;
+      if (c.kt + 1 >= tiles[c.t].nkt) return first_of(c.t + grid);
+      if (c.k0 + kTcBK < pairs[c.p].K) return Cursor{c.t, c.p, c.k0 + kTcBK, c.kt + 1};
+      return Cursor{c.t, c.p + 1, 0, c.kt + 1};
+    };
+    auto load = [&](const Cursor& c, float (&ra)[kCH][4], float (&rb)[kCH][4]) {
+      const TcTile tl = tiles[c.t];
+      const GemmCBlock cb = cblocks[tl.cb];
+      const GemmPair pr = pairs[c.p];
+      const int ma = SWAP ? cb.N : cb.M, nbv = SWAP ? cb.M : cb.N;
+      const int kv = min(kTcBK, pr.K - c.k0);
+      const int64_t lda = SWAP ? pr.ldy : pr.ldx, ldb = SWAP ? pr.ldx : pr.ldy;
+      const float* pa = SWAP ? Y + pr.y_off : X + pr.x_off;
+      const float* pb = SWAP ? X + pr.x_off : Y + pr.y_off;
+      pa += A_KC ? static_cast<int64_t>(tl.a0) * lda + c.k0 : tl.a0 + static_cast<int64_t>(c.k0) * lda;
+      pb += B_KC ? static_cast<int64_t>(tl.b0) * ldb + c.k0 : tl.b0 + static_cast<int64_t>(c.k0) * ldb;
+      load_tile<A_KC>(ra, pa, lda, min(128, ma - tl.a0), kv, tid);
+      load_tile<B_KC>(rb, pb, ldb, min(tl.nb, nbv - tl.b0), kv, tid);
+    };
+    float ra0[kCH][4], rb0[kCH][4], ra1[kCH][4], rb1[kCH][4];
+    Cursor cur = first_of(static_cast<int>(blockIdx.x));
+    Cursor nxt = advance(cur);
+    if (cur.t < nz_begin) load(cur, ra0, rb0);
+    if (nxt.t < nz_begin) load(nxt, ra1, rb1);
+    uint32_t g = 0;
+    auto produce = [&](float (&ra)[kCH][4], float (&rb)[kCH][4], const Cursor& ahead2) {
+      const int s = static_cast<int>(g % kTcStages);
+      if (g >= kTcStages && !failed) failed = !mbar_wait(bar_empty0 + 8 * s, ((g / kTcStages) - 1) & 1, status);
+      const uint32_t sa_hi = base + s * kTcStageBytes, sa_lo = sa_hi + kTcImg;
+      const uint32_t sb_hi = sa_hi + 2 * kTcImg, sb_lo = sb_hi + kTcImg;
+      store_tile<A_KC>(ra, sa_hi, sa_lo, split, tid);
+      store_tile<B_KC>(rb, sb_hi, sb_lo, split, tid);
+      fence_proxy_async();
+      mbar_arrive(bar_full0 + 8 * s);
+      if (ahead2.t < nz_begin) load(ahead2, ra, rb);  // in flight during the next two k-tiles
+      ++g;
+    };
+    while (cur.t < nz_begin && !failed) {
+      const Cursor n2 = advance(nxt);
+      produce(ra0, rb0, n2);
+      cur = nxt;
+      nxt = n2;
+      if (cur.t >= nz_begin || failed) break;
+      const Cursor n3 = advance(nxt);
+      produce(ra1, rb1, n3);
+      cur = nxt;
+      nxt = n3;
+    }
+  } else if (warp == kTcMmaWarp) {
+    // ── MMA issue (one thread) ────────────────────────────────────────────
+    if (lane == 0) {
+      bool failed = false;
+      uint32_t g = 0, cg = 0;
+      for (int t = static_cast<int>(blockIdx.x); t < nz_begin && !failed; t += grid) {
+        const TcTile tl = tiles[t];
+        const uint32_t idesc = idesc_tf32(tl.nb);
+        for (int kt = 0; kt < tl.nkt && !failed; ++kt) {
+          const bool chunk_first = kt % kc == 0;
+          const bool chunk_last = kt + 1 == tl.nkt || (kt + 1) % kc == 0;
+          const uint32_t b = cg & 1;
+          if (chunk_first && cg >= 2) failed = !mbar_wait(bar_acce0 + 8 * b, ((cg >> 1) - 1) & 1, status);
+          const int s = static_cast<int>(g % kTcStages);
+          if (!failed) failed = !mbar_wait(bar_full0 + 8 * s, (g / kTcStages) & 1, status);
+          if (failed) break;
+          tc_fence_after();
+          const uint32_t acc = tmem + 128 * b;
+          const uint32_t sa_hi = base + s * kTcStageBytes, sa_lo = sa_hi + kTcImg;
+          const uint32_t sb_hi = sa_hi + 2 * kTcImg, sb_lo = sb_hi + kTcImg;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          if (ch.first) {
-            sm[j] = v[j];
-            cm[j] = 0.0f;
-          } else {  // Kahan: s + v, lost low part kept (negated) in c
-            const float y = v[j] - cm[j];
-            const float t = sm[j] + y;
-            cm[j] = (t - sm[j]) - y;
-            sm[j] = t;
+          for (int kk = 0; kk < kTcBK / 8; ++kk) {
+            const uint64_t ah = smem_desc(sa_hi + 32 * kk), bh = smem_desc(sb_hi + 32 * kk);
+            bool accum = !(chunk_first && kk == 0);
+            if (split) {
+              mma_tf32(acc, ah, smem_desc(sb_lo + 32 * kk), idesc, accum);
+              mma_tf32(acc, smem_desc(sa_lo + 32 * kk), bh, idesc, true);
+              accum = true;
+            }
+            mma_tf32(acc, ah, bh, idesc, accum);
           }
+          mma_commit(bar_empty0 + 8 * s);
+          if (chunk_last) {
+            mma_commit(bar_accf0 + 8 * b);
+            ++cg;
+          }
+          ++g;
         }
-        if (!ch.last) {
-          tmem_st16(t_sum + lanes + cc, sm);
-          tmem_st16(t_comp + lanes + cc, cm);
-          continue;
-        }
-        if (failed || rows_ok <= 0) continue;
-        if (tl.part >= 0) {
-          // partial tile (column-major 128 x 128): lanes write consecutive rows
-          double* pt = partial + static_cast<int64_t>(tl.part) * (128 * 128) + 32 * sub + lane;
-          if (lane < rows_ok)
-#pragma unroll
-            for (int j = 0; j < 16; ++j)
-              pt[(cc + j) * 128] = static_cast<double>(sm[j]) - static_cast<double>(cm[j]);
-          continue;
-        }
-        if (!SWAP) {
-          // C(i = arow, j = bcol) at arow + bcol * ldc: lanes write consecutive rows
-          if (lane < rows_ok)
+      }
+    }
+  } else {
+    // ── drain: warps 9-12, TMEM lane quarter q = warp % 4 ─────────────────
+    bool failed = false;
+    const int q = warp & 3;
+    const uint32_t lanes = static_cast<uint32_t>(32 * q) << 16;
+    float* const epi = reinterpret_cast<float*>(smem_raw + (epi_addr - raw)) + (warp - kTcEpiWarp0) * 1024;
+    const uint32_t t_sum = tmem + 256, t_comp = tmem + 384;
+    uint32_t cg = 0;
+    for (int t = static_cast<int>(blockIdx.x); t < nz_begin; t += grid) {
+      const TcTile tl = tiles[t];
+      const GemmCBlock cb = cblocks[tl.cb];
+      const int ma = SWAP ? cb.N : cb.M, nbv = SWAP ? cb.M : cb.N;
+      const int arow0 = tl.a0 + 32 * q;         // first A-side row of this warp
+      const int arow = arow0 + lane;            // A-side row of this thread
+      const int rows_ok = min(32, ma - arow0);  // valid rows of this warp (may be <= 0)
+      const int nch = (tl.nkt + kc - 1) / kc;
+      for (int ch = 0; ch < nch; ++ch, ++cg) {
+        const bool first = ch == 0, last = ch + 1 == nch;
+        const uint32_t b = cg & 1;
+        if (!failed) failed = !mbar_wait(bar_accf0 + 8 * b, (cg >> 1) & 1, status);
+        tc_fence_after();
+        const uint32_t acc = tmem + 128 * b;
+        for (int col0 = 0; col0 < tl.nb; col0 += 32) {
+          const int nh = col0 + 16 < tl.nb ? 2 : 1;  // 16-column halves inside nb
+          for (int h = 0; h < nh; ++h) {
+            const int cc = col0 + 16 * h;
+            float v[16], sm[16], cm[16];
+            tmem_ld16(acc + lanes + cc, v);
+            if (!first) {
+              tmem_ld16(t_sum + lanes + cc, sm);
+              tmem_ld16(t_comp + lanes + cc, cm);
+            }
+            tmem_wait_ld();
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
-              const int bcol = tl.b0 + cc + j;
-              if (bcol >= nbv) break;
-              const int64_t off = cb.c_off + arow + static_cast<int64_t>(bcol) * cb.ldc;
-              if (OUT64) static_cast<double*>(Cv)[off] = static_cast<double>(sm[j]) - static_cast<double>(cm[j]);
-              else static_cast<float*>(Cv)[off] = sm[j] - cm[j];
+              if (first) {
+                sm[j] = v[j];
+                cm[j] = 0.0f;
+              } else {  // Kahan: s + v, lost low part kept (negated) in c
+                const float y = v[j] - cm[j];
+                const float tt = sm[j] + y;
+                cm[j] = (tt - sm[j]) - y;
+                sm[j] = tt;
+              }
             }
-          continue;
-        }
-        // SWAP: stage the warp's 32 rows x 16 columns in its shared buffer
-        // (XOR-swizzled: no bank conflicts either way) for the transposed store
+            if (!last) {
+              tmem_st16(t_sum + lanes + cc, sm);
+              tmem_st16(t_comp + lanes + cc, cm);
+              continue;
+            }
+            if (failed || rows_ok <= 0) continue;
+            if (tl.part >= 0) {
+              // partial tile (column-major 128 x 128): lanes write consecutive rows
+              double* pt = partial + static_cast<int64_t>(tl.part) * (128 * 128) + 32 * q + lane;
+              if (lane < rows_ok)
 #pragma unroll
-        for (int j = 0; j < 16; ++j) epi[lane * 32 + ((16 * h + j) ^ lane)] = sm[j] - cm[j];
-      }
-      if (!SWAP || !ch.last || tl.part >= 0) continue;
-      // C(i = bcol, j = arow) at bcol + arow * ldc: lanes write consecutive
-      // columns of one row
-      __syncwarp();
-      if (!failed && rows_ok > 0) {
-        const int bcol = tl.b0 + col0 + lane;
-        const bool col_ok = bcol < nbv && lane < 16 * nh;
-        for (int r = 0; r < rows_ok; ++r) {
-          const float val = epi[r * 32 + (lane ^ r)];
-          if (!col_ok) continue;
-          const int64_t off = cb.c_off + bcol + static_cast<int64_t>(arow0 + r) * cb.ldc;
-          if (OUT64) static_cast<double*>(Cv)[off] = static_cast<double>(val);
-          else static_cast<float*>(Cv)[off] = val;
-        }
-      }
-      __syncwarp();
-    }
-    if (!ch.last) tmem_wait_st();
-    tc_fence_before();
-  };
-
-  Cursor cur = first_of(static_cast<int>(blockIdx.x));
-  Cursor nxt = advance(cur);   // k-tile held in the second register set
-  if (cur.t < nz_begin) load(cur, ra0, rb0);
-  if (nxt.t < nz_begin) load(nxt, ra1, rb1);
-
-  uint32_t g = 0;    // k-tiles staged by this CTA so far
-  uint32_t cg = 0;   // chunks started by this CTA so far
-  Chunk pending{0, 0, false, false};
-  bool has_pending = false;
-  int chunk_first_kt = 0;  // kt at which the current chunk started
-
-  // One k-tile: stage the registers of cursor c, prefetch two ahead into the
-  // same registers, issue the MMAs, fold a pending chunk.
-  auto step = [&](const Cursor& c, float (&ra)[kCH][4], float (&rb)[kCH][4], const Cursor& ahead2) {
-    const int s = static_cast<int>(g % kTcStages);
-    if (g >= kTcStages && !failed) failed = !mbar_wait(bar_empty0 + 8 * s, ((g / kTcStages) - 1) & 1, status);
-    const uint32_t sa_hi = base + s * kTcStageBytes, sa_lo = sa_hi + kTcImg;
-    const uint32_t sb_hi = sa_hi + 2 * kTcImg, sb_lo = sb_hi + kTcImg;
-    store_tile<A_KC>(ra, sa_hi, sa_lo, split, tid);
-    store_tile<B_KC>(rb, sb_hi, sb_lo, split, tid);
-    fence_proxy_async();
-    if (ahead2.t < nz_begin) load(ahead2, ra, rb);  // in flight during the next two k-tiles
-    __syncthreads();
-    const Cursor n1 = advance(c);
-    const bool tile_last = n1.t != c.t;
-    if (c.kt == 0) chunk_first_kt = 0;
-    const bool chunk_first = c.kt == chunk_first_kt;
-    const bool chunk_last = tile_last || (c.kt + 1 - chunk_first_kt) == kc;
-    const TcTile tl = tiles[c.t];
-    const uint32_t acc = tmem + 128 * (cg & 1);
-    if (tid == 0 && !failed) {
-      tc_fence_after();
-      const uint32_t idesc = idesc_tf32(tl.nb);
+                for (int j = 0; j < 16; ++j)
+                  pt[(cc + j) * 128] = static_cast<double>(sm[j]) - static_cast<double>(cm[j]);
+              continue;
+            }
+            if (!SWAP) {
+              // C(i = arow, j = bcol) at arow + bcol * ldc: lanes write consecutive rows
+              if (lane < rows_ok)
 #pragma unroll
-      for (int kk = 0; kk < kTcBK / 8; ++kk) {
-        const uint64_t ah = smem_desc(sa_hi + 32 * kk), bh = smem_desc(sb_hi + 32 * kk);
-        bool accum = !(chunk_first && kk == 0);
-        if (split) {
-          mma_tf32(acc, ah, smem_desc(sb_lo + 32 * kk), idesc, accum);
-          mma_tf32(acc, smem_desc(sa_lo + 32 * kk), bh, idesc, true);
-          accum = true;
+                for (int j = 0; j < 16; ++j) {
+                  const int bcol = tl.b0 + cc + j;
+                  if (bcol >= nbv) break;
+                  const int64_t off = cb.c_off + arow + static_cast<int64_t>(bcol) * cb.ldc;
+                  if (OUT64) static_cast<double*>(Cv)[off] = static_cast<double>(sm[j]) - static_cast<double>(cm[j]);
+                  else static_cast<float*>(Cv)[off] = sm[j] - cm[j];
+                }
+              continue;
+            }
+            // SWAP: stage 32 rows x 16 columns in the warp's shared buffer
+            // (XOR-swizzled: no bank conflicts either way) for the transposed store
+            if constexpr (SWAP) {
+#pragma unroll
+              for (int j = 0; j < 16; ++j) epi[lane * 32 + ((16 * h + j) ^ lane)] = sm[j] - cm[j];
+            }
+          }
+          if constexpr (SWAP) {
+            if (!last || tl.part >= 0) continue;
+            // C(i = bcol, j = arow) at bcol + arow * ldc: lanes write consecutive
+            // columns of one row
+            __syncwarp();
+            if (!failed && rows_ok > 0) {
+              const int bcol = tl.b0 + col0 + lane;
+              const bool col_ok = bcol < nbv && lane < 16 * nh;
+              for (int r = 0; r < rows_ok; ++r) {
+                const float val = epi[r * 32 + (lane ^ r)];
+                if (!col_ok) continue;
+                const int64_t off = cb.c_off + bcol + static_cast<int64_t>(arow0 + r) * cb.ldc;
+                if (OUT64) static_cast<double*>(Cv)[off] = static_cast<double>(val);
+                else static_cast<float*>(Cv)[off] = val;
+              }
+            }
+            __syncwarp();
+          }
         }
-        mma_tf32(acc, ah, bh, idesc, accum);
+        if (!last) tmem_wait_st();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(bar_acce0 + 8 * b);
       }
-      mma_commit(bar_empty0 + 8 * s);
-      if (chunk_last) mma_commit(bar_acc0 + 8 * (cg & 1));
     }
-    ++g;
-    if (has_pending) {  // the tensor core now works on the other accumulator
-      finish_chunk(pending);
-      has_pending = false;
-    }
-    if (chunk_last) {
-      pending = Chunk{c.t, cg, chunk_first_kt == 0, tile_last};
-      has_pending = true;
-      ++cg;
-      chunk_first_kt = c.kt + 1;
-    }
-  };
-
-  while (cur.t < nz_begin) {
-    const Cursor n2 = advance(nxt);
-    step(cur, ra0, rb0, n2);
-    cur = nxt;
-    nxt = n2;
-    if (cur.t >= nz_begin) break;
-    const Cursor n3 = advance(nxt);
-    step(cur, ra1, rb1, n3);
-    cur = nxt;
-    nxt = n3;
-  }
-  if (has_pending) finish_chunk(pending);
-
-  // C blocks without pairs (tiles [nz_begin, ntiles)): zeros
-  for (int t = nz_begin + static_cast<int>(blockIdx.x); t < ntiles; t += static_cast<int>(gridDim.x)) {
-    const TcTile tl = tiles[t];
-    const GemmCBlock cb = cblocks[tl.cb];
-    const int ma = SWAP ? cb.N : cb.M, nbv = SWAP ? cb.M : cb.N;
-    const int rows = min(128, ma - tl.a0), cols = min(tl.nb, nbv - tl.b0);
-    for (int e = tid; e < rows * cols; e += kTcThreads) {
-      const int r = tl.a0 + e % rows, c = tl.b0 + e / rows;
-      const int64_t off = cb.c_off + (SWAP ? c + static_cast<int64_t>(r) * cb.ldc : r + static_cast<int64_t>(c) * cb.ldc);
-      if (OUT64) static_cast<double*>(Cv)[off] = 0.0;
-      else static_cast<float*>(Cv)[off] = 0.0f;
+    // C blocks without pairs (items [nz_begin, ntiles)): zeros
+    const int et = tid - kTcEpiWarp0 * 32;
+    for (int t = nz_begin + static_cast<int>(blockIdx.x); t < ntiles; t += grid) {
+      const TcTile tl = tiles[t];
+      const GemmCBlock cb = cblocks[tl.cb];
+      const int ma = SWAP ? cb.N : cb.M, nbv = SWAP ? cb.M : cb.N;
+      const int rows = min(128, ma - tl.a0), cols = min(tl.nb, nbv - tl.b0);
+      for (int e = et; e < rows * cols; e += 128) {
+        const int r = tl.a0 + e % rows, c = tl.b0 + e / rows;
+        const int64_t off =
+            cb.c_off + (SWAP ? c + static_cast<int64_t>(r) * cb.ldc : r + static_cast<int64_t>(c) * cb.ldc);
+        if (OUT64) static_cast<double*>(Cv)[off] = 0.0;
+        else static_cast<float*>(Cv)[off] = 0.0f;
+      }
     }
   }
 
@@ -506,7 +529,8 @@ cudaError_t launch_tc_t(const float* X, const float* Y, void* C, const GemmCBloc
     grid = sms;
   }
   const unsigned g = static_cast<unsigned>(std::min<int64_t>(ntiles, grid));
-  kern<<<g, kTcThreads, kTcSmemBytes, s>>>(X, Y, C, cb, pr, tiles, ntiles, nz_begin, passes, kc, partial, status);
+  kern<<<g, kTcAllThreads, kTcSmemBytes, s>>>(X, Y, C, cb, pr, tiles, ntiles, nz_begin, passes, kc, partial,
+                                               status);
   return cudaGetLastError();
 }
 
