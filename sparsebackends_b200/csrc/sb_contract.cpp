@@ -368,7 +368,9 @@ struct GemmPlan {
   void launch(Ctx* ctx, const double* X, const double* Y, double* C, bool xT, bool yT) {
     prepare(ctx, xT, yT).run(ctx, X, Y, C);
   }
-  GemmLaunch prepare(Ctx* ctx, bool xT, bool yT) {
+  // f32mask: bit 0 = X, bit 1 = Y, bit 2 = C hold FP32 values (FP32-stored
+  // tensors); the thin kernel takes them only as its long operand and result.
+  GemmLaunch prepare(Ctx* ctx, bool xT, bool yT, int f32mask = 0) {
     GemmLaunch g;
     g.xT = xT;
     g.yT = yT;
@@ -391,7 +393,13 @@ struct GemmPlan {
     // (ragged chi=1024 H_eff: 0.11 ms against 0.20 ms per MPO step).
     const bool skinny_n = Kmax <= 16 && N <= 16;
     const bool skinny_m = Kmax <= 16 && M <= 16;
-    if ((skinny_n || skinny_m) && ctx->gemm_tile < 0 && ctx->gemm_thin != 0) {
+    bool thin_types = true;
+    if (f32mask != 0) {  // FP32 values: persistent thin kernel only (it needs a pair in every C block)
+      for (auto& c : cbs) thin_types = thin_types && c.pair_end > c.pair_begin;
+      const bool long_f32 = (f32mask >> (skinny_m ? 1 : 0)) & 1, short_f32 = (f32mask >> (skinny_m ? 0 : 1)) & 1;
+      thin_types = thin_types && long_f32 == ((f32mask >> 2) & 1) && !short_f32 && ctx->gemm_thin != 1;
+    }
+    if ((skinny_n || skinny_m) && ctx->gemm_tile < 0 && ctx->gemm_thin != 0 && thin_types) {
       const bool small_rows = skinny_m;
       std::vector<int> group;
       const bool interleaved = group_shared_long(small_rows, group);
@@ -1396,7 +1404,9 @@ void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0
       else gp.add_pair(yb, xa, d.k, d.k, d.m);
     }
   }
-  GemmLaunch g = athenb ? gp.prepare(ctx, false, false) : gp.prepare(ctx, true, true);
+  const int f32mask = athenb ? (A->f32 ? 1 : 0) | (B->f32 ? 2 : 0) | (C.f32 ? 4 : 0)
+                              : (B->f32 ? 1 : 0) | (A->f32 ? 2 : 0) | (C.f32 ? 4 : 0);
+  GemmLaunch g = athenb ? gp.prepare(ctx, false, false, f32mask) : gp.prepare(ctx, true, true, f32mask);
   if (athenb) g.run_io(ctx, *A, *B, C);
   else g.run_io(ctx, *B, *A, C);
   if (cache) {

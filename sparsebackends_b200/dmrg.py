@@ -98,10 +98,16 @@ def _host(t):
 class DMRG:
     """Two-site DMRG of the XXZ chain on ``n`` sites from the Néel state."""
 
-    def __init__(self, n: int, delta: float = 1.0, ctx=None):
+    def __init__(self, n: int, delta: float = 1.0, ctx=None, precision: str = "f64"):
+        """``precision``: the H_eff applies inside Lanczos run in that context
+        precision ("tf32x3": tcgen05 3xTF32 with FP32 intermediates); the
+        Lanczos vectors, orthogonalisation, the split and the environments stay
+        FP64, and each bond's energy is the FP64 Rayleigh quotient of its Ritz
+        vector (``krylov.eigsolve(..., correction=)``)."""
         import sparsebackends_b200 as sb
         self.sb = sb
         self.ctx = ctx or sb.default_context()
+        self.precision = precision
         self.n = n
         self.W = mpo_tensor(self.ctx, delta)
         self.sites, self.bonds = neel_state(self.ctx, n)
@@ -133,8 +139,11 @@ class DMRG:
     def _update(self, i: int, absorb: str, maxdim: int, cutoff: float, krylovdim: int, maxiter: int):
         from . import krylov
         lay, x = self._two_site(i)
-        op = qn.HeffOperator(lay, self.Lenv[i - 1], self.W, self.W, self.Renv[i + 1], self.ctx)
-        vals, vecs, _ = krylov.eigsolve(op, x, 1, "SR", krylovdim=krylovdim, maxiter=maxiter, tol=1e-14)
+        ops = (lay, self.Lenv[i - 1], self.W, self.W, self.Renv[i + 1], self.ctx)
+        op = qn.HeffOperator(*ops, precision=self.precision)
+        corr = qn.HeffOperator(*ops) if self.precision != "f64" else None
+        vals, vecs, _ = krylov.eigsolve(op, x, 1, "SR", krylovdim=krylovdim, maxiter=maxiter, tol=1e-14,
+                                        correction=corr, optol=op.accuracy)
         self.energy = float(vals[0])
         (ak, ad, ae), (bk, bd, be), link, _, err = qn.split_two_site(lay, *_host(vecs[0]), maxdim=maxdim,
                                                                    cutoff=cutoff, absorb=absorb)

@@ -28,6 +28,15 @@ algorithm (KrylovKit ``src/eigsolve/lanczos.jl`` and
 
 The operator ``A`` maps a vector to a new vector with the same block layout
 (``qn.HeffOperator`` wraps the two-site H_eff chain that way).
+
+Mixed precision: ``A`` may run its block GEMMs on the tensor cores (3xTF32,
+``HeffOperator(..., precision="tf32x3")``) while every Lanczos vector,
+inner product, norm and the tridiagonal eigenproblem stay FP64.  With
+``correction`` (the same operator in FP64) each returned Ritz vector x gets
+one FP64 apply: its value becomes the FP64 Rayleigh quotient <x, A x>/<x, x>
+and ``info.residuals`` the FP64 residual norms |A x - E x| / |x|, so the
+energy carries the tensor-core error only at second order in the vector's
+error.
 """
 from __future__ import annotations
 
@@ -109,12 +118,19 @@ def _combine(V: List["sb._Tensor"], c: np.ndarray):
 
 
 def eigsolve(A: Callable, x0, howmany: int = 1, which: str = "SR", *, krylovdim: int = 30, maxiter: int = 100,
-             tol: float = 1e-12, eta: float = ETA, ishermitian: bool = True):
+             tol: float = 1e-12, eta: float = ETA, ishermitian: bool = True, correction: Callable = None,
+             optol: float = 0.0):
     """``eigsolve(A, x0, howmany, which; ishermitian=true, krylovdim, maxiter, tol)``.
 
     Returns (values, vectors, info) like KrylovKit: ``values[i]`` and device
     tensors ``vectors[i]`` for the ``howmany`` selected Ritz pairs (more when
-    more converged), and a ConvergenceInfo."""
+    more converged), and a ConvergenceInfo.  ``correction``: an FP64 operator
+    for the residual correction of the returned pairs (module docstring).
+    ``optol``: relative accuracy of ``A`` (0 for FP64); a new residual norm
+    below ``optol`` times the largest recurrence coefficient so far is the
+    operator's rounding noise, so the Krylov space counts as invariant, as a
+    residual below ``tol`` does (a tensor-core operator on a space smaller
+    than ``krylovdim`` would otherwise expand it with noise vectors)."""
     if not ishermitian:
         raise NotImplementedError("only the Hermitian (Lanczos) eigensolver is provided")
     if which not in _SELECT:
@@ -148,6 +164,9 @@ def eigsolve(A: Callable, x0, howmany: int = 1, which: str = "SR", *, krylovdim:
     while True:
         beta = betas[-1]
         K = len(V)
+        scale = max(max(abs(a) for a in alphas), max(betas))
+        if optol > 0.0 and beta <= optol * scale:
+            beta = 0.0  # numerically invariant for the operator's accuracy
         if beta <= tol and K < howmany:
             howmany = K
         if K == krylovdim or beta <= tol:
@@ -199,4 +218,13 @@ def eigsolve(A: Callable, x0, howmany: int = 1, which: str = "SR", *, krylovdim:
     values = [float(x) for x in D[:howmany]]
     vectors = [_combine(V, U[:, i]) for i in range(howmany)]
     normres = [abs(float(f[i])) for i in range(howmany)]
-    return values, vectors, ConvergenceInfo(converged, normres, numiter, numops)
+    info = ConvergenceInfo(converged, normres, numiter, numops)
+    if correction is not None:
+        for i, x in enumerate(vectors):
+            y = correction(x)
+            xx = sb.dot(x, x)
+            e = sb.dot(x, y) / xx
+            sb.axpy_(-e, x, y)
+            info.residuals.append(float(np.sqrt(max(sb.dot(y, y), 0.0) / xx)))
+            values[i] = float(e)
+    return values, vectors, info

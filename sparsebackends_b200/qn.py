@@ -365,28 +365,58 @@ class HeffOperator:
     each call runs the contraction chain and copies the result out of the
     chain's reused output buffer."""
 
-    def __init__(self, layout: HeffLayout, L, W1, W2, R, ctx=None, graph_like=None, w12: bool = False):
+    def __init__(self, layout: HeffLayout, L, W1, W2, R, ctx=None, graph_like=None, w12: bool = False,
+                 precision: str = "f64", f32_intermediates: bool = None):
         """With ``graph_like`` (a vector with the layout of the inputs to come)
         the chain is captured once as a CUDA graph on a private input buffer;
         each call copies its input there and replays the graph.  ``w12`` picks
-        the chain ψ·L·(W1·W2)·R (``HeffChain``)."""
+        the chain ψ·L·(W1·W2)·R (``HeffChain``).  ``precision``: the context
+        precision the chain's block GEMMs run in (``Context.set_precision``;
+        set for each apply and restored after it); in a tensor-core precision
+        the intermediates are FP32 unless ``f32_intermediates`` is False."""
         import sparsebackends_b200 as sb
         self.sb = sb
-        self.chain = HeffChain(layout, ctx, w12=w12)
+        self.ctx = ctx or L.ctx
+        self.precision = precision
+        # relative accuracy of one apply (krylov.eigsolve's optol): measured
+        # per-block errors of the tensor-core GEMMs are a few 1e-7 to 1e-6
+        # (3xTF32) and 3e-4 (TF32); the bound leaves a margin
+        self.accuracy = {"f64": 0.0, "tf32x3": 1e-5, "tf32": 3e-2}[precision]
+        if f32_intermediates is None:
+            f32_intermediates = precision != "f64"
+        self.chain = HeffChain(layout, self.ctx, w12=w12, f32_intermediates=f32_intermediates)
         self.ops = (L, W1, W2, R)
         self.calls = 0
         self.graph = None
         if graph_like is not None:
             self.x = sb.copy(graph_like)
-            self.graph = self.chain.capture(self.x, *self.ops)
+            prev = self._enter()
+            try:
+                self.graph = self.chain.capture(self.x, *self.ops)
+            finally:
+                self._leave(prev)
+
+    def _enter(self) -> str:
+        prev = self.ctx.precision
+        if prev != self.precision:
+            self.ctx.set_precision(self.precision)
+        return prev
+
+    def _leave(self, prev: str) -> None:
+        if prev != self.precision:
+            self.ctx.set_precision(prev)
 
     def __call__(self, psi):
         self.calls += 1
-        if self.graph is not None:
-            self.sb.map_(self.x, psi, self.sb.MAP_COPY)
-            self.graph.launch()
-            return self.sb.copy(self.chain.out["T4"])
-        return self.sb.copy(self.chain.apply(psi, *self.ops))
+        prev = self._enter()
+        try:
+            if self.graph is not None:
+                self.sb.map_(self.x, psi, self.sb.MAP_COPY)
+                self.graph.launch()
+                return self.sb.copy(self.chain.out["T4"])
+            return self.sb.copy(self.chain.apply(psi, *self.ops))
+        finally:
+            self._leave(prev)
 
 
 def contract_new(labelsC, n2C, A, labelsA, B, labelsB):
