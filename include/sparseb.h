@@ -361,13 +361,16 @@ SB_API sb_status sb_blocksparse_svd(sb_ctx* ctx, const sb_tensor* A, int ortho_r
  * written exactly once (no accumulation into prior C contents).
  * The caller passes device pointers for inputs and outputs and the plan in
  * host arrays; the function calls no cudaMalloc/cudaFree or any allocating
- * routine: the plan is copied into a static device array of 640 KiB that
+ * routine: the plan is copied into a static device array of 672 KiB that
  * every GPU loading the library holds until exit.
  * Limits: n_cblocks <= 4096 and c_pair_begin[n_cblocks] <= 16384; larger
  * plans are rejected with SB_ERR_INVALID_ARG and a message in err (if given).
- * The first call on a device resolves the array's device address (set-up);
- * make that first call before any stream capture.  All calls share the array:
- * calls that overlap on the GPU (e.g. on different streams) race.            */
+ * The first call on a device resolves the array's device address (set-up).
+ * A call on a stream that is capturing is rejected (SB_ERR_INVALID_ARG): the
+ * plan is copied from host memory at call time.  Negative offsets and
+ * leading dimensions below a block's contiguous extent are rejected too.
+ * All calls share the array: calls that overlap on the GPU (e.g. on
+ * different streams) race.                                                   */
 SB_API sb_status sb_block_gemm_f64_noalloc(void* stream, const double* d_X, const double* d_Y, double* d_C,
                                            int32_t n_cblocks, const int64_t* c_off, const int32_t* c_rows,
                                            const int32_t* c_cols, const int32_t* c_pair_begin,

@@ -6,6 +6,7 @@
 // straight across the pairs of one C block (the K loops of all pairs feeding a
 // C tile are concatenated), so one CTA owns one C tile and writes it once.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 
 #include "../../include/sparseb.h"
@@ -382,7 +383,7 @@ cudaError_t launch_t(const double* X, const double* Y, double* C, const GemmCBlo
   constexpr int threads = (BM / WM) * (BN / WN) * 32;
   constexpr int smem = TileLayout<BM, BN, XT, YT, BK, ST>::bytes();
   auto kern = k_gemm_f64<BM, BN, WM, WN, XT, YT, BK, ST>;
-  static unsigned long long configured = 0;  // one bit per device ordinal
+  static std::atomic<unsigned long long> configured{0};  // one bit per device ordinal (host threads may race)
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
@@ -390,7 +391,7 @@ cudaError_t launch_t(const double* X, const double* Y, double* C, const GemmCBlo
   if (!(configured & bit)) {
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    configured |= bit;
+    configured.fetch_or(bit);
   }
   if (ntiles <= 0) return cudaSuccess;
   if (splitk < 1 || ntiles * splitk > 0x7fffffffLL || (splitk > 1 && !partial)) return cudaErrorInvalidValue;
@@ -888,7 +889,7 @@ cudaError_t launch_edges_t(const double* X, const double* Y, double* C, const Ge
   constexpr int smem = std::max(std::max(TileLayout<64, 64, XT, YT>::bytes(), TileLayout<64, 32, XT, YT>::bytes()),
                                 TileLayout<32, 64, XT, YT>::bytes());
   auto kern = k_gemm_f64_edges<XT, YT>;
-  static unsigned long long configured = 0;  // one bit per device ordinal
+  static std::atomic<unsigned long long> configured{0};  // one bit per device ordinal (host threads may race)
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
@@ -896,7 +897,7 @@ cudaError_t launch_edges_t(const double* X, const double* Y, double* C, const Ge
   if (!(configured & bit)) {
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    configured |= bit;
+    configured.fetch_or(bit);
   }
   kern<<<static_cast<unsigned>(ntiles * splitk), kEdgeThreads, smem, s>>>(X, Y, C, cb, ncb, pr, splitk,
                                                                           static_cast<int32_t>(ntiles), partial);
@@ -950,7 +951,7 @@ cudaError_t launch_gemm_f64(const double* X, const double* Y, double* C,
 // device buffers live instead in this file-scope device array, which every GPU
 // that loads the library holds until process exit.  Limits: at most
 // kNoAllocMaxCBlocks output blocks and kNoAllocMaxPairs block pairs per call
-// (640 KiB of scratch).
+// (672 KiB of scratch).
 namespace {
 
 constexpr int kNoAllocMaxCBlocks = 4096;
@@ -963,7 +964,7 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 // Device address of g_noalloc_scratch per device ordinal, resolved once per
 // device (with that device current) by cudaGetSymbolAddress.
 constexpr int kMaxDevices = 64;
-void* g_scratch_addr[kMaxDevices] = {};
+std::atomic<void*> g_scratch_addr[kMaxDevices] = {};
 
 // Host staging of the plan; per thread so concurrent host threads do not share it.
 thread_local sb::GemmCBlock t_cblocks[kNoAllocMaxCBlocks];
@@ -1011,14 +1012,21 @@ extern "C" SB_API sb_status sb_block_gemm_f64_noalloc(void* stream, const double
     return noalloc_fail(SB_ERR_CUDA, "no usable current CUDA device");
   // One-time set-up on this device (the first call on a device must not be
   // inside a stream capture).
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) return noalloc_fail(SB_ERR_CUDA, cudaGetErrorString(e));
-    g_scratch_addr[dev] = p;
+  void* scratch = g_scratch_addr[dev].load();
+  if (!scratch) {
+    const cudaError_t e = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
+    if (e != cudaSuccess || !scratch) return noalloc_fail(SB_ERR_CUDA, cudaGetErrorString(e));
+    g_scratch_addr[dev].store(scratch);  // every thread resolves the same address
   }
-  auto* d_cb = static_cast<sb::GemmCBlock*>(g_scratch_addr[dev]);
-  auto* d_pr = reinterpret_cast<sb::GemmPair*>(static_cast<unsigned char*>(g_scratch_addr[dev]) +
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // The plan is copied from host arrays at call time, which a captured graph
+  // could not repeat: calls on a capturing stream are rejected.
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+    return noalloc_fail(SB_ERR_INVALID_ARG, "the stream is capturing (or cannot be queried); the plan copy reads "
+                                            "host memory at call time");
+  auto* d_cb = static_cast<sb::GemmCBlock*>(scratch);
+  auto* d_pr = reinterpret_cast<sb::GemmPair*>(static_cast<unsigned char*>(scratch) +
                                                kNoAllocMaxCBlocks * sizeof(sb::GemmCBlock));
 
   // Tile shape: same rule as the library's allocating path.
@@ -1044,11 +1052,17 @@ extern "C" SB_API sb_status sb_block_gemm_f64_noalloc(void* stream, const double
                                   static_cast<int32_t>(ntiles), static_cast<int32_t>(mt), c_rows[c], 0};
     ntiles += mt * nt;
   }
-  for (int32_t p = 0; p < n_pairs; ++p) {
-    if (K[p] < 1) return noalloc_fail(SB_ERR_INVALID_ARG, "pair K must be >= 1");
-    t_pairs[p] = sb::GemmPair{x_off[p], y_off[p], K[p], ldx[p], ldy[p], 0};
+  for (int32_t c = 0; c < n_cblocks; ++c) {
+    if (c_off[c] < 0) return noalloc_fail(SB_ERR_INVALID_ARG, "negative c_off");
+    for (int32_t p = c_pair_begin[c]; p < c_pair_begin[c + 1]; ++p) {
+      if (K[p] < 1) return noalloc_fail(SB_ERR_INVALID_ARG, "pair K must be >= 1");
+      if (x_off[p] < 0 || y_off[p] < 0) return noalloc_fail(SB_ERR_INVALID_ARG, "negative x_off or y_off");
+      // leading dimensions at least the contiguous extent of each operand block
+      if (ldx[p] < (x_trans ? K[p] : c_rows[c]) || ldy[p] < (y_trans ? c_cols[c] : K[p]))
+        return noalloc_fail(SB_ERR_INVALID_ARG, "ldx or ldy below the block's leading extent");
+      t_pairs[p] = sb::GemmPair{x_off[p], y_off[p], K[p], ldx[p], ldy[p], 0};
+    }
   }
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   // Every call rewrites the descriptors it uses; nothing in the scratch has to
   // start at zero.  Copies from pageable host memory return once the data is
   // staged, so the thread-local host arrays may be reused on the next call.
