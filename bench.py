@@ -138,16 +138,18 @@ def measured_hbm_gbs():
 
 # DRAM bytes (read + write) per launch from one ncu capture of this bench at the
 # given chi (--metrics dram__bytes_read.sum,dram__bytes_write.sum), averaged
-# over the captured launches of each kernel; see profiles/ for the commands.
+# over the captured launches of each kernel.  A constant of that capture (its
+# date below), not a measurement of this run: it goes stale when the kernel
+# changes.
 TRAFFIC = {
-    (2048, "k_gemm_f64"): (1121.8e6, "profiles/heff_chi2048_dram_traffic.md (mean of the psi*L and R*T3 launches)"),
-    (2048, "k_gemm_thin"): (1315.3e6, "profiles/heff_chi2048_dram_traffic.md (mean of the T1*W1 and T2*W2 launches)"),
+    (2048, "k_gemm_f64"): (1121.8e6, "ncu capture of 2026-12-03, mean of the psi*L and R*T3 launches"),
+    (2048, "k_gemm_thin"): (1315.3e6, "ncu capture of 2026-12-03, mean of the T1*W1 and T2*W2 launches"),
 }
 
 
 def traffic_per_launch(chi: int, kernel: str):
     t = TRAFFIC.get((chi, kernel))
-    return None if t is None else {"bytes": t[0], "source": t[1]}
+    return None if t is None else {"bytes": t[0], "source": t[1], "kind": "constant from a dated capture"}
 
 
 def cublas_block_lists(layout, steps: int = 10):
@@ -307,6 +309,55 @@ def fp64_peak_tflops():
     del a, b
     torch.cuda.empty_cache()
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def tf32_peak_tflops():
+    """Dense TF32 tensor-core rate: torch.matmul float32 with TF32 allowed, 8192^3, best of 10."""
+    import torch
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    try:
+        n = 8192
+        a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        for _ in range(2):
+            torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = math.inf
+        for _ in range(10):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch.matmul(a, b)
+            e.record()
+            e.synchronize()
+            best = min(best, s.elapsed_time(e))
+        del a, b
+        torch.cuda.empty_cache()
+        return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+
+
+def mixed_dmrg_energy(local: int):
+    """Two-site DMRG of the N = 12 Heisenberg chain in FP64 and with the
+    tensor-core (3xTF32) H_eff applies plus the FP64 Rayleigh-quotient
+    correction, same schedule; energies against each other and exact
+    diagonalisation of the 2Sz = 0 sector."""
+    import sparsebackends_b200 as sb
+    from sparsebackends_b200 import dmrg
+    n, sched = 12, [8, 16, 32, 64, 64]
+    out = {"model": f"Heisenberg chain N={n}, OBC, U(1) 2Sz=0, chi schedule {sched}, cutoff 1e-14, "
+                    "krylovdim 8, maxiter 3"}
+    for prec in ("f64", "tf32x3"):
+        t0 = time.perf_counter()
+        d = dmrg.DMRG(n, 1.0, sb.Context(local), precision=prec)
+        e, _ = d.run(sched, cutoff=1e-14, krylovdim=8, maxiter=3)
+        out[prec] = {"energy": e, "seconds": time.perf_counter() - t0}
+    exact = dmrg.exact_ground_energy(n, 1.0)
+    out["exact"] = exact
+    out["rel_diff_tf32x3_vs_f64"] = abs(out["tf32x3"]["energy"] - out["f64"]["energy"]) / abs(out["f64"]["energy"])
+    out["rel_err_f64_vs_exact"] = abs(out["f64"]["energy"] - exact) / abs(exact)
+    return out
 
 
 # ── the CPU baseline: the oracle port of the reference path ──────────────
@@ -531,6 +582,46 @@ def run_ours(args, world, rank, local):
     _, _, prof_w = timed(apply_w, args.steps, profile=True)
     value_w = replica_rate(world, args.steps, ms_w)
 
+    # ── mixed precision: the tiled steps on the tcgen05 tensor cores (3xTF32),
+    # FP32-stored intermediates, in both associations of the chain
+    ctx_mx = sb.Context(local)
+    ctx_mx.set_precision("tf32x3")
+    dev_mx = {n: sb.NewBlockSparseSorted(layout.dims[n], layout.n2[n], k, None, d, ctx=ctx_mx, block_dims=e)
+              for n, (k, d, e) in host_r.items()}
+    stream_mx = torch.cuda.ExternalStream(ctx_mx.stream)
+    mixed = {}
+    for name, w12 in (("psi_L_W1_W2_R", False), ("w12", True)):
+        ch = qn.HeffChain(layout, ctx_mx, w12=w12, f32_intermediates=True)
+        fn = (lambda c=ch: c.apply(dev_mx["psi"], dev_mx["L"], dev_mx["W1"], dev_mx["W2"], dev_mx["R"]))
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        barrier(world)
+        ctx_mx.synchronize()
+        s_m, e_m = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s_m.record(stream_mx)
+        for _ in range(args.steps):
+            fn()
+        e_m.record(stream_mx)
+        ctx_mx.synchronize()
+        barrier(world)
+        ms_m = reduce_max(s_m.elapsed_time(e_m), world)
+        ctx_mx.set_profiling(True)
+        for _ in range(args.steps):
+            fn()
+        ctx_mx.synchronize()
+        pm = {k: ctx_mx.profile(k) for k in ("gemm_tc", "gemm_thin", "other")}
+        ctx_mx.set_profiling(False)
+        ref_d = chain_r.out["T4"].data
+        got_d = ch.out["T4"].data
+        gb, rb = ch.out["T4"].blocks_by_key(), chain_r.out["T4"].blocks_by_key()
+        blk_err = max(float(np.linalg.norm(gb[k] - v) / max(np.linalg.norm(v), 1e-300)) for k, v in rb.items())
+        mixed[name] = {"value": replica_rate(world, args.steps, ms_m), "ms_per_step": ms_m / args.steps,
+                       "rel_err_vs_fp64": float(np.linalg.norm(got_d - ref_d) / np.linalg.norm(ref_d)),
+                       "max_block_rel_err_vs_fp64": blk_err,
+                       "kernel_ms_per_step": {k: v["ms"] / args.steps for k, v in pm.items()},
+                       "prof": pm}
+        del ch
+
     # ── end to end through the public API (pinned host psi in, H·psi out) ──
     lib = ctx._lib
 
@@ -704,6 +795,30 @@ def run_ours(args, world, rank, local):
 
     if rank != 0:
         return
+    tf32_peak = tf32_peak_tflops()
+    mx_energy = mixed_dmrg_energy(local)
+    tcp = mixed["w12"]["prof"]["gemm_tc"]
+    tc_alg = tcp["flops"] / (tcp["ms"] * 1e-3) / 1e12 if tcp["ms"] > 0 else 0.0
+    for m in mixed.values():
+        m.pop("prof")
+    mixed_line = {
+        "value": mixed["w12"]["value"], "unit": UNIT,
+        "form": "block GEMMs of psi*L and R*T3 on tcgen05 in 3xTF32 (TF32 hi/lo split of every operand, FP32 "
+                "accumulation in Kahan-summed chunks), MPO steps in FP64 arithmetic on FP32-stored intermediates; "
+                "association psi*L*(W1*W2)*R; Lanczos vectors, inner products and norms FP64",
+        "dtype": "tf32x3",
+        "ratio_vs_plain_fp64": mixed["w12"]["value"] / value,
+        "ratio_vs_plain_fp64_same_association": mixed["w12"]["value"] / value_w,
+        "forms": mixed,
+        "roofline": {"bound": "tensor", "kernel": "k_gemm_tc (tcgen05.mma kind::tf32, 128xN tiles, warp-specialized)",
+                     "achieved_tf32_ops": 3.0 * tc_alg, "peak": tf32_peak, "unit": "TFLOP/s",
+                     "frac": 3.0 * tc_alg / tf32_peak if tf32_peak else None,
+                     "achieved_algorithmic": tc_alg,
+                     "note": "three TF32 products per FP64 multiply-add (3xTF32); peak measured live: torch.matmul "
+                             "float32 with TF32 allowed, 8192^3, best of 10",
+                     "launches": tcp["launches"], "kernel_ms_per_step": tcp["ms"] / args.steps},
+        "dmrg_energy": mx_energy,
+    }
     g = prof["gemm"]
     achieved = g["flops"] / (g["ms"] * 1e-3) / 1e12 if g["ms"] > 0 else 0.0
     th = prof["gemm_thin"]
@@ -772,6 +887,7 @@ def run_ours(args, world, rank, local):
                 "serial": {"value": e2e_serial, "unit": UNIT,
                            "mode": "one request at a time: upload, apply, blocking read-back"}},
         "lanczos": lanczos,
+        "mixed_precision": mixed_line,
         "graph_replay": graph_leg,
         "gpu_launches": launches,
         "clocks": clocks,
