@@ -93,6 +93,21 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* st
   }
 }
 
+// The same wait for roles that sit out most of a k-tile (the drain warps):
+// between polls the warp sleeps, leaving its issue slots to the producers.
+__device__ __forceinline__ bool mbar_wait_idle(uint32_t bar, uint32_t parity, int* status) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (true) {
+    __nanosleep(256);
+    if (mbar_try(bar, parity)) return true;
+    if (global_ns() - t0 > kWaitNs) {
+      atomicExch(status, 1);
+      return false;
+    }
+  }
+}
+
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
@@ -399,7 +414,7 @@ __global__ void __launch_bounds__(kTcAllThreads, 1)
       for (int ch = 0; ch < nch; ++ch, ++cg) {
         const bool first = ch == 0, last = ch + 1 == nch;
         const uint32_t b = cg & 1;
-        if (!failed) failed = !mbar_wait(bar_accf0 + 8 * b, (cg >> 1) & 1, status);
+        if (!failed) failed = !mbar_wait_idle(bar_accf0 + 8 * b, (cg >> 1) & 1, status);
         tc_fence_after();
         const uint32_t acc = tmem + 128 * b;
         for (int col0 = 0; col0 < tl.nb; col0 += 32) {

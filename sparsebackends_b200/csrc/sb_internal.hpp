@@ -99,7 +99,7 @@ struct Ctx {
   int precision = SB_PRECISION_F64;
   // k-tiles (32 deep) per FP32 accumulation chunk of the tensor-core GEMM
   // (SPARSEB_TC_KC); chunks are summed with Kahan compensation.
-  int tc_kc = 16;
+  int tc_kc = 8;
   // SPARSEB_POISON_OUTPUT=1: contract! outputs are filled with NaN before the
   // kernels write them (a test aid that exposes unwritten elements).
   bool poison_output = false;
