@@ -182,3 +182,137 @@ def exact_ground_energy(n: int, delta: float = 1.0) -> float:
             H += c * M
     idx = [s for s in range(dim) if bin(s).count("1") == n // 2]
     return float(np.linalg.eigvalsh(H[np.ix_(idx, idx)])[0])
+
+
+# ── the single two-site H_eff of a canonical Heisenberg MPS (N = 16, chi = 64) ──
+
+# Sector dimension profile over |2Sz| of the part left of a link: the centre
+# link of N = 16 gets {4, 12, 32, 12, 4} on 2Sz = -4..4; every link keeps the
+# charges of this profile that its sites allow, each at most the sector's
+# Schmidt bound min(binom(b, .), binom(n - b, .)).
+CENTER_PROFILE = {0: 32, 1: 22, 2: 12, 3: 8, 4: 4}
+
+
+def profile_link(n: int, b: int) -> qn.U1Link:
+    """Link after b of n sites: charges Q = 2Sz of the first b sites."""
+    from math import comb
+    m = min(b, n - b)
+    charges, dims = [], []
+    for q in range(-m, m + 1, 2):
+        d = CENTER_PROFILE.get(abs(q), 0)
+        bound = min(comb(b, (b + q) // 2), comb(n - b, (n - b - q) // 2))
+        if d > 0 and bound > 0:
+            charges.append(q)
+            dims.append(min(d, bound))
+    return qn.U1Link(charges, dims)
+
+
+def _site_blocks(left: qn.U1Link, right: qn.U1Link, rng):
+    """Seeded N(0, 1) blocks of A[(ql, s, qr) | (ml, mr)] on every allowed key."""
+    out = {}
+    for il, ql in enumerate(left.charges):
+        for s in range(2):
+            q = ql + qn.PHYS[s]
+            if q in right.charges:
+                ir = right.index(q)
+                out[(il + 1, s + 1, ir + 1)] = rng.standard_normal((left.dims[il], right.dims[ir]))
+    return out
+
+
+def _bs_from_blocks(ctx, left, right, blocks):
+    import sparsebackends_b200 as sb
+    keys = sorted(blocks, key=lambda k: k[::-1])
+    data = np.concatenate([blocks[k].reshape(-1, order="F") for k in keys])
+    return sb.NewBlockSparseSorted((left.S, 2, right.S, left.D, right.D), 2, keys, None, data, ctx=ctx,
+                                   block_dims=[blocks[k].shape for k in keys])
+
+
+def _sector_qr(ctx, rows):
+    """QR of one charge sector through the library's blocksparse_left_qr
+    (ops_factorize.jl:8-43): ``rows`` = list of (s, matrix r_j x c) whose row
+    blocks stack to M (sum r_j rows, c columns), given as A[(l, r) | (1)]
+    (every row its own l, a unit tail).  Returns (the Q row blocks as (s,
+    r_j x k), R (k x c)), M = Q R."""
+    import sparsebackends_b200 as sb
+    M = np.vstack([m for _, m in rows])
+    nl, c = M.shape
+    keys = [(l + 1, r + 1) for r in range(c) for l in range(nl)]
+    data = np.array([M[l - 1, r - 1] for l, r in keys])
+    A = sb.NewBlockSparseSorted((nl, c, 1), 1, keys, None, data, ctx=ctx)
+    Q, R, lv, rv = sb.blocksparse_left_qr(A)
+    Rm = R.to_numpy()
+    k = Rm.shape[0]
+    qb = Q.blocks_by_key()
+    qfull = np.zeros((nl, k))
+    for l in lv:
+        qfull[l - 1] = np.asarray(qb[(l,)]).reshape(k)
+    Rfull = np.zeros((k, c))
+    Rfull[:, [r - 1 for r in rv]] = Rm
+    out, off = [], 0
+    for s, m in rows:
+        out.append((s, qfull[off: off + m.shape[0]]))
+        off += m.shape[0]
+    return out, Rfull
+
+
+def canonical_center_problem(ctx, n: int = 16, seed: int = 2026):
+    """The two-site H_eff problem of a Heisenberg chain at its centre bond:
+    links by ``profile_link`` (chi <= 64, centre {4, 12, 32, 12, 4}), seeded
+    N(0, 1) site tensors, sites 1..n/2-1 left-canonicalised and sites
+    n/2+2..n right-canonicalised by QR per charge sector (the library's
+    blocksparse_left_qr), L and R built from the boundaries by make_L / make_R,
+    and psi Gaussian on the flux-0 blocks of sites n/2, n/2+1, normalised.
+    Returns (layout, psi, L, W, R)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    links = [profile_link(n, b) for b in range(n + 1)]
+    sites = [_site_blocks(links[i], links[i + 1], rng) for i in range(n)]
+    c = n // 2  # centre bond between sites c and c+1 (1-based)
+    # left-canonicalise sites 1..c-1, absorbing R into the next site
+    for i in range(c - 1):
+        left, right = links[i], links[i + 1]
+        newdims = list(right.dims)
+        rs = {}
+        for ir, q in enumerate(right.charges):
+            rows = [(k[1], m) for k, m in sites[i].items() if k[2] == ir + 1]
+            if not rows:
+                continue
+            qrows, R = _sector_qr(ctx, rows)
+            for (s, qm), (k, _) in zip(qrows, [(k, m) for k, m in sites[i].items() if k[2] == ir + 1]):
+                sites[i][k] = qm
+            rs[ir] = R
+            newdims[ir] = R.shape[0]
+        for k in list(sites[i + 1]):
+            if k[0] - 1 in rs:
+                sites[i + 1][k] = rs[k[0] - 1] @ sites[i + 1][k]
+        links[i + 1] = qn.U1Link(list(right.charges), newdims)
+    # right-canonicalise sites n..c+2, absorbing R^T into the previous site
+    for i in range(n - 1, c, -1):
+        left = links[i]
+        newdims = list(left.dims)
+        rs = {}
+        for il, q in enumerate(left.charges):
+            items = [(k, m) for k, m in sites[i].items() if k[0] == il + 1]
+            if not items:
+                continue
+            # transposed: rows (mr, s), columns ml
+            qrows, R = _sector_qr(ctx, [(k[1], m.T) for k, m in items])
+            for (s, qm), (k, _) in zip(qrows, items):
+                sites[i][k] = qm.T
+            rs[il] = R
+            newdims[il] = R.shape[0]
+        for k in list(sites[i - 1]):
+            if k[2] - 1 in rs:
+                sites[i - 1][k] = sites[i - 1][k] @ rs[k[2] - 1].T
+        links[i] = qn.U1Link(list(left.charges), newdims)
+    W = mpo_tensor(ctx, 1.0)
+    L, R = boundary_envs(ctx)
+    for i in range(c - 1):
+        L = qn.make_L(L, _bs_from_blocks(ctx, links[i], links[i + 1], sites[i]), W)
+    for i in range(n - 1, c, -1):
+        R = qn.make_R(R, _bs_from_blocks(ctx, links[i], links[i + 1], sites[i]), W)
+    lay = qn.HeffLayout(links[c - 1], links[c + 1], MPO_LINK)
+    import sparsebackends_b200 as sb
+    keys, data, exts = qn.random_block_tensor(lay, "psi", rng, 1.0, ragged=True)
+    data = data / np.linalg.norm(data)
+    psi = sb.NewBlockSparseSorted(lay.dims["psi"], lay.n2["psi"], keys, None, data, ctx=ctx, block_dims=exts)
+    return lay, psi, L, W, R
