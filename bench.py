@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=60.0)
+    ap.add_argument("--leg", default="all", choices=["all", "mixed"],
+                    help="mixed: only the 3xTF32 tensor-core chain (psi*L*(W1*W2)*R, FP32 intermediates), "
+                         "a short case for kernel profiling; prints its own line, not the headline")
     return ap.parse_args()
 
 
@@ -362,7 +365,7 @@ def mixed_dmrg_energy(local: int):
 
 # ── the CPU baseline: the oracle port of the reference path ──────────────
 
-def cpu_matvec_rate(layout, host, budget_s: float, max_runs: int):
+def cpu_matvec_rate(layout, host, budget_s: float, max_runs: int, keep=None):
     from oracle import sparse_oracle as so
     from sparsebackends_b200 import qn
     t = {}
@@ -378,11 +381,13 @@ def cpu_matvec_rate(layout, host, budget_s: float, max_runs: int):
 
     runs, start = 0, time.perf_counter()
     while runs < max_runs:
-        one()
+        t4 = one()
         runs += 1
         if time.perf_counter() - start > budget_s:
             break
     el = time.perf_counter() - start
+    if keep is not None:
+        keep.append(t4)
     return runs / el, runs, el
 
 
@@ -765,6 +770,50 @@ def run_ours(args, world, rank, local):
         return {"chi": chi_s, "eager_matvec_per_s": replica_rate(world, steps, ms_e),
                 "graph_matvec_per_s": replica_rate(world, steps, ms_s)}
 
+    def centre_problem_leg(steps):
+        """The two-site H_eff at the centre bond of a canonical Heisenberg MPS
+        (N = 16, chi = 64, centre link {4, 12, 32, 12, 4}): the reference's
+        plain FP64 CPU matvec case, eager and replayed from a graph, against the
+        oracle's chain on the zero-padded operands."""
+        from sparsebackends_b200 import dmrg
+        lay1, psi1, L1, W1_, R1 = dmrg.canonical_center_problem(ctx)
+        a1 = (psi1, L1, W1_, W1_, R1)
+        ch = qn.HeffChain(lay1, ctx)
+        for _ in range(3):
+            ch.apply(*a1)
+        ms_e, _, _ = timed(lambda: ch.apply(*a1), steps)
+        chg = qn.HeffChain(lay1, ctx)
+        g1 = chg.capture(*a1)
+        for _ in range(3):
+            g1.launch()
+        ms_s, _, _ = timed(g1.launch, steps)
+        assert np.array_equal(chg.out["T4"].data, ch.out["T4"].data)
+        out = {"workload": "two-site H_eff matvec at the centre bond of a canonical Heisenberg MPS, N=16, "
+                           "chi=64 (centre link 2Sz=-4..4 at {4,12,32,12,4}; psi on links {8,22,22,8}), MPO w=5",
+               "eager_matvec_per_s": replica_rate(world, steps, ms_e),
+               "graph_matvec_per_s": replica_rate(world, steps, ms_s),
+               "gflop_per_matvec_algorithmic": qn.chain_flops(lay1, padded=False) / 1e9,
+               "l2": "inputs L2-resident (a few MB)"}
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            host1 = {}
+            for name, t in (("psi", psi1), ("L", L1), ("W1", W1_), ("W2", W1_), ("R", R1)):
+                u = sb.to_uniform(t)
+                host1[name] = (u.keys, np.array(u.data, copy=True))
+            last = []
+            rate, runs, el = cpu_matvec_rate(lay1, host1, 5.0, 400, keep=last)
+            got = sb.to_uniform(ch.out["T4"])
+            ref = last[-1]
+            assert got.keys == ref.keys
+            gb = got.blocks_by_key()
+            out["max_block_rel_err_vs_oracle"] = max(
+                float(np.linalg.norm(np.asarray(gb[k]) - v) / max(np.linalg.norm(v), 1e-300))
+                for k, v in ref.blocks_by_key().items())
+            out["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": blas_threads(), "kind": "port",
+                                   "sample": f"{runs} matvecs in {el:.1f} s, oracle chain on the uniform blocks"}
+        return out
+
+    centre_leg = centre_problem_leg(max(200, args.steps))
+
     graph_leg = {"value": replica_rate(world, args.steps, ms_g), "unit": UNIT,
                  "note": "the H_eff chain captured once (sb_ctx_capture_begin/end) and replayed with sb_graph_launch",
                  "small_chi": small_chi_rates(256, 200)}
@@ -889,17 +938,52 @@ def run_ours(args, world, rank, local):
         "lanczos": lanczos,
         "mixed_precision": mixed_line,
         "graph_replay": graph_leg,
+        "centre_bond_n16_chi64": centre_leg,
         "gpu_launches": launches,
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
 
 
+def run_mixed_only(args, world, rank, local):
+    """The 3xTF32 chain alone (W12 association, FP32 intermediates): warm-up
+    and timed steps on the device-resident operands of ``workload(chi)``."""
+    import torch
+    import sparsebackends_b200 as sb
+    from sparsebackends_b200 import qn
+    torch.cuda.set_device(local)
+    layout = workload(args.chi)
+    _, host_r = host_tensors(layout, args.seed, with_ragged=True)
+    ctx = sb.Context(local)
+    ctx.set_precision("tf32x3")
+    dev = {n: sb.NewBlockSparseSorted(layout.dims[n], layout.n2[n], k, None, d, ctx=ctx, block_dims=e)
+           for n, (k, d, e) in host_r.items()}
+    ch = qn.HeffChain(layout, ctx, w12=True, f32_intermediates=True)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    for _ in range(max(args.warmup, 3)):
+        ch.apply(dev["psi"], dev["L"], dev["W1"], dev["W2"], dev["R"])
+    barrier(world)
+    ctx.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    for _ in range(args.steps):
+        ch.apply(dev["psi"], dev["L"], dev["W1"], dev["W2"], dev["R"])
+    e.record(stream)
+    ctx.synchronize()
+    barrier(world)
+    ms = reduce_max(s.elapsed_time(e), world)
+    if rank == 0:
+        print(json.dumps({"leg": "mixed", "chi": args.chi, "steps": args.steps, "ms_per_step": ms / args.steps,
+                          "value": replica_rate(world, args.steps, ms), "unit": UNIT}), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     try:
-        if args.impl == "reference":
+        if args.impl == "ours" and args.leg == "mixed":
+            run_mixed_only(args, world, rank, local)
+        elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
             run_ours(args, world, rank, local)

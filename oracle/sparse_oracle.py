@@ -519,8 +519,36 @@ def _advance_run(keys: List[Key], i0: int, n: int, pos: List[int]) -> int:
     return i
 
 
+# Order in which the merge-join compares the join tuples of two keys.
+# "sorted" (default): from the last join axis down, the order the keys are
+# sorted in.  "reference": from the first join axis up, exactly as
+# ``_cmp_join_tuple`` (contract_bs_bs.jl:430-442) does; with two or more join
+# axes whose value sets differ between the operands that merge can skip matched
+# pairs, and this mode reproduces the reference's output there.
+JOIN_ORDER = "sorted"
+
+
+class join_order:
+    """Context manager: ``with join_order("reference"): so.contract(...)``."""
+
+    def __init__(self, mode: str):
+        _assert(mode in ("sorted", "reference"), f"unknown join order {mode!r}")
+        self.mode = mode
+
+    def __enter__(self):
+        global JOIN_ORDER
+        self.prev, JOIN_ORDER = JOIN_ORDER, self.mode
+        return self
+
+    def __exit__(self, *exc):
+        global JOIN_ORDER
+        JOIN_ORDER = self.prev
+        return False
+
+
 def _cmp_join(akey, bkey, posA, posB) -> int:
-    """``_cmp_join_tuple`` (contract_bs_bs.jl:430-442), with one correction.
+    """``_cmp_join_tuple`` (contract_bs_bs.jl:430-442), with one correction
+    unless ``JOIN_ORDER`` is "reference".
 
     The join axes are the last prefix axes of the permuted operands and keys
     are sorted column-major, so the last join axis is the most significant; the
@@ -528,7 +556,10 @@ def _cmp_join(akey, bkey, posA, posB) -> int:
     whose value sets differ between the operands its merge skips matched pairs.
     Comparing from the last join axis down keeps the merge consistent with the
     sort; wherever the reference's merge finds every match the two agree."""
-    for pa, pb in reversed(list(zip(posA, posB))):
+    pairs = list(zip(posA, posB))
+    if JOIN_ORDER == "sorted":
+        pairs.reverse()
+    for pa, pb in pairs:
         av, bv = akey[pa - 1], bkey[pb - 1]
         if av < bv:
             return -1

@@ -37,9 +37,9 @@ def xxz_terms(delta: float = 1.0):
             (4, 5, delta * SZ)]
 
 
-def mpo_tensor(ctx, delta: float = 1.0):
-    """W[(qwl, s', s, qwr) | (mwl, mwr)], ragged (every block at its channel-sector extents)."""
-    import sparsebackends_b200 as sb
+def mpo_blocks(delta: float = 1.0):
+    """Host blocks of W[(qwl, s', s, qwr) | (mwl, mwr)]: key -> matrix at the
+    key's channel-sector extents."""
     w = MPO_LINK
     blocks = {}
     for wl, wr, op in xxz_terms(delta):
@@ -51,6 +51,14 @@ def mpo_tensor(ctx, delta: float = 1.0):
                 k = (ql, sp + 1, s + 1, qr)
                 blk = blocks.setdefault(k, np.zeros((w.dims[ql - 1], w.dims[qr - 1])))
                 blk[ml - 1, mr - 1] += op[sp, s]
+    return blocks
+
+
+def mpo_tensor(ctx, delta: float = 1.0):
+    """W[(qwl, s', s, qwr) | (mwl, mwr)], ragged (every block at its channel-sector extents)."""
+    import sparsebackends_b200 as sb
+    w = MPO_LINK
+    blocks = mpo_blocks(delta)
     keys = sorted(blocks, key=lambda k: k[::-1])
     data = np.concatenate([blocks[k].reshape(-1, order="F") for k in keys])
     return sb.NewBlockSparseSorted((w.S, 2, 2, w.S, w.D, w.D), 2, keys, None, data, ctx=ctx,

@@ -430,6 +430,34 @@ def contract_new(labelsC, n2C, A, labelsA, B, labelsB):
     return sb.contract_(C, labelsC, A, labelsA, B, labelsB)
 
 
+# The three contract! calls of each environment update: (labels of the result,
+# its tail count, labels of the left operand, labels of the right operand).
+# make_L: E1 = L*A, E2 = E1*W, L' = E2*A;  make_R: F1 = R*B, F2 = F1*W, R' = F2*B.
+MAKE_L_STEPS = (
+    (["qlp", "qwl", "s1", "qr", "mr", "mlp", "mwl"], 3,
+     ["qlp", "qwl", "ql", "mlp", "mwl", "ml"], ["ql", "s1", "qr", "ml", "mr"]),
+    (["qlp", "qr", "s1p", "qwm", "mr", "mlp", "mwm"], 3,
+     ["qlp", "qwl", "s1", "qr", "mr", "mlp", "mwl"], ["qwl", "s1p", "s1", "qwm", "mwl", "mwm"]),
+    (["qrp", "qwm", "qr", "mrp", "mwm", "mr"], 3,
+     ["qlp", "qr", "s1p", "qwm", "mr", "mlp", "mwm"], ["qlp", "s1p", "qrp", "mlp", "mrp"]),
+)
+MAKE_R_STEPS = (
+    (["qrp", "qwm", "ql", "s1", "ml", "mrp", "mwm"], 3,
+     ["qrp", "qwm", "qr", "mrp", "mwm", "mr"], ["ql", "s1", "qr", "ml", "mr"]),
+    (["qrp", "ql", "s1p", "qwl", "ml", "mrp", "mwl"], 3,
+     ["qrp", "qwm", "ql", "s1", "ml", "mrp", "mwm"], ["qwl", "s1p", "s1", "qwm", "mwl", "mwm"]),
+    (["qlp", "qwl", "ql", "mlp", "mwl", "ml"], 3,
+     ["qrp", "ql", "s1p", "qwl", "ml", "mrp", "mwl"], ["qlp", "s1p", "qrp", "mlp", "mrp"]),
+)
+
+
+def _env_update(steps, E, A, W):
+    (c1, n1, la1, lb1), (c2, n2, la2, lb2), (c3, n3, la3, lb3) = steps
+    E1 = contract_new(c1, n1, E, la1, A, lb1)
+    E2 = contract_new(c2, n2, E1, la2, W, lb2)
+    return contract_new(c3, n3, E2, la3, A, lb3)
+
+
 def make_L(L, A, W):
     """Left environment update, ITensorMPS ``makeL!``: L' = L · A · W · Ā.
 
@@ -437,13 +465,7 @@ def make_L(L, A, W):
     A[(ql, ml), s, (qr, mr)] W[(qw, mw), s', s, (qw', mw')] A[(ql', ml'), s', (qr', mr')]
     as three ``contract!`` calls on the device (real tensors: Ā = A).  The
     result has the layout of the environments (labels q', qw, q | m', mw, m)."""
-    E1 = contract_new(["qlp", "qwl", "s1", "qr", "mr", "mlp", "mwl"], 3,
-                      L, ["qlp", "qwl", "ql", "mlp", "mwl", "ml"], A, ["ql", "s1", "qr", "ml", "mr"])
-    E2 = contract_new(["qlp", "qr", "s1p", "qwm", "mr", "mlp", "mwm"], 3,
-                      E1, ["qlp", "qwl", "s1", "qr", "mr", "mlp", "mwl"], W,
-                      ["qwl", "s1p", "s1", "qwm", "mwl", "mwm"])
-    return contract_new(["qrp", "qwm", "qr", "mrp", "mwm", "mr"], 3,
-                        E2, ["qlp", "qr", "s1p", "qwm", "mr", "mlp", "mwm"], A, ["qlp", "s1p", "qrp", "mlp", "mrp"])
+    return _env_update(MAKE_L_STEPS, L, A, W)
 
 
 def make_R(R, B, W):
@@ -451,13 +473,7 @@ def make_R(R, B, W):
 
     R'[(ql', ml'), (qw, mw), (ql, ml)] = sum R[(qr', mr'), (qw', mw'), (qr, mr)]
     B[(ql, ml), s, (qr, mr)] W[(qw, mw), s', s, (qw', mw')] B[(ql', ml'), s', (qr', mr')]."""
-    F1 = contract_new(["qrp", "qwm", "ql", "s1", "ml", "mrp", "mwm"], 3,
-                      R, ["qrp", "qwm", "qr", "mrp", "mwm", "mr"], B, ["ql", "s1", "qr", "ml", "mr"])
-    F2 = contract_new(["qrp", "ql", "s1p", "qwl", "ml", "mrp", "mwl"], 3,
-                      F1, ["qrp", "qwm", "ql", "s1", "ml", "mrp", "mwm"], W,
-                      ["qwl", "s1p", "s1", "qwm", "mwl", "mwm"])
-    return contract_new(["qlp", "qwl", "ql", "mlp", "mwl", "ml"], 3,
-                        F2, ["qrp", "ql", "s1p", "qwl", "ml", "mrp", "mwl"], B, ["qlp", "s1p", "qrp", "mlp", "mrp"])
+    return _env_update(MAKE_R_STEPS, R, B, W)
 
 
 class HeffChain:
