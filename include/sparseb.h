@@ -110,7 +110,8 @@ SB_API sb_status sb_ctx_set_profiling(sb_ctx* ctx, int enable);
  * kind 0 = tiled block GEMM (with its split-K reduction), 1 = permute,
  * 2 = outer-product accumulation, 3 = segmented axpy, 4 = other (QR/SVD,
  * gathers), 5 = vector-space operations, 6 = thin block GEMM (K <= 16),
- * 7 = tensor-core (tcgen05) block GEMM.
+ * 7 = tensor-core (tcgen05) block GEMM, 8 = packing of its operands (TF32
+ * hi/lo split into the tensor core's shared-memory image layout).
  * Synchronises the context stream.                                           */
 SB_API sb_status sb_ctx_profile_summary(sb_ctx* ctx, int kind, int64_t* launches, double* total_ms,
                                         double* flops, double* bytes);

@@ -116,7 +116,7 @@ class Context:
         return int(self._lib.sb_ctx_launch_count(self._h))
 
     PROFILE_KINDS = {"gemm": 0, "permute": 1, "outer": 2, "axpy": 3, "other": 4, "vector": 5, "gemm_thin": 6,
-                     "gemm_tc": 7}
+                     "gemm_tc": 7, "tc_pack": 8}
 
     PRECISIONS = {"f64": 0, "tf32x3": 1, "tf32": 2}
 

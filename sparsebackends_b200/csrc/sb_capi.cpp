@@ -611,7 +611,7 @@ sb_status sb_tensor_export_dense(sb_ctx* ctx, const sb_tensor* t, double* data) 
 sb_status sb_tensor_device_data(const sb_tensor* t, double** d_ptr, int64_t* len) {
   return guard(t ? t->owner : nullptr, [&] {
     check_t(t);
-    ++t->impl->version;  // the caller may write through the pointer
+    t->impl->version = next_version();  // the caller may write through the pointer
     if (d_ptr) *d_ptr = t->impl->data.d();
     if (len) *len = t->impl->payload_len();
   });
@@ -767,7 +767,7 @@ sb_status sb_tensor_scale(sb_ctx* ctx, sb_tensor* A, double alpha) {
     check_ctx(ctx);
     check_t(A);
     SB_CK(cudaSetDevice(ctx->impl.device));
-    ++A->impl->version;
+    A->impl->version = next_version();
     tensor_scale(&ctx->impl, *A->impl, alpha);
   });
 }
@@ -777,7 +777,7 @@ sb_status sb_tensor_fill(sb_ctx* ctx, sb_tensor* A, double x) {
     check_ctx(ctx);
     check_t(A);
     SB_CK(cudaSetDevice(ctx->impl.device));
-    ++A->impl->version;
+    A->impl->version = next_version();
     tensor_fill(&ctx->impl, *A->impl, x);
   });
 }
@@ -788,7 +788,7 @@ sb_status sb_tensor_map(sb_ctx* ctx, sb_tensor* R, const sb_tensor* A, int op, d
     check_t(R);
     check_t(A);
     SB_CK(cudaSetDevice(ctx->impl.device));
-    ++R->impl->version;
+    R->impl->version = next_version();
     tensor_map(&ctx->impl, *R->impl, *A->impl, op, alpha, beta);
   });
 }

@@ -237,7 +237,7 @@ struct CKeys {
 // payload buffer is kept when its size does not change: every element of it
 // is rewritten by the kernel that follows.
 void reset_output(Ctx* ctx, Tensor& C, int64_t nkeys, int64_t payload) {
-  ++C.version;
+  C.version = next_version();
   C.keys.clear();
   C.alias_ids.clear();
   C.nkeys = nkeys;
@@ -271,31 +271,75 @@ struct GemmLaunch {
   int32_t nz_begin = 0, nsplits = 0, nparts = 0;
   bool swap = false;
   int passes = 3, kc = 16;
-  int64_t x_len = 0, y_len = 0;  // elements of X and Y the pairs read (from offset 0)
+  // packed operand images (launch_tc_pack): descriptors of the A side (the
+  // 128-row side: Y with swap, else X) and of the B side, per-pair locations,
+  // image bytes, and the elements the packing reads
+  DevBuf dpk, dimg_a, dimg_b;
+  int64_t nimg_a = 0, nimg_b = 0, pack_a_bytes = 0, pack_b_bytes = 0, pack_a_elems = 0, pack_b_elems = 0;
+  // the images of the last call, reused while the operand's payload and
+  // version are unchanged (an environment across the matvecs of a solve);
+  // never inside a graph capture
+  mutable DevBuf pk_a, pk_b;
+  mutable const void* pk_a_src = nullptr;
+  mutable const void* pk_b_src = nullptr;
+  mutable uint64_t pk_a_ver = 0, pk_b_ver = 0;
   double flops = 0.0, bytes = 0.0;
   char desc[sizeof(Ctx::gemm_desc)] = "";
-  // Tensor-core launch on FP32 operands; C FP64 or FP32.
-  void run_tc(Ctx* ctx, const float* X, const float* Y, void* C, bool c_f64) const {
+  // Tensor-core launch: X and Y FP64 or FP32 arrays (versions 0 = unknown,
+  // packed every call), C FP64 or FP32.
+  void run_tc(Ctx* ctx, const void* X, bool x64, uint64_t xver, const void* Y, bool y64, uint64_t yver, void* C,
+              bool c_f64) const {
     require(ctx->tc_status.raw() != nullptr, SB_ERR_INVALID_ARG, "tensor-core GEMM without a status word");
     std::memcpy(ctx->gemm_desc, desc, sizeof(desc));
+    const void* A = swap ? Y : X;
+    const void* B = swap ? X : Y;
+    const bool a64 = swap ? y64 : x64, b64 = swap ? x64 : y64;
+    const uint64_t aver = swap ? yver : xver, bver = swap ? xver : yver;
+    DevBuf sa, sb;  // scratch images inside a capture
+    auto images = [&](DevBuf& cache, const void*& key, uint64_t& kver, DevBuf& scratch, const void* src, bool f64,
+                      uint64_t ver, const DevBuf& imgs, int64_t nimg, int64_t bytes, int64_t elems) -> const void* {
+      if (bytes == 0) return nullptr;
+      DevBuf* buf = &cache;
+      if (ctx->capturing) {
+        scratch = DevBuf(ctx, bytes);
+        buf = &scratch;
+      } else if (ver != 0 && key == src && kver == ver && cache.bytes() == static_cast<size_t>(bytes)) {
+        return cache.raw();
+      }
+      if (!ctx->capturing && cache.bytes() != static_cast<size_t>(bytes)) cache = DevBuf(ctx, bytes);
+      {
+        ProfScope ps(ctx, PROF_TC_PACK, 0.0,
+                     static_cast<double>(elems) * (f64 ? 8 : 4) + static_cast<double>(bytes) / (passes == 3 ? 1 : 2));
+        SB_CK(launch_tc_pack(src, f64, imgs.as<TcImage>(), nimg, buf->raw(), passes, ctx->stream));
+      }
+      ctx->note_launch();
+      if (!ctx->capturing) {
+        key = src;
+        kver = ver;
+      }
+      return buf->raw();
+    };
+    const void* pa = images(pk_a, pk_a_src, pk_a_ver, sa, A, a64, aver, dimg_a, nimg_a, pack_a_bytes, pack_a_elems);
+    const void* pb = images(pk_b, pk_b_src, pk_b_ver, sb, B, b64, bver, dimg_b, nimg_b, pack_b_bytes, pack_b_elems);
     DevBuf part;  // k-segment partial tiles of split tiles (stream-ordered scratch)
     if (nparts > 0) part = DevBuf(ctx, static_cast<size_t>(nparts) * 128 * 128 * sizeof(double));
     {
       ProfScope ps(ctx, PROF_GEMM_TC, flops, bytes);
-      SB_CK(launch_gemm_tc(X, Y, C, c_f64, dc.as<GemmCBlock>(), dp.as<GemmPair>(), dt.as<TcTile>(),
-                           static_cast<int32_t>(n), nz_begin, xT, yT, swap, passes, kc, part.d(),
+      SB_CK(launch_gemm_tc(pa, pb, C, c_f64, dc.as<GemmCBlock>(), dp.as<GemmPair>(), dpk.as<TcPack>(),
+                           dt.as<TcTile>(), static_cast<int32_t>(n), nz_begin, swap, passes, kc, part.d(),
                            dsplit.as<TcSplit>(), nsplits, ctx->tc_status.as<int>(), ctx->stream));
     }
     ctx->tc_launched = true;
     ctx->note_launch(nsplits > 0 ? 2 : 1);
   }
   // Operands and result as tensors: FP32-stored tensors (the intermediates of
-  // a tensor-core H_eff chain) go to the launches that read or write them,
-  // FP64 operands of a tensor-core launch through their FP32 copies.
+  // a tensor-core H_eff chain) go to the launches that read or write them;
+  // a tensor-core launch packs FP64 and FP32 operands alike.
   void run_io(Ctx* ctx, const Tensor& Xt, const Tensor& Yt, Tensor& Ct) const {
     if (kind == NONE) return;
     if (kind == TC) {
-      run_tc(ctx, f32_payload(ctx, Xt), f32_payload(ctx, Yt), Ct.data.raw(), !Ct.f32);
+      run_tc(ctx, Xt.payload(), !Xt.f32, Xt.owner().version, Yt.payload(), !Yt.f32, Yt.owner().version,
+             Ct.data.raw(), !Ct.f32);
       return;
     }
     if (kind == THIN) {
@@ -314,12 +358,7 @@ struct GemmLaunch {
   void run(Ctx* ctx, const double* X, const double* Y, double* C, bool long_f32 = false) const {
     if (kind == NONE) return;
     if (kind == TC) {
-      // FP32 copies of the operand ranges the pairs read (no tensor to keep them with)
-      DevBuf x32(ctx, x_len * sizeof(float)), y32(ctx, y_len * sizeof(float));
-      SB_CK(launch_to_f32(X, x32.as<float>(), x_len, ctx->stream));
-      SB_CK(launch_to_f32(Y, y32.as<float>(), y_len, ctx->stream));
-      ctx->note_launch(2);
-      run_tc(ctx, x32.as<float>(), y32.as<float>(), C, true);
+      run_tc(ctx, X, true, 0, Y, true, 0, C, true);  // no tensors: packed every call
       return;
     }
     std::memcpy(ctx->gemm_desc, desc, sizeof(desc));
@@ -592,13 +631,55 @@ struct GemmPlan {
     g.swap = swap;
     g.passes = ctx->precision == SB_PRECISION_TF32 ? 1 : 3;
     g.kc = ctx->tc_kc;
-    for (size_t c = 0; c < cbs.size(); ++c)
-      for (int p = cbs[c].pair_begin; p < cbs[c].pair_end; ++p) {
-        const GemmPair& q = pairs[p];
-        const int64_t M = cbs[c].M, N = cbs[c].N, K = q.K;
-        g.x_len = std::max(g.x_len, q.x_off + (g.xT ? (M - 1) * q.ldx + K : (K - 1) * q.ldx + M));
-        g.y_len = std::max(g.y_len, q.y_off + (g.yT ? (K - 1) * q.ldy + N : (N - 1) * q.ldy + K));
+    // packed images: one set per distinct A-side block (128-row tiles) and per
+    // distinct B-side block (nbs-row tiles, nbs as in the item geometry), each
+    // with the block's k-tiles; a block that several C blocks read is packed once
+    {
+      const bool akc = swap ? !g.yT : g.xT;  // A side K-contiguous
+      const bool bkc = swap ? g.xT : !g.yT;
+      std::vector<TcPack> pk(pairs.size(), TcPack{0, 0, 0, 0});
+      std::vector<TcImage> ia, ib;
+      struct Seen { int64_t base, K, ld; };
+      std::unordered_map<int64_t, Seen> sa, sb;
+      auto add = [&](std::unordered_map<int64_t, Seen>& seen, std::vector<TcImage>& out, int64_t& total,
+                     int64_t& elems, int64_t off, int64_t ld, int64_t K, int64_t rows, int64_t tile, bool kc) -> int64_t {
+        auto it = seen.find(off);
+        if (it != seen.end()) {
+          require(it->second.K == K && it->second.ld == ld, SB_ERR_ASSERTION, "operand block packed twice differently");
+          return it->second.base;
+        }
+        const int64_t base = total, nkt = (K + 31) / 32, plane = tile * 128;
+        for (int64_t r0 = 0; r0 < rows; r0 += tile)
+          for (int64_t j = 0; j < nkt; ++j) {
+            const int64_t k0 = 32 * j;
+            out.push_back(TcImage{off + (kc ? r0 * ld + k0 : r0 + k0 * ld), ld, total,
+                                  static_cast<int32_t>(std::min(tile, rows - r0)),
+                                  static_cast<int32_t>(std::min<int64_t>(32, K - k0)), static_cast<int32_t>(plane),
+                                  kc ? 1 : 0});
+            elems += std::min(tile, rows - r0) * std::min<int64_t>(32, K - k0);
+            total += 2 * plane;
+          }
+        seen.emplace(off, Seen{base, K, ld});
+        return base;
+      };
+      for (size_t c = 0; c < cbs.size(); ++c) {
+        const int64_t ma = swap ? cbs[c].N : cbs[c].M, nbx = swap ? cbs[c].M : cbs[c].N;
+        const int64_t nbt = (nbx + kTcMaxN - 1) / kTcMaxN, nbs = up((nbx + nbt - 1) / nbt, 16);
+        for (int p = cbs[c].pair_begin; p < cbs[c].pair_end; ++p) {
+          const GemmPair& q = pairs[p];
+          const int64_t ab = add(sa, ia, g.pack_a_bytes, g.pack_a_elems, swap ? q.y_off : q.x_off,
+                                 swap ? q.ldy : q.ldx, q.K, ma, 128, akc);
+          const int64_t bb = add(sb, ib, g.pack_b_bytes, g.pack_b_elems, swap ? q.x_off : q.y_off,
+                                 swap ? q.ldx : q.ldy, q.K, nbx, nbs, bkc);
+          pk[p] = TcPack{ab, bb, static_cast<int32_t>((q.K + 31) / 32), static_cast<int32_t>(nbs)};
+        }
       }
+      g.dpk = upload(ctx, pk);
+      g.dimg_a = upload(ctx, ia);
+      g.dimg_b = upload(ctx, ib);
+      g.nimg_a = static_cast<int64_t>(ia.size());
+      g.nimg_b = static_cast<int64_t>(ib.size());
+    }
     g.flops = flops;
     g.bytes = bytes;
     std::snprintf(g.desc, sizeof(g.desc), "tcgen05 %s 128xN%s items:%lld split:%d", g.passes == 3 ? "3xtf32" : "tf32",

@@ -3,27 +3,34 @@
 // FP64 result.
 //
 // Same plan as the FP64 DMMA kernels (GemmCBlock / GemmPair: for every C block
-// C_c = sum over its pairs of X_p * Y_p).  Every FP32 operand value is split
-// on its way into shared memory:  x = hi + lo  with  hi = tf32(x) and
+// C_c = sum over its pairs of X_p * Y_p).  Every operand value (FP64 or FP32)
+// is rounded to FP32 and split  x = hi + lo  with  hi = tf32(x) and
 // lo = tf32(x - hi),  and each product is  a_hi*b_lo + a_lo*b_hi + a_hi*b_hi
 // (the lo*lo term is below FP32 rounding); single-pass TF32 keeps hi*hi.
-// FP64 operands are given to this kernel as FP32 copies (the host keeps them
-// per tensor), which keeps 24 of their bits, more than the 22 the split uses.
+//
+// Two kernels.  k_tc_pack converts every operand tile once: for each k-tile
+// (32 deep) of each 128-row tile of an A-side block and of each nbs-row tile
+// of a B-side block it writes the hi and lo planes in the exact layout the
+// tensor core reads from shared memory (K-major, 128-byte swizzle: row r of an
+// 8-row group at r*128 bytes, 16-byte chunk c at position c ^ r), so a tile
+// that several output tiles share is split once.  k_gemm_tc then moves those
+// images into shared memory with bulk asynchronous copies (cp.async.bulk
+// completing on an mbarrier, no thread work), which leaves the tensor core as
+// the only busy unit of the main loop.
 //
 // Roles.  tcgen05.mma computes D[m, n] = sum_k A[m, k] * B[n, k] with M = 128
 // rows of A (TMEM lanes) and N <= 128 rows of B (TMEM columns).  A tile is
 // (C block, 128 rows on the A side, nb rows on the B side).  Without SWAP the
 // A side is X (rows i of C) and the B side is Y^T (columns j of C); with SWAP
-// the roles exchange.
-//
-// Pipeline of one k-tile (32 deep): all 256 threads hold the FP32 elements
-// of the k-tile two ahead in registers (loads in flight across two k-tiles of
-// tensor-core work), split the current one and store 16-byte chunks into
-// K-major 128-byte-swizzled images (the canonical SWIZZLE_128B K-major operand
-// layout: row r of an 8-row group at r*128 bytes, 16-byte chunk c at position
-// c ^ r), in one of three stages.  After a proxy fence and a CTA barrier one
-// thread issues the MMAs of the k-tile and commits them to the stage's
-// mbarrier, which the threads wait on before they overwrite that stage.
+// the roles exchange.  Warp 0 (one thread) issues the copies of a k-tile into
+// one of three stages and arms the stage's "full" barrier with their byte
+// count; warp 1 (one thread) waits for it, issues the k-tile's MMAs into the
+// accumulator of the current chunk and commits them to the stage's "empty"
+// barrier (and, at a chunk's end, to the accumulator's "full" barrier);
+// warps 2-5 drain (each owns one quarter of the TMEM lanes, the rows of the A
+// side): they fold a finished chunk into the Kahan pair or write the item,
+// then arrive on the accumulator's "empty" barrier.  The three roles walk the
+// same sequence of items, k-tiles and chunks.
 //
 // Accumulation.  The tensor core accumulates in FP32 and its error grows with
 // the number of accumulation steps (measured: ~9e-5 relative over 17 000
@@ -37,6 +44,7 @@
 // that runs out sets *status = 1, and the CTA stops issuing MMAs and waiting,
 // so the kernel always returns and the host reports SB_ERR_TIMEOUT.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 
 #include "sb_kernels.hpp"
@@ -112,7 +120,6 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -181,55 +188,63 @@ __device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) 
   lo = l;
 }
 
-__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
-}
-
 // Byte offset of the 16-byte chunk c (k = 4c..4c+3) of row r in a K-major
 // SWIZZLE_128B image.
 __device__ __forceinline__ uint32_t img_off(int r, int c) {
   return static_cast<uint32_t>((r >> 3) * 1024 + (r & 7) * 128 + ((c ^ (r & 7)) << 4));
 }
 
-// Operand tile of 128 rows x 32 k: four chunks of four k values per thread.
-// K-contiguous sources (element (r, k) at r*ld + k): a warp covers 4 rows x 8
-// chunks; row-contiguous sources (at r + k*ld): a warp covers 32 consecutive
-// rows of one chunk, so each of its four loads reads 128 contiguous bytes.
-constexpr int kCH = 4;
-template <bool KC>
-__device__ __forceinline__ int map_row(int tid, int it) { return KC ? (tid >> 3) + 32 * it : tid & 127; }
-template <bool KC>
-__device__ __forceinline__ int map_chunk(int tid, int it) { return KC ? (tid & 7) : (tid >> 7) + 2 * it; }
-
-// Loads one k-tile of an operand: rows [0, rows) of the tile (the rest are
-// zero), k in [0, kv) from src (zero past kv).
-template <bool KC>
-__device__ __forceinline__ void load_tile(float (&r)[kCH][4], const float* __restrict__ src, int64_t ld, int rows,
-                                          int kv, int tid) {
-#pragma unroll
-  for (int it = 0; it < kCH; ++it) {
-    const int row = map_row<KC>(tid, it), c = map_chunk<KC>(tid, it);
-    const bool rv = row < rows;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int k = 4 * c + j;
-      const float* p = KC ? src + static_cast<int64_t>(row) * ld + k : src + row + static_cast<int64_t>(k) * ld;
-      r[it][j] = (rv && k < kv) ? __ldg(p) : 0.0f;
-    }
-  }
+// 16-byte global store (packed images).
+__device__ __forceinline__ void st_global_v4(void* p, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  asm volatile("st.global.v4.b32 [%0], {%1, %2, %3, %4};" ::"l"(p), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
 }
 
-template <bool KC>
-__device__ __forceinline__ void store_tile(const float (&r)[kCH][4], uint32_t s_hi, uint32_t s_lo, bool split,
-                                           int tid) {
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// Bulk asynchronous copy global -> this CTA's shared memory, completing
+// `bytes` of transaction count on the mbarrier (16-byte aligned addresses,
+// size a multiple of 16).
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
+// One packed k-tile image: rows [0, rows) x k [0, kv) of the operand tile at
+// src (element (r, k) at src + r*ld + k when kc, else src + r + k*ld), the rest
+// zero; hi plane at dst, lo plane at dst + plane (plane = image rows x 128 B).
+template <bool F64>
+__global__ void __launch_bounds__(256)
+    k_tc_pack(const void* __restrict__ srcv, const TcImage* __restrict__ imgs, int64_t nimg,
+              unsigned char* __restrict__ dst, int32_t passes) {
+  const int tid = static_cast<int>(threadIdx.x);
+  for (int64_t i = blockIdx.x; i < nimg; i += gridDim.x) {
+    const TcImage im = imgs[i];
+    const int rows_img = im.plane >> 7;
+    const int nchunks = rows_img * 8;
+    unsigned char* const d = dst + im.dst;
+    for (int ch = tid; ch < nchunks; ch += 256) {
+      // k-contiguous sources: consecutive threads take the chunks of one row;
+      // row-contiguous sources: consecutive rows of one chunk
+      const int r = im.kc ? ch >> 3 : ch % rows_img, c = im.kc ? ch & 7 : ch / rows_img;
+      uint32_t h[4], l[4];
 #pragma unroll
-  for (int it = 0; it < kCH; ++it) {
-    const uint32_t off = img_off(map_row<KC>(tid, it), map_chunk<KC>(tid, it));
-    uint32_t h[4], l[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) split_tf32(r[it][j], h[j], l[j]);
-    st_shared_v4(s_hi + off, h[0], h[1], h[2], h[3]);
-    if (split) st_shared_v4(s_lo + off, l[0], l[1], l[2], l[3]);
+      for (int j = 0; j < 4; ++j) {
+        const int k = 4 * c + j;
+        float x = 0.0f;
+        if (r < im.rows && k < im.kv) {
+          const int64_t e = im.src + (im.kc ? static_cast<int64_t>(r) * im.ld + k : r + static_cast<int64_t>(k) * im.ld);
+          x = F64 ? __double2float_rn(static_cast<const double*>(srcv)[e]) : static_cast<const float*>(srcv)[e];
+        }
+        split_tf32(x, h[j], l[j]);
+      }
+      const uint32_t off = img_off(r, c);
+      st_global_v4(d + off, h[0], h[1], h[2], h[3]);
+      if (passes == 3) st_global_v4(d + im.plane + off, l[0], l[1], l[2], l[3]);
+    }
   }
 }
 
@@ -239,28 +254,16 @@ struct Cursor {
   int t, p, k0, kt;
 };
 
-// Roles (13 warps).  Warps 0-7 produce: they load the FP32 operand values of
-// a k-tile (two k-tiles ahead, in registers), split them and store the hi/lo
-// images into one of three shared-memory stages, then arrive on the stage's
-// "full" barrier.  Warp 8 issues the MMAs: it waits for a full stage, issues
-// the k-tile's MMAs into the accumulator of the current chunk and commits
-// them to the stage's "empty" barrier (and, at a chunk's end, to the
-// accumulator's "full" barrier).  Warps 9-12 drain: each owns one quarter of
-// the TMEM lanes (rows of the A side); for a finished chunk they fold it into
-// the Kahan pair, or write the item, then arrive on the accumulator's "empty"
-// barrier so that the MMA warp can start the chunk after next in it.  The
-// three roles walk the same sequence of items, k-tiles and chunks.
-constexpr int kTcProducers = 256;  // warps 0-7 (the operand loads map 256 threads)
-constexpr int kTcMmaWarp = 8;
-constexpr int kTcEpiWarp0 = 9;     // warps 9-12
-constexpr int kTcAllThreads = 13 * 32;
+constexpr int kTcMmaWarp = 1;
+constexpr int kTcEpiWarp0 = 2;  // warps 2-5
+constexpr int kTcAllThreads = 6 * 32;
 
-template <bool SWAP, bool A_KC, bool B_KC, bool OUT64>
+template <bool SWAP, bool OUT64>
 __global__ void __launch_bounds__(kTcAllThreads, 1)
-    k_gemm_tc(const float* __restrict__ X, const float* __restrict__ Y, void* __restrict__ Cv,
-              const GemmCBlock* __restrict__ cblocks, const GemmPair* __restrict__ pairs,
-              const TcTile* __restrict__ tiles, int32_t ntiles, int32_t nz_begin, int32_t passes, int32_t kc,
-              double* __restrict__ partial, int* __restrict__ status) {
+    k_gemm_tc(const unsigned char* __restrict__ pack_a, const unsigned char* __restrict__ pack_b,
+              void* __restrict__ Cv, const GemmCBlock* __restrict__ cblocks, const GemmPair* __restrict__ pairs,
+              const TcPack* __restrict__ packs, const TcTile* __restrict__ tiles, int32_t ntiles, int32_t nz_begin,
+              int32_t passes, int32_t kc, double* __restrict__ partial, int* __restrict__ status) {
   extern __shared__ unsigned char smem_raw[];
   const int tid = static_cast<int>(threadIdx.x);
   const int warp = tid >> 5, lane = tid & 31;
@@ -279,7 +282,7 @@ __global__ void __launch_bounds__(kTcAllThreads, 1)
 
   if (tid == 0) {
     for (int s = 0; s < kTcStages; ++s) {
-      mbar_init(bar_full0 + 8 * s, kTcProducers);
+      mbar_init(bar_full0 + 8 * s, 1);  // the producer's arrive + the copies' bytes
       mbar_init(bar_empty0 + 8 * s, 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -298,62 +301,47 @@ __global__ void __launch_bounds__(kTcAllThreads, 1)
   tc_fence_after();
   const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(tmem_slot_ptr);
 
-  if (warp < kTcProducers / 32) {
-    // ── producers ─────────────────────────────────────────────────────────
-    bool failed = false;
-    auto first_of = [&](int t) -> Cursor {
-      if (t >= nz_begin) return Cursor{t, 0, 0, 0};
-      const TcTile tl = tiles[t];
-      return Cursor{t, tl.p0, tl.k0, 0};
-    };
-    auto advance = [&](Cursor c) -> Cursor {
-      if (c.t >= nz_begin) return c;
-      if (c.kt + 1 >= tiles[c.t].nkt) return first_of(c.t + grid);
-      if (c.k0 + kTcBK < pairs[c.p].K) return Cursor{c.t, c.p, c.k0 + kTcBK, c.kt + 1};
-      return Cursor{c.t, c.p + 1, 0, c.kt + 1};
-    };
-    auto load = [&](const Cursor& c, float (&ra)[kCH][4], float (&rb)[kCH][4]) {
-      const TcTile tl = tiles[c.t];
-      const GemmCBlock cb = cblocks[tl.cb];
-      const GemmPair pr = pairs[c.p];
-      const int ma = SWAP ? cb.N : cb.M, nbv = SWAP ? cb.M : cb.N;
-      const int kv = min(kTcBK, pr.K - c.k0);
-      const int64_t lda = SWAP ? pr.ldy : pr.ldx, ldb = SWAP ? pr.ldx : pr.ldy;
-      const float* pa = SWAP ? Y + pr.y_off : X + pr.x_off;
-      const float* pb = SWAP ? X + pr.x_off : Y + pr.y_off;
-      pa += A_KC ? static_cast<int64_t>(tl.a0) * lda + c.k0 : tl.a0 + static_cast<int64_t>(c.k0) * lda;
-      pb += B_KC ? static_cast<int64_t>(tl.b0) * ldb + c.k0 : tl.b0 + static_cast<int64_t>(c.k0) * ldb;
-      load_tile<A_KC>(ra, pa, lda, min(128, ma - tl.a0), kv, tid);
-      load_tile<B_KC>(rb, pb, ldb, min(tl.nb, nbv - tl.b0), kv, tid);
-    };
-    float ra0[kCH][4], rb0[kCH][4], ra1[kCH][4], rb1[kCH][4];
-    Cursor cur = first_of(static_cast<int>(blockIdx.x));
-    Cursor nxt = advance(cur);
-    if (cur.t < nz_begin) load(cur, ra0, rb0);
-    if (nxt.t < nz_begin) load(nxt, ra1, rb1);
-    uint32_t g = 0;
-    auto produce = [&](float (&ra)[kCH][4], float (&rb)[kCH][4], const Cursor& ahead2) {
-      const int s = static_cast<int>(g % kTcStages);
-      if (g >= kTcStages && !failed) failed = !mbar_wait(bar_empty0 + 8 * s, ((g / kTcStages) - 1) & 1, status);
-      const uint32_t sa_hi = base + s * kTcStageBytes, sa_lo = sa_hi + kTcImg;
-      const uint32_t sb_hi = sa_hi + 2 * kTcImg, sb_lo = sb_hi + kTcImg;
-      store_tile<A_KC>(ra, sa_hi, sa_lo, split, tid);
-      store_tile<B_KC>(rb, sb_hi, sb_lo, split, tid);
-      fence_proxy_async();
-      mbar_arrive(bar_full0 + 8 * s);
-      if (ahead2.t < nz_begin) load(ahead2, ra, rb);  // in flight during the next two k-tiles
-      ++g;
-    };
-    while (cur.t < nz_begin && !failed) {
-      const Cursor n2 = advance(nxt);
-      produce(ra0, rb0, n2);
-      cur = nxt;
-      nxt = n2;
-      if (cur.t >= nz_begin || failed) break;
-      const Cursor n3 = advance(nxt);
-      produce(ra1, rb1, n3);
-      cur = nxt;
-      nxt = n3;
+  if (warp == 0) {
+    // ── producer (one thread): bulk copies of the packed images ───────────
+    if (lane == 0) {
+      bool failed = false;
+      auto first_of = [&](int t) -> Cursor {
+        if (t >= nz_begin) return Cursor{t, 0, 0, 0};
+        const TcTile tl = tiles[t];
+        return Cursor{t, tl.p0, tl.k0, 0};
+      };
+      auto advance = [&](Cursor c) -> Cursor {
+        if (c.kt + 1 >= tiles[c.t].nkt) return first_of(c.t + grid);
+        if (c.k0 + kTcBK < pairs[c.p].K) return Cursor{c.t, c.p, c.k0 + kTcBK, c.kt + 1};
+        return Cursor{c.t, c.p + 1, 0, c.kt + 1};
+      };
+      uint32_t g = 0;
+      for (Cursor c = first_of(static_cast<int>(blockIdx.x)); c.t < nz_begin && !failed; c = advance(c), ++g) {
+        const int s = static_cast<int>(g % kTcStages);
+        if (g >= kTcStages) failed = !mbar_wait(bar_empty0 + 8 * s, ((g / kTcStages) - 1) & 1, status);
+        if (failed) break;
+        const TcTile tl = tiles[c.t];
+        const TcPack pk = packs[c.p];
+        const int j = c.k0 / kTcBK;  // k-tile of the pair
+        const unsigned char* ga =
+            pack_a + pk.a_base + (static_cast<int64_t>(tl.a0 >> 7) * pk.nkt + j) * (2 * kTcImg);
+        const int64_t bimg = 2LL * pk.nbs * 128;
+        const unsigned char* gb = pack_b + pk.b_base + (static_cast<int64_t>(tl.b0 / pk.nbs) * pk.nkt + j) * bimg;
+        const uint32_t bplane = static_cast<uint32_t>(tl.nb) * 128u;
+        const uint32_t sa = base + s * kTcStageBytes, sbh = sa + 2 * kTcImg;
+        const uint32_t full = bar_full0 + 8 * s;
+        mbar_expect_tx(full, split ? 2u * kTcImg + 2u * bplane : static_cast<uint32_t>(kTcImg) + bplane);
+        bulk_g2s(sa, ga, kTcImg, full);
+        bulk_g2s(sbh, gb, bplane, full);
+        if (split) {
+          bulk_g2s(sa + kTcImg, ga + kTcImg, kTcImg, full);
+          bulk_g2s(sbh + kTcImg, gb + pk.nbs * 128, bplane, full);
+        }
+      }
+      // copies still in flight land before the CTA exits: wait (bounded) for
+      // the last stages issued; consumed stages have completed already
+      for (uint32_t q = g > kTcStages ? g - kTcStages : 0; q < g; ++q)
+        mbar_wait(bar_full0 + 8 * (q % kTcStages), (q / kTcStages) & 1, status);
     }
   } else if (warp == kTcMmaWarp) {
     // ── MMA issue (one thread) ────────────────────────────────────────────
@@ -373,7 +361,7 @@ __global__ void __launch_bounds__(kTcAllThreads, 1)
           if (failed) break;
           tc_fence_after();
           const uint32_t acc = tmem + 128 * b;
-          const uint32_t sa_hi = base + s * kTcStageBytes, sa_lo = sa_hi + kTcImg;
+          const uint32_t sa_hi = base + s * kTcStageBytes, sa_lo = sa_hi + kTcImg;  // planes: A hi, A lo, B hi, B lo
           const uint32_t sb_hi = sa_hi + 2 * kTcImg, sb_lo = sb_hi + kTcImg;
 #pragma unroll
           for (int kk = 0; kk < kTcBK / 8; ++kk) {
@@ -525,27 +513,26 @@ __global__ void __launch_bounds__(kTcAllThreads, 1)
   }
 }
 
-template <bool SWAP, bool A_KC, bool B_KC, bool OUT64>
-cudaError_t launch_tc_t(const float* X, const float* Y, void* C, const GemmCBlock* cb, const GemmPair* pr,
-                        const TcTile* tiles, int32_t ntiles, int32_t nz_begin, int passes, int kc, double* partial,
-                        int* status, cudaStream_t s) {
-  auto kern = k_gemm_tc<SWAP, A_KC, B_KC, OUT64>;
-  static int grid_of[64] = {};  // one CTA per SM, per device ordinal
+template <bool SWAP, bool OUT64>
+cudaError_t launch_tc_t(const unsigned char* pa, const unsigned char* pb, void* C, const GemmCBlock* cb,
+                        const GemmPair* pr, const TcPack* packs, const TcTile* tiles, int32_t ntiles,
+                        int32_t nz_begin, int passes, int kc, double* partial, int* status, cudaStream_t s) {
+  auto kern = k_gemm_tc<SWAP, OUT64>;
+  static std::atomic<int> grid_of[64] = {};  // one CTA per SM, per device ordinal
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  int& grid = grid_of[dev & 63];
+  int grid = grid_of[dev & 63].load();
   if (grid == 0) {
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes);
     if (e != cudaSuccess) return e;
-    int sms = 0;
-    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    e = cudaDeviceGetAttribute(&grid, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    grid = sms;
+    grid_of[dev & 63].store(grid);
   }
   const unsigned g = static_cast<unsigned>(std::min<int64_t>(ntiles, grid));
-  kern<<<g, kTcAllThreads, kTcSmemBytes, s>>>(X, Y, C, cb, pr, tiles, ntiles, nz_begin, passes, kc, partial,
-                                               status);
+  kern<<<g, kTcAllThreads, kTcSmemBytes, s>>>(pa, pb, C, cb, pr, packs, tiles, ntiles, nz_begin, passes, kc,
+                                               partial, status);
   return cudaGetLastError();
 }
 
@@ -576,20 +563,41 @@ __global__ void k_tc_reduce(const double* __restrict__ partial, void* __restrict
 
 }  // namespace
 
-cudaError_t launch_gemm_tc_main(const float* X, const float* Y, void* C, bool c_f64, const GemmCBlock* d_cblocks,
-                                const GemmPair* d_pairs, const TcTile* d_tiles, int32_t ntiles, int32_t nz_begin,
-                                bool xT, bool yT, bool swap, int passes, int kc, double* d_partial, int* d_status,
-                                cudaStream_t s);
+cudaError_t launch_tc_pack(const void* src, bool src_f64, const TcImage* d_imgs, int64_t nimg, void* dst, int passes,
+                           cudaStream_t s) {
+  if (nimg <= 0) return cudaSuccess;
+  if (passes != 1 && passes != 3) return cudaErrorInvalidValue;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const unsigned g = static_cast<unsigned>(std::min<int64_t>(nimg, 8LL * sms));
+  if (src_f64)
+    k_tc_pack<true><<<g, 256, 0, s>>>(src, d_imgs, nimg, static_cast<unsigned char*>(dst), passes);
+  else
+    k_tc_pack<false><<<g, 256, 0, s>>>(src, d_imgs, nimg, static_cast<unsigned char*>(dst), passes);
+  return cudaGetLastError();
+}
 
-cudaError_t launch_gemm_tc(const float* X, const float* Y, void* C, bool c_f64, const GemmCBlock* d_cblocks,
-                           const GemmPair* d_pairs, const TcTile* d_tiles, int32_t ntiles, int32_t nz_begin,
-                           bool xT, bool yT, bool swap, int passes, int kc, double* d_partial,
+cudaError_t launch_gemm_tc(const void* pack_a, const void* pack_b, void* C, bool c_f64, const GemmCBlock* d_cblocks,
+                           const GemmPair* d_pairs, const TcPack* d_packs, const TcTile* d_tiles, int32_t ntiles,
+                           int32_t nz_begin, bool swap, int passes, int kc, double* d_partial,
                            const TcSplit* d_splits, int32_t nsplits, int* d_status, cudaStream_t s) {
   if (ntiles <= 0) return cudaSuccess;
   if ((passes != 1 && passes != 3) || kc < 1 || (nsplits > 0 && (!d_partial || !d_splits)))
     return cudaErrorInvalidValue;
-  cudaError_t e = launch_gemm_tc_main(X, Y, C, c_f64, d_cblocks, d_pairs, d_tiles, ntiles, nz_begin, xT, yT, swap,
-                                      passes, kc, d_partial, d_status, s);
+  const auto* pa = static_cast<const unsigned char*>(pack_a);
+  const auto* pb = static_cast<const unsigned char*>(pack_b);
+  cudaError_t e;
+  if (swap)
+    e = c_f64 ? launch_tc_t<true, true>(pa, pb, C, d_cblocks, d_pairs, d_packs, d_tiles, ntiles, nz_begin, passes, kc,
+                                        d_partial, d_status, s)
+              : launch_tc_t<true, false>(pa, pb, C, d_cblocks, d_pairs, d_packs, d_tiles, ntiles, nz_begin, passes,
+                                         kc, d_partial, d_status, s);
+  else
+    e = c_f64 ? launch_tc_t<false, true>(pa, pb, C, d_cblocks, d_pairs, d_packs, d_tiles, ntiles, nz_begin, passes,
+                                         kc, d_partial, d_status, s)
+              : launch_tc_t<false, false>(pa, pb, C, d_cblocks, d_pairs, d_packs, d_tiles, ntiles, nz_begin, passes,
+                                          kc, d_partial, d_status, s);
   if (e != cudaSuccess || nsplits <= 0) return e;
   if (swap) {
     if (c_f64) k_tc_reduce<true, true><<<nsplits, 256, 0, s>>>(d_partial, C, d_cblocks, d_splits);
@@ -598,41 +606,6 @@ cudaError_t launch_gemm_tc(const float* X, const float* Y, void* C, bool c_f64, 
     if (c_f64) k_tc_reduce<false, true><<<nsplits, 256, 0, s>>>(d_partial, C, d_cblocks, d_splits);
     else k_tc_reduce<false, false><<<nsplits, 256, 0, s>>>(d_partial, C, d_cblocks, d_splits);
   }
-  return cudaGetLastError();
-}
-
-cudaError_t launch_gemm_tc_main(const float* X, const float* Y, void* C, bool c_f64, const GemmCBlock* d_cblocks,
-                                const GemmPair* d_pairs, const TcTile* d_tiles, int32_t ntiles, int32_t nz_begin,
-                                bool xT, bool yT, bool swap, int passes, int kc, double* d_partial, int* d_status,
-                                cudaStream_t s) {
-  // A side K-contiguous: X with xT (no swap) or Y without yT (swap); B side the other operand
-  const bool akc = swap ? !yT : xT;
-  const bool bkc = swap ? xT : !yT;
-#define SB_TC(SW, AK, BK)                                                                                       \
-  if (swap == SW && akc == AK && bkc == BK)                                                                     \
-    return c_f64 ? launch_tc_t<SW, AK, BK, true>(X, Y, C, d_cblocks, d_pairs, d_tiles, ntiles, nz_begin, passes, \
-                                                  kc, d_partial, d_status, s)                                   \
-                 : launch_tc_t<SW, AK, BK, false>(X, Y, C, d_cblocks, d_pairs, d_tiles, ntiles, nz_begin, passes, \
-                                                   kc, d_partial, d_status, s);
-  SB_TC(false, false, false) SB_TC(false, false, true) SB_TC(false, true, false) SB_TC(false, true, true)
-  SB_TC(true, false, false) SB_TC(true, false, true) SB_TC(true, true, false) SB_TC(true, true, true)
-#undef SB_TC
-  return cudaErrorInvalidValue;
-}
-
-// FP32 copy of FP64 values (operands of the tensor-core GEMM).
-__global__ void k_to_f32(const double* __restrict__ src, float* __restrict__ dst, int64_t n) {
-  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x * 2;
-  for (int64_t i = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 2; i < n; i += stride) {
-    dst[i] = __double2float_rn(src[i]);
-    if (i + 1 < n) dst[i + 1] = __double2float_rn(src[i + 1]);
-  }
-}
-
-cudaError_t launch_to_f32(const double* src, float* dst, int64_t n, cudaStream_t s) {
-  if (n <= 0) return cudaSuccess;
-  const unsigned g = static_cast<unsigned>(std::min<int64_t>((n + 511) / 512, 148LL * 16));
-  k_to_f32<<<g, 256, 0, s>>>(src, dst, n);
   return cudaGetLastError();
 }
 

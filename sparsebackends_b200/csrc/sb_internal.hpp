@@ -57,7 +57,7 @@ class DevBuf {
 // Kernel classes reported by the in-library profiler.
 enum ProfKind : int {
   PROF_GEMM = 0, PROF_PERMUTE = 1, PROF_OUTER = 2, PROF_AXPY = 3, PROF_OTHER = 4, PROF_VECTOR = 5,
-  PROF_GEMM_THIN = 6, PROF_GEMM_TC = 7, PROF_NKINDS = 8
+  PROF_GEMM_THIN = 6, PROF_GEMM_TC = 7, PROF_TC_PACK = 8, PROF_NKINDS = 9
 };
 
 struct Ctx {
@@ -195,6 +195,9 @@ std::vector<T> download(Ctx* ctx, const void* dptr, size_t n) {
 
 enum Kind : int { DENSE = SB_KIND_DENSE, COO = SB_KIND_COO, BS = SB_KIND_BLOCKSPARSE, ALIASED = SB_KIND_ALIASED };
 
+// A fresh payload version, unique across all tensors of the process.
+uint64_t next_version();
+
 struct Tensor {
   Ctx* ctx = nullptr;
   Kind kind = DENSE;
@@ -228,12 +231,11 @@ struct Tensor {
   // path reads or writes such tensors (the intermediates of a TF32 H_eff
   // chain); every other kernel rejects them.
   bool f32 = false;
-  // Bumped by every library call that writes the payload (contract! output,
-  // vector-space updates, a device pointer handed out).  The FP32 copy of an
-  // FP64 payload used by the tensor-core GEMMs is kept while it matches.
-  uint64_t version = 0;
-  mutable DevBuf shadow;
-  mutable uint64_t shadow_version = ~0ull;
+  // Renewed (next_version) by every library call that writes the payload
+  // (contract! output, vector-space updates, a device pointer handed out);
+  // unique across tensors, so (payload, version) names the values.  The
+  // packed tensor-core images of an operand are kept while it matches.
+  uint64_t version = next_version();
 
   int N() const { return static_cast<int>(dims.size()); }
   int P() const { return N() - n2; }
@@ -306,11 +308,6 @@ void copy_blocks(Ctx* ctx, const double* src, double* dst, const std::vector<int
 void require_uniform(const Tensor& t, const char* what);
 // Rejects FP32-stored tensors on paths that only handle FP64 payloads.
 void require_f64(const Tensor& t, const char* what);
-// FP32 values of a tensor's payload at its own element offsets: the payload
-// itself for FP32 storage, else the owner's FP32 copy (made on first use and
-// kept while the owner's version is unchanged; always remade while a capture
-// is open, so that a replay converts the current values).
-const float* f32_payload(Ctx* ctx, const Tensor& t);
 void check_no_cross_perm(const std::vector<int>& perm1, int N, int P);
 bool is_identity(const std::vector<int>& perm1);
 

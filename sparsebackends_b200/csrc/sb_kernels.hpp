@@ -117,12 +117,31 @@ struct TcSplit {
   int32_t part0, nparts, pad0, pad1;
 };
 constexpr int kTcMaxN = 128;
-cudaError_t launch_gemm_tc(const float* X, const float* Y, void* C, bool c_f64, const GemmCBlock* d_cblocks,
-                           const GemmPair* d_pairs, const TcTile* d_tiles, int32_t ntiles, int32_t nz_begin,
-                           bool xT, bool yT, bool swap, int passes, int kc, double* d_partial,
+// Operands arrive packed (launch_tc_pack): per pair p, packs[p] locates the
+// images of its A-side block (a_base: 128-row tiles, nkt k-tiles each, 32 KB
+// per k-tile: hi plane then lo plane) and of its B-side block (b_base: tiles
+// of nbs rows, 2*nbs*128 bytes per k-tile); item rows a0 and b0 select the
+// tile (a0 / 128, b0 / nbs).
+struct TcPack {
+  int64_t a_base, b_base;
+  int32_t nkt, nbs;
+};
+cudaError_t launch_gemm_tc(const void* pack_a, const void* pack_b, void* C, bool c_f64, const GemmCBlock* d_cblocks,
+                           const GemmPair* d_pairs, const TcPack* d_packs, const TcTile* d_tiles, int32_t ntiles,
+                           int32_t nz_begin, bool swap, int passes, int kc, double* d_partial,
                            const TcSplit* d_splits, int32_t nsplits, int* d_status, cudaStream_t s);
-// dst[i] = (float)src[i], i < n (FP32 operand copies for launch_gemm_tc).
-cudaError_t launch_to_f32(const double* src, float* dst, int64_t n, cudaStream_t s);
+// One packed k-tile image of one operand tile: rows [0, rows) x k [0, kv)
+// (element (r, k) at src + r*ld + k when kc, else src + r + k*ld; elements of
+// the FP64 or FP32 operand array), zero elsewhere, written at byte dst as the
+// hi plane and (passes = 3) the lo plane plane bytes further; plane = image
+// rows x 128 bytes in the K-major 128-byte-swizzled layout the tensor core
+// reads.
+struct TcImage {
+  int64_t src, ld, dst;
+  int32_t rows, kv, plane, kc;
+};
+cudaError_t launch_tc_pack(const void* src, bool src_f64, const TcImage* d_imgs, int64_t nimg, void* dst, int passes,
+                           cudaStream_t s);
 
 // ── outer-product accumulation (K = 1 pairs) on CUDA cores ─────────────────
 //

@@ -4,6 +4,7 @@
 // src/coo/{storage,conversions}.jl, src/aliased/{storage,conversions}.jl.
 // Keys (integer metadata) live on the host; every payload value lives on and
 // is produced by the device.
+#include <atomic>
 #include <algorithm>
 #include <cstring>
 #include <numeric>
@@ -198,22 +199,9 @@ void require_f64(const Tensor& t, const char* what) {
                              "contract_shared! (BS x BS) and the exports only");
 }
 
-const float* f32_payload(Ctx* ctx, const Tensor& t) {
-  if (t.f32) return reinterpret_cast<const float*>(t.payload());
-  const Tensor& o = t.owner();
-  const int64_t n = o.payload_len();
-  if (n == 0) return nullptr;
-  if (!ctx->capturing && o.shadow.raw() && o.shadow_version == o.version &&
-      o.shadow.bytes() == static_cast<size_t>(n) * sizeof(float))
-    return o.shadow.as<const float>();
-  if (o.shadow.bytes() != static_cast<size_t>(n) * sizeof(float)) o.shadow = DevBuf(ctx, n * sizeof(float));
-  {
-    ProfScope ps(ctx, PROF_OTHER, 0.0, 12.0 * n);
-    SB_CK(launch_to_f32(o.payload(), o.shadow.as<float>(), n, ctx->stream));
-  }
-  ctx->note_launch();
-  o.shadow_version = ctx->capturing ? ~0ull : o.version;
-  return o.shadow.as<const float>();
+uint64_t next_version() {
+  static std::atomic<uint64_t> counter{0};
+  return counter.fetch_add(1, std::memory_order_relaxed) + 1;
 }
 
 void copy_blocks(Ctx* ctx, const double* src, double* dst, const std::vector<int64_t>& src_off,

@@ -213,3 +213,54 @@ def test_f32_tensors_rejected_outside_the_chain_kernels(sb, ctxs):
     Cref = so.contract(so.BS.empty((2, 2, 20, 10), 2), ["i", "j", "m", "n"], A, ["i", "q", "m", "k"], B,
                        ["q", "j", "k", "n"])
     check(C2, Cref, TOL_X3)
+
+
+def _pair(sb, ctx, seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    A = rand_bs(rng, (2, 3, 150, 90), 2)
+    B = rand_bs(rng, (3, 2, 90, 70), 2)
+    a = sb.NewBlockSparseSorted(A.dims, 2, A.keys, A.ids, A.data, ctx=ctx)
+    b = sb.NewBlockSparseSorted(B.dims, 2, B.keys, B.ids, B.data, ctx=ctx)
+    return a, b
+
+
+LC, LA, LB = ["i", "j", "m", "n"], ["i", "q", "m", "k"], ["q", "j", "k", "n"]
+
+
+def test_tc_packed_operands_follow_writes(sb, ctxs):
+    """The packed (split, swizzled) operand images are reused while an operand
+    is unchanged and rebuilt after a library call writes it: scaling A by 2 in
+    place doubles C exactly (the split of 2x is the split of x, doubled)."""
+    ctx = ctxs["tf32x3"]
+    a, b = _pair(sb, ctx, 31)
+    C = sb.NewBlockSparseSorted.empty((2, 2, 150, 70), 2, ctx=ctx)
+    sb.contract_(C, LC, a, LA, b, LB)
+    c1 = np.array(C.data, copy=True)
+    sb.contract_(C, LC, a, LA, b, LB)  # unchanged operands: cached images
+    assert np.array_equal(np.array(C.data), c1)
+    sb.scale_(a, 2.0)
+    sb.contract_(C, LC, a, LA, b, LB)
+    assert np.array_equal(np.array(C.data), 2.0 * c1)
+    sb.fill_(a, 0.0)
+    sb.contract_(C, LC, a, LA, b, LB)
+    ctx.synchronize()
+    assert not np.any(np.array(C.data))
+
+
+def test_tc_graph_replay_reads_current_values(sb, ctxs):
+    """A captured tensor-core contraction packs its operands inside the graph:
+    a replay after an in-place write of an operand uses the new values."""
+    ctx = ctxs["tf32x3"]
+    a, b = _pair(sb, ctx, 33)
+    C = sb.NewBlockSparseSorted.empty((2, 2, 150, 70), 2, ctx=ctx)
+    sb.contract_(C, LC, a, LA, b, LB)
+    c1 = np.array(C.data, copy=True)
+    g = ctx.capture(lambda: sb.contract_(C, LC, a, LA, b, LB), keep=(a, b, C))
+    g.launch()
+    ctx.synchronize()
+    assert np.array_equal(np.array(C.data), c1)
+    sb.scale_(b, 0.5)
+    g.launch()
+    ctx.synchronize()
+    assert np.array_equal(np.array(C.data), 0.5 * c1)
+    del g
