@@ -81,18 +81,18 @@ SB_API int64_t sb_ctx_launch_count(const sb_ctx* ctx);
  * reference runs in FP64).  Tensors stay FP64 unless created with
  * sb_tensor_create_bs_f32.
  *   SB_PRECISION_F64    FP64 tensor-core (DMMA) GEMMs, the drop-in (default);
- *   SB_PRECISION_TF32X3 tcgen05 tensor cores on FP32 copies of the operands,
- *                       every value split into TF32 hi + lo and the three
- *                       significant products summed in FP32 chunks that are
- *                       added with Kahan compensation (a few 1e-7 to 1e-6
- *                       relative per block);
+ *   SB_PRECISION_TF32X3 tcgen05 tensor cores: every operand value rounded
+ *                       to FP32 and split into TF32 hi + lo, the three
+ *                       significant products accumulated in FP32 chunks of
+ *                       kc k-tiles that are then added in FP32 (a few 1e-7 to
+ *                       a few 1e-6 relative per block);
  *   SB_PRECISION_TF32   tcgen05, one TF32 product (about 3e-4 relative).
  * Only the tiled GEMMs change; the K <= 16 (MPO) steps, outer products,
  * Kahan sums and axpys compute in FP64.  Operands must lie in FP32's range.
- * The FP32 copy of an FP64 operand is kept with its tensor and remade after
- * the library writes the tensor or hands out its device pointer
- * (sb_tensor_device_data); inside a captured graph it is remade on every
- * replay.  Not while a capture is open.  A bounded wait of the tensor-core
+ * The split operand images of a contraction are kept with its plan and
+ * remade after the library writes the operand tensor or hands out its device
+ * pointer (sb_tensor_device_data); inside a captured graph they are remade on
+ * every replay.  Not while a capture is open.  A bounded wait of the tensor-core
  * kernel that runs out is reported by the next sb_ctx_synchronize as
  * SB_ERR_TIMEOUT.                                                           */
 typedef enum sb_precision {

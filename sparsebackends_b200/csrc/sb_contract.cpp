@@ -269,7 +269,7 @@ struct GemmLaunch {
   // tensor-core launches: explicit tile list, tiles [nz_begin, n) are the
   // pair-less C blocks; swap puts Y on the 128-row side; passes 3 or 1
   int32_t nz_begin = 0, nsplits = 0, nparts = 0;
-  bool swap = false;
+  bool swap = false, fold = false;
   int passes = 3, kc = 16;
   // packed operand images (launch_tc_pack): descriptors of the A side (the
   // 128-row side: Y with swap, else X) and of the B side, per-pair locations,
@@ -322,11 +322,11 @@ struct GemmLaunch {
     const void* pa = images(pk_a, pk_a_src, pk_a_ver, sa, A, a64, aver, dimg_a, nimg_a, pack_a_bytes, pack_a_elems);
     const void* pb = images(pk_b, pk_b_src, pk_b_ver, sb, B, b64, bver, dimg_b, nimg_b, pack_b_bytes, pack_b_elems);
     DevBuf part;  // k-segment partial tiles of split tiles (stream-ordered scratch)
-    if (nparts > 0) part = DevBuf(ctx, static_cast<size_t>(nparts) * 128 * 128 * sizeof(double));
+    if (nparts > 0) part = DevBuf(ctx, static_cast<size_t>(nparts) * kTcPartElems * sizeof(double));
     {
       ProfScope ps(ctx, PROF_GEMM_TC, flops, bytes);
       SB_CK(launch_gemm_tc(pa, pb, C, c_f64, dc.as<GemmCBlock>(), dp.as<GemmPair>(), dpk.as<TcPack>(),
-                           dt.as<TcTile>(), static_cast<int32_t>(n), nz_begin, swap, passes, kc, part.d(),
+                           dt.as<TcTile>(), static_cast<int32_t>(n), nz_begin, swap, passes, kc, fold, part.d(),
                            dsplit.as<TcSplit>(), nsplits, ctx->tc_status.as<int>(), ctx->stream));
     }
     ctx->tc_launched = true;
@@ -630,7 +630,13 @@ struct GemmPlan {
     g.nz_begin = static_cast<int32_t>(items.size());
     g.swap = swap;
     g.passes = ctx->precision == SB_PRECISION_TF32 ? 1 : 3;
-    g.kc = ctx->tc_kc;
+    // chunks: items of at most 2*kc k-tiles run as one chunk each (two
+    // accumulators alternate, no running sum); longer items fold chunks of kc
+    // k-tiles into a sum kept in TMEM (one accumulator)
+    int64_t max_nkt = 1;
+    for (const W& w : items) max_nkt = std::max<int64_t>(max_nkt, w.t.nkt);
+    g.fold = max_nkt > 2LL * ctx->tc_kc;
+    g.kc = g.fold ? ctx->tc_kc : static_cast<int>(max_nkt);
     // packed images: one set per distinct A-side block (128-row tiles) and per
     // distinct B-side block (nbs-row tiles, nbs as in the item geometry), each
     // with the block's k-tiles; a block that several C blocks read is packed once
@@ -682,8 +688,9 @@ struct GemmPlan {
     }
     g.flops = flops;
     g.bytes = bytes;
-    std::snprintf(g.desc, sizeof(g.desc), "tcgen05 %s 128xN%s items:%lld split:%d", g.passes == 3 ? "3xtf32" : "tf32",
-                  swap ? " swapped" : "", static_cast<long long>(g.n), g.nsplits);
+    std::snprintf(g.desc, sizeof(g.desc), "tcgen05 %s 128xN%s items:%lld split:%d chunk:%d%s",
+                  g.passes == 3 ? "3xtf32" : "tf32", swap ? " swapped" : "", static_cast<long long>(g.n), g.nsplits,
+                  g.kc, g.fold ? " fold" : "");
   }
 
   // Thin launches (K <= 16): output blocks whose pairs read the same block of

@@ -19,26 +19,29 @@
 // the only busy unit of the main loop.
 //
 // Roles.  tcgen05.mma computes D[m, n] = sum_k A[m, k] * B[n, k] with M = 128
-// rows of A (TMEM lanes) and N <= 128 rows of B (TMEM columns).  A tile is
-// (C block, 128 rows on the A side, nb rows on the B side).  Without SWAP the
-// A side is X (rows i of C) and the B side is Y^T (columns j of C); with SWAP
-// the roles exchange.  Warp 0 (one thread) issues the copies of a k-tile into
-// one of three stages and arms the stage's "full" barrier with their byte
-// count; warp 1 (one thread) waits for it, issues the k-tile's MMAs into the
-// accumulator of the current chunk and commits them to the stage's "empty"
-// barrier (and, at a chunk's end, to the accumulator's "full" barrier);
-// warps 2-5 drain (each owns one quarter of the TMEM lanes, the rows of the A
-// side): they fold a finished chunk into the Kahan pair or write the item,
-// then arrive on the accumulator's "empty" barrier.  The three roles walk the
-// same sequence of items, k-tiles and chunks.
+// rows of A (TMEM lanes) and N <= 256 rows of B (TMEM columns): the widest
+// single-CTA form, which the tensor core runs at 1.4x the rate per flop of
+// N = 128 (measured on B200: 1.10 against 0.79 PFLOP/s of TF32 products).  A
+// tile is (C block, 128 rows on the A side, nb rows on the B side).  Without
+// SWAP the A side is X (rows i of C) and the B side is Y^T (columns j of C);
+// with SWAP the roles exchange.  Warp 0 (one thread) issues the copies of a
+// k-tile into one of two stages and arms the stage's "full" barrier with their
+// byte count; warp 1 (one thread) waits for it, issues the k-tile's MMAs into
+// the accumulator of the current chunk and commits them to the stage's
+// "empty" barrier (and, at a chunk's end, to the accumulator's "full"
+// barrier); warps 2-9 drain (warp w reads TMEM lane quarter w % 4, the rows of
+// the A side, and one half of the columns): they add a finished chunk to
+// their register sums, arrive on the accumulator's "empty" barrier and, after
+// an item's last chunk, write it.  The three roles walk the same sequence of
+// items, k-tiles and chunks.
 //
 // Accumulation.  The tensor core accumulates in FP32 and its error grows with
 // the number of accumulation steps (measured: ~9e-5 relative over 17 000
 // terms).  The k-tiles of a tile are therefore cut into chunks of kc k-tiles;
 // each chunk accumulates from zero in one of two TMEM accumulators (the next
-// chunk runs in the other one), and the threads fold a finished chunk into a
-// Kahan pair (sum, compensation) also kept in TMEM: 4 x 128 columns in all.
-// A tile of one chunk is written straight from its accumulator.
+// chunk runs in the other one), and the drain adds the chunks in FP32 with
+// round-to-nearest adds (a compensated sum measured the same error: the
+// chunks' own accumulation dominates).
 //
 // Every mbarrier wait is bounded (about two seconds of %globaltimer); a wait
 // that runs out sets *status = 1, and the CTA stops issuing MMAs and waiting,
@@ -53,12 +56,14 @@ namespace sb {
 namespace {
 
 constexpr int kTcBK = 32;                 // k-tile: 32 TF32 values = one 128-byte swizzle row
-constexpr int kTcStages = 3;
-constexpr int kTcImg = 128 * 128;         // bytes of one plane image (128 rows x 128 B)
-constexpr int kTcStageBytes = 4 * kTcImg;  // hi and lo planes of A and B
-constexpr int kTcEpiBytes = 4 * 32 * 32 * 4;   // per-warp 32 x 32 FP32 transpose buffers of the drain warps
+constexpr int kTcStages = 2;
+constexpr int kTcImg = 128 * 128;                  // bytes of one A plane (128 rows x 128 B)
+constexpr int kTcBPlane = kTcMaxN * 128;           // bytes reserved for one B plane (up to 256 rows)
+constexpr int kTcStageBytes = 2 * kTcImg + 2 * kTcBPlane;  // A hi, A lo, B hi, B lo
+constexpr int kTcDrainWarps = 8;
+constexpr int kTcEpiBytes = kTcDrainWarps * 32 * 32 * 4;  // per-warp 32 x 32 FP32 transpose buffers
 constexpr int kTcSmemBytes = kTcStages * kTcStageBytes + kTcEpiBytes + 1024 /*alignment*/ + 256 /*barriers*/;
-constexpr int kTcTmemCols = 512;          // acc0, acc1, Kahan sum, Kahan compensation
+constexpr int kTcTmemCols = 512;                   // two accumulators of up to 256 columns
 constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of every mbarrier wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -175,6 +180,16 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16]) 
       "r"(__float_as_uint(v[15])));
 }
 
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  tmem_ld16(taddr, *reinterpret_cast<float(*)[16]>(&v[0]));
+  tmem_ld16(taddr + 16, *reinterpret_cast<float(*)[16]>(&v[16]));
+}
+
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float (&v)[32]) {
+  tmem_st16(taddr, *reinterpret_cast<const float(*)[16]>(&v[0]));
+  tmem_st16(taddr + 16, *reinterpret_cast<const float(*)[16]>(&v[16]));
+}
+
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
@@ -255,15 +270,16 @@ struct Cursor {
 };
 
 constexpr int kTcMmaWarp = 1;
-constexpr int kTcEpiWarp0 = 2;  // warps 2-5
-constexpr int kTcAllThreads = 6 * 32;
+constexpr int kTcEpiWarp0 = 2;  // warps 2-9
+constexpr int kTcAllThreads = (2 + kTcDrainWarps) * 32;
+static_assert(kTcSmemBytes <= 227 * 1024, "shared memory of the tensor-core GEMM");
 
 template <bool SWAP, bool OUT64>
 __global__ void __launch_bounds__(kTcAllThreads, 1)
     k_gemm_tc(const unsigned char* __restrict__ pack_a, const unsigned char* __restrict__ pack_b,
               void* __restrict__ Cv, const GemmCBlock* __restrict__ cblocks, const GemmPair* __restrict__ pairs,
               const TcPack* __restrict__ packs, const TcTile* __restrict__ tiles, int32_t ntiles, int32_t nz_begin,
-              int32_t passes, int32_t kc, double* __restrict__ partial, int* __restrict__ status) {
+              int32_t passes, int32_t kc, int32_t fold, double* __restrict__ partial, int* __restrict__ status) {
   extern __shared__ unsigned char smem_raw[];
   const int tid = static_cast<int>(threadIdx.x);
   const int warp = tid >> 5, lane = tid & 31;
@@ -287,7 +303,7 @@ __global__ void __launch_bounds__(kTcAllThreads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(bar_accf0 + 8 * b, 1);
-      mbar_init(bar_acce0 + 8 * b, 4);
+      mbar_init(bar_acce0 + 8 * b, kTcDrainWarps);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -335,7 +351,7 @@ __global__ void __launch_bounds__(kTcAllThreads, 1)
         bulk_g2s(sbh, gb, bplane, full);
         if (split) {
           bulk_g2s(sa + kTcImg, ga + kTcImg, kTcImg, full);
-          bulk_g2s(sbh + kTcImg, gb + pk.nbs * 128, bplane, full);
+          bulk_g2s(sbh + kTcBPlane, gb + pk.nbs * 128, bplane, full);
         }
       }
       // copies still in flight land before the CTA exits: wait (bounded) for
@@ -354,15 +370,18 @@ __global__ void __launch_bounds__(kTcAllThreads, 1)
         for (int kt = 0; kt < tl.nkt && !failed; ++kt) {
           const bool chunk_first = kt % kc == 0;
           const bool chunk_last = kt + 1 == tl.nkt || (kt + 1) % kc == 0;
-          const uint32_t b = cg & 1;
-          if (chunk_first && cg >= 2) failed = !mbar_wait(bar_acce0 + 8 * b, ((cg >> 1) - 1) & 1, status);
+          // fold: one accumulator, freed by the drain after every chunk;
+          // otherwise two, alternating per chunk
+          const uint32_t b = fold ? 0u : (cg & 1);
+          if (chunk_first && fold && cg >= 1) failed = !mbar_wait(bar_acce0, (cg - 1) & 1, status);
+          if (chunk_first && !fold && cg >= 2) failed = !mbar_wait(bar_acce0 + 8 * b, ((cg >> 1) - 1) & 1, status);
           const int s = static_cast<int>(g % kTcStages);
           if (!failed) failed = !mbar_wait(bar_full0 + 8 * s, (g / kTcStages) & 1, status);
           if (failed) break;
           tc_fence_after();
-          const uint32_t acc = tmem + 128 * b;
+          const uint32_t acc = tmem + 256 * b;
           const uint32_t sa_hi = base + s * kTcStageBytes, sa_lo = sa_hi + kTcImg;  // planes: A hi, A lo, B hi, B lo
-          const uint32_t sb_hi = sa_hi + 2 * kTcImg, sb_lo = sb_hi + kTcImg;
+          const uint32_t sb_hi = sa_hi + 2 * kTcImg, sb_lo = sb_hi + kTcBPlane;
 #pragma unroll
           for (int kk = 0; kk < kTcBK / 8; ++kk) {
             const uint64_t ah = smem_desc(sa_hi + 32 * kk), bh = smem_desc(sb_hi + 32 * kk);
@@ -384,12 +403,15 @@ __global__ void __launch_bounds__(kTcAllThreads, 1)
       }
     }
   } else {
-    // ── drain: warps 9-12, TMEM lane quarter q = warp % 4 ─────────────────
+    // ── drain: warps 2-9; warp w reads TMEM lane quarter w % 4 (32 rows of
+    // the A side) and column half h = (w - 2) / 4 ([128h, 128h + 128)).  With
+    // fold the chunks of an item are added into a sum kept in TMEM columns
+    // [256, 512) (FP32, round to nearest); otherwise items have one chunk. ──
     bool failed = false;
-    const int q = warp & 3;
+    const int dw = warp - kTcEpiWarp0;
+    const int q = warp & 3, h = dw >> 2;
     const uint32_t lanes = static_cast<uint32_t>(32 * q) << 16;
-    float* const epi = reinterpret_cast<float*>(smem_raw + (epi_addr - raw)) + (warp - kTcEpiWarp0) * 1024;
-    const uint32_t t_sum = tmem + 256, t_comp = tmem + 384;
+    float* const epi = reinterpret_cast<float*>(smem_raw + (epi_addr - raw)) + dw * 1024;
     uint32_t cg = 0;
     for (int t = static_cast<int>(blockIdx.x); t < nz_begin; t += grid) {
       const TcTile tl = tiles[t];
@@ -398,86 +420,67 @@ __global__ void __launch_bounds__(kTcAllThreads, 1)
       const int arow0 = tl.a0 + 32 * q;         // first A-side row of this warp
       const int arow = arow0 + lane;            // A-side row of this thread
       const int rows_ok = min(32, ma - arow0);  // valid rows of this warp (may be <= 0)
+      const int c_lo = 128 * h;                 // this warp's columns [c_lo, c_hi) of the item
+      const int c_hi = min(tl.nb, c_lo + 128);
       const int nch = (tl.nkt + kc - 1) / kc;
       for (int ch = 0; ch < nch; ++ch, ++cg) {
         const bool first = ch == 0, last = ch + 1 == nch;
-        const uint32_t b = cg & 1;
-        if (!failed) failed = !mbar_wait_idle(bar_accf0 + 8 * b, (cg >> 1) & 1, status);
+        const uint32_t b = fold ? 0u : (cg & 1);
+        const uint32_t parity = fold ? (cg & 1) : ((cg >> 1) & 1);
+        if (!failed) failed = !mbar_wait_idle(bar_accf0 + 8 * b, parity, status);
         tc_fence_after();
-        const uint32_t acc = tmem + 128 * b;
-        for (int col0 = 0; col0 < tl.nb; col0 += 32) {
-          const int nh = col0 + 16 < tl.nb ? 2 : 1;  // 16-column halves inside nb
-          for (int h = 0; h < nh; ++h) {
-            const int cc = col0 + 16 * h;
-            float v[16], sm[16], cm[16];
-            tmem_ld16(acc + lanes + cc, v);
-            if (!first) {
-              tmem_ld16(t_sum + lanes + cc, sm);
-              tmem_ld16(t_comp + lanes + cc, cm);
-            }
-            tmem_wait_ld();
+        const uint32_t acc = tmem + 256 * b + static_cast<uint32_t>(c_lo) + lanes;
+        const uint32_t tsum = tmem + 256 + static_cast<uint32_t>(c_lo) + lanes;
+        for (int gp = 0; gp < 4; ++gp) {  // 32 columns per TMEM wait
+          const int c0 = c_lo + 32 * gp;  // item column of v[0]
+          if (c0 >= c_hi) break;
+          float v[32], sm[32];
+          tmem_ld32(acc + 32 * gp, v);
+          if (fold && !first) tmem_ld32(tsum + 32 * gp, sm);
+          tmem_wait_ld();
+          if (fold && !first)
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-              if (first) {
-                sm[j] = v[j];
-                cm[j] = 0.0f;
-              } else {  // Kahan: s + v, lost low part kept (negated) in c
-                const float y = v[j] - cm[j];
-                const float tt = sm[j] + y;
-                cm[j] = (tt - sm[j]) - y;
-                sm[j] = tt;
-              }
-            }
-            if (!last) {
-              tmem_st16(t_sum + lanes + cc, sm);
-              tmem_st16(t_comp + lanes + cc, cm);
-              continue;
-            }
-            if (failed || rows_ok <= 0) continue;
-            if (tl.part >= 0) {
-              // partial tile (column-major 128 x 128): lanes write consecutive rows
-              double* pt = partial + static_cast<int64_t>(tl.part) * (128 * 128) + 32 * q + lane;
-              if (lane < rows_ok)
-#pragma unroll
-                for (int j = 0; j < 16; ++j)
-                  pt[(cc + j) * 128] = static_cast<double>(sm[j]) - static_cast<double>(cm[j]);
-              continue;
-            }
-            if (!SWAP) {
-              // C(i = arow, j = bcol) at arow + bcol * ldc: lanes write consecutive rows
-              if (lane < rows_ok)
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                  const int bcol = tl.b0 + cc + j;
-                  if (bcol >= nbv) break;
-                  const int64_t off = cb.c_off + arow + static_cast<int64_t>(bcol) * cb.ldc;
-                  if (OUT64) static_cast<double*>(Cv)[off] = static_cast<double>(sm[j]) - static_cast<double>(cm[j]);
-                  else static_cast<float*>(Cv)[off] = sm[j] - cm[j];
-                }
-              continue;
-            }
-            // SWAP: stage 32 rows x 16 columns in the warp's shared buffer
-            // (XOR-swizzled: no bank conflicts either way) for the transposed store
-            if constexpr (SWAP) {
-#pragma unroll
-              for (int j = 0; j < 16; ++j) epi[lane * 32 + ((16 * h + j) ^ lane)] = sm[j] - cm[j];
-            }
+            for (int j = 0; j < 32; ++j) v[j] += sm[j];
+          if (!last) {
+            tmem_st32(tsum + 32 * gp, v);
+            continue;
           }
-          if constexpr (SWAP) {
-            if (!last || tl.part >= 0) continue;
-            // C(i = bcol, j = arow) at bcol + arow * ldc: lanes write consecutive
-            // columns of one row
-            __syncwarp();
-            if (!failed && rows_ok > 0) {
-              const int bcol = tl.b0 + col0 + lane;
-              const bool col_ok = bcol < nbv && lane < 16 * nh;
-              for (int r = 0; r < rows_ok; ++r) {
-                const float val = epi[r * 32 + (lane ^ r)];
-                if (!col_ok) continue;
-                const int64_t off = cb.c_off + bcol + static_cast<int64_t>(arow0 + r) * cb.ldc;
-                if (OUT64) static_cast<double*>(Cv)[off] = static_cast<double>(val);
-                else static_cast<float*>(Cv)[off] = val;
+          if (failed || rows_ok <= 0) continue;
+          if (tl.part >= 0) {
+            // partial tile (column-major 128 x 256): lanes write consecutive rows
+            double* pt = partial + static_cast<int64_t>(tl.part) * kTcPartElems + 32 * q + lane;
+            if (lane < rows_ok)
+#pragma unroll
+              for (int j = 0; j < 32; ++j)
+                if (c0 + j < c_hi) pt[(c0 + j) * 128] = static_cast<double>(v[j]);
+            continue;
+          }
+          if constexpr (!SWAP) {
+            // C(i = arow, j = bcol) at arow + bcol * ldc: lanes write consecutive rows
+            if (lane < rows_ok)
+#pragma unroll
+              for (int j = 0; j < 32; ++j) {
+                const int bcol = tl.b0 + c0 + j;
+                if (c0 + j >= c_hi || bcol >= nbv) break;
+                const int64_t off = cb.c_off + arow + static_cast<int64_t>(bcol) * cb.ldc;
+                if (OUT64) static_cast<double*>(Cv)[off] = static_cast<double>(v[j]);
+                else static_cast<float*>(Cv)[off] = v[j];
               }
+          } else {
+            // SWAP: stage 32 rows x 32 columns in the warp's shared buffer
+            // (XOR-swizzled: no bank conflicts either way), then lanes write
+            // consecutive columns of one row: C(i = bcol, j = arow) at bcol + arow * ldc
+#pragma unroll
+            for (int j = 0; j < 32; ++j) epi[lane * 32 + (j ^ lane)] = v[j];
+            __syncwarp();
+            const int bcol = tl.b0 + c0 + lane;
+            const bool col_ok = bcol < nbv && c0 + lane < c_hi;
+            for (int r = 0; r < rows_ok; ++r) {
+              const float val = epi[r * 32 + (lane ^ r)];
+              if (!col_ok) continue;
+              const int64_t off = cb.c_off + bcol + static_cast<int64_t>(arow0 + r) * cb.ldc;
+              if (OUT64) static_cast<double*>(Cv)[off] = static_cast<double>(val);
+              else static_cast<float*>(Cv)[off] = val;
             }
             __syncwarp();
           }
@@ -495,7 +498,7 @@ __global__ void __launch_bounds__(kTcAllThreads, 1)
       const GemmCBlock cb = cblocks[tl.cb];
       const int ma = SWAP ? cb.N : cb.M, nbv = SWAP ? cb.M : cb.N;
       const int rows = min(128, ma - tl.a0), cols = min(tl.nb, nbv - tl.b0);
-      for (int e = et; e < rows * cols; e += 128) {
+      for (int e = et; e < rows * cols; e += 32 * kTcDrainWarps) {
         const int r = tl.a0 + e % rows, c = tl.b0 + e / rows;
         const int64_t off =
             cb.c_off + (SWAP ? c + static_cast<int64_t>(r) * cb.ldc : r + static_cast<int64_t>(c) * cb.ldc);
@@ -516,7 +519,8 @@ __global__ void __launch_bounds__(kTcAllThreads, 1)
 template <bool SWAP, bool OUT64>
 cudaError_t launch_tc_t(const unsigned char* pa, const unsigned char* pb, void* C, const GemmCBlock* cb,
                         const GemmPair* pr, const TcPack* packs, const TcTile* tiles, int32_t ntiles,
-                        int32_t nz_begin, int passes, int kc, double* partial, int* status, cudaStream_t s) {
+                        int32_t nz_begin, int passes, int kc, bool fold, double* partial, int* status,
+                        cudaStream_t s) {
   auto kern = k_gemm_tc<SWAP, OUT64>;
   static std::atomic<int> grid_of[64] = {};  // one CTA per SM, per device ordinal
   int dev = 0;
@@ -532,7 +536,7 @@ cudaError_t launch_tc_t(const unsigned char* pa, const unsigned char* pb, void* 
   }
   const unsigned g = static_cast<unsigned>(std::min<int64_t>(ntiles, grid));
   kern<<<g, kTcAllThreads, kTcSmemBytes, s>>>(pa, pb, C, cb, pr, packs, tiles, ntiles, nz_begin, passes, kc,
-                                               partial, status);
+                                               fold ? 1 : 0, partial, status);
   return cudaGetLastError();
 }
 
@@ -552,7 +556,7 @@ __global__ void k_tc_reduce(const double* __restrict__ partial, void* __restrict
     if (r >= rows) continue;
     double acc = 0.0;
     for (int q = 0; q < sp.nparts; ++q)
-      acc += partial[static_cast<int64_t>(sp.part0 + q) * (128 * 128) + r + c * 128];
+      acc += partial[static_cast<int64_t>(sp.part0 + q) * kTcPartElems + r + c * 128];
     const int arow = sp.a0 + r, bcol = sp.b0 + c;
     const int64_t off = cb.c_off + (SWAP ? bcol + static_cast<int64_t>(arow) * cb.ldc
                                          : arow + static_cast<int64_t>(bcol) * cb.ldc);
@@ -580,7 +584,7 @@ cudaError_t launch_tc_pack(const void* src, bool src_f64, const TcImage* d_imgs,
 
 cudaError_t launch_gemm_tc(const void* pack_a, const void* pack_b, void* C, bool c_f64, const GemmCBlock* d_cblocks,
                            const GemmPair* d_pairs, const TcPack* d_packs, const TcTile* d_tiles, int32_t ntiles,
-                           int32_t nz_begin, bool swap, int passes, int kc, double* d_partial,
+                           int32_t nz_begin, bool swap, int passes, int kc, bool fold, double* d_partial,
                            const TcSplit* d_splits, int32_t nsplits, int* d_status, cudaStream_t s) {
   if (ntiles <= 0) return cudaSuccess;
   if ((passes != 1 && passes != 3) || kc < 1 || (nsplits > 0 && (!d_partial || !d_splits)))
@@ -590,14 +594,14 @@ cudaError_t launch_gemm_tc(const void* pack_a, const void* pack_b, void* C, bool
   cudaError_t e;
   if (swap)
     e = c_f64 ? launch_tc_t<true, true>(pa, pb, C, d_cblocks, d_pairs, d_packs, d_tiles, ntiles, nz_begin, passes, kc,
-                                        d_partial, d_status, s)
+                                        fold, d_partial, d_status, s)
               : launch_tc_t<true, false>(pa, pb, C, d_cblocks, d_pairs, d_packs, d_tiles, ntiles, nz_begin, passes,
-                                         kc, d_partial, d_status, s);
+                                         kc, fold, d_partial, d_status, s);
   else
     e = c_f64 ? launch_tc_t<false, true>(pa, pb, C, d_cblocks, d_pairs, d_packs, d_tiles, ntiles, nz_begin, passes,
-                                         kc, d_partial, d_status, s)
+                                         kc, fold, d_partial, d_status, s)
               : launch_tc_t<false, false>(pa, pb, C, d_cblocks, d_pairs, d_packs, d_tiles, ntiles, nz_begin, passes,
-                                          kc, d_partial, d_status, s);
+                                          kc, fold, d_partial, d_status, s);
   if (e != cudaSuccess || nsplits <= 0) return e;
   if (swap) {
     if (c_f64) k_tc_reduce<true, true><<<nsplits, 256, 0, s>>>(d_partial, C, d_cblocks, d_splits);

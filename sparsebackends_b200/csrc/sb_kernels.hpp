@@ -94,17 +94,20 @@ void gemm_tile_dims(GemmShape shape, int* bm, int* bn);
 // the TF32-rounded operands once.
 // Work items are listed explicitly: item i covers rows [a0, a0 + 128) of the
 // A side and [b0, b0 + nb) of the B side of C block cb (nb a multiple of 16
-// in 16..128), and nkt k-tiles (32 deep) of its C block's concatenated pair
+// in 16..256), and nkt k-tiles (32 deep) of its C block's concatenated pair
 // K ranges starting at pair p0, offset k0 (a multiple of 32).  Without swap
 // the A side is X (rows of C) and the B side Y (columns of C); with swap the
 // other way round.  An item with part < 0 covers the whole K range and
 // writes C; part >= 0 marks a k-segment of a split tile, written in FP64 to
-// partial tile `part` (column-major 128 x 128 doubles) and summed in segment
+// partial tile `part` (column-major 128 x 256 doubles) and summed in segment
 // order into C by the reduction that follows (one TcSplit per split tile:
 // its geometry and its parts [part0, part0 + nparts)).  Items [nz_begin,
 // ntiles) belong to C blocks without pairs and are written as zeros.  Within
-// an item the k-tiles accumulate in FP32 chunks of kc k-tiles that are summed
-// with Kahan compensation.  A persistent grid of one CTA per SM walks the list
+// an item the k-tiles accumulate in FP32 chunks of kc k-tiles (the tensor
+// core's accumulation error grows with the chunk length) whose sum is formed
+// in FP32 with round-to-nearest adds.  fold must be set when an item has
+// more than kc k-tiles (one accumulator and the running sum in TMEM; without
+// it two accumulators alternate and every item is one chunk).  A persistent grid of one CTA per SM walks the list
 // with stride gridDim.x, so the list order (the host sorts by work) balances
 // the load.  *d_status is set to 1 if a bounded wait on the tensor core ran
 // out (the results are then invalid).
@@ -116,7 +119,8 @@ struct TcSplit {
   int32_t cb, a0, b0, nb;
   int32_t part0, nparts, pad0, pad1;
 };
-constexpr int kTcMaxN = 128;
+constexpr int kTcMaxN = 256;
+constexpr int64_t kTcPartElems = 128 * kTcMaxN;  // doubles of one partial tile
 // Operands arrive packed (launch_tc_pack): per pair p, packs[p] locates the
 // images of its A-side block (a_base: 128-row tiles, nkt k-tiles each, 32 KB
 // per k-tile: hi plane then lo plane) and of its B-side block (b_base: tiles
@@ -128,7 +132,7 @@ struct TcPack {
 };
 cudaError_t launch_gemm_tc(const void* pack_a, const void* pack_b, void* C, bool c_f64, const GemmCBlock* d_cblocks,
                            const GemmPair* d_pairs, const TcPack* d_packs, const TcTile* d_tiles, int32_t ntiles,
-                           int32_t nz_begin, bool swap, int passes, int kc, double* d_partial,
+                           int32_t nz_begin, bool swap, int passes, int kc, bool fold, double* d_partial,
                            const TcSplit* d_splits, int32_t nsplits, int* d_status, cudaStream_t s);
 // One packed k-tile image of one operand tile: rows [0, rows) x k [0, kv)
 // (element (r, k) at src + r*ld + k when kc, else src + r + k*ld; elements of
