@@ -53,9 +53,14 @@ def parse():
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=60.0)
-    ap.add_argument("--leg", default="all", choices=["all", "mixed"],
+    ap.add_argument("--leg", default="all", choices=["all", "mixed", "dmrg", "cpu"],
                     help="mixed: only the 3xTF32 tensor-core chain (psi*L*(W1*W2)*R, FP32 intermediates), "
-                         "a short case for kernel profiling; prints its own line, not the headline")
+                         "a short case for kernel profiling; dmrg: the full two-site DMRG of the Heisenberg "
+                         "chain (N=100, chi 64->512, 5 sweeps) in FP64 and in 3xTF32; cpu: the oracle port "
+                         "of the reference's algorithm on the host cores at 1 thread and at all threads, for the "
+                         "chi=2048 matvec and the N=16 chi=64 centre-bond matvec; each prints its own line, not "
+                         "the headline")
+    ap.add_argument("--dmrg-n", type=int, default=100)
     return ap.parse_args()
 
 
@@ -977,12 +982,85 @@ def run_mixed_only(args, world, rank, local):
                           "value": replica_rate(world, args.steps, ms), "unit": UNIT}), flush=True)
 
 
+def run_dmrg_leg(args, world, rank, local):
+    """Two-site DMRG of the Heisenberg chain (J = 1, open, U(1) 2Sz = 0) from
+    the Neel state: 5 sweeps with maxdim 64, 128, 256, 512, 512, cutoff 1e-10,
+    krylovdim 3, maxiter 1 per bond, in plain FP64 and in the 3xTF32 form (the
+    H_eff applies on the tensor cores, FP64 Rayleigh-quotient energies).  Every
+    step runs on the device (contractions, Lanczos vector operations, the SVD
+    per centre charge); the host holds keys, the tridiagonal eigenproblem and
+    the singular values for the truncation."""
+    import torch
+    import sparsebackends_b200 as sb
+    from sparsebackends_b200 import dmrg
+    torch.cuda.set_device(local)
+    sched = [64, 128, 256, 512, 512]
+    kinds = ("gemm", "gemm_thin", "gemm_tc", "tc_pack", "permute", "outer", "axpy", "vector", "other")
+    out = {}
+    for prec in ("f64", "tf32x3"):
+        ctx = sb.Context(local)
+        d = dmrg.DMRG(args.dmrg_n, 1.0, ctx, precision=prec)
+        ctx.set_profiling(True)
+        energies, secs = [], []
+        for m in sched:
+            t0 = time.perf_counter()
+            energies.append(d.sweep(m, cutoff=1e-10, krylovdim=3, maxiter=1))
+            ctx.synchronize()
+            secs.append(time.perf_counter() - t0)
+        prof = {k: ctx.profile(k) for k in kinds}
+        ctx.set_profiling(False)
+        out[prec] = {"energy": energies[-1], "sweep_energies": energies, "sweep_seconds": secs,
+                     "max_bond": max(sum(b.dims) for b in d.bonds), "truncerr": d.truncerr,
+                     "kernel_ms": {k: v["ms"] for k, v in prof.items()},
+                     "kernel_launches": {k: v["launches"] for k, v in prof.items()}}
+    if rank == 0:
+        e64, e32 = out["f64"]["energy"], out["tf32x3"]["energy"]
+        print(json.dumps({"leg": "dmrg", "model": f"Heisenberg chain N={args.dmrg_n}, OBC, U(1) 2Sz=0, Neel start",
+                          "schedule": {"maxdim": sched, "cutoff": 1e-10, "krylovdim": 3, "maxiter": 1},
+                          "forms": out, "rel_diff_tf32x3_vs_f64": abs(e32 - e64) / abs(e64)}), flush=True)
+
+
+def run_cpu_leg(args):
+    """The CPU restatement of the reference (oracle port: numpy + OpenBLAS) on
+    this host's cores, 1 thread and all threads: one chi=2048 matvec (the
+    headline workload, uniform zero-padded blocks as the reference stores
+    them) and repeated N=16 chi=64 centre-bond matvecs."""
+    from threadpoolctl import threadpool_limits
+    import sparsebackends_b200 as sb
+    from sparsebackends_b200 import dmrg, qn
+    layout = workload(args.chi)
+    host = host_tensors(layout, args.seed)
+    ctx = sb.Context(0)
+    lay1, psi1, L1, W1_, R1 = dmrg.canonical_center_problem(ctx)
+    host1 = {}
+    for name, t in (("psi", psi1), ("L", L1), ("W1", W1_), ("W2", W1_), ("R", R1)):
+        u = sb.to_uniform(t)
+        host1[name] = (u.keys, np.array(u.data, copy=True))
+    out = {"host_cores": os.cpu_count()}
+    for threads in (1, blas_threads()):
+        with threadpool_limits(limits=threads, user_api="blas"):
+            r, n, el = cpu_matvec_rate(layout, host, 0.0, 1)
+            r1, n1, el1 = cpu_matvec_rate(lay1, host1, 5.0, 2000)
+        out[f"threads_{threads}"] = {
+            "chi2048": {"value": r, "unit": UNIT, "sample": f"{n} matvec in {el:.1f} s",
+                        "gflops_algorithmic": qn.chain_flops(layout, padded=False) * r / 1e9},
+            "centre_n16_chi64": {"value": r1, "unit": UNIT, "sample": f"{n1} matvecs in {el1:.1f} s",
+                                 "gflops_algorithmic": qn.chain_flops(lay1, padded=False) * r1 / 1e9}}
+    print(json.dumps({"leg": "cpu", "kind": "port", "what": "oracle restatement of the reference (numpy + OpenBLAS), "
+                      "not the reference itself", **out}), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     try:
         if args.impl == "ours" and args.leg == "mixed":
             run_mixed_only(args, world, rank, local)
+        elif args.impl == "ours" and args.leg == "dmrg":
+            run_dmrg_leg(args, world, rank, local)
+        elif args.impl == "ours" and args.leg == "cpu":
+            if rank == 0:
+                run_cpu_leg(args)
         elif args.impl == "reference":
             run_reference(args, world, rank)
         else:

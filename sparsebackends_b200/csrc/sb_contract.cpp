@@ -588,7 +588,10 @@ struct GemmPlan {
     int64_t seg = 0;
     if (static_cast<int64_t>(geo.size()) < target && total_kt > 0)
       seg = std::max<int64_t>(ctx->tc_kc, (total_kt + target - 1) / target);
-    struct W { TcTile t; int64_t work; };
+    // group = (C block, k-segment): its items read the same operand images
+    // (A rows for every b0, B rows for every a0) and are kept adjacent, so
+    // that consecutive CTAs run them together and the images come from L2
+    struct W { TcTile t; int64_t work; int64_t group; };
     std::vector<W> items;
     std::vector<TcSplit> splits;
     int32_t nparts = 0;
@@ -601,7 +604,7 @@ struct GemmPlan {
         const int64_t kb = kt * q / nseg, ke = kt * (q + 1) / nseg;
         items.push_back(W{TcTile{t.c, t.a0, t.b0, t.nb, p, k0, static_cast<int32_t>(ke - kb),
                                  nseg > 1 ? nparts + static_cast<int32_t>(q) : -1},
-                          (ke - kb) * t.nb});
+                          (ke - kb) * t.nb, (static_cast<int64_t>(t.c) << 32) | q});
         for (int64_t i = kb; i < ke; ++i) {  // advance to k-tile ke
           k0 += 32;
           if (k0 >= pairs[p].K) {
@@ -612,7 +615,14 @@ struct GemmPlan {
       }
       if (nseg > 1) nparts += static_cast<int32_t>(nseg);
     }
-    std::stable_sort(items.begin(), items.end(), [](const W& a, const W& b) { return a.work > b.work; });
+    // heaviest groups first (load balance of the persistent grid), a group's
+    // items together
+    std::unordered_map<int64_t, int64_t> gwork;
+    for (const W& w : items) gwork[w.group] += w.work;
+    std::stable_sort(items.begin(), items.end(), [&](const W& a, const W& b) {
+      const int64_t wa = gwork[a.group], wb = gwork[b.group];
+      return wa != wb ? wa > wb : a.group < b.group;
+    });
     std::vector<TcTile> tiles;
     tiles.reserve(items.size() + zero.size());
     for (auto& w : items) tiles.push_back(w.t);

@@ -64,6 +64,7 @@ constexpr int kTcDrainWarps = 8;
 constexpr int kTcEpiBytes = kTcDrainWarps * 32 * 32 * 4;  // per-warp 32 x 32 FP32 transpose buffers
 constexpr int kTcSmemBytes = kTcStages * kTcStageBytes + kTcEpiBytes + 1024 /*alignment*/ + 256 /*barriers*/;
 constexpr int kTcTmemCols = 512;                   // two accumulators of up to 256 columns
+constexpr int kTcReduceSlices = kTcMaxN / 32;      // 32-column slices of a split tile
 constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of every mbarrier wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -541,27 +542,40 @@ cudaError_t launch_tc_t(const unsigned char* pa, const unsigned char* pb, void* 
 }
 
 // Sum of the k-segment partial tiles of split tiles, in segment order (FP64,
-// deterministic), into C.  One CTA per split tile; element e of the
-// column-major 128 x nb tile is (A-side row e % 128, B-side row e / 128).
+// deterministic), into C.  Element (r, c) of the column-major partial tile is
+// (A-side row r, B-side row c).
 template <bool SWAP, bool OUT64>
-__global__ void k_tc_reduce(const double* __restrict__ partial, void* __restrict__ Cv,
-                            const GemmCBlock* __restrict__ cblocks, const TcSplit* __restrict__ splits) {
-  const TcSplit sp = splits[blockIdx.x];
+__global__ void __launch_bounds__(256) k_tc_reduce(const double* __restrict__ partial, void* __restrict__ Cv,
+                                                   const GemmCBlock* __restrict__ cblocks,
+                                                   const TcSplit* __restrict__ splits) {
+  // block = (split tile, 32-column slice): partials read along rows, summed in
+  // segment order, staged, and written along C's contiguous direction
+  __shared__ double S[32][129];
+  const TcSplit sp = splits[blockIdx.x / kTcReduceSlices];
+  const int c0 = 32 * static_cast<int>(blockIdx.x % kTcReduceSlices);
   const GemmCBlock cb = cblocks[sp.cb];
   const int ma = SWAP ? cb.N : cb.M, nbv = SWAP ? cb.M : cb.N;
-  const int rows = min(128, ma - sp.a0), cols = min(sp.nb, nbv - sp.b0);
-  for (int e = static_cast<int>(threadIdx.x); e < 128 * cols; e += static_cast<int>(blockDim.x)) {
-    // SWAP: consecutive threads take consecutive B-side rows (contiguous in C)
-    const int r = SWAP ? e / cols : e % 128, c = SWAP ? e % cols : e / 128;
-    if (r >= rows) continue;
+  const int rows = min(128, ma - sp.a0), cols = min(sp.nb, nbv - sp.b0) - c0;
+  if (cols <= 0) return;
+  const int tid = static_cast<int>(threadIdx.x);
+  for (int e = tid; e < 128 * 32; e += 256) {
+    const int r = e & 127, c = e >> 7;
     double acc = 0.0;
-    for (int q = 0; q < sp.nparts; ++q)
-      acc += partial[static_cast<int64_t>(sp.part0 + q) * kTcPartElems + r + c * 128];
-    const int arow = sp.a0 + r, bcol = sp.b0 + c;
+    if (r < rows && c < cols)
+      for (int q = 0; q < sp.nparts; ++q)
+        acc += partial[static_cast<int64_t>(sp.part0 + q) * kTcPartElems + r + (c0 + c) * 128];
+    S[c][r] = acc;
+  }
+  __syncthreads();
+  for (int e = tid; e < 128 * 32; e += 256) {
+    // SWAP: consecutive threads take consecutive B-side rows (contiguous in C)
+    const int r = SWAP ? e >> 5 : e & 127, c = SWAP ? e & 31 : e >> 7;
+    if (r >= rows || c >= cols) continue;
+    const int arow = sp.a0 + r, bcol = sp.b0 + c0 + c;
     const int64_t off = cb.c_off + (SWAP ? bcol + static_cast<int64_t>(arow) * cb.ldc
                                          : arow + static_cast<int64_t>(bcol) * cb.ldc);
-    if (OUT64) static_cast<double*>(Cv)[off] = acc;
-    else static_cast<float*>(Cv)[off] = static_cast<float>(acc);
+    if (OUT64) static_cast<double*>(Cv)[off] = S[c][r];
+    else static_cast<float*>(Cv)[off] = static_cast<float>(S[c][r]);
   }
 }
 
@@ -604,11 +618,11 @@ cudaError_t launch_gemm_tc(const void* pack_a, const void* pack_b, void* C, bool
                                           kc, fold, d_partial, d_status, s);
   if (e != cudaSuccess || nsplits <= 0) return e;
   if (swap) {
-    if (c_f64) k_tc_reduce<true, true><<<nsplits, 256, 0, s>>>(d_partial, C, d_cblocks, d_splits);
-    else k_tc_reduce<true, false><<<nsplits, 256, 0, s>>>(d_partial, C, d_cblocks, d_splits);
+    if (c_f64) k_tc_reduce<true, true><<<nsplits * kTcReduceSlices, 256, 0, s>>>(d_partial, C, d_cblocks, d_splits);
+    else k_tc_reduce<true, false><<<nsplits * kTcReduceSlices, 256, 0, s>>>(d_partial, C, d_cblocks, d_splits);
   } else {
-    if (c_f64) k_tc_reduce<false, true><<<nsplits, 256, 0, s>>>(d_partial, C, d_cblocks, d_splits);
-    else k_tc_reduce<false, false><<<nsplits, 256, 0, s>>>(d_partial, C, d_cblocks, d_splits);
+    if (c_f64) k_tc_reduce<false, true><<<nsplits * kTcReduceSlices, 256, 0, s>>>(d_partial, C, d_cblocks, d_splits);
+    else k_tc_reduce<false, false><<<nsplits * kTcReduceSlices, 256, 0, s>>>(d_partial, C, d_cblocks, d_splits);
   }
   return cudaGetLastError();
 }

@@ -5,7 +5,7 @@
 Per bond (i, i+1) of a sweep: ψ = A_i·A_{i+1} (``contract!``), the lowest
 eigenpair of the two-site H_eff by the device Lanczos (``krylov.eigsolve`` on
 ``qn.HeffOperator``), the U(1) split of the eigenvector
-(``qn.split_two_site``, host SVD per centre charge) into the new site tensors,
+(``qn.split_two_site_device``, one GPU SVD per centre charge) into the new site tensors,
 and the environment update (``qn.make_L`` / ``qn.make_R``).  Site tensors are
 ragged block tensors A[(ql, s, qr) | (ml, mr)] in the "A" layout of
 ``qn.HeffLayout``; links are ``qn.U1Link`` with charge = 2Sz of the sites to
@@ -106,16 +106,19 @@ def _host(t):
 class DMRG:
     """Two-site DMRG of the XXZ chain on ``n`` sites from the Néel state."""
 
-    def __init__(self, n: int, delta: float = 1.0, ctx=None, precision: str = "f64"):
+    def __init__(self, n: int, delta: float = 1.0, ctx=None, precision: str = "f64", device_split: bool = True):
         """``precision``: the H_eff applies inside Lanczos run in that context
         precision ("tf32x3": tcgen05 3xTF32 with FP32 intermediates); the
         Lanczos vectors, orthogonalisation, the split and the environments stay
         FP64, and each bond's energy is the FP64 Rayleigh quotient of its Ritz
-        vector (``krylov.eigsolve(..., correction=)``)."""
+        vector (``krylov.eigsolve(..., correction=)``).  ``device_split``: the
+        SVD per centre charge runs on the GPU (``qn.split_two_site_device``);
+        False uses the host numpy split."""
         import sparsebackends_b200 as sb
         self.sb = sb
         self.ctx = ctx or sb.default_context()
         self.precision = precision
+        self.device_split = device_split
         self.n = n
         self.W = mpo_tensor(self.ctx, delta)
         self.sites, self.bonds = neel_state(self.ctx, n)
@@ -153,12 +156,17 @@ class DMRG:
         vals, vecs, _ = krylov.eigsolve(op, x, 1, "SR", krylovdim=krylovdim, maxiter=maxiter, tol=1e-14,
                                         correction=corr, optol=op.accuracy)
         self.energy = float(vals[0])
-        (ak, ad, ae), (bk, bd, be), link, _, err = qn.split_two_site(lay, *_host(vecs[0]), maxdim=maxdim,
-                                                                   cutoff=cutoff, absorb=absorb)
+        if self.device_split:
+            A, B, link, _, err = qn.split_two_site_device(lay, vecs[0], maxdim=maxdim, cutoff=cutoff, absorb=absorb)
+        else:
+            (ak, ad, ae), (bk, bd, be), link, _, err = qn.split_two_site(lay, *_host(vecs[0]), maxdim=maxdim,
+                                                                       cutoff=cutoff, absorb=absorb)
+            A = _site(self.ctx, self.bonds[i - 1], link, ak, ad, ae)
+            B = _site(self.ctx, link, self.bonds[i + 1], bk, bd, be)
         self.truncerr = max(self.truncerr, err)
         self.bonds[i] = link
-        self.sites[i - 1] = _site(self.ctx, self.bonds[i - 1], link, ak, ad, ae)
-        self.sites[i] = _site(self.ctx, link, self.bonds[i + 1], bk, bd, be)
+        self.sites[i - 1] = A
+        self.sites[i] = B
 
     def sweep(self, maxdim: int, cutoff: float = 0.0, krylovdim: int = 3, maxiter: int = 1) -> float:
         """One left-to-right and one right-to-left pass; returns the last energy."""

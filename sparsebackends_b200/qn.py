@@ -317,6 +317,117 @@ def split_two_site(layout: HeffLayout, keys, data, exts, maxdim: int = 2 ** 62, 
     return pack(A_blocks), pack(B_blocks), link, np.array([t[0] for t in allsv[:m]]), float(w[m:].sum())
 
 
+def _device_view(t):
+    """The device payload of library tensor ``t`` as a torch float64 vector (no copy)."""
+    import torch
+    ptr, n = t.device_ptr()
+
+    class _Payload:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 3,
+                                    "stream": None}
+
+    return torch.as_tensor(_Payload(), device=f"cuda:{t.ctx.device}")
+
+
+def split_two_site_device(layout: HeffLayout, psi, maxdim: int = 2 ** 62, cutoff: float = 0.0,
+                          absorb: str = "right"):
+    """``split_two_site`` on the device: the same grouping by centre charge,
+    truncation rule and output layout, with the matrices assembled from the
+    library tensor ``psi``'s device payload and factorised on the GPU
+    (torch.linalg.svd, FP64; only the singular values travel to the host for
+    the global truncation).  Returns (A, B, link, svals, truncerr) with A and B
+    library tensors in the "A" layout of ``HeffLayout(left, link)`` and
+    ``HeffLayout(link, right)``."""
+    import torch
+    import sparsebackends_b200 as sb
+    if absorb not in ("left", "right"):
+        raise ValueError("absorb must be 'left' or 'right'")
+    ctx = psi.ctx
+    left, right = layout.left, layout.right
+    keys = [tuple(k) for k in psi.keys]
+    exts = [tuple(int(x) for x in e) for e in psi.block_dims]
+    offs = np.concatenate([[0], np.cumsum([e[0] * e[1] for e in exts])]).astype(np.int64)
+    rows, cols = {}, {}
+    for (ql, s1, s2, qr) in keys:
+        c = left.charges[ql - 1] + PHYS[s1 - 1]
+        rows.setdefault(c, set()).add((ql, s1))
+        cols.setdefault(c, set()).add((s2, qr))
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{ctx.device}")
+    svd = {}
+    with torch.cuda.stream(stream):
+        flat = _device_view(psi)
+        for c in sorted(rows):
+            rseg = sorted(rows[c], key=lambda x: (x[1], x[0]))
+            cseg = sorted(cols[c], key=lambda x: (x[1], x[0]))
+            roff, coff, r0, c0 = {}, {}, 0, 0
+            for ql, s1 in rseg:
+                roff[(ql, s1)] = r0
+                r0 += left.dims[ql - 1]
+            for s2, qr in cseg:
+                coff[(s2, qr)] = c0
+                c0 += right.dims[qr - 1]
+            M = torch.zeros((r0, c0), dtype=torch.float64, device=flat.device)
+            for i, (ql, s1, s2, qr) in enumerate(keys):
+                if left.charges[ql - 1] + PHYS[s1 - 1] != c:
+                    continue
+                dl, dr = exts[i]
+                r, cc = roff[(ql, s1)], coff[(s2, qr)]
+                M[r: r + dl, cc: cc + dr] = flat[offs[i]: offs[i + 1]].view(dr, dl).t()
+            U, S, Vh = torch.linalg.svd(M, full_matrices=False)
+            svd[c] = (U, S, Vh, rseg, roff, cseg, coff)
+        shost = {c: v[1].cpu().numpy() for c, v in svd.items()}
+    allsv = sorted(((float(sv), c, i) for c, S in shost.items() for i, sv in enumerate(S)),
+                   key=lambda t: (-t[0], t[1], t[2]))
+    w = np.array([t[0] ** 2 for t in allsv])
+    total = float(w.sum())
+    m = len(allsv)
+    if total > 0.0 and cutoff > 0.0:
+        tail = np.cumsum(w[::-1])[::-1]
+        m = next((i for i in range(1, len(allsv) + 1) if i == len(allsv) or tail[i] <= cutoff * total), m)
+    m = max(1, min(m, maxdim, len(allsv)))
+    kept = {}
+    for sv, c, i in allsv[:m]:
+        kept[c] = kept.get(c, 0) + 1
+    charges = sorted(kept)
+    link = U1Link(charges, [kept[c] for c in charges])
+    A_blocks, B_blocks = {}, {}
+    with torch.cuda.stream(stream):
+        for qc, c in enumerate(charges, start=1):
+            U, S, Vh, rseg, roff, cseg, coff = svd[c]
+            k = kept[c]
+            Uk, Sk, Vk = U[:, :k], S[:k], Vh[:k, :]
+            if absorb == "right":
+                Vk = Sk[:, None] * Vk
+            else:
+                Uk = Uk * Sk[None, :]
+            for ql, s1 in rseg:
+                r = roff[(ql, s1)]
+                A_blocks[(ql, s1, qc)] = Uk[r: r + left.dims[ql - 1], :]
+            for s2, qr in cseg:
+                cc = coff[(s2, qr)]
+                B_blocks[(qc, s2, qr)] = Vk[:, cc: cc + right.dims[qr - 1]]
+
+    def make(bl, lo: U1Link, hi: U1Link):
+        ks = sorted(bl, key=lambda k: k[::-1])
+        ex = [tuple(bl[k].shape) for k in ks]
+        n = int(sum(a * b for a, b in ex))
+        t = sb.NewBlockSparseSorted((lo.S, 2, hi.S, lo.D, hi.D), 2, ks, None, np.zeros(max(n, 1))[:n], ctx=ctx,
+                                    block_dims=ex)
+        if n:
+            with torch.cuda.stream(stream):
+                view = _device_view(t)
+                o = 0
+                for k, e in zip(ks, ex):
+                    view[o: o + e[0] * e[1]] = bl[k].t().reshape(-1)  # column-major block
+                    o += e[0] * e[1]
+        return t
+
+    A = make(A_blocks, left, link)
+    B = make(B_blocks, link, right)
+    stream.synchronize()
+    return A, B, link, np.array([t[0] for t in allsv[:m]]), float(w[m:].sum())
+
+
 def _channel_conj(layout: HeffLayout, qw: int) -> int:
     """1-based sector index of the conjugate MPO channel sector (charge -c)."""
     w = layout.mpo

@@ -34,3 +34,45 @@ def test_dmrg_reference_lanczos_setting_converges():
     exact = dmrg.exact_ground_energy(8, 1.0)
     assert abs(e - exact) <= 1e-6 * abs(exact), (e, exact, es)
     assert all(b <= a + 1e-10 for a, b in zip(es, es[1:])), es
+
+
+def test_device_split_matches_host_split():
+    """qn.split_two_site_device (SVD per centre charge on the GPU) against the
+    host split on the same two-site tensor: the same bond sectors, singular
+    values to 1e-12, and A*B reproducing the truncated psi of the host split."""
+    import sparsebackends_b200 as sb
+    from sparsebackends_b200 import qn
+    ctx = sb.Context(0)
+    left = qn.U1Link([-3, -1, 1, 3], [3, 9, 9, 3])
+    right = qn.U1Link([-2, 0, 2], [6, 11, 6])
+    lay = qn.HeffLayout(left, right, qn.mpo_link({-2: 1, 0: 3, 2: 1}))
+    keys, data, exts = qn.random_block_tensor(lay, "psi", np.random.Generator(np.random.PCG64(17)), 1.0,
+                                              ragged=True)
+    psi = sb.NewBlockSparseSorted(lay.dims["psi"], lay.n2["psi"], keys, None, data, ctx=ctx, block_dims=exts)
+    for absorb in ("right", "left"):
+        (ak, ad, ae), (bk, bd, be), link_h, sv_h, err_h = qn.split_two_site(lay, keys, data, exts, maxdim=20,
+                                                                           cutoff=1e-3, absorb=absorb)
+        A, B, link_d, sv_d, err_d = qn.split_two_site_device(lay, psi, maxdim=20, cutoff=1e-3, absorb=absorb)
+        assert link_d.charges == link_h.charges and link_d.dims == link_h.dims
+        assert np.allclose(sv_d, sv_h, rtol=1e-12, atol=0) and abs(err_d - err_h) <= 1e-12
+        assert A.keys == ak and B.keys == bk
+        Ah = sb.NewBlockSparseSorted(A.dims, 2, ak, None, ad, ctx=ctx, block_dims=ae)
+        Bh = sb.NewBlockSparseSorted(B.dims, 2, bk, None, bd, ctx=ctx, block_dims=be)
+        lab = (["ql", "s1", "s2", "qr", "ml", "mr"], ["ql", "s1", "qc", "ml", "mc"], ["qc", "s2", "qr", "mc", "mr"])
+        pd = qn.contract_new(lab[0], 2, A, lab[1], B, lab[2])
+        ph = qn.contract_new(lab[0], 2, Ah, lab[1], Bh, lab[2])
+        assert pd.keys == ph.keys
+        gd, gh = pd.blocks_by_key(), ph.blocks_by_key()
+        nrm = np.linalg.norm(np.array(ph.data))
+        assert max(np.abs(np.asarray(gd[k]) - np.asarray(v)).max() for k, v in gh.items()) <= 1e-12 * nrm
+
+
+def test_dmrg_device_split_energy():
+    import sparsebackends_b200 as sb
+    from sparsebackends_b200 import dmrg
+    sched = [4, 16, 32, 32, 32, 32]
+    e_d, _ = dmrg.DMRG(10, 1.0, sb.Context(0), device_split=True).run(sched, cutoff=1e-14, krylovdim=8, maxiter=3)
+    e_h, _ = dmrg.DMRG(10, 1.0, sb.Context(0), device_split=False).run(sched, cutoff=1e-14, krylovdim=8, maxiter=3)
+    assert abs(e_d - e_h) <= 1e-12 * abs(e_h), (e_d, e_h)
+    exact = dmrg.exact_ground_energy(10, 1.0)
+    assert abs(e_d - exact) <= 1e-9 * abs(exact)
