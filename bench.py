@@ -994,30 +994,37 @@ def run_dmrg_leg(args, world, rank, local):
     import sparsebackends_b200 as sb
     from sparsebackends_b200 import dmrg
     torch.cuda.set_device(local)
-    sched = [64, 128, 256, 512, 512]
     kinds = ("gemm", "gemm_thin", "gemm_tc", "tc_pack", "permute", "outer", "axpy", "vector", "other")
-    out = {}
-    for prec in ("f64", "tf32x3"):
-        ctx = sb.Context(local)
-        d = dmrg.DMRG(args.dmrg_n, 1.0, ctx, precision=prec)
-        ctx.set_profiling(True)
-        energies, secs = [], []
-        for m in sched:
-            t0 = time.perf_counter()
-            energies.append(d.sweep(m, cutoff=1e-10, krylovdim=3, maxiter=1))
-            ctx.synchronize()
-            secs.append(time.perf_counter() - t0)
-        prof = {k: ctx.profile(k) for k in kinds}
-        ctx.set_profiling(False)
-        out[prec] = {"energy": energies[-1], "sweep_energies": energies, "sweep_seconds": secs,
-                     "max_bond": max(sum(b.dims) for b in d.bonds), "truncerr": d.truncerr,
-                     "kernel_ms": {k: v["ms"] for k, v in prof.items()},
-                     "kernel_launches": {k: v["launches"] for k, v in prof.items()}}
-    if rank == 0:
+
+    def run(sched, krylovdim, maxiter):
+        out = {}
+        for prec in ("f64", "tf32x3"):
+            ctx = sb.Context(local)
+            d = dmrg.DMRG(args.dmrg_n, 1.0, ctx, precision=prec)
+            ctx.set_profiling(True)
+            energies, secs = [], []
+            for m in sched:
+                t0 = time.perf_counter()
+                energies.append(d.sweep(m, cutoff=1e-10, krylovdim=krylovdim, maxiter=maxiter))
+                ctx.synchronize()
+                secs.append(time.perf_counter() - t0)
+            prof = {k: ctx.profile(k) for k in kinds}
+            ctx.set_profiling(False)
+            out[prec] = {"energy": energies[-1], "sweep_energies": energies, "sweep_seconds": secs,
+                         "max_bond": max(sum(b.dims) for b in d.bonds), "truncerr": d.truncerr,
+                         "kernel_ms": {k: v["ms"] for k, v in prof.items()},
+                         "kernel_launches": {k: v["launches"] for k, v in prof.items()}}
         e64, e32 = out["f64"]["energy"], out["tf32x3"]["energy"]
+        return {"schedule": {"maxdim": sched, "cutoff": 1e-10, "krylovdim": krylovdim, "maxiter": maxiter},
+                "forms": out, "rel_diff_tf32x3_vs_f64": abs(e32 - e64) / abs(e64)}
+
+    # the configuration as specified (5 sweeps: not converged, so the two
+    # forms' truncations take different paths), then sweeps to convergence
+    spec = run([64, 128, 256, 512, 512], 3, 1)
+    conv = run([64, 128, 256, 512] + [512] * 8, 6, 2)
+    if rank == 0:
         print(json.dumps({"leg": "dmrg", "model": f"Heisenberg chain N={args.dmrg_n}, OBC, U(1) 2Sz=0, Neel start",
-                          "schedule": {"maxdim": sched, "cutoff": 1e-10, "krylovdim": 3, "maxiter": 1},
-                          "forms": out, "rel_diff_tf32x3_vs_f64": abs(e32 - e64) / abs(e64)}), flush=True)
+                          "as_specified": spec, "converged": conv}), flush=True)
 
 
 def run_cpu_leg(args):

@@ -167,6 +167,9 @@ def eigsolve(A: Callable, x0, howmany: int = 1, which: str = "SR", *, krylovdim:
         scale = max(max(abs(a) for a in alphas), max(betas))
         if optol > 0.0 and beta <= optol * scale:
             beta = 0.0  # numerically invariant for the operator's accuracy
+        # a Ritz residual at the operator's noise level counts as converged:
+        # restarting below it only mixes that noise into the basis
+        ctol = max(tol, optol * scale)
         if beta <= tol and K < howmany:
             howmany = K
         if K == krylovdim or beta <= tol:
@@ -176,7 +179,7 @@ def eigsolve(A: Callable, x0, howmany: int = 1, which: str = "SR", *, krylovdim:
             D, U = D[p], U[:, p]
             f = beta * U[K - 1, :]
             converged = 0
-            while converged < K and abs(f[converged]) <= tol:
+            while converged < K and abs(f[converged]) <= ctol:
                 converged += 1
             if converged >= howmany:
                 break

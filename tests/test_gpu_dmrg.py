@@ -44,7 +44,7 @@ def test_device_split_matches_host_split():
     from sparsebackends_b200 import qn
     ctx = sb.Context(0)
     left = qn.U1Link([-3, -1, 1, 3], [3, 9, 9, 3])
-    right = qn.U1Link([-2, 0, 2], [6, 11, 6])
+    right = qn.U1Link([-3, -1, 1, 3], [5, 11, 11, 5])
     lay = qn.HeffLayout(left, right, qn.mpo_link({-2: 1, 0: 3, 2: 1}))
     keys, data, exts = qn.random_block_tensor(lay, "psi", np.random.Generator(np.random.PCG64(17)), 1.0,
                                               ragged=True)
