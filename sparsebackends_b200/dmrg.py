@@ -99,6 +99,9 @@ def neel_state(ctx, n: int):
     return sites, bonds
 
 
+DEVICE_SPLIT_ROWS = 48
+
+
 def _host(t):
     return t.keys, np.array(t.data, copy=True), t.block_dims
 
@@ -106,14 +109,16 @@ def _host(t):
 class DMRG:
     """Two-site DMRG of the XXZ chain on ``n`` sites from the Néel state."""
 
-    def __init__(self, n: int, delta: float = 1.0, ctx=None, precision: str = "f64", device_split: bool = True):
+    def __init__(self, n: int, delta: float = 1.0, ctx=None, precision: str = "f64", device_split="auto"):
         """``precision``: the H_eff applies inside Lanczos run in that context
         precision ("tf32x3": tcgen05 3xTF32 with FP32 intermediates); the
         Lanczos vectors, orthogonalisation, the split and the environments stay
         FP64, and each bond's energy is the FP64 Rayleigh quotient of its Ritz
-        vector (``krylov.eigsolve(..., correction=)``).  ``device_split``: the
-        SVD per centre charge runs on the GPU (``qn.split_two_site_device``);
-        False uses the host numpy split."""
+        vector (``krylov.eigsolve(..., correction=)``).  ``device_split``: True,
+        the SVD per centre charge runs on the GPU (``qn.split_two_site_device``);
+        False, the host numpy split; "auto", the GPU for bonds whose largest
+        centre-charge matrix has at least ``DEVICE_SPLIT_ROWS`` rows (below
+        that the launches of the device path cost more than the work)."""
         import sparsebackends_b200 as sb
         self.sb = sb
         self.ctx = ctx or sb.default_context()
@@ -163,7 +168,14 @@ class DMRG:
         vals, vecs, _ = krylov.eigsolve(op, x, 1, "SR", krylovdim=krylovdim, maxiter=maxiter, tol=1e-14,
                                         correction=corr, optol=self.optol)
         self.energy = float(vals[0])
-        if self.device_split:
+        on_device = self.device_split
+        if on_device == "auto":
+            rows = {}
+            for (ql, s1, s2, qr) in lay.keys["psi"]:
+                c = lay.left.charges[ql - 1] + qn.PHYS[s1 - 1]
+                rows.setdefault(c, set()).add((ql, s1))
+            on_device = max(sum(lay.left.dims[ql - 1] for ql, _ in r) for r in rows.values()) >= DEVICE_SPLIT_ROWS
+        if on_device:
             A, B, link, _, err = qn.split_two_site_device(lay, vecs[0], maxdim=maxdim, cutoff=cutoff, absorb=absorb)
         else:
             (ak, ad, ae), (bk, bd, be), link, _, err = qn.split_two_site(lay, *_host(vecs[0]), maxdim=maxdim,
