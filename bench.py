@@ -262,40 +262,38 @@ def permute_stage(ctx, L, hbm_peak, reps: int = 5):
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)", "cases": out}
 
 
-def serving_leg(ctx, seed: int, nreq: int = 16):
-    """Ground-state solves served one at a time: a seeded stream of XXZ chains
-    (Delta ~ U[0.5, 1.5], N ~ U{8..12}, chi_max ~ log-uniform [8, 32], two-site
-    DMRG from the Neel state, 4 sweeps, cutoff 1e-10, krylovdim 3, maxiter 1)
-    through ``sparsebackends_b200.dmrg``.  The request shape of the serving
-    workload (N up to 128, chi_max up to 1024) is reduced so that the leg takes
-    seconds; requests run back to back, without batching.  Latency is the wall
-    time of one solve, synchronised at its end."""
-    from sparsebackends_b200 import dmrg
-    rng = np.random.Generator(np.random.PCG64(seed))
-    reqs = [(int(rng.integers(8, 13)), float(rng.uniform(0.5, 1.5)),
-             int(round(math.exp(rng.uniform(math.log(8), math.log(32)))))) for _ in range(nreq)]
-    dmrg.DMRG(8, 1.0, ctx).run([8], cutoff=1e-10)  # warm-up
-    ctx.synchronize()
-    lat, energies = [], []
-    t0 = time.perf_counter()
-    for n, delta, chi in reqs:
-        t = time.perf_counter()
-        e, _ = dmrg.DMRG(n, delta, ctx).run([chi] * 4, cutoff=1e-10, krylovdim=3, maxiter=1)
-        ctx.synchronize()
-        lat.append((time.perf_counter() - t) * 1e3)
-        energies.append(e)
-    total = time.perf_counter() - t0
-    srt = sorted(lat)
-
-    def pct(p):  # nearest rank
-        return srt[max(0, math.ceil(p / 100.0 * len(srt)) - 1)]
-
-    return {"solves_per_s": nreq / total, "p50_ms": pct(50), "p99_ms": pct(99), "requests": nreq,
-            "stream": "XXZ, Delta~U[0.5,1.5], N~U{8..12}, chi_max~logU[8,32], 4 sweeps, cutoff 1e-10, "
-                      "krylovdim 3, maxiter 1 (reduced from N<=128, chi_max<=1024)",
-            "mode": "plain FP64, one request at a time (no continuous batching)",
-            "energy_per_site_range": [min(e / n for e, (n, _, _) in zip(energies, reqs)),
-                                      max(e / n for e, (n, _, _) in zip(energies, reqs))]}
+def serving_leg(seed: int, nreq: int = 24):
+    """The serving loop (``sparsebackends_b200.serving``): a seeded stream of
+    XXZ ground-state solves (Delta ~ U[0.5, 1.5], N ~ U{8..24}, chi_max ~
+    log-uniform [8, 64], two-site DMRG from the Neel state, 4 sweeps, cutoff
+    1e-10, krylovdim 3, maxiter 1; reduced from N <= 128, chi_max <= 1024 so that
+    the leg takes under a minute).  The baseline is the plain FP64 form served
+    one request at a time; the served forms keep 4 requests in flight (own
+    contexts and streams, admission by memory footprint), FP64 and 3xTF32.
+    Arrival rates: 0.5, 1 and 2 times the baseline's capacity."""
+    from sparsebackends_b200 import serving
+    reqs = serving.random_requests(nreq, seed)
+    warm = serving.Server(slots=1)
+    warm.run(serving.random_requests(2, seed + 1, n_range=(8, 8), chi_range=(8, 8)))
+    first = serving.Server(slots=1).run(reqs)  # all arrive at t = 0: the one-at-a-time capacity
+    cap = serving.summary(first)
+    out = {"stream": f"{nreq} XXZ solves, Delta~U[0.5,1.5], N~U{{8..24}}, chi_max~logU[8,64], 4 sweeps, cutoff "
+                     "1e-10, krylovdim 3, maxiter 1 (reduced from N<=128, chi_max<=1024)",
+           "baseline_capacity_solves_per_s": cap["solves_per_s"], "rates": []}
+    base = {r.rid: r.energy for r in first}
+    for f in (0.5, 1.0, 2.0):
+        rate = f * cap["solves_per_s"]
+        stream = serving.poisson_arrivals(reqs, rate, seed + 7)
+        row = {"arrival_rate_per_s": rate, "fraction_of_baseline_capacity": f}
+        for name, server in (("fp64_one_at_a_time", serving.Server(slots=1)),
+                             ("fp64_4_in_flight", serving.Server(slots=4)),
+                             ("tf32x3_4_in_flight", serving.Server(slots=4, precision="tf32x3"))):
+            res = server.run(stream)
+            row[name] = serving.summary(res)
+            row[name]["max_rel_energy_diff_vs_fp64"] = max(abs(r.energy - base[r.rid]) / abs(base[r.rid])
+                                                           for r in res)
+        out["rates"].append(row)
+    return out
 
 
 def fp64_peak_tflops():
@@ -884,7 +882,7 @@ def run_ours(args, world, rank, local):
     hbm_peak = measured_hbm_gbs()
     gu, gtu = prof_u["gemm"], prof_u["gemm_thin"]
     permute = permute_stage(ctx, dev_u["L"], hbm_peak)
-    serving = serving_leg(ctx, args.seed)
+    serving = serving_leg(args.seed)
     # the vendor library on the same block lists, after every timed leg (its
     # many small launches stay out of the launch lists profiled from this run)
     library = cublas_block_lists(layout)
