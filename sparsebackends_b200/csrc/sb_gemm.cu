@@ -818,11 +818,11 @@ __global__ void __launch_bounds__(kThinThreads, 5)
 template <bool SR, bool XT, bool YT, bool LF = false>
 cudaError_t launch_thin_p(const double* X, const double* Y, double* C, const GemmCBlock* cb, int32_t ncb,
                           const GemmPair* pr, int64_t nctas, cudaStream_t s) {
-  static int grid_of[64] = {};
+  static std::atomic<int> grid_of[64] = {};  // host threads may race on the first call
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  int& grid = grid_of[dev & 63];
+  int grid = grid_of[dev & 63].load();
   if (grid == 0) {
     int sms = 0, per_sm = 0;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -830,6 +830,7 @@ cudaError_t launch_thin_p(const double* X, const double* Y, double* C, const Gem
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gemm_thin_p<SR, XT, YT, LF>, kThinThreads, 0);
     if (e != cudaSuccess) return e;
     grid = sms * std::max(per_sm, 1);
+    grid_of[dev & 63].store(grid);
   }
   const unsigned g = static_cast<unsigned>(std::min<int64_t>(nctas, grid));
   k_gemm_thin_p<SR, XT, YT, LF><<<g, kThinThreads, 0, s>>>(X, Y, C, cb, ncb, pr, static_cast<int32_t>(nctas));

@@ -3,6 +3,7 @@
 // segmented accumulation with the reference's rounding, structure flags,
 // gathers/scatters and the scalar programs of the aliased format.
 #include <algorithm>
+#include <atomic>
 
 #include "sb_kernels.hpp"
 
@@ -555,14 +556,14 @@ cudaError_t launch_permute_blocks(const double* src, double* dst, const int64_t*
     const int pitch = static_cast<int>(td.dv) | 1;
     int64_t tu = kNarrowSmem / 8 / pitch;
     tu = td.du <= tu ? td.du : tu / 32 * 32;
-    static bool configured[64] = {};
+    static std::atomic<bool> configured[64] = {};  // host threads may race on the first call
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (!configured[dev & 63]) {
+    if (!configured[dev & 63].load()) {
       e = cudaFuncSetAttribute(k_permute_narrow, cudaFuncAttributeMaxDynamicSharedMemorySize, kNarrowSmem);
       if (e != cudaSuccess) return e;
-      configured[dev & 63] = true;
+      configured[dev & 63].store(true);
     }
     td.tiles_u = (td.du + tu - 1) / tu;
     td.tiles_v = 1;
@@ -576,11 +577,11 @@ cudaError_t launch_permute_blocks(const double* src, double* dst, const int64_t*
   td.tiles_v = (td.dv + kTileV - 1) / kTileV;
   const int64_t total = nblocks * td.nbatch * td.tiles_u * td.tiles_v;
   constexpr int smem = 2 * kTileElems * static_cast<int>(sizeof(double));
-  static int grid_of[64] = {};
+  static std::atomic<int> grid_of[64] = {};  // host threads may race on the first call
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  int& grid = grid_of[dev & 63];
+  int grid = grid_of[dev & 63].load();
   if (grid == 0) {
     e = cudaFuncSetAttribute(k_permute_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
@@ -590,6 +591,7 @@ cudaError_t launch_permute_blocks(const double* src, double* dst, const int64_t*
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_permute_tiled, 256, smem);
     if (e != cudaSuccess) return e;
     grid = sms * std::max(per_sm, 1);
+    grid_of[dev & 63].store(grid);
   }
   const unsigned g = static_cast<unsigned>(total < grid ? total : grid);
   k_permute_tiled<<<g, dim3(32, 8), smem, s>>>(src, dst, d_src_off, blk, td, total);
