@@ -156,6 +156,12 @@ SB_API sb_status sb_tensor_create_bs_ragged(sb_ctx* ctx, int nd, const int64_t* 
 SB_API sb_status sb_tensor_create_bs_f32(sb_ctx* ctx, int nd, const int64_t* dims, int n_tail, sb_tensor** out);
 /* *f32 = 1 for FP32 storage (sb_tensor_create_bs_f32), else 0.              */
 SB_API sb_status sb_tensor_storage_f32(const sb_tensor* t, int* f32);
+/* *dense = 1 when every combination of the prefix axes has a block (a dense
+ * tensor, or a block-sparse one with no prefix), else 0: `is_dense`
+ * (src/blocksparse/storage.jl:413-425), which the wrappers use to return a plain
+ * dense ITensor (src/tensor_wrappers.jl:389-427).  COO and aliased tensors:
+ * SB_ERR_UNSUPPORTED_TYPES (the reference defines it for NewBlockSparseSorted). */
+SB_API sb_status sb_tensor_is_dense(const sb_tensor* t, int* dense);
 /* COOTensor{T,N}(dims, keys, vals, dirty) (src/coo/storage.jl:1-15).        */
 SB_API sb_status sb_tensor_create_coo(sb_ctx* ctx, int nd, const int64_t* dims, int64_t nnz,
                                const int64_t* keys, const double* vals, int dirty, sb_tensor** out);

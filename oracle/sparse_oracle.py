@@ -275,6 +275,14 @@ def blocksparse_from_dense(A: np.ndarray, n2: int, atol=0.0, rtol=0.0, dropzeros
     return out
 
 
+def bs_is_dense(A: BS) -> bool:
+    """``is_dense`` (src/blocksparse/storage.jl:413-425)."""
+    if A.P == 0:
+        _assert(len(A.keys) <= 1, "P=0 means no prefix, so at most one block (the whole tensor) is allowed")
+        return True
+    return len(A.keys) == _prod(A.dims[: A.P])
+
+
 def bs_to_dense(B: BS) -> np.ndarray:
     """``to_dense(::NewBlockSparseSorted)`` (conversions.jl:83-187), no merge."""
     out = np.zeros(B.dims)

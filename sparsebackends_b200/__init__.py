@@ -653,6 +653,14 @@ def fuse_axes(A: _Tensor, ax1: int, ax2: int) -> _Tensor:
 
 # ── block factorisations (src/ops_factorize.jl) ────────────────────────────
 
+def is_dense(A: _Tensor) -> bool:
+    """``is_dense(A)`` (src/blocksparse/storage.jl:413-425): every prefix
+    combination has a block."""
+    v = C.c_int()
+    _check(A.ctx, A.ctx._lib.sb_tensor_is_dense(A._h, C.byref(v)))
+    return bool(v.value)
+
+
 def blocksparse_left_qr(A: NewBlockSparseSorted):
     """``blocksparse_left_qr(A)`` (ops_factorize.jl:8-43) for A with prefix
     (l, r) and dense tail (s).  Returns (Q, R, l_vals, r_vals): Q block-sparse

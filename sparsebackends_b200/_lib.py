@@ -41,6 +41,7 @@ SIGNATURES = {
     "sb_tensor_block_dims": (C.c_int, [vp, P_int, P_i64, P_i64]),
     "sb_tensor_create_bs_f32": (C.c_int, [vp, C.c_int, P_i64, C.c_int, C.POINTER(vp)]),
     "sb_tensor_storage_f32": (C.c_int, [vp, P_int]),
+    "sb_tensor_is_dense": (C.c_int, [vp, P_int]),
     "sb_tensor_to_uniform": (C.c_int, [vp, vp, C.POINTER(vp)]),
     "sb_tensor_to_ragged": (C.c_int, [vp, vp, P_i64, C.c_int, C.POINTER(vp)]),
     "sb_tensor_crop_padding": (C.c_int, [vp, vp, C.POINTER(vp)]),

@@ -561,6 +561,29 @@ sb_status sb_tensor_storage_f32(const sb_tensor* t, int* f32) {
   });
 }
 
+// is_dense (src/blocksparse/storage.jl:413-425): every prefix combination has a
+// block (no prefix: the one whole-tensor block, at most one key).
+sb_status sb_tensor_is_dense(const sb_tensor* t, int* dense) {
+  return guard(t ? t->owner : nullptr, [&] {
+    check_t(t);
+    require(dense != nullptr, SB_ERR_INVALID_ARG, "dense is NULL");
+    const Tensor& A = *t->impl;
+    if (A.kind == DENSE) {
+      *dense = 1;
+      return;
+    }
+    require(A.kind == BS, SB_ERR_UNSUPPORTED_TYPES, "is_dense: block-sparse or dense tensors only");
+    if (A.P() == 0) {
+      require(A.nkeys <= 1, SB_ERR_ASSERTION, "P=0 means no prefix, so at most one block (the whole tensor) is allowed");
+      *dense = 1;
+      return;
+    }
+    int64_t combos = 1;
+    for (int i = 0; i < A.P(); ++i) combos *= A.dims[i];
+    *dense = A.nkeys == combos ? 1 : 0;
+  });
+}
+
 sb_status sb_tensor_export_coo(sb_ctx* ctx, const sb_tensor* t, int64_t* keys, double* vals) {
   return guard(ctx, [&] {
     check_ctx(ctx);

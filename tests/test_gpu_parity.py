@@ -371,3 +371,14 @@ def test_random_splitk_gemm(sb, seed):
     for lC, dims in ((["i", "j", "m", "n"], (2, 2, 70, 50)), (["i", "j", "n", "m"], (2, 2, 50, 70))):
         Cg, Cref = run_both(sb, so.BS.empty(dims, 2), lC, A, lA, B, lB)
         assert_bs_equal(Cg, Cref)
+
+
+def test_is_dense_matches_oracle():
+    import sparsebackends_b200 as sb
+    rng = np.random.Generator(np.random.PCG64(8))
+    for density in (1.0, 0.5):
+        A = rng.standard_normal((3, 2, 4, 5)) * (rng.random((3, 2, 1, 1)) < density)
+        Bo = so.blocksparse_from_dense(A, 2)
+        Bg = sb.NewBlockSparseSorted(Bo.dims, 2, Bo.keys, Bo.ids, Bo.data)
+        assert sb.is_dense(Bg) == so.bs_is_dense(Bo)
+    assert sb.is_dense(sb.DenseTensor(np.ones((2, 3))))

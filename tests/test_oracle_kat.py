@@ -215,3 +215,13 @@ def test_aliased_coo_dense_demotion():
     # keys (3,) and its rv=2 template is shared with nobody else but stays aliased
     j = Cal.keys.index((3,))
     assert Cal.scalars[j] == 0.5
+
+
+def test_bs_is_dense():
+    """is_dense (src/blocksparse/storage.jl:413-425): every prefix combination has a block."""
+    full = so.blocksparse_from_dense(np.arange(1.0, 25.0).reshape(2, 3, 4), 1)
+    assert so.bs_is_dense(full)
+    A = np.zeros((2, 3, 4))
+    A[0, 1] = 1.0
+    assert not so.bs_is_dense(so.blocksparse_from_dense(A, 1))
+    assert so.bs_is_dense(so.blocksparse_from_dense(np.ones((3, 4)), 2))  # no prefix
