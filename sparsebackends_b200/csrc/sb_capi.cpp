@@ -129,6 +129,7 @@ sb_status sb_ctx_create(int device, unsigned flags, sb_ctx** out) {
     if (const char* sk = std::getenv("SPARSEB_GEMM_SPLITK")) c->impl.gemm_splitk = std::max(0, std::atoi(sk));
     if (const char* kc = std::getenv("SPARSEB_TC_KC")) c->impl.tc_kc = std::max(1, std::atoi(kc));
     if (const char* po = std::getenv("SPARSEB_POISON_OUTPUT")) c->impl.poison_output = std::atoi(po) != 0;
+    if (const char* at = std::getenv("SPARSEB_AUTOTUNE")) c->impl.autotune = std::atoi(at) != 0;
     // Keep freed device memory cached in the stream-ordered pool.
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {

@@ -25,6 +25,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <numeric>
 #include <unordered_map>
 
@@ -1254,6 +1255,80 @@ std::vector<uint64_t> shared_signature(const Tensor& C, const Labels& lC, const 
   return sig;
 }
 
+// Autotuner of the FP64 tiled block GEMM (SPARSEB_AUTOTUNE=1).  Key: the
+// histogram of the pairs' (M, N, K) by powers of two (and the count of pairs
+// per bin, also by powers of two) plus the operand order; the same key on a
+// later plan reuses the choice.  Candidates: the heuristic's own choice (edge
+// tiles included) and every tile shape forced; each runs twice on this call's
+// operands (the first run warms it) and the second run is timed with events on
+// the context stream.  The chosen launch then writes C once more, so C is what
+// that launch computes.
+uint64_t histogram_key(const GemmPlan& gp, bool athenb) {
+  auto lg = [](int64_t v) { int b = 0; while ((1LL << b) < v) ++b; return b; };
+  std::map<std::tuple<int, int, int>, int64_t> h;
+  for (const auto& c : gp.cbs)
+    for (int p = c.pair_begin; p < c.pair_end; ++p) ++h[{lg(c.M), lg(c.N), lg(gp.pairs[p].K)}];
+  uint64_t x = 1469598103934665603ull ^ (athenb ? 1 : 2);
+  auto mix = [&](uint64_t v) { x = (x ^ v) * 1099511628211ull; };
+  for (const auto& [k, n] : h) {
+    mix(static_cast<uint64_t>(std::get<0>(k)));
+    mix(static_cast<uint64_t>(std::get<1>(k)));
+    mix(static_cast<uint64_t>(std::get<2>(k)));
+    mix(static_cast<uint64_t>(lg(n)));
+  }
+  return x;
+}
+
+template <class Run>
+GemmLaunch autotune_gemm(Ctx* ctx, const GemmPlan& gp, bool athenb, GemmLaunch g0, Run run_g) {
+  const uint64_t key = histogram_key(gp, athenb);
+  const int tile0 = ctx->gemm_tile, edges0 = ctx->gemm_edges;
+  auto with = [&](int tile, int edges) {
+    ctx->gemm_tile = tile;
+    ctx->gemm_edges = edges;
+    GemmPlan gc = gp;
+    GemmLaunch gl = athenb ? gc.prepare(ctx, false, false, 0) : gc.prepare(ctx, true, true, 0);
+    ctx->gemm_tile = tile0;
+    ctx->gemm_edges = edges0;
+    return gl;
+  };
+  auto it = ctx->tune_table.find(key);
+  if (it != ctx->tune_table.end()) {
+    if (it->second.first == -2) return g0;  // the heuristic's choice won
+    return with(it->second.first, it->second.second);
+  }
+  cudaEvent_t e0, e1;
+  SB_CK(cudaEventCreate(&e0));
+  SB_CK(cudaEventCreate(&e1));
+  auto time_ms = [&](const GemmLaunch& gl) {
+    run_g(gl);
+    SB_CK(cudaEventRecord(e0, ctx->stream));
+    run_g(gl);
+    SB_CK(cudaEventRecord(e1, ctx->stream));
+    SB_CK(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    SB_CK(cudaEventElapsedTime(&ms, e0, e1));
+    return ms;
+  };
+  float best = time_ms(g0);
+  std::pair<int, int> choice{-2, 0};
+  GemmLaunch best_g = std::move(g0);
+  for (int tile = 0; tile <= 5; ++tile) {  // every shape forced (no edge tiles)
+    GemmLaunch gl = with(tile, 0);
+    if (gl.kind != GemmLaunch::TILED && gl.kind != GemmLaunch::EDGES) continue;
+    const float ms = time_ms(gl);
+    if (ms < best) {
+      best = ms;
+      best_g = std::move(gl);
+      choice = {tile, 0};
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ctx->tune_table[key] = choice;
+  return best_g;
+}
+
 void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0, const Labels& shared);
 
 struct CropScratch {
@@ -1504,9 +1579,15 @@ void shared_bb(Ctx* ctx, Tensor& C, const Labels& lC, const Op& A0, const Op& B0
   }
   const int f32mask = athenb ? (A->f32 ? 1 : 0) | (B->f32 ? 2 : 0) | (C.f32 ? 4 : 0)
                               : (B->f32 ? 1 : 0) | (A->f32 ? 2 : 0) | (C.f32 ? 4 : 0);
+  auto run_g = [&](const GemmLaunch& gl) {
+    if (athenb) gl.run_io(ctx, *A, *B, C);
+    else gl.run_io(ctx, *B, *A, C);
+  };
   GemmLaunch g = athenb ? gp.prepare(ctx, false, false, f32mask) : gp.prepare(ctx, true, true, f32mask);
-  if (athenb) g.run_io(ctx, *A, *B, C);
-  else g.run_io(ctx, *B, *A, C);
+  if (ctx->autotune && !ctx->capturing && f32mask == 0 && ctx->precision == SB_PRECISION_F64 &&
+      (g.kind == GemmLaunch::TILED || g.kind == GemmLaunch::EDGES))
+    g = autotune_gemm(ctx, gp, athenb, std::move(g), run_g);
+  run_g(g);
   if (cache) {
     auto e = std::make_unique<SharedPlanEntry>();
     e->sig = std::move(sig);

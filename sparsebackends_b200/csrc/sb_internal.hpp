@@ -8,6 +8,7 @@
 #include <stdexcept>
 #include <string>
 #include <utility>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/sparseb.h"
@@ -92,6 +93,13 @@ struct Ctx {
   // SPARSEB_GEMM_EDGES=0 keeps 64x64-tile launches in one tile shape (tuning);
   // -1 = auto: column / row edges of <= 32 go to 64x32 / 32x64 tiles.
   int gemm_edges = -1;
+  // SPARSEB_AUTOTUNE=1: the first FP64 tiled block GEMM of a block-shape
+  // histogram times the candidate tile shapes on its own operands and keeps the
+  // fastest; later launches with the same histogram take it without timing
+  // (histogram key -> (gemm_tile, gemm_edges)).  Off by default: the choice
+  // depends on measured times, so two processes may pick differently.
+  bool autotune = false;
+  std::unordered_map<uint64_t, std::pair<int, int>> tune_table;
   // Arithmetic of the tiled block GEMMs (sb_ctx_set_precision): SB_PRECISION_F64
   // (DMMA, the drop-in), SB_PRECISION_TF32X3 or SB_PRECISION_TF32 (tcgen05).
   // The thin K <= 16 launches compute in FP64 in every mode (they are

@@ -140,3 +140,32 @@ def test_heff_chain_and_eviction(sb_mod, capfd):
 def sb_mod():
     import sparsebackends_b200 as sb
     return sb
+
+
+def test_autotuned_gemm_matches_oracle(monkeypatch):
+    """SPARSEB_AUTOTUNE=1: the first launch of a block-shape histogram times the
+    tile shapes and keeps the fastest; results stay within the drop-in
+    tolerance, a second call (same histogram) reuses the choice, and repeated
+    calls are bit-identical."""
+    import numpy as np
+    import sparsebackends_b200 as sb
+    from oracle import sparse_oracle as so
+    monkeypatch.setenv("SPARSEB_AUTOTUNE", "1")
+    ctx = sb.Context(0)
+    rng = np.random.Generator(np.random.PCG64(19))
+    A = so.blocksparse_from_dense(rng.standard_normal((2, 3, 200, 150)), 2)
+    B = so.blocksparse_from_dense(rng.standard_normal((3, 2, 150, 90)), 2)
+    lC, lA, lB = ["i", "j", "m", "n"], ["i", "q", "m", "k"], ["q", "j", "k", "n"]
+    ref = so.contract(so.BS.empty((2, 2, 200, 90), 2), lC, A, lA, B, lB)
+    a = sb.NewBlockSparseSorted(A.dims, 2, A.keys, A.ids, A.data, ctx=ctx)
+    b = sb.NewBlockSparseSorted(B.dims, 2, B.keys, B.ids, B.data, ctx=ctx)
+    outs = []
+    for _ in range(3):
+        C = sb.NewBlockSparseSorted.empty((2, 2, 200, 90), 2, ctx=ctx)
+        sb.contract_(C, lC, a, lA, b, lB)
+        outs.append(np.array(C.data, copy=True))
+        assert C.keys == ref.keys
+        gb = C.blocks_by_key()
+        for k, v in ref.blocks_by_key().items():
+            assert np.linalg.norm(np.asarray(gb[k]) - v) <= 1e-12 * np.linalg.norm(v)
+    assert np.array_equal(outs[1], outs[2])
