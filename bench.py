@@ -53,13 +53,14 @@ def parse():
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=60.0)
-    ap.add_argument("--leg", default="all", choices=["all", "mixed", "dmrg", "cpu"],
+    ap.add_argument("--leg", default="all", choices=["all", "mixed", "dmrg", "cpu", "pxp"],
                     help="mixed: only the 3xTF32 tensor-core chain (psi*L*(W1*W2)*R, FP32 intermediates), "
                          "a short case for kernel profiling; dmrg: the full two-site DMRG of the Heisenberg "
                          "chain (N=100, chi 64->512, 5 sweeps) in FP64 and in 3xTF32; cpu: the oracle port "
                          "of the reference's algorithm on the host cores at 1 thread and at all threads, for the "
                          "chi=2048 matvec and the N=16 chi=64 centre-bond matvec; each prints its own line, not "
-                         "the headline")
+                         "the headline; pxp: the PXP chain (N=64, chi=256, MPO in COO) H_eff matvec in FP64 and "
+                         "3xTF32 and the MPO x MPS apply, with the oracle port on the host cores")
     ap.add_argument("--dmrg-n", type=int, default=100)
     return ap.parse_args()
 
@@ -912,6 +913,7 @@ def run_ours(args, world, rank, local):
     gu, gtu = prof_u["gemm"], prof_u["gemm_thin"]
     permute = permute_stage(ctx, dev_u["L"], hbm_peak)
     serving = serving_leg(args.seed)
+    pxp_line = pxp_leg(local, args.steps)
     # the vendor library on the same block lists, after every timed leg (its
     # many small launches stay out of the launch lists profiled from this run)
     library = cublas_block_lists(layout)
@@ -944,6 +946,7 @@ def run_ours(args, world, rank, local):
         "library_baseline": library,
         "permute_stage": permute,
         "serving": serving,
+        "pxp_chain": pxp_line,
         "uniform_format": {"value": value_u, "ms_per_step": ms_u / args.steps,
                            "note": "contract! on the reference's zero-padded blocks; psi*L and R*T3 crop the padding "
                                    "inside contract_shared! (scan, harmonised extents, ragged GEMM, padded result)",
@@ -980,6 +983,103 @@ def run_ours(args, world, rank, local):
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
+
+
+def pxp_leg(local: int, steps: int, cpu_budget_s: float = 0.0, seed: int = 64):
+    """The PXP chain (N = 64, chi = 256, MPO bond 4 in COO): the two-site
+    H_eff matvec in plain FP64 and with its two dense contractions in 3xTF32
+    (error of the 3xTF32 result against the FP64 one), and the MPO x MPS apply
+    on every site tensor (COO x block-sparse scaled adds).  With
+    ``cpu_budget_s`` > 0 the oracle port runs the same matvec on the host
+    cores beside it."""
+    import torch
+    import sparsebackends_b200 as sb
+    from sparsebackends_b200 import pxp
+    torch.cuda.set_device(local)
+    ctx = sb.Context(local)
+    t0 = time.perf_counter()
+    prob = pxp.PxpProblem(64, 256, seed, ctx=ctx)
+    ctx.synchronize()
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    dims = pxp.bond_dims(prob.n, prob.chi)
+    dl, dr = dims[prob.c - 1], dims[prob.c + 1]
+    # T1 = L*psi: 4 channels x 4 (s1, s2) blocks of dl x dl x dr; T4 = T3*R:
+    # 16 (s1', s2', wr) products of dl x dr x dr
+    nl, nr = len(prob.L.keys), len(prob.R.keys)
+    flops = 2.0 * (nl * 4 * dl * dl * dr + 4 * nr * dl * dr * dr)
+
+    def timed(fn, n):
+        for _ in range(3):
+            fn()
+        ctx.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(n):
+            fn()
+        e.record(stream)
+        ctx.synchronize()
+        return s.elapsed_time(e) / n
+
+    kinds = ("gemm", "gemm_thin", "gemm_tc", "tc_pack", "permute", "outer", "axpy", "vector", "other")
+
+    def forms():
+        """eager ms, graph-replay ms and per-kind kernel ms of one matvec"""
+        out = prob.apply(prob.psi)
+        ms = timed(lambda: prob.apply(prob.psi), steps)
+        ctx.set_profiling(True)
+        for _ in range(5):
+            prob.apply(prob.psi)
+        ctx.synchronize()
+        kern = {k: ctx.profile(k)["ms"] / 5 for k in kinds}
+        ctx.set_profiling(False)
+        graph, gout = prob.capture(prob.psi)
+        ms_g = timed(graph.launch, steps)
+        del graph, gout
+        return out, ms, ms_g, {k: v for k, v in kern.items() if v > 0}
+
+    out64, ms64, ms64g, kern64 = forms()
+    ctx.set_precision("tf32x3")
+    try:
+        out32, ms32, ms32g, kern32 = forms()
+    finally:
+        ctx.set_precision("f64")
+    b64, b32 = out64.blocks_by_key(), out32.blocks_by_key()
+    scale = max(float(np.max(np.abs(v))) for v in b64.values())
+    err = max(float(np.max(np.abs(b32[k] - v))) for k, v in b64.items()) / scale
+    sites = [prob._bs(*pxp.site_blocks(a)) for a in prob.sites if a is not None]
+    site_bytes = sum(8 * a.size for a in prob.sites if a is not None)
+    outs = [prob.apply_mpo(a) for a in sites]
+    out_bytes = sum(8 * len(o.keys) * o.blksize for o in outs)
+    ms_mpo = timed(lambda: [prob.apply_mpo(a) for a in sites], max(3, steps // 10))
+    res = {"workload": "PXP chain N=64, OBC, no U(1); MPO bond 4 (8 nonzeros) in COO; random MPS chi=256; "
+                       "two-site H_eff at the centre (sites 32, 33), environments built on the device",
+           "setup_s": setup_s,
+           "heff_fp64": {"value": 1e3 / ms64, "unit": "matvec/s", "ms": ms64, "gflops_algorithmic": flops / ms64 / 1e6,
+                         "graph": {"value": 1e3 / ms64g, "ms": ms64g, "gflops_algorithmic": flops / ms64g / 1e6},
+                         "kernel_ms": kern64},
+           "heff_tf32x3": {"value": 1e3 / ms32, "unit": "matvec/s", "ms": ms32,
+                           "gflops_algorithmic": flops / ms32 / 1e6,
+                           "graph": {"value": 1e3 / ms32g, "ms": ms32g, "gflops_algorithmic": flops / ms32g / 1e6},
+                           "kernel_ms": kern32,
+                           "rel_err_vs_fp64": err,
+                           "form": "psi*L and T3*R on tcgen05 in 3xTF32 (FP32 accumulation); the MPO steps are "
+                                   "scaled adds by the exact 0/1 entries in FP64"},
+           "mpo_apply": {"sites": len(sites), "ms_all_sites": ms_mpo, "sites_per_s": 1e3 * len(sites) / ms_mpo,
+                         "gb_per_s_algorithmic": (site_bytes + out_bytes) / ms_mpo / 1e6,
+                         "form": "COO x block-sparse (contract_prefix!), FP64"},
+           "flops_per_matvec": flops}
+    if cpu_budget_s > 0:
+        from oracle.pxp_oracle import OracleProblem
+        ora = OracleProblem(64, 256, seed)
+        n, t0 = 0, time.perf_counter()
+        while n < 2 or (time.perf_counter() - t0 < cpu_budget_s and n < 200):
+            ora.apply(ora.psi)
+            n += 1
+        el = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": n / el, "unit": "matvec/s", "cores": blas_threads(), "kind": "port",
+                               "sample": f"{n} matvecs in {el:.1f} s, oracle restatement (numpy + OpenBLAS)"}
+    return res
 
 
 def run_mixed_only(args, world, rank, local):
@@ -1101,6 +1201,9 @@ def main():
             run_mixed_only(args, world, rank, local)
         elif args.impl == "ours" and args.leg == "dmrg":
             run_dmrg_leg(args, world, rank, local)
+        elif args.impl == "ours" and args.leg == "pxp":
+            if rank == 0:
+                print(json.dumps({"leg": "pxp", **pxp_leg(local, args.steps, 10.0)}), flush=True)
         elif args.impl == "ours" and args.leg == "cpu":
             if rank == 0:
                 run_cpu_leg(args)

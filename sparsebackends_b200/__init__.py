@@ -176,6 +176,12 @@ class Graph:
     def launch(self) -> None:
         _check(self.ctx, self.ctx._lib.sb_graph_launch(self.ctx._h, self._h))
 
+    def hold(self, *tensors: Any) -> None:
+        """Keep tensors alive as long as the graph: outputs that the captured
+        calls created (their storage was allocated at capture, and every
+        replay writes it)."""
+        self._keep.extend(tensors)
+
     def __del__(self):
         h = getattr(self, "_h", None)
         ctx = getattr(self, "ctx", None)
