@@ -1044,6 +1044,9 @@ def pxp_leg(local: int, steps: int, cpu_budget_s: float = 0.0, seed: int = 64):
         out32, ms32, ms32g, kern32 = forms()
     finally:
         ctx.set_precision("f64")
+    ops = prob.aliased_operands()
+    psi_d = sb.DenseTensor(prob.psi_host, ctx=ctx)
+    ms_al = timed(lambda: prob.apply_aliased(psi_d, ops), steps)
     b64, b32 = out64.blocks_by_key(), out32.blocks_by_key()
     scale = max(float(np.max(np.abs(v))) for v in b64.values())
     err = max(float(np.max(np.abs(b32[k] - v))) for k, v in b64.items()) / scale
@@ -1065,6 +1068,9 @@ def pxp_leg(local: int, steps: int, cpu_budget_s: float = 0.0, seed: int = 64):
                            "rel_err_vs_fp64": err,
                            "form": "psi*L and T3*R on tcgen05 in 3xTF32 (FP32 accumulation); the MPO steps are "
                                    "scaled adds by the exact 0/1 entries in FP64"},
+           "heff_aliased_fp64": {"value": 1e3 / ms_al, "unit": "matvec/s", "ms": ms_al,
+                                 "form": "W aliased (templates I, P, X), dense psi and environments: "
+                                         "contract_shared! of the aliased backend, FP64 block GEMMs"},
            "mpo_apply": {"sites": len(sites), "ms_all_sites": ms_mpo, "sites_per_s": 1e3 * len(sites) / ms_mpo,
                          "gb_per_s_algorithmic": (site_bytes + out_bytes) / ms_mpo / 1e6,
                          "form": "COO x block-sparse (contract_prefix!), FP64"},

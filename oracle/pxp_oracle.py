@@ -67,6 +67,23 @@ class OracleProblem:
         """H_eff . psi (the table HEFF_STEPS)."""
         return o_run(pxp.HEFF_STEPS, {"psi": psi, "L": self.L, "R": self.R, "W1f": self.Wf, "W2f": self.Wf})["T4"]
 
+    def apply_aliased(self, psi_d):
+        """H_eff . psi with W aliased and dense psi (l, s1, s2, r) and
+        environments (the table ALIASED_HEFF_STEPS); returns the dense result."""
+        dims, tm, keys, aids, sc = pxp.mpo_aliased()
+        Wa = so.Aliased(dims, 2, tm, 3, list(keys), list(aids), list(sc))
+        ops = {"W1a": Wa, "W2a": Wa, "psi_d": psi_d,
+               "Ld": pxp.env_dense(self.L.keys, self.L.blocks_by_key(), self.L.dims, right=False),
+               "Rd": pxp.env_dense(self.R.keys, self.R.blocks_by_key(), self.R.dims, right=True)}
+
+        def contract(lc, n2, A, la, B, lb):
+            ext = dict(zip(la, so.dims_of(A)))
+            ext.update(zip(lb, so.dims_of(B)))
+            return so.contract(so.Aliased.empty(tuple(ext[x] for x in lc), n2), lc, A, la, B, lb)
+
+        X4 = pxp.run_steps(pxp.ALIASED_HEFF_STEPS, ops, dict(pxp.ALIASED_LABELS), contract, None)["X4"]
+        return X4
+
     def apply_mpo(self, A):
         """MPO x MPS on one oracle site tensor (contract_prefix!)."""
         dims = (pxp.D, pxp.W, pxp.W, 1, 1) + tuple(A.dims[3:])

@@ -53,6 +53,28 @@ LABELS = {
     "W2f": ("s2p", "wr", "x2"),
 }
 
+# The aliased form: W as AliasedBlockSparse (prefix (wl, wr) | tail (s', s)),
+# one template per distinct one-site operator (I, P, X), and dense psi and
+# environments.  Every step is a contract_shared! / contract! of the aliased
+# backend (contract_aliased_shared.jl:103-302 Aliased x Dense,
+# :325-523 Aliased x Aliased; contract_aliased.jl:244-365): the MPO products
+# are formed once per (template, template) or (template, slice) pair and
+# shared by every key that uses them; keys that collect several distinct
+# products are accumulated into a block of their own.
+ALIASED_LABELS = {
+    "psi_d": ("l", "s1", "s2", "r"),
+    "Ld": ("lp", "wl", "l"),
+    "Rd": ("rp", "wr", "r"),
+    "W1a": ("wl", "wm", "s1p", "s1"),
+    "W2a": ("wm", "wr", "s2p", "s2"),
+}
+ALIASED_HEFF_STEPS = (
+    ("contract", "X1", ("wl", "wm", "s1p", "l", "s2", "r"), 4, "W1a", "psi_d"),
+    ("contract", "X2", ("wl", "wr", "s1p", "l", "r", "s2p"), 4, "W2a", "X1"),
+    ("contract", "X3", ("wr", "lp", "s1p", "r", "s2p"), 4, "X2", "Ld"),
+    ("contract", "X4", ("lp", "s1p", "s2p", "rp"), 4, "X3", "Rd"),  # no prefix: one key (), H_eff . psi
+)
+
 # ("contract", result, result labels, result tail count, left, right) or
 # ("fuse", result, operand, ax1, ax2, fused label); ax1 is the fast index.
 ENV_L_STEPS = (
@@ -111,6 +133,28 @@ def mpo_entries():
     idx = np.argwhere(Wd != 0.0)
     keys = sorted((tuple(int(i) + 1 for i in k) for k in idx), key=lambda k: tuple(reversed(k)))
     return keys, [float(Wd[tuple(x - 1 for x in k)]) for k in keys]
+
+
+def mpo_aliased():
+    """(dims, templates, keys, alias_ids, scalars) of W as an aliased tensor
+    (wl, wr | s', s): templates I, P, X (column-major 2x2), keys sorted
+    column-major, every scalar 1."""
+    names = ("I", "P", "X")
+    keys = sorted(((wl + 1, wr + 1) for wl, wr, _ in CHANNELS), key=lambda k: (k[1], k[0]))
+    op = {(wl + 1, wr + 1): o for wl, wr, o in CHANNELS}
+    templates = np.concatenate([OPS[m].reshape(-1, order="F") for m in names])
+    return (W, W, D, D), templates, keys, [names.index(op[k]) + 1 for k in keys], [1.0] * len(keys)
+
+
+def env_dense(keys: Sequence, blocks: Dict, dims: Sequence[int], right: bool) -> np.ndarray:
+    """Dense E[m', w, m] from environment blocks (left layout (q', w, q | m',
+    m); right layout (q', w, q | m, m'))."""
+    m1, m2 = dims[3], dims[4]
+    out = np.zeros((m2, dims[1], m1) if right else (m1, dims[1], m2))
+    for k in keys:
+        b = np.asarray(blocks[k]).reshape(m1, m2, order="F")
+        out[:, k[1] - 1, :] = b.T if right else b
+    return out
 
 
 def bond_dims(n: int, chi: int) -> List[int]:
@@ -232,6 +276,31 @@ class PxpProblem:
         order), four contractions and two fusions."""
         return self._run(HEFF_STEPS, {"psi": psi, "L": self.L, "R": self.R, "W1f": self.Wf,
                                       "W2f": self.Wf})["T4"]
+
+    def aliased_operands(self):
+        """The aliased form's operands on the device: W as an aliased tensor
+        and dense L, R (converted from the block environments once)."""
+        sb = self.sb
+        dims, tm, keys, aids, sc = mpo_aliased()
+        Wa = sb.AliasedBlockSparse(dims, 2, tm, keys, aids, sc, ctx=self.ctx)
+        Ld = sb.DenseTensor(env_dense(self.L.keys, self.L.blocks_by_key(), self.L.dims, right=False), ctx=self.ctx)
+        Rd = sb.DenseTensor(env_dense(self.R.keys, self.R.blocks_by_key(), self.R.dims, right=True), ctx=self.ctx)
+        return {"W1a": Wa, "W2a": Wa, "Ld": Ld, "Rd": Rd}
+
+    def apply_aliased(self, psi_d, ops):
+        """H_eff . psi with the MPO in aliased storage: ``psi_d`` a dense
+        DenseTensor (l, s1, s2, r), ``ops`` from ``aliased_operands``.  Returns
+        an aliased tensor with one key () whose logical block is H_eff . psi in
+        psi's layout."""
+        sb = self.sb
+
+        def contract(lc, n2, A, la, B, lb):
+            ext = dict(zip(la, A.dims))
+            ext.update(zip(lb, B.dims))
+            C = sb.AliasedBlockSparse.empty(tuple(ext[x] for x in lc), n2, ctx=self.ctx)
+            return sb.contract_(C, lc, A, la, B, lb)
+
+        return run_steps(ALIASED_HEFF_STEPS, {"psi_d": psi_d, **ops}, dict(ALIASED_LABELS), contract, None)["X4"]
 
     def capture(self, psi):
         """Run the matvec once, then capture it as one CUDA graph bound to

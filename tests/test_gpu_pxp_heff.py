@@ -143,3 +143,26 @@ def test_heff_graph_replay(sb, pair, precision):
     assert set(got) == set(want)
     for k, v in want.items():
         assert np.array_equal(got[k], v), k
+
+
+def test_heff_aliased(sb, pair):
+    """The aliased form of the matvec (W as templates I, P, X; dense psi and
+    environments): same template structure as the oracle, the same H_eff . psi
+    as the oracle and as the COO form, to 1e-13."""
+    dev, ora = pair
+    ops = dev.aliased_operands()
+    psi_d = sb.DenseTensor(dev.psi_host, ctx=dev.ctx)
+    got = dev.apply_aliased(psi_d, ops)
+    ref = ora.apply_aliased(ora.psi_host)
+    assert got.keys == ref.keys == [()]
+    assert got.n_templates == ref.n_templates
+    g, r = got.logical_blocks()[()], ref.logical_blocks()[()]
+    assert np.max(np.abs(g - r)) <= FP64_RTOL * np.max(np.abs(r))
+    coo = pxp.psi_from_blocks(*_keys_data(dev.apply(dev.psi)), dev.psi.dims)
+    assert np.max(np.abs(g.reshape(coo.shape, order="F") - coo)) <= FP64_RTOL * np.max(np.abs(coo))
+
+
+def _keys_data(T):
+    b = T.blocks_by_key()
+    keys = sorted(b, key=lambda k: tuple(reversed(k)))
+    return keys, np.concatenate([b[k] for k in keys])

@@ -99,3 +99,15 @@ def test_both_join_orders_agree(prob):
     assert base.keys == ref.keys
     for i, j in zip(base.ids, ref.ids):
         assert np.array_equal(base.block(i), ref.block(j))
+
+
+def test_aliased_heff_matches_dense(prob):
+    """The aliased form (W as templates I, P, X; dense psi and environments)
+    gives the same H_eff . psi."""
+    X4 = prob.apply_aliased(prob.psi_host)
+    assert X4.keys == [()]
+    got = X4.logical_blocks()[()].reshape(prob.psi_host.shape, order="F")
+    want = pr.dense_heff(pr.dense_env_L(prob.sites, prob.c), pr.dense_env_R(prob.sites, N, prob.c), prob.psi_host)
+    assert np.max(np.abs(got - want)) <= 1e-12 * np.max(np.abs(want))
+    dims, tm, keys, aids, sc = pxp.mpo_aliased()
+    assert len(keys) == 5 and len(tm) == 3 * pxp.D * pxp.D
