@@ -70,12 +70,27 @@ def label_key(lab: Any) -> Tuple[int, int]:
     return int.from_bytes(h, "little"), 0
 
 
+# Packed label arrays of label lists made of strings, by the tuple of strings
+# (strings compare and hash by value, so a hit is exact).  The C side copies
+# the labels, so one array serves every call; the cache is bounded.
+_LABELS_CACHE: dict = {}
+_LABELS_CACHE_MAX = 4096
+
+
 def _labels(labels: Sequence[Any]):
+    key = tuple(labels)
+    strs = all(type(l) is str for l in key)
+    if strs:
+        hit = _LABELS_CACHE.get(key)
+        if hit is not None:
+            return hit
     flat = []
-    for l in labels:
+    for l in key:
         flat.extend(label_key(l))
-    arr = (C.c_uint64 * max(len(flat), 1))(*flat)
-    return arr, len(labels)
+    out = ((C.c_uint64 * max(len(flat), 1))(*flat), len(key))
+    if strs and len(_LABELS_CACHE) < _LABELS_CACHE_MAX:
+        _LABELS_CACHE[key] = out
+    return out
 
 
 def _i64(xs) -> "C.Array":
@@ -227,7 +242,12 @@ class _Tensor:
 
     @property
     def dims(self) -> Tuple[int, ...]:
-        return self._info()["dims"]
+        # a tensor's dims never change after creation (contract! and the
+        # vector-space updates rewrite keys and payload only)
+        d = self.__dict__.get("_dims")
+        if d is None:
+            d = self._dims = self._info()["dims"]
+        return d
 
     def size(self) -> Tuple[int, ...]:
         return self.dims
