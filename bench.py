@@ -53,15 +53,20 @@ def parse():
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=60.0)
-    ap.add_argument("--leg", default="all", choices=["all", "mixed", "dmrg", "cpu", "pxp"],
+    ap.add_argument("--leg", default="all", choices=["all", "mixed", "dmrg", "cpu", "pxp", "j1j2"],
                     help="mixed: only the 3xTF32 tensor-core chain (psi*L*(W1*W2)*R, FP32 intermediates), "
                          "a short case for kernel profiling; dmrg: the full two-site DMRG of the Heisenberg "
                          "chain (N=100, chi 64->512, 5 sweeps) in FP64 and in 3xTF32; cpu: the oracle port "
                          "of the reference's algorithm on the host cores at 1 thread and at all threads, for the "
                          "chi=2048 matvec and the N=16 chi=64 centre-bond matvec; each prints its own line, not "
                          "the headline; pxp: the PXP chain (N=64, chi=256, MPO in COO) H_eff matvec in FP64 and "
-                         "3xTF32 and the MPO x MPS apply, with the oracle port on the host cores")
+                         "3xTF32 and the MPO x MPS apply, with the oracle port on the host cores; j1j2: two-site DMRG "
+                         "of the J1-J2 model on the 6x6 cylinder (N=36, maxdim to --j1j2-maxdim) in FP64 and "
+                         "3xTF32")
     ap.add_argument("--dmrg-n", type=int, default=100)
+    ap.add_argument("--j1j2-maxdim", type=int, default=2048)
+    ap.add_argument("--j1j2-budget-s", type=float, default=150.0,
+                    help="no new FP64 sweep starts after this many seconds (the schedule is cut there)")
     return ap.parse_args()
 
 
@@ -1169,6 +1174,59 @@ def run_dmrg_leg(args, world, rank, local):
                           "as_specified": spec, "converged": conv}), flush=True)
 
 
+def run_j1j2_leg(args, world, rank, local):
+    """Two-site DMRG of the J1-J2 Heisenberg model (J1 = 1, J2 = 0.5) on the
+    6 x 6 cylinder (open along x, periodic along y), snake order, N = 36, U(1)
+    2Sz = 0, from the Neel state along the snake; the MPO is the automaton
+    construction of ``j1j2.J1J2Cylinder``.  Sweeps with maxdim doubling from 64
+    to ``--j1j2-maxdim`` (then one more at the maximum), cutoff 1e-10,
+    krylovdim 3, maxiter 1, in plain FP64 and in the 3xTF32 form (the H_eff
+    applies on the tensor cores, FP64 Rayleigh-quotient energies).  Reports
+    the energies, their relative difference, per-sweep seconds and the device
+    time per kernel kind."""
+    import torch
+    import sparsebackends_b200 as sb
+    from sparsebackends_b200 import dmrg, j1j2
+    torch.cuda.set_device(local)
+    kinds = ("gemm", "gemm_thin", "gemm_tc", "tc_pack", "permute", "outer", "axpy", "vector", "other")
+    m = j1j2.J1J2Cylinder(6, 6, 1.0, 0.5)
+    sched = []
+    x = 64
+    while x < args.j1j2_maxdim:
+        sched.append(x)
+        x *= 2
+    sched += [args.j1j2_maxdim] * 2
+    out = {}
+    for prec in ("f64", "tf32x3"):
+        ctx = sb.Context(local)
+        d = dmrg.DMRG(m.n, ctx=ctx, precision=prec, device_split=True, mpo=m)
+        ctx.set_profiling(True)
+        energies, secs = [], []
+        t_start = time.perf_counter()
+        for mx in sched:
+            if prec == "f64" and time.perf_counter() - t_start > args.j1j2_budget_s:
+                sched = sched[:len(energies)]  # the 3xTF32 form runs the same sweeps
+                break
+            t0 = time.perf_counter()
+            energies.append(d.sweep(mx, cutoff=1e-10, krylovdim=3, maxiter=1))
+            ctx.synchronize()
+            secs.append(time.perf_counter() - t0)
+        prof = {k: ctx.profile(k) for k in kinds}
+        ctx.set_profiling(False)
+        out[prec] = {"energy": energies[-1], "energy_per_site": energies[-1] / m.n, "sweep_energies": energies,
+                     "sweep_seconds": secs, "max_bond": max(sum(b.dims) for b in d.bonds), "truncerr": d.truncerr,
+                     "kernel_ms": {k: v["ms"] for k, v in prof.items() if v["launches"]},
+                     "tc_gemm_tflops_algorithmic": prof["gemm_tc"]["flops"] / (prof["gemm_tc"]["ms"] * 1e-3) / 1e12
+                     if prof["gemm_tc"]["ms"] > 0 else None}
+    e64, e32 = out["f64"]["energy"], out["tf32x3"]["energy"]
+    if rank == 0:
+        print(json.dumps({"leg": "j1j2", "model": "J1-J2 Heisenberg (J1=1, J2=0.5), 6x6 cylinder (open x, periodic y), "
+                          "snake order, N=36, U(1) 2Sz=0, Neel start",
+                          "mpo_link": {"charges": m.link.charges, "dims": m.link.dims},
+                          "schedule": {"maxdim": sched, "cutoff": 1e-10, "krylovdim": 3, "maxiter": 1},
+                          "forms": out, "rel_diff_tf32x3_vs_f64": abs(e32 - e64) / abs(e64)}), flush=True)
+
+
 def run_cpu_leg(args):
     """The CPU restatement of the reference (oracle port: numpy + OpenBLAS) on
     this host's cores, 1 thread and all threads: one chi=2048 matvec (the
@@ -1207,6 +1265,8 @@ def main():
             run_mixed_only(args, world, rank, local)
         elif args.impl == "ours" and args.leg == "dmrg":
             run_dmrg_leg(args, world, rank, local)
+        elif args.impl == "ours" and args.leg == "j1j2":
+            run_j1j2_leg(args, world, rank, local)
         elif args.impl == "ours" and args.leg == "pxp":
             if rank == 0:
                 print(json.dumps({"leg": "pxp", **pxp_leg(local, args.steps, 10.0)}), flush=True)

@@ -109,7 +109,8 @@ def _host(t):
 class DMRG:
     """Two-site DMRG of the XXZ chain on ``n`` sites from the Néel state."""
 
-    def __init__(self, n: int, delta: float = 1.0, ctx=None, precision: str = "f64", device_split="auto"):
+    def __init__(self, n: int, delta: float = 1.0, ctx=None, precision: str = "f64", device_split="auto",
+                 mpo=None):
         """``precision``: the H_eff applies inside Lanczos run in that context
         precision ("tf32x3": tcgen05 3xTF32 with FP32 intermediates); the
         Lanczos vectors, orthogonalisation, the split and the environments stay
@@ -118,7 +119,10 @@ class DMRG:
         the SVD per centre charge runs on the GPU (``qn.split_two_site_device``);
         False, the host numpy split; "auto", the GPU for bonds whose largest
         centre-charge matrix has at least ``DEVICE_SPLIT_ROWS`` rows (below
-        that the launches of the device path cost more than the work)."""
+        that the launches of the device path cost more than the work).
+        ``mpo``: a site-dependent MPO (``j1j2.J1J2Cylinder``: ``link``,
+        ``tensors(ctx)``, ``boundary_envs(ctx)``) instead of the XXZ chain's;
+        ``delta`` is then unused."""
         import sparsebackends_b200 as sb
         self.sb = sb
         self.ctx = ctx or sb.default_context()
@@ -132,15 +136,21 @@ class DMRG:
         self.optol = {"f64": 0.0, "tf32x3": 1e-7, "tf32": 3e-2}[precision]
         self.device_split = device_split
         self.n = n
-        self.W = mpo_tensor(self.ctx, delta)
+        if mpo is None:
+            self.mpo_link = MPO_LINK
+            self.Ws = [mpo_tensor(self.ctx, delta)] * n
+            L0, R0 = boundary_envs(self.ctx)
+        else:
+            self.mpo_link = mpo.link
+            self.Ws = mpo.tensors(self.ctx)
+            L0, R0 = mpo.boundary_envs(self.ctx)
         self.sites, self.bonds = neel_state(self.ctx, n)
-        L0, R0 = boundary_envs(self.ctx)
         # Lenv[b]: sites 1..b, Renv[b]: sites b+1..n
         self.Lenv: List = [None] * (n + 1)
         self.Renv: List = [None] * (n + 1)
         self.Lenv[0], self.Renv[n] = L0, R0
         for b in range(n - 1, 0, -1):
-            self.Renv[b] = qn.make_R(self.Renv[b + 1], self.sites[b], self.W)
+            self.Renv[b] = qn.make_R(self.Renv[b + 1], self.sites[b], self.Ws[b])
         self.energy: Optional[float] = None
         self.truncerr = 0.0
 
@@ -150,7 +160,7 @@ class DMRG:
         A, B = self.sites[i - 1], self.sites[i]
         psi = qn.contract_new(["ql", "s1", "s2", "qr", "ml", "mr"], 2, A, ["ql", "s1", "qc", "ml", "mc"],
                               B, ["qc", "s2", "qr", "mc", "mr"])
-        lay = qn.HeffLayout(self.bonds[i - 1], self.bonds[i + 1], MPO_LINK)
+        lay = qn.HeffLayout(self.bonds[i - 1], self.bonds[i + 1], self.mpo_link)
         have = psi.blocks_by_key()
         keys = sorted(lay.keys["psi"], key=lambda k: k[::-1])
         exts = [lay.valid_extent("psi", k) for k in keys]
@@ -162,7 +172,7 @@ class DMRG:
     def _update(self, i: int, absorb: str, maxdim: int, cutoff: float, krylovdim: int, maxiter: int):
         from . import krylov
         lay, x = self._two_site(i)
-        ops = (lay, self.Lenv[i - 1], self.W, self.W, self.Renv[i + 1], self.ctx)
+        ops = (lay, self.Lenv[i - 1], self.Ws[i - 1], self.Ws[i], self.Renv[i + 1], self.ctx)
         op = qn.HeffOperator(*ops, precision=self.precision)
         corr = qn.HeffOperator(*ops) if self.precision != "f64" else None
         vals, vecs, _ = krylov.eigsolve(op, x, 1, "SR", krylovdim=krylovdim, maxiter=maxiter, tol=1e-14,
@@ -192,10 +202,10 @@ class DMRG:
         n = self.n
         for i in range(1, n):
             self._update(i, "right", maxdim, cutoff, krylovdim, maxiter)
-            self.Lenv[i] = qn.make_L(self.Lenv[i - 1], self.sites[i - 1], self.W)
+            self.Lenv[i] = qn.make_L(self.Lenv[i - 1], self.sites[i - 1], self.Ws[i - 1])
         for i in range(n - 1, 0, -1):
             self._update(i, "left", maxdim, cutoff, krylovdim, maxiter)
-            self.Renv[i] = qn.make_R(self.Renv[i + 1], self.sites[i], self.W)
+            self.Renv[i] = qn.make_R(self.Renv[i + 1], self.sites[i], self.Ws[i])
         return self.energy
 
     def run(self, maxdims: List[int], cutoff: float = 0.0, krylovdim: int = 3, maxiter: int = 1) -> Tuple[float, list]:

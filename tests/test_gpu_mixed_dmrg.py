@@ -40,7 +40,7 @@ def test_mixed_eigsolve_correction_on_heisenberg_heff():
     d.run([16, 16, 16], cutoff=1e-14, krylovdim=8, maxiter=3)
     i = 4
     lay, x = d._two_site(i)
-    args = (lay, d.Lenv[i - 1], d.W, d.W, d.Renv[i + 1], ctx)
+    args = (lay, d.Lenv[i - 1], d.Ws[i - 1], d.Ws[i], d.Renv[i + 1], ctx)
     op64 = qn.HeffOperator(*args)
     opmx = qn.HeffOperator(*args, precision="tf32x3")
     v64, _, _ = krylov.eigsolve(op64, x, 1, "SR", krylovdim=12, maxiter=4, tol=1e-14)
