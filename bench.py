@@ -1218,6 +1218,8 @@ def run_j1j2_leg(args, world, rank, local):
                      "kernel_ms": {k: v["ms"] for k, v in prof.items() if v["launches"]},
                      "tc_gemm_tflops_algorithmic": prof["gemm_tc"]["flops"] / (prof["gemm_tc"]["ms"] * 1e-3) / 1e12
                      if prof["gemm_tc"]["ms"] > 0 else None}
+        if rank == 0:  # each form as soon as it ends (a long run cut short keeps what finished)
+            print(json.dumps({"leg": "j1j2_form", "precision": prec, "maxdim": sched, **out[prec]}), flush=True)
     e64, e32 = out["f64"]["energy"], out["tf32x3"]["energy"]
     if rank == 0:
         print(json.dumps({"leg": "j1j2", "model": "J1-J2 Heisenberg (J1=1, J2=0.5), 6x6 cylinder (open x, periodic y), "
