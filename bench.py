@@ -65,6 +65,8 @@ def parse():
                          "3xTF32")
     ap.add_argument("--dmrg-n", type=int, default=100)
     ap.add_argument("--j1j2-maxdim", type=int, default=2048)
+    ap.add_argument("--j1j2-split", default="gram", choices=["svd", "gram"],
+                    help="factorisation of the two-site split (qn.split_two_site_device method)")
     ap.add_argument("--j1j2-budget-s", type=float, default=150.0,
                     help="no new FP64 sweep starts after this many seconds (the schedule is cut there)")
     return ap.parse_args()
@@ -1199,7 +1201,7 @@ def run_j1j2_leg(args, world, rank, local):
     out = {}
     for prec in ("f64", "tf32x3"):
         ctx = sb.Context(local)
-        d = dmrg.DMRG(m.n, ctx=ctx, precision=prec, device_split=True, mpo=m)
+        d = dmrg.DMRG(m.n, ctx=ctx, precision=prec, device_split=True, mpo=m, split_method=args.j1j2_split)
         ctx.set_profiling(True)
         energies, secs = [], []
         t_start = time.perf_counter()
@@ -1226,6 +1228,7 @@ def run_j1j2_leg(args, world, rank, local):
                           "snake order, N=36, U(1) 2Sz=0, Neel start",
                           "mpo_link": {"charges": m.link.charges, "dims": m.link.dims},
                           "schedule": {"maxdim": sched, "cutoff": 1e-10, "krylovdim": 3, "maxiter": 1},
+                          "split": args.j1j2_split,
                           "forms": out, "rel_diff_tf32x3_vs_f64": abs(e32 - e64) / abs(e64)}), flush=True)
 
 

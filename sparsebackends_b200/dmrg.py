@@ -110,7 +110,7 @@ class DMRG:
     """Two-site DMRG of the XXZ chain on ``n`` sites from the Néel state."""
 
     def __init__(self, n: int, delta: float = 1.0, ctx=None, precision: str = "f64", device_split="auto",
-                 mpo=None):
+                 mpo=None, split_method: str = "svd"):
         """``precision``: the H_eff applies inside Lanczos run in that context
         precision ("tf32x3": tcgen05 3xTF32 with FP32 intermediates); the
         Lanczos vectors, orthogonalisation, the split and the environments stay
@@ -122,7 +122,8 @@ class DMRG:
         that the launches of the device path cost more than the work).
         ``mpo``: a site-dependent MPO (``j1j2.J1J2Cylinder``: ``link``,
         ``tensors(ctx)``, ``boundary_envs(ctx)``) instead of the XXZ chain's;
-        ``delta`` is then unused."""
+        ``delta`` is then unused.  ``split_method``: the device split's
+        factorisation, "svd" or "gram" (``qn.split_two_site_device``)."""
         import sparsebackends_b200 as sb
         self.sb = sb
         self.ctx = ctx or sb.default_context()
@@ -135,6 +136,7 @@ class DMRG:
         # (bonds whose residual falls below it stop improving)
         self.optol = {"f64": 0.0, "tf32x3": 1e-7, "tf32": 3e-2}[precision]
         self.device_split = device_split
+        self.split_method = split_method
         self.n = n
         if mpo is None:
             self.mpo_link = MPO_LINK
@@ -186,7 +188,8 @@ class DMRG:
                 rows.setdefault(c, set()).add((ql, s1))
             on_device = max(sum(lay.left.dims[ql - 1] for ql, _ in r) for r in rows.values()) >= DEVICE_SPLIT_ROWS
         if on_device:
-            A, B, link, _, err = qn.split_two_site_device(lay, vecs[0], maxdim=maxdim, cutoff=cutoff, absorb=absorb)
+            A, B, link, _, err = qn.split_two_site_device(lay, vecs[0], maxdim=maxdim, cutoff=cutoff, absorb=absorb,
+                                                          method=self.split_method)
         else:
             (ak, ad, ae), (bk, bd, be), link, _, err = qn.split_two_site(lay, *_host(vecs[0]), maxdim=maxdim,
                                                                        cutoff=cutoff, absorb=absorb)

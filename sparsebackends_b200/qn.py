@@ -330,18 +330,30 @@ def _device_view(t):
 
 
 def split_two_site_device(layout: HeffLayout, psi, maxdim: int = 2 ** 62, cutoff: float = 0.0,
-                          absorb: str = "right"):
+                          absorb: str = "right", method: str = "svd"):
     """``split_two_site`` on the device: the same grouping by centre charge,
     truncation rule and output layout, with the matrices assembled from the
-    library tensor ``psi``'s device payload and factorised on the GPU
-    (torch.linalg.svd, FP64; only the singular values travel to the host for
-    the global truncation).  Returns (A, B, link, svals, truncerr) with A and B
-    library tensors in the "A" layout of ``HeffLayout(left, link)`` and
-    ``HeffLayout(link, right)``."""
+    library tensor ``psi``'s device payload and factorised on the GPU in FP64
+    (only the singular values travel to the host for the global truncation).
+    Returns (A, B, link, svals, truncerr) with A and B library tensors in the
+    "A" layout of ``HeffLayout(left, link)`` and ``HeffLayout(link, right)``.
+
+    ``method``: "svd" (torch.linalg.svd of each centre-charge matrix M, as the
+    reference's blocksparse_svd), or "gram": the density-matrix decomposition
+    (ITensors' ``factorize(...; which_decomp="eigen")``): the eigenvectors of
+    M M^T (absorb "right") or M^T M (absorb "left") by torch.linalg.eigh give
+    the isometry, the singular values are the square roots of the eigenvalues,
+    and the other factor is the projection U^T M (or M V), so A B is exactly
+    the projection of psi on the kept states.  The eigenvalues carry an
+    absolute error of order eps * sigma_max^2, well below a truncation cutoff
+    on the discarded weight; singular values under about 1e-8 sigma_max are
+    not resolved."""
     import torch
     import sparsebackends_b200 as sb
     if absorb not in ("left", "right"):
         raise ValueError("absorb must be 'left' or 'right'")
+    if method not in ("svd", "gram"):
+        raise ValueError("method must be 'svd' or 'gram'")
     ctx = psi.ctx
     left, right = layout.left, layout.right
     keys = [tuple(k) for k in psi.keys]
@@ -373,8 +385,18 @@ def split_two_site_device(layout: HeffLayout, psi, maxdim: int = 2 ** 62, cutoff
                 dl, dr = exts[i]
                 r, cc = roff[(ql, s1)], coff[(s2, qr)]
                 M[r: r + dl, cc: cc + dr] = flat[offs[i]: offs[i + 1]].view(dr, dl).t()
-            U, S, Vh = torch.linalg.svd(M, full_matrices=False)
-            svd[c] = (U, S, Vh, rseg, roff, cseg, coff)
+            if method == "svd":
+                U, S, Vh = torch.linalg.svd(M, full_matrices=False)
+            else:
+                r = min(r0, c0)
+                if absorb == "right":
+                    lam, U = torch.linalg.eigh(M @ M.t())
+                    U, Vh = U.flip(1)[:, :r], None
+                else:
+                    lam, V = torch.linalg.eigh(M.t() @ M)
+                    U, Vh = None, V.flip(1)[:, :r].t()
+                S = lam.flip(0)[:r].clamp_min(0.0).sqrt()
+            svd[c] = (U, S, Vh, rseg, roff, cseg, coff, M)
         shost = {c: v[1].cpu().numpy() for c, v in svd.items()}
     allsv = sorted(((float(sv), c, i) for c, S in shost.items() for i, sv in enumerate(S)),
                    key=lambda t: (-t[0], t[1], t[2]))
@@ -393,13 +415,21 @@ def split_two_site_device(layout: HeffLayout, psi, maxdim: int = 2 ** 62, cutoff
     A_blocks, B_blocks = {}, {}
     with torch.cuda.stream(stream):
         for qc, c in enumerate(charges, start=1):
-            U, S, Vh, rseg, roff, cseg, coff = svd[c]
+            U, S, Vh, rseg, roff, cseg, coff, M = svd[c]
             k = kept[c]
-            Uk, Sk, Vk = U[:, :k], S[:k], Vh[:k, :]
-            if absorb == "right":
-                Vk = Sk[:, None] * Vk
+            if method == "gram":
+                if absorb == "right":
+                    Uk = U[:, :k]
+                    Vk = Uk.t() @ M
+                else:
+                    Vk = Vh[:k, :]
+                    Uk = M @ Vk.t()
             else:
-                Uk = Uk * Sk[None, :]
+                Uk, Sk, Vk = U[:, :k], S[:k], Vh[:k, :]
+                if absorb == "right":
+                    Vk = Sk[:, None] * Vk
+                else:
+                    Uk = Uk * Sk[None, :]
             for ql, s1 in rseg:
                 r = roff[(ql, s1)]
                 A_blocks[(ql, s1, qc)] = Uk[r: r + left.dims[ql - 1], :]

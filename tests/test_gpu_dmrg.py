@@ -76,3 +76,43 @@ def test_dmrg_device_split_energy():
     assert abs(e_d - e_h) <= 1e-12 * abs(e_h), (e_d, e_h)
     exact = dmrg.exact_ground_energy(10, 1.0)
     assert abs(e_d - exact) <= 1e-9 * abs(exact)
+
+
+def test_device_split_gram_matches_svd():
+    """The density-matrix split (method="gram": eigh of M M^T or M^T M) against
+    the SVD split on the same two-site tensor: the same bond sectors, singular
+    values to 1e-10 of the largest, the same discarded weight, the isometry
+    orthonormal to 1e-12 and A*B equal to the SVD truncation's to 1e-10."""
+    import sparsebackends_b200 as sb
+    from sparsebackends_b200 import qn
+    ctx = sb.Context(0)
+    left = qn.U1Link([-3, -1, 1, 3], [3, 9, 9, 3])
+    right = qn.U1Link([-3, -1, 1, 3], [5, 11, 11, 5])
+    lay = qn.HeffLayout(left, right, qn.mpo_link({-2: 1, 0: 3, 2: 1}))
+    keys, data, exts = qn.random_block_tensor(lay, "psi", np.random.Generator(np.random.PCG64(23)), 1.0,
+                                              ragged=True)
+    psi = sb.NewBlockSparseSorted(lay.dims["psi"], lay.n2["psi"], keys, None, data, ctx=ctx, block_dims=exts)
+    lab = (["ql", "s1", "s2", "qr", "ml", "mr"], ["ql", "s1", "qc", "ml", "mc"], ["qc", "s2", "qr", "mc", "mr"])
+    for absorb in ("right", "left"):
+        A1, B1, l1, sv1, e1 = qn.split_two_site_device(lay, psi, maxdim=20, cutoff=1e-3, absorb=absorb)
+        A2, B2, l2, sv2, e2 = qn.split_two_site_device(lay, psi, maxdim=20, cutoff=1e-3, absorb=absorb,
+                                                       method="gram")
+        assert l1.charges == l2.charges and l1.dims == l2.dims
+        assert np.allclose(sv2, sv1, rtol=0, atol=1e-10 * sv1[0]) and abs(e1 - e2) <= 1e-12
+        p1 = qn.contract_new(lab[0], 2, A1, lab[1], B1, lab[2]).blocks_by_key()
+        p2 = qn.contract_new(lab[0], 2, A2, lab[1], B2, lab[2]).blocks_by_key()
+        assert set(p1) == set(p2)
+        nrm = np.sqrt(sum(float(np.sum(np.asarray(v) ** 2)) for v in p1.values()))
+        assert max(np.abs(np.asarray(p2[k]) - np.asarray(v)).max() for k, v in p1.items()) <= 1e-10 * nrm
+        # the isometry: A's rows (absorb right) or B's columns (absorb left) orthonormal per bond sector
+        iso = A2 if absorb == "right" else B2
+        blocks = iso.blocks_by_key()
+        dims = dict(zip(iso.keys, iso.block_dims))
+        for qc in range(1, l2.S + 1):
+            if absorb == "right":
+                parts = [np.asarray(blocks[k]).reshape(dims[k], order="F") for k in iso.keys if k[2] == qc]
+                Q = np.vstack(parts)
+            else:
+                parts = [np.asarray(blocks[k]).reshape(dims[k], order="F") for k in iso.keys if k[0] == qc]
+                Q = np.hstack(parts).T
+            assert np.allclose(Q.T @ Q, np.eye(Q.shape[1]), atol=1e-12)
