@@ -921,6 +921,7 @@ def run_ours(args, world, rank, local):
     permute = permute_stage(ctx, dev_u["L"], hbm_peak)
     serving = serving_leg(args.seed)
     pxp_line = pxp_leg(local, args.steps)
+    j1j2_line = j1j2_leg(local, 2048, 60.0, "gram")
     # the vendor library on the same block lists, after every timed leg (its
     # many small launches stay out of the launch lists profiled from this run)
     library = cublas_block_lists(layout)
@@ -954,6 +955,7 @@ def run_ours(args, world, rank, local):
         "permute_stage": permute,
         "serving": serving,
         "pxp_chain": pxp_line,
+        "j1j2_cylinder_dmrg": j1j2_line,
         "uniform_format": {"value": value_u, "ms_per_step": ms_u / args.steps,
                            "note": "contract! on the reference's zero-padded blocks; psi*L and R*T3 crop the padding "
                                    "inside contract_shared! (scan, harmonised extents, ragged GEMM, padded result)",
@@ -1176,16 +1178,18 @@ def run_dmrg_leg(args, world, rank, local):
                           "as_specified": spec, "converged": conv}), flush=True)
 
 
-def run_j1j2_leg(args, world, rank, local):
+def j1j2_leg(local: int, maxdim: int = 2048, budget_s: float = 150.0, split: str = "gram", emit=None):
     """Two-site DMRG of the J1-J2 Heisenberg model (J1 = 1, J2 = 0.5) on the
     6 x 6 cylinder (open along x, periodic along y), snake order, N = 36, U(1)
     2Sz = 0, from the Neel state along the snake; the MPO is the automaton
     construction of ``j1j2.J1J2Cylinder``.  Sweeps with maxdim doubling from 64
-    to ``--j1j2-maxdim`` (then one more at the maximum), cutoff 1e-10,
-    krylovdim 3, maxiter 1, in plain FP64 and in the 3xTF32 form (the H_eff
-    applies on the tensor cores, FP64 Rayleigh-quotient energies).  Reports
-    the energies, their relative difference, per-sweep seconds and the device
-    time per kernel kind."""
+    to ``maxdim`` (then one more at the maximum), cutoff 1e-10, krylovdim 3,
+    maxiter 1, in plain FP64 and in the 3xTF32 form (the H_eff applies on the
+    tensor cores, FP64 Rayleigh-quotient energies).  No new FP64 sweep starts
+    after ``budget_s`` seconds (the schedule is cut there, and the 3xTF32 form
+    runs the same sweeps).  Returns the energies, their relative difference,
+    per-sweep seconds and the device time per kernel kind; ``emit(form)`` is
+    called with each form's record as soon as it ends."""
     import torch
     import sparsebackends_b200 as sb
     from sparsebackends_b200 import dmrg, j1j2
@@ -1194,20 +1198,20 @@ def run_j1j2_leg(args, world, rank, local):
     m = j1j2.J1J2Cylinder(6, 6, 1.0, 0.5)
     sched = []
     x = 64
-    while x < args.j1j2_maxdim:
+    while x < maxdim:
         sched.append(x)
         x *= 2
-    sched += [args.j1j2_maxdim] * 2
+    sched += [maxdim] * 2
     out = {}
     for prec in ("f64", "tf32x3"):
         ctx = sb.Context(local)
-        d = dmrg.DMRG(m.n, ctx=ctx, precision=prec, device_split=True, mpo=m, split_method=args.j1j2_split)
+        d = dmrg.DMRG(m.n, ctx=ctx, precision=prec, device_split=True, mpo=m, split_method=split)
         ctx.set_profiling(True)
         energies, secs = [], []
         t_start = time.perf_counter()
         for mx in sched:
-            if prec == "f64" and time.perf_counter() - t_start > args.j1j2_budget_s:
-                sched = sched[:len(energies)]  # the 3xTF32 form runs the same sweeps
+            if prec == "f64" and time.perf_counter() - t_start > budget_s:
+                sched = sched[:len(energies)]
                 break
             t0 = time.perf_counter()
             energies.append(d.sweep(mx, cutoff=1e-10, krylovdim=3, maxiter=1))
@@ -1220,16 +1224,25 @@ def run_j1j2_leg(args, world, rank, local):
                      "kernel_ms": {k: v["ms"] for k, v in prof.items() if v["launches"]},
                      "tc_gemm_tflops_algorithmic": prof["gemm_tc"]["flops"] / (prof["gemm_tc"]["ms"] * 1e-3) / 1e12
                      if prof["gemm_tc"]["ms"] > 0 else None}
-        if rank == 0:  # each form as soon as it ends (a long run cut short keeps what finished)
-            print(json.dumps({"leg": "j1j2_form", "precision": prec, "maxdim": sched, **out[prec]}), flush=True)
+        if emit is not None:
+            emit({"precision": prec, "maxdim": sched, **out[prec]})
     e64, e32 = out["f64"]["energy"], out["tf32x3"]["energy"]
+    return {"model": "J1-J2 Heisenberg (J1=1, J2=0.5), 6x6 cylinder (open x, periodic y), snake order, N=36, "
+                     "U(1) 2Sz=0, Neel start",
+            "mpo_link": {"charges": m.link.charges, "dims": m.link.dims},
+            "schedule": {"maxdim": sched, "cutoff": 1e-10, "krylovdim": 3, "maxiter": 1},
+            "split": split, "forms": out, "rel_diff_tf32x3_vs_f64": abs(e32 - e64) / abs(e64)}
+
+
+def run_j1j2_leg(args, world, rank, local):
+    """``j1j2_leg`` with the command line's maxdim, budget and split; each form
+    is printed when it ends (a long run cut short keeps what finished)."""
+    def emit(form):
+        if rank == 0:
+            print(json.dumps({"leg": "j1j2_form", **form}), flush=True)
+    res = j1j2_leg(local, args.j1j2_maxdim, args.j1j2_budget_s, args.j1j2_split, emit)
     if rank == 0:
-        print(json.dumps({"leg": "j1j2", "model": "J1-J2 Heisenberg (J1=1, J2=0.5), 6x6 cylinder (open x, periodic y), "
-                          "snake order, N=36, U(1) 2Sz=0, Neel start",
-                          "mpo_link": {"charges": m.link.charges, "dims": m.link.dims},
-                          "schedule": {"maxdim": sched, "cutoff": 1e-10, "krylovdim": 3, "maxiter": 1},
-                          "split": args.j1j2_split,
-                          "forms": out, "rel_diff_tf32x3_vs_f64": abs(e32 - e64) / abs(e64)}), flush=True)
+        print(json.dumps({"leg": "j1j2", **res}), flush=True)
 
 
 def run_cpu_leg(args):
