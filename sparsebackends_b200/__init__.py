@@ -388,24 +388,28 @@ class NewBlockSparseSorted(_Tensor):
     def blksize(self) -> int:
         return self._info()["blksize"]
 
-    def _export(self):
+    def _export(self, with_data: bool = True):
+        """(keys, ids, payload); without ``with_data`` the payload is None and
+        nothing is copied from the device (keys live on the host)."""
         i = self._info()
-        P, n, blk = len(i["dims"]) - i["n2"], i["nkeys"], i["blksize"]
-        _, _, plen = self._layout()
+        P, n = len(i["dims"]) - i["n2"], i["nkeys"]
         keys = (C.c_int64 * max(n * P, 1))()
         ids = (C.c_int64 * max(n, 1))()
-        data = np.empty(plen, dtype=np.float64)
+        data = None
+        if with_data:
+            _, _, plen = self._layout()
+            data = np.empty(plen, dtype=np.float64)
         _check(self.ctx, self.ctx._lib.sb_tensor_export_bs(self.ctx._h, self._h, keys, ids, _f64ptr(data)))
         klist = [tuple(keys[j * P + t] for t in range(P)) for j in range(n)]
         return klist, [ids[j] for j in range(n)], data
 
     @property
     def keys(self) -> List[Tuple[int, ...]]:
-        return self._export()[0]
+        return self._export(with_data=False)[0]
 
     @property
     def ids(self) -> List[int]:
-        return self._export()[1]
+        return self._export(with_data=False)[1]
 
     @property
     def data(self) -> np.ndarray:
@@ -511,10 +515,12 @@ class AliasedBlockSparse(_Tensor):
                                                       _i64(alias_ids or []), _f64ptr(sc), C.byref(h)))
         super().__init__(ctx, h)
 
-    def _export(self):
+    def _export(self, with_templates: bool = True):
+        """(templates, keys, alias_ids, scalars); without ``with_templates``
+        the templates are None and not copied from the device."""
         i = self._info()
         P, n, blk, ntm = len(i["dims"]) - i["n2"], i["nkeys"], i["blksize"], i["n_templates"]
-        tm = np.empty(ntm * blk, dtype=np.float64)
+        tm = np.empty(ntm * blk, dtype=np.float64) if with_templates else None
         keys = (C.c_int64 * max(n * P, 1))()
         aids = (C.c_int64 * max(n, 1))()
         sc = np.empty(n, dtype=np.float64)
@@ -532,7 +538,7 @@ class AliasedBlockSparse(_Tensor):
 
     @property
     def keys(self):
-        return self._export()[1]
+        return self._export(with_templates=False)[1]
 
     def logical_blocks(self) -> dict:
         """Per-key ``scalar * template`` (the unit the reference's tests compare)."""
