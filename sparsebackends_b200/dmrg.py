@@ -163,9 +163,11 @@ class DMRG:
         psi = qn.contract_new(["ql", "s1", "s2", "qr", "ml", "mr"], 2, A, ["ql", "s1", "qc", "ml", "mc"],
                               B, ["qc", "s2", "qr", "mc", "mr"])
         lay = qn.HeffLayout(self.bonds[i - 1], self.bonds[i + 1], self.mpo_link)
-        have = psi.blocks_by_key()
         keys = sorted(lay.keys["psi"], key=lambda k: k[::-1])
         exts = [lay.valid_extent("psi", k) for k in keys]
+        if psi.keys == keys and [tuple(e) for e in psi.block_dims] == [tuple(e) for e in exts]:
+            return lay, psi  # every allowed block already there, at its extents
+        have = psi.blocks_by_key()
         parts = [have[k] if k in have else np.zeros(int(np.prod(e))) for k, e in zip(keys, exts)]
         data = np.concatenate(parts) if parts else np.zeros(0)
         x = sb.NewBlockSparseSorted(lay.dims["psi"], 2, keys, None, data, ctx=self.ctx, block_dims=exts)
