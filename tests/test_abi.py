@@ -73,6 +73,26 @@ def test_label_key_mapping():
     assert sb.label_key("r") != sb.label_key("i")
 
 
+def test_packed_labels_cache_is_exact():
+    """String-label lists are packed once and reused; every other label list
+    is packed afresh; both give the words of label_key."""
+    import sparsebackends_b200 as sb
+
+    def words(labels):
+        return [w for l in labels for w in sb.label_key(l)]
+
+    strs = ["ql", "s1", "s2", "qr", "ml", "mr"]
+    a1, n1 = sb._labels(strs)
+    a2, n2 = sb._labels(list(strs))
+    assert a1 is a2 and n1 == n2 == 6 and list(a1) == words(strs)
+    mixed = ["ql", (7, 1), 3]
+    b1, _ = sb._labels(mixed)
+    b2, _ = sb._labels(mixed)
+    assert b1 is not b2 and list(b1) == list(b2) == words(mixed)
+    # equal-comparing labels of different types keep their own words
+    assert list(sb._labels([1])[0]) != list(sb._labels([1.0])[0])
+
+
 def test_output_inds_order():
     """output_inds (src/tensor_wrappers.jl:477-526): links by level, non-links, dense tail."""
     import sparsebackends_b200 as sb
