@@ -402,6 +402,34 @@ def cpu_matvec_rate(layout, host, budget_s: float, max_runs: int, keep=None):
     return runs / el, runs, el
 
 
+def cpp_matvec_rate(layout, host, budget_s: float, max_runs: int, keep=None):
+    """``cpu_matvec_rate`` on the C++ restatement of contract_shared!
+    (``oracle/cpu_ref``: compiled loops, one OpenBLAS dgemm per block pair, as
+    the reference's mul!), operands resident on the C++ side."""
+    from oracle import cpu_ref
+    from sparsebackends_b200 import qn
+    cpu_ref.build()
+    t = {n: cpu_ref.Tensor(layout.dims[n], layout.n2[n], keys, data) for n, (keys, data) in host.items()}
+    lab = layout.labels
+
+    def one():
+        tt = dict(t)
+        for c, a, b in qn.HeffChain.STEPS:
+            tt[c] = cpu_ref.contract(layout.dims[c], layout.n2[c], lab[c], tt[a], lab[a], tt[b], lab[b])
+        return tt["T4"]
+
+    runs, start = 0, time.perf_counter()
+    while runs < max_runs:
+        t4 = one()
+        runs += 1
+        if time.perf_counter() - start > budget_s:
+            break
+    el = time.perf_counter() - start
+    if keep is not None:
+        keep.append(t4)
+    return runs / el, runs, el
+
+
 def blas_threads():
     try:
         from threadpoolctl import threadpool_info
@@ -459,8 +487,8 @@ def run_reference(args, world, rank):
     from sparsebackends_b200 import qn
     flops = qn.chain_flops(layout, padded=False)
     if args.warmup > 0:
-        cpu_matvec_rate(layout, host, 0.0, 1)
-    rate, runs, el = cpu_matvec_rate(layout, host, args.cpu_budget_s, max(1, args.steps))
+        cpp_matvec_rate(layout, host, 0.0, 1)
+    rate, runs, el = cpp_matvec_rate(layout, host, args.cpu_budget_s, max(1, args.steps))
     line = {
         "metric": METRIC, "value": rate, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": runs, "steps_requested": args.steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 / rate,
@@ -470,8 +498,9 @@ def run_reference(args, world, rank):
                    "l2": "inputs larger than L2"},
         "gflops_algorithmic": flops * rate / 1e9,
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": blas_threads(), "kind": "port",
-                         "sample": f"{runs} full matvec(s) of the same chi={args.chi} workload, oracle (numpy + "
-                                   f"OpenBLAS) restatement of contract_bs_bs.jl contract_shared!"},
+                         "sample": f"{runs} full matvec(s) of the same chi={args.chi} workload, C++ restatement "
+                                   f"of contract_bs_bs.jl contract_shared! (g++ -O3, OpenBLAS 0.3.30 dgemm per "
+                                   f"block pair)"},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -844,7 +873,8 @@ def run_ours(args, world, rank, local):
                 u = sb.to_uniform(t)
                 host1[name] = (u.keys, np.array(u.data, copy=True))
             last = []
-            rate, runs, el = cpu_matvec_rate(lay1, host1, 5.0, 400, keep=last)
+            cpu_matvec_rate(lay1, host1, 0.0, 1, keep=last)  # the oracle's result, for the check below
+            rate, runs, el = cpp_matvec_rate(lay1, host1, 5.0, 4000)
             got = sb.to_uniform(ch.out["T4"])
             ref = last[-1]
             assert got.keys == ref.keys
@@ -853,7 +883,8 @@ def run_ours(args, world, rank, local):
                 float(np.linalg.norm(np.asarray(gb[k]) - v) / max(np.linalg.norm(v), 1e-300))
                 for k, v in ref.blocks_by_key().items())
             out["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": blas_threads(), "kind": "port",
-                                   "sample": f"{runs} matvecs in {el:.1f} s, oracle chain on the uniform blocks"}
+                                   "sample": f"{runs} matvecs in {el:.1f} s, C++ restatement of contract_shared! "
+                                             f"(g++ -O3, OpenBLAS dgemm per block pair) on the uniform blocks"}
         return out
 
     centre_leg = centre_problem_leg(max(200, args.steps))
@@ -880,11 +911,11 @@ def run_ours(args, world, rank, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, runs, el = cpu_matvec_rate(layout, host, args.cpu_budget_s, 8)
+        rate, runs, el = cpp_matvec_rate(layout, host, args.cpu_budget_s, 8)
         cpu = {"value": rate, "unit": UNIT, "cores": blas_threads(), "kind": "port",
-               "sample": f"{runs} full matvec(s) of the same workload in {el:.1f} s, oracle (numpy + OpenBLAS) "
-                         f"restatement of contract_shared! (contract_bs_bs.jl:572-730) on the reference's "
-                         f"uniform (zero-padded) blocks"}
+               "sample": f"{runs} full matvec(s) of the same workload in {el:.1f} s, C++ restatement of "
+                         f"contract_shared! (contract_bs_bs.jl:572-730; g++ -O3, one OpenBLAS 0.3.30 dgemm per "
+                         f"block pair as the reference's mul!) on the reference's uniform (zero-padded) blocks"}
 
     if rank != 0:
         return
@@ -1263,16 +1294,21 @@ def run_cpu_leg(args):
         host1[name] = (u.keys, np.array(u.data, copy=True))
     out = {"host_cores": os.cpu_count()}
     for threads in (1, blas_threads()):
-        with threadpool_limits(limits=threads, user_api="blas"):
-            r, n, el = cpu_matvec_rate(layout, host, 0.0, 1)
-            r1, n1, el1 = cpu_matvec_rate(lay1, host1, 5.0, 2000)
-        out[f"threads_{threads}"] = {
-            "chi2048": {"value": r, "unit": UNIT, "sample": f"{n} matvec in {el:.1f} s",
-                        "gflops_algorithmic": qn.chain_flops(layout, padded=False) * r / 1e9},
-            "centre_n16_chi64": {"value": r1, "unit": UNIT, "sample": f"{n1} matvecs in {el1:.1f} s",
-                                 "gflops_algorithmic": qn.chain_flops(lay1, padded=False) * r1 / 1e9}}
-    print(json.dumps({"leg": "cpu", "kind": "port", "what": "oracle restatement of the reference (numpy + OpenBLAS), "
-                      "not the reference itself", **out}), flush=True)
+        row = {}
+        for impl, fn in (("cpp", cpp_matvec_rate), ("numpy", cpu_matvec_rate)):
+            with threadpool_limits(limits=threads, user_api="blas"):
+                r, n, el = fn(layout, host, 0.0, 1)
+                r1, n1, el1 = fn(lay1, host1, 5.0, 4000)
+            row[impl] = {
+                "chi2048": {"value": r, "unit": UNIT, "sample": f"{n} matvec in {el:.1f} s",
+                            "gflops_algorithmic": qn.chain_flops(layout, padded=False) * r / 1e9},
+                "centre_n16_chi64": {"value": r1, "unit": UNIT, "sample": f"{n1} matvecs in {el1:.1f} s",
+                                     "gflops_algorithmic": qn.chain_flops(lay1, padded=False) * r1 / 1e9}}
+        out[f"threads_{threads}"] = row
+    print(json.dumps({"leg": "cpu", "kind": "port",
+                      "what": "restatements of the reference, not the reference itself: cpp = C++ contract_shared! "
+                              "(g++ -O3, one OpenBLAS dgemm per block pair), numpy = the oracle (numpy + OpenBLAS)",
+                      **out}), flush=True)
 
 
 def main():
