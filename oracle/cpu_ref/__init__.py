@@ -58,6 +58,9 @@ def load():
         lib.oref_info.argtypes = [VP, P(I64), P(I64)]
         lib.oref_export.argtypes = [VP, P(I64), P(C.c_double)]
         lib.oref_contract_shared.argtypes = [C.c_int, P(I64), C.c_int, P(I64), VP, P(I64), VP, P(I64), P(VP)]
+        lib.oref_fuse_prefix.argtypes = [VP, C.c_int, C.c_int, P(VP)]
+        lib.oref_contract_coo_prefix.argtypes = [C.c_int, P(I64), C.c_int, P(I64), C.c_int, P(I64), I64, P(I64),
+                                                 P(C.c_double), P(I64), VP, P(I64), P(VP)]
         blas = openblas()
         fn = getattr(blas, "scipy_cblas_dgemm64_")
         lib.oref_set_dgemm(C.cast(fn, VP))
@@ -144,3 +147,50 @@ def contract(dimsC, n2C, labelsC, A: Tensor, labelsA, B: Tensor, labelsB) -> Ten
 def contract_shared(C0, labelsC, A, labelsA, B, labelsB):
     """Oracle-typed convenience: BS operands in, BS result out (C0 gives dims and n2)."""
     return contract(C0.dims, C0.n2, labelsC, Tensor.from_bs(A), labelsA, Tensor.from_bs(B), labelsB).to_bs()
+
+
+def fuse_prefix(A: Tensor, ax1: int, ax2: int) -> Tensor:
+    """fuse_two_axes! of two prefix axes (1-based)."""
+    lib = load()
+    h = C.c_void_p()
+    _check(lib.oref_fuse_prefix(A._h, int(ax1), int(ax2), C.byref(h)))
+    a1, a2 = min(ax1, ax2), max(ax1, ax2)
+    dims = tuple(A.dims[a1 - 1] * A.dims[a2 - 1] if i == a1 else A.dims[i - 1]
+                 for i in range(1, len(A.dims) + 1) if i != a2)
+    return Tensor(dims, A.n2, None, None, _handle=h)
+
+
+def contract_coo_prefix(dimsC, n2C, labelsC, A, labelsA, B: Tensor, labelsB) -> Tensor:
+    """contract_prefix! with an oracle COO ``A`` and a C++-side ``B``."""
+    lib = load()
+    h = C.c_void_p()
+    keys = [int(x) for k in A.keys for x in k]
+    vals = np.ascontiguousarray(np.asarray(A.vals, dtype=np.float64))
+    _check(lib.oref_contract_coo_prefix(len(dimsC), _i64(dimsC), int(n2C), _i64(_label_ids(labelsC)), len(A.dims),
+                                        _i64(A.dims), len(A.vals), _i64(keys),
+                                        vals.ctypes.data_as(C.POINTER(C.c_double)), _i64(_label_ids(labelsA)),
+                                        B._h, _i64(_label_ids(labelsB)), C.byref(h)))
+    return Tensor(dimsC, n2C, None, None, _handle=h)
+
+
+def pxp_heff_runner(prob):
+    """The PXP matvec (``sparsebackends_b200.pxp.HEFF_STEPS``) on the C++
+    side for an ``oracle.pxp_oracle.OracleProblem``: returns ``apply(psi)``
+    taking and returning C++ tensors, with L, R and psi resident."""
+    from sparsebackends_b200 import pxp
+    from oracle import sparse_oracle as so
+    L, R, psi = Tensor.from_bs(prob.L), Tensor.from_bs(prob.R), Tensor.from_bs(prob.psi)
+
+    def contract_any(lc, n2, A, la, B, lb):
+        ext = dict(zip(la, A.dims))
+        ext.update(zip(lb, B.dims))
+        dims = tuple(ext[x] for x in lc)
+        if isinstance(A, so.COO):
+            return contract_coo_prefix(dims, n2, lc, A, la, B, lb)
+        return contract(dims, n2, lc, A, la, B, lb)
+
+    def apply(x):
+        t = {"psi": x, "L": L, "R": R, "W1f": prob.Wf, "W2f": prob.Wf}
+        return pxp.run_steps(pxp.HEFF_STEPS, t, dict(pxp.LABELS), contract_any, fuse_prefix)["T4"]
+
+    return apply, psi

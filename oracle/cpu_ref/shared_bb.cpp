@@ -294,6 +294,139 @@ T contract_shared(const std::vector<i64>& dimsC, int n2C, const std::vector<i64>
   return C;
 }
 
+// fuse_two_axes! for two prefix axes (blocksparse/conversions.jl:228-262):
+// the fused key (k[a2] - 1) * d[a1] + k[a1] sits at a1, axis a2 is dropped,
+// the blocks are unchanged; the keys are kept sorted.
+T fuse_prefix(const T& A, int ax1, int ax2) {
+  const int N = A.N(), P = A.P();
+  const int a1 = std::min(ax1, ax2), a2 = std::max(ax1, ax2);
+  require(a1 >= 1 && a2 <= P && a1 != a2, "prefix axes must be distinct and in 1:P");
+  T B;
+  B.n2 = A.n2;
+  for (int i = 1; i <= N; ++i)
+    if (i != a2) B.dims.push_back(i == a1 ? A.dims[a1 - 1] * A.dims[a2 - 1] : A.dims[i - 1]);
+  const i64 n = A.nkeys();
+  for (i64 r = 0; r < n; ++r) {
+    const i64* k = A.key(r);
+    for (int j = 1; j <= P; ++j) {
+      if (j == a2) continue;
+      B.keys.push_back(j == a1 ? (k[a2 - 1] - 1) * A.dims[a1 - 1] + k[a1 - 1] : k[j - 1]);
+    }
+  }
+  B.data = A.data;
+  sort_keys(B);
+  return B;
+}
+
+struct Coo {
+  std::vector<i64> dims;
+  std::vector<i64> keys;  // nnz x N, 1-based
+  std::vector<double> vals;
+  int N() const { return static_cast<int>(dims.size()); }
+  i64 nnz() const { return static_cast<i64>(vals.size()); }
+  const i64* key(i64 i) const { return keys.data() + i * N(); }
+};
+
+// contract_prefix! COO x BS (contract_coo_bs.jl:51-124) for one reduced label r
+// in B's prefix: A's keys with r last, sorted column-major
+// (ensure_rlab_last_and_sorted, contract_coo.jl:48-82), B with r as its last
+// prefix axis; for every A entry and B block with equal r,
+// C[key] += a * B_block (_scale_add_block!, :4-10).
+T contract_coo_prefix(const std::vector<i64>& dimsC, int n2C, const std::vector<i64>& lC, const Coo& A0,
+                      const std::vector<i64>& lA0, const T& B0, const std::vector<i64>& lB0) {
+  std::vector<i64> shared;
+  for (i64 l : lA0)
+    if (find(lB0, l) >= 0) shared.push_back(l);
+  require(shared.size() == 1 && find(lC, shared[0]) < 0, "contract_prefix! reduces exactly one label");
+  const i64 r = shared[0];
+  const int NA = A0.N(), PB0 = B0.P(), NC = static_cast<int>(dimsC.size()), PC = NC - n2C;
+  require(find(lB0, r) < PB0, "the reduced label must be in B's prefix");
+  require(PC == NA + PB0 - 2, "PC must equal NA + PB - 2");
+  // A: r last, keys sorted column-major (last axis slowest)
+  std::vector<int> pa;
+  for (int j = 0; j < NA; ++j)
+    if (lA0[j] != r) pa.push_back(j);
+  pa.push_back(find(lA0, r));
+  Coo A;
+  std::vector<i64> lA;
+  for (int j : pa) {
+    A.dims.push_back(A0.dims[j]);
+    lA.push_back(lA0[j]);
+  }
+  std::vector<i64> order(A0.nnz());
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](i64 x, i64 y) {
+    for (int t = NA - 1; t >= 0; --t) {
+      const i64 a = A0.key(x)[pa[t]], b = A0.key(y)[pa[t]];
+      if (a != b) return a < b;
+    }
+    return false;
+  });
+  for (i64 e : order) {
+    for (int j : pa) A.keys.push_back(A0.key(e)[j]);
+    A.vals.push_back(A0.vals[e]);
+  }
+  // B: r to the last prefix position (r_to_last_prefix)
+  std::vector<int> pb;
+  const int br = find(lB0, r);
+  for (int j = 0; j < PB0; ++j)
+    if (j != br) pb.push_back(j + 1);
+  pb.push_back(br + 1);
+  for (int j = PB0; j < B0.N(); ++j) pb.push_back(j + 1);
+  bool ident = true;
+  for (size_t j = 0; j < pb.size(); ++j) ident = ident && pb[j] == static_cast<int>(j) + 1;
+  T Bp;
+  if (!ident) Bp = permute(B0, pb);
+  const T& B = ident ? B0 : Bp;
+  std::vector<i64> lB;
+  for (int p : pb) lB.push_back(lB0[p - 1]);
+  T C;
+  C.dims = dimsC;
+  C.n2 = n2C;
+  require(C.blk() == B.blk(), "C.blksize must equal B.blksize");
+  std::vector<int> src;  // >0: A position + 1, <0: -(B prefix position + 1)
+  for (int j = 0; j < PC; ++j) {
+    const int ia = find(lA, lC[j]), ib = find(lB, lC[j]);
+    if (ia >= 0) src.push_back(ia + 1);
+    else if (ib >= 0 && ib < B.P()) src.push_back(-(ib + 1));
+    else throw std::runtime_error("C prefix label must come from A or B prefix");
+  }
+  const int aR = NA - 1, bR = B.P() - 1;
+  const i64 blk = B.blk();
+  std::map<i64, std::pair<std::vector<i64>, i64>> cmap;
+  std::vector<std::vector<double>> slots;
+  std::vector<i64> ck(PC);
+  i64 iA = 0, iB = 0;
+  const i64 nA = A.nnz(), nB = B.nkeys();
+  while (iA < nA && iB < nB) {
+    const i64 rA = A.key(iA)[aR], rB = B.key(iB)[bR];
+    if (rA < rB) { while (iA < nA && A.key(iA)[aR] == rA) ++iA; continue; }
+    if (rB < rA) { while (iB < nB && B.key(iB)[bR] == rB) ++iB; continue; }
+    const i64 blo = iB;
+    while (iB < nB && B.key(iB)[bR] == rA) ++iB;
+    for (; iA < nA && A.key(iA)[aR] == rA; ++iA)
+      for (i64 b = blo; b < iB; ++b) {
+        for (int q = 0; q < PC; ++q) ck[q] = src[q] > 0 ? A.key(iA)[src[q] - 1] : B.key(b)[-src[q] - 1];
+        const i64 lin = prefix_lin(ck.data(), C.dims, PC);
+        auto it = cmap.find(lin);
+        if (it == cmap.end()) {
+          slots.emplace_back(blk, 0.0);
+          it = cmap.emplace(lin, std::make_pair(ck, static_cast<i64>(slots.size()) - 1)).first;
+        }
+        double* c = slots[it->second.second].data();
+        const double a = A.vals[iA];
+        const double* x = B.block(b);
+        for (i64 e = 0; e < blk; ++e) c[e] += a * x[e];
+      }
+  }
+  for (auto& kv : cmap) {
+    C.keys.insert(C.keys.end(), kv.second.first.begin(), kv.second.first.end());
+    const auto& sl = slots[kv.second.second];
+    C.data.insert(C.data.end(), sl.begin(), sl.end());
+  }
+  return C;
+}
+
 thread_local std::string g_err;
 
 template <class F>
@@ -359,6 +492,27 @@ int oref_contract_shared(int ndC, const int64_t* dimsC, int n2C, const int64_t* 
     const T& b = *static_cast<T*>(B);
     std::vector<i64> dc(dimsC, dimsC + ndC), lc(lC, lC + ndC), la(lA, lA + a.N()), lb(lB, lB + b.N());
     *out = new T(contract_shared(dc, n2C, lc, a, la, b, lb));
+  });
+}
+
+// fuse_two_axes! of two prefix axes (1-based); *out receives a new tensor.
+int oref_fuse_prefix(void* A, int ax1, int ax2, void** out) {
+  return guard([&] { *out = new T(fuse_prefix(*static_cast<T*>(A), ax1, ax2)); });
+}
+
+// contract_prefix! (COO x block-sparse, one reduced label in B's prefix); the
+// COO operand as (nd, dims, nnz, keys nnz x nd row-major 1-based, vals).
+int oref_contract_coo_prefix(int ndC, const int64_t* dimsC, int n2C, const int64_t* lC, int ndA, const int64_t* dimsA,
+                             int64_t nnz, const int64_t* keysA, const double* valsA, const int64_t* lA, void* B,
+                             const int64_t* lB, void** out) {
+  return guard([&] {
+    Coo a;
+    a.dims.assign(dimsA, dimsA + ndA);
+    a.keys.assign(keysA, keysA + nnz * ndA);
+    a.vals.assign(valsA, valsA + nnz);
+    const T& b = *static_cast<T*>(B);
+    std::vector<i64> dc(dimsC, dimsC + ndC), lc(lC, lC + ndC), la(lA, lA + ndA), lb(lB, lB + b.N());
+    *out = new T(contract_coo_prefix(dc, n2C, lc, a, la, b, lb));
   });
 }
 

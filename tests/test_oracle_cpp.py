@@ -89,3 +89,38 @@ def test_heff_chain_matches_numpy_oracle():
     rb, gb = ref.blocks_by_key(), got.blocks_by_key()
     scale = max(np.max(np.abs(v)) for v in rb.values())
     assert max(np.max(np.abs(gb[k] - v)) for k, v in rb.items()) <= 1e-12 * scale
+
+
+def test_pxp_matvec_matches_numpy_oracle():
+    """The whole PXP matvec (contract_shared!, fuse_two_axes!, contract_prefix!)
+    through the C++ restatement, as the PXP leg's CPU baseline runs it."""
+    from oracle.pxp_oracle import OracleProblem, o_run
+    from sparsebackends_b200 import pxp
+    prob = OracleProblem(12, 16, 5)
+    apply, psi = cpu_ref.pxp_heff_runner(prob)
+    got = apply(psi).to_bs()
+    ref = prob.apply(prob.psi)
+    assert got.keys == ref.keys
+    for k, v in ref.blocks_by_key().items():
+        assert np.max(np.abs(got.blocks_by_key()[k] - v)) <= 1e-13 * max(1.0, np.max(np.abs(v))), k
+    # the scaled adds alone are bit-exact: T2 from the oracle's own T1f
+    t = o_run(pxp.HEFF_STEPS, {"psi": prob.psi, "L": prob.L, "R": prob.R, "W1f": prob.Wf, "W2f": prob.Wf})
+    t1f = cpu_ref.Tensor.from_bs(t["T1f"])
+    t2 = cpu_ref.contract_coo_prefix(t["T2"].dims, 2, list(pxp.HEFF_STEPS[2][2]), prob.Wf,
+                                     list(pxp.LABELS["W1f"]), t1f, ["qlp", "s2", "qr", "x1", "lp", "r"]).to_bs()
+    assert t2.keys == t["T2"].keys
+    for k, v in t["T2"].blocks_by_key().items():
+        assert np.array_equal(t2.blocks_by_key()[k], v), k
+
+
+def test_fuse_prefix_matches_oracle():
+    rng = np.random.Generator(np.random.PCG64(8))
+    A = so.blocksparse_from_dense(rng.standard_normal((2, 3, 4, 5, 6)) * (rng.random((2, 3, 4, 1, 1)) < 0.6), 2)
+    for ax1, ax2 in ((1, 2), (2, 3), (2, 1)):
+        got = cpu_ref.fuse_prefix(cpu_ref.Tensor.from_bs(A), ax1, ax2).to_bs()
+        ref = so.fuse_two_axes(A, ax1, ax2)
+        assert got.dims == ref.dims
+        rb = ref.blocks_by_key()
+        assert sorted(got.keys, key=lambda k: k[::-1]) == got.keys and set(got.keys) == set(rb)
+        for k, v in rb.items():
+            assert np.array_equal(got.blocks_by_key()[k], v)
