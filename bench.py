@@ -374,9 +374,11 @@ def mixed_dmrg_energy(local: int):
     return out
 
 
-# ── the CPU baseline: the oracle port of the reference path ──────────────
+# ── the CPU baseline: restatements of the reference path (numpy oracle, C++) ──
 
 def cpu_matvec_rate(layout, host, budget_s: float, max_runs: int, keep=None):
+    """Whole H_eff matvecs of the numpy oracle on the uniform reference blocks:
+    (matvecs per second, matvecs, seconds)."""
     from oracle import sparse_oracle as so
     from sparsebackends_b200 import qn
     t = {}
