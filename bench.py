@@ -13,8 +13,11 @@ format (every block at its sector extents); the reference's uniform format
 
 Beside the headline the line carries the reference's zero-padded layout
 (cropped inside contract! and not), the permute stage, CUDA-graph replay, one
-Lanczos solve, the cuBLAS block-list baseline and a small serving leg
-(two-site DMRG solves one at a time, solves/s with p50/p99).
+Lanczos solve, the cuBLAS block-list baseline, the 3xTF32 tensor-core form,
+the N = 16 centre-bond problem, the serving loop (DMRG solves at three arrival
+rates, solves/s with p50/p99), the PXP chain (N = 64, chi = 256, MPO in COO
+and aliased storage) and the J1-J2 6x6 cylinder DMRG to chi = 2048, and the
+CPU baseline: the C++ restatement of the reference path (oracle/cpu_ref).
 
 Prints one JSON line (rank 0).  `value` is whole-job matvecs/s with inputs
 resident in HBM; `e2e` is the same through the public API with psi uploaded
