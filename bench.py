@@ -955,9 +955,11 @@ def run_ours(args, world, rank, local):
     hbm_peak = measured_hbm_gbs()
     gu, gtu = prof_u["gemm"], prof_u["gemm_thin"]
     permute = permute_stage(ctx, dev_u["L"], hbm_peak)
-    serving = serving_leg(args.seed)
-    pxp_line = pxp_leg(local, args.steps)
-    j1j2_line = j1j2_leg(local, 2048, 60.0, "gram")
+    # single-GPU studies: measured at N = 1 only, so that a replica run does not
+    # hold every GPU while rank 0 alone runs them
+    serving = serving_leg(args.seed) if world == 1 else None
+    pxp_line = pxp_leg(local, args.steps) if world == 1 else None
+    j1j2_line = j1j2_leg(local, 2048, 60.0, "gram") if world == 1 else None
     # the vendor library on the same block lists, after every timed leg (its
     # many small launches stay out of the launch lists profiled from this run)
     library = cublas_block_lists(layout)
