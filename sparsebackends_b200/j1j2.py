@@ -33,29 +33,32 @@ def snake_index(x: int, y: int, ly: int) -> int:
 
 
 def cylinder_couplings(lx: int, ly: int, j1: float = 1.0, j2: float = 0.5) -> Dict[Tuple[int, int], float]:
-    """{(i, j): J_ij} over 0-based snake-ordered sites, i < j; a pair reached
-    twice (narrow cylinders) sums its couplings."""
-    out: Dict[Tuple[int, int], float] = {}
+    """{(i, j): J_ij} over 0-based snake-ordered sites, i < j.  Each nearest-
+    and next-nearest-neighbour pair counts once, also on a narrow cylinder
+    where the periodic wrap reaches the same site twice."""
+    nn, nnn = set(), set()
 
-    def add(a, b, j):
-        if a == b or j == 0.0:
-            return
-        k = (min(a, b), max(a, b))
-        out[k] = out.get(k, 0.0) + j
+    def pair(a, b):
+        return (min(a, b), max(a, b))
 
     for x in range(lx):
         for y in range(ly):
             a = snake_index(x, y, ly)
             if ly > 1:
-                add(a, snake_index(x, (y + 1) % ly, ly), j1)
+                nn.add(pair(a, snake_index(x, (y + 1) % ly, ly)))
             if x + 1 < lx:
-                add(a, snake_index(x + 1, y, ly), j1)
+                nn.add(pair(a, snake_index(x + 1, y, ly)))
                 if ly > 1:
-                    add(a, snake_index(x + 1, (y + 1) % ly, ly), j2)
-                    add(a, snake_index(x + 1, (y - 1) % ly, ly), j2)
-    if ly == 2:  # (y+1) and (y-1) mod 2 are the same neighbour: each listed pair was added twice
-        out = {k: v / 2.0 for k, v in out.items()}
-    return out
+                    nnn.add(pair(a, snake_index(x + 1, (y + 1) % ly, ly)))
+                    nnn.add(pair(a, snake_index(x + 1, (y - 1) % ly, ly)))
+    out: Dict[Tuple[int, int], float] = {}
+    for p in nn:
+        if p[0] != p[1] and j1 != 0.0:
+            out[p] = out.get(p, 0.0) + j1
+    for p in nnn:
+        if p[0] != p[1] and j2 != 0.0:
+            out[p] = out.get(p, 0.0) + j2
+    return dict(sorted(out.items()))
 
 
 class J1J2Cylinder:

@@ -59,3 +59,12 @@ def test_blocks_conserve_charge():
     for k in range(m.n):
         for (ql, sp, s, qr) in m.site_blocks(k):
             assert w.charges[qr - 1] == w.charges[ql - 1] + qn.PHYS[sp - 1] - qn.PHYS[s - 1]
+
+
+def test_narrow_cylinder_counts_each_pair_once():
+    """On a width-2 cylinder the periodic wrap meets the direct bond: one J1
+    per rung, one J1 per leg bond and one J2 per diagonal."""
+    J = j1j2.cylinder_couplings(3, 2, 1.0, 0.5)
+    assert sum(1 for v in J.values() if v == 1.0) == 3 + 2 * 2   # rungs + legs
+    assert sum(1 for v in J.values() if v == 0.5) == 2 * 2       # two diagonals per plaquette
+    assert set(J.values()) == {1.0, 0.5}
